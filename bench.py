@@ -1,0 +1,407 @@
+"""Benchmark of the cone-beam operators on the FDK workload (256^3, 360 x 384^2).
+
+One step = forward projection of a 256^3 twelve-ellipsoid phantom onto 360
+views of a 384x384 detector (sid 1000, sod 600, pixel 1, step 0.5, voxel 1)
+followed by ``reconstruct_fdk`` of those projections into 256^3 -- the
+"plain FDK at medium size" workload.  ``value`` is rays per second through the
+whole step (Grays/s) with inputs resident in HBM; the forward projector alone
+(Grays/s) and the backprojection alone (Gvoxel-views/s) are reported beside it.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs under torch.distributed (one process per GPU, NCCL): every rank
+reconstructs its own phantom (independent objects, weak scaling, no data-path
+collective); time = max over ranks.  ``--impl reference`` times the
+reference's CPU path (the FP64 oracle port of its CPU checks) on the host
+cores over a bounded sample of the same workload and prints the same line.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+for _p in (str(ROOT / "diff-geocali_b200"), str(ROOT)):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+WORKLOAD = dict(name="fdk256: project 256^3 -> 360x384^2, then reconstruct_fdk 256^3",
+                D=256, H=256, W=256, A=360, U=384, V=384, sid=1000.0, sod=600.0, pixel=1.0,
+                step=0.5, voxel=1.0, ellipsoids=12, alpha=0.8)
+METRIC = "fwd Grays/s, backproj Gvoxel-views/s; calib time to 0.1 px reproj, NN vs plain"
+UNIT = "Grays/s"
+# Per-launch DRAM bytes of fp_forward_kernel from an ncu capture (see
+# profiles/fp_forward_kernel_fdk256.md); None until measured.
+FWD_DRAM_BYTES_PER_LAUNCH = None
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse_args(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args(argv)
+
+
+# ----------------------------------------------------------------- distributed
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def init_dist(world, backend):
+    import datetime
+
+    import torch.distributed as dist
+
+    if world > 1 and not dist.is_initialized():
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return dist if world > 1 else None
+
+
+def max_over_ranks(value: float, dist, device) -> float:
+    """Maximum of a per-rank float over all ranks (identity for one rank)."""
+    if dist is None:
+        return value
+    import torch
+
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def instance_seed(rank: int) -> int:
+    """Each rank reconstructs its own phantom (independent objects)."""
+    return 1000 + rank
+
+
+# ---------------------------------------------------------------------- clocks
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.proc = None
+        self.file = None
+        self.device_index = device_index
+
+    def __enter__(self):
+        try:
+            import torch
+
+            uuid = str(torch.cuda.get_device_properties(self.device_index).uuid)
+            target = uuid if uuid.startswith("GPU-") else "GPU-" + uuid
+        except Exception:
+            target = str(self.device_index)
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", target], stdout=self.file, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        return False
+
+    def summary(self):
+        if self.proc is None or self.file is None:
+            return None
+        self.file.flush()
+        rows = []
+        with open(self.file.name) as fh:
+            for line in fh:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9 and parts[1].replace(".", "").isdigit():
+                    rows.append(parts)
+        os.unlink(self.file.name)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows]
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v == "Active"})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(rows[0][2]),
+                "reasons": reasons, "samples": len(rows),
+                "power_w_max": max(float(r[3]) for r in rows if r[3].replace(".", "").isdigit())}
+
+
+# ------------------------------------------------------------------- workload
+
+
+def make_instance(device, seed):
+    import torch
+
+    from cbct_backprojector.phantoms import circular_geometry, ellipsoid_phantom
+
+    w = WORKLOAD
+    vol = ellipsoid_phantom((w["D"], w["H"], w["W"]), n=w["ellipsoids"], seed=seed,
+                            voxel_size=w["voxel"], device=device)
+    geom = circular_geometry(w["A"], w["U"], w["V"], w["sid"], w["sod"], w["pixel"], device=device)
+    torch.cuda.synchronize(device)
+    return vol, geom
+
+
+def step(vol, geom):
+    import cbct_backprojector as cb
+
+    w = WORKLOAD
+    proj = cb.project(vol, *geom, w["pixel"], w["U"], w["V"], step_size=w["step"],
+                      voxel_size=w["voxel"])
+    recon = cb.reconstruct_fdk(proj, *geom, w["pixel"], (w["D"], w["H"], w["W"]), w["voxel"],
+                               alpha=w["alpha"])
+    return proj, recon
+
+
+def measured_peak_hbm():
+    path = ROOT / "MEASURED_PEAKS.json"
+    try:
+        data = json.loads(path.read_text())
+        return float(data["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+# ------------------------------------------------------------- CPU baseline
+
+
+def cpu_baseline_sample(vol_np, geom_np, threads=None):
+    """Time the FP64 oracle (a port of the reference's CPU checks) on a bounded sample.
+
+    Sample: the forward projection of 2 full views (2 x 384^2 rays), the FDK
+    filter of 2 views, and the backprojection of an 8-slice z-slab over all 360
+    views.  Each part is scaled to the full step by its share of the work.
+    Returns (seconds per full step, threads used, description).
+    """
+    import numpy as np
+
+    from oracle import oracle
+
+    if threads:
+        oracle.set_num_threads(threads)
+    w = WORKLOAD
+    A, U, V = w["A"], w["U"], w["V"]
+    nv = 2
+    t0 = time.perf_counter()
+    rays = np.arange(0, nv * U * V, dtype=np.int64)
+    oracle.project_rays(vol_np, geom_np, w["pixel"], U, V, w["step"], w["voxel"], rays, mode=1)
+    t_fwd = (time.perf_counter() - t0) * (A / nv)
+    proj_part = np.ones((nv, U, V), np.float32)
+    t0 = time.perf_counter()
+    filt = oracle.fdk_filter(proj_part, w["pixel"], geom_np[2][:nv], geom_np[1][:nv], w["alpha"])
+    t_filt = (time.perf_counter() - t0) * (A / nv)
+    slab = 8
+    proj_all = np.broadcast_to(filt[:1], (A, U, V))
+    t0 = time.perf_counter()
+    # the central slab: slab voxel z' sits where full-volume voxel D/2 - slab/2 + z' does
+    oracle.backproject(proj_all, geom_np, w["pixel"], (slab, w["H"], w["W"]), w["voxel"],
+                       offset=(0.0, 0.0, 0.0))
+    t_bp = (time.perf_counter() - t0) * (w["D"] / slab)
+    desc = (f"FP64 oracle on {oracle.num_threads()} threads: forward of {nv} full views, "
+            f"filter of {nv} views, backprojection of a {slab}-slice slab over {A} views; "
+            "each scaled to the full step")
+    return t_fwd + t_filt + t_bp, oracle.num_threads(), desc
+
+
+# ------------------------------------------------------------------------ arms
+
+
+def run_reference(args):
+    """The reference's CPU path (oracle port) on the host cores; rank 0 only."""
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    import numpy as np
+    import torch
+
+    from cbct_backprojector.phantoms import ellipsoid_parameters  # noqa: F401
+
+    w = WORKLOAD
+    # the same phantom as the GPU arm, generated on the CPU
+    from cbct_backprojector.phantoms import circular_geometry, ellipsoid_phantom
+
+    vol = ellipsoid_phantom((w["D"], w["H"], w["W"]), n=w["ellipsoids"], seed=instance_seed(0),
+                            voxel_size=w["voxel"], device="cpu").numpy()
+    geom = [g.numpy().astype(np.float64) for g in
+            circular_geometry(w["A"], w["U"], w["V"], w["sid"], w["sod"], w["pixel"], device="cpu")]
+    for _ in range(args.warmup):
+        cpu_baseline_sample(vol, geom)
+    times = []
+    threads, desc = 1, ""
+    for _ in range(args.steps):
+        t, threads, desc = cpu_baseline_sample(vol, geom)
+        times.append(t)
+    t_step = sum(times) / len(times)
+    rays = w["A"] * w["U"] * w["V"]
+    value = rays / t_step / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_step * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": {"workload": w["name"]},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": desc},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    del torch
+    return 0
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    from cbct_backprojector import _native, _ops
+
+    world, rank, local = dist_env()
+    if not torch.cuda.is_available():
+        raise RuntimeError("bench.py needs CUDA devices")
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    dist = init_dist(world, "nccl")
+    w = WORKLOAD
+    vol, geom = make_instance(device, instance_seed(rank))
+    R = w["A"] * w["U"] * w["V"]
+    N = w["D"] * w["H"] * w["W"] * w["A"]
+    counts = _ops.project_sample_counts((w["D"], w["H"], w["W"]), geom, w["pixel"], w["U"], w["V"],
+                                        w["step"], w["voxel"])
+    S = int(counts.sum().item())
+    del counts
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
+
+    for _ in range(max(args.warmup, 1)):
+        step(vol, geom)
+    torch.cuda.synchronize(device)
+
+    # ---- device-resident timed region
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    stops = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize(device)
+    with ClockSampler(local) as clocks, _native.trace() as tr:
+        for i in range(args.steps):
+            flush.zero_()  # L2 flush between timed steps (outside the events)
+            starts[i].record()
+            step(vol, geom)
+            stops[i].record()
+        torch.cuda.synchronize(device)
+    if dist is not None:
+        dist.barrier()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, stops)]
+    total_ms = max_over_ranks(sum(step_ms), dist, device)
+    ms_per_step = total_ms / args.steps
+    value = world * R * args.steps / (total_ms * 1e-3) / 1e9
+    kern = {}
+    for name, ms in tr.records:
+        kern.setdefault(name, []).append(ms)
+    launches = len(tr.records)
+    fwd_ms = statistics.mean(kern["fp_forward_kernel"])
+    bp_ms = statistics.mean(kern["bp_forward_kernel<fdk>"])
+    fwd_ms = max_over_ranks(fwd_ms, dist, device)
+    bp_ms = max_over_ranks(bp_ms, dist, device)
+
+    # ---- end to end through the public API with host buffers
+    vol_host = vol.cpu().pin_memory()
+    out_host = torch.empty_like(vol_host).pin_memory()
+    e_start = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    e_stop = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    vol_dev = torch.empty_like(vol)
+    for _ in range(max(1, min(args.warmup, 2))):
+        vol_dev.copy_(vol_host, non_blocking=True)
+        _, r = step(vol_dev, geom)
+        out_host.copy_(r, non_blocking=True)
+    torch.cuda.synchronize(device)
+    if dist is not None:
+        dist.barrier()
+    for i in range(args.steps):
+        flush.zero_()
+        e_start[i].record()
+        vol_dev.copy_(vol_host, non_blocking=True)
+        _, r = step(vol_dev, geom)
+        out_host.copy_(r, non_blocking=True)
+        e_stop[i].record()
+    torch.cuda.synchronize(device)
+    e2e_ms = max_over_ranks(sum(s.elapsed_time(e) for s, e in zip(e_start, e_stop)), dist, device)
+    e2e_value = world * R * args.steps / (e2e_ms * 1e-3) / 1e9
+    nbytes = vol.numel() * 4
+
+    # ---- roofline of the dominant kernel (forward projector)
+    peak, peak_kind = measured_peak_hbm()
+    alg_bytes = 32 * S + 4 * R  # trilinear gathers + projection writes per launch
+    achieved = alg_bytes / (fwd_ms * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "kernel": "fp_forward_kernel", "achieved": achieved, "peak": peak,
+                "unit": "GB/s", "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",
+                "traffic": FWD_DRAM_BYTES_PER_LAUNCH, "algorithmic_bytes": alg_bytes,
+                "samples": S, "ms": fwd_ms}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": w["name"], "volume": [w["D"], w["H"], w["W"]],
+                   "views": w["A"], "detector": [w["U"], w["V"]], "sid": w["sid"], "sod": w["sod"],
+                   "step": w["step"], "ellipsoids": w["ellipsoids"],
+                   "l2": "flushed between timed steps (256 MiB write)",
+                   "parallelism": f"independent objects x{world}"},
+        "fwd_grays_per_s": world * R / (fwd_ms * 1e-3) / 1e9,
+        "backproj_gvoxel_views_per_s": world * N / (bp_ms * 1e-3) / 1e9,
+        "kernel_ms": {k: statistics.mean(v) for k, v in kern.items()},
+        "gpu_launches": launches,
+        "roofline": roofline,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": nbytes,
+                "d2h_bytes_per_step": nbytes},
+        "clocks": clocks.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        vol_np = vol.cpu().numpy()
+        geom_np = [g.cpu().numpy().astype(np.float64) for g in geom]
+        t_cpu, threads, desc = cpu_baseline_sample(vol_np, geom_np)
+        line["cpu_baseline"] = {"value": R / t_cpu / 1e9, "unit": UNIT, "cores": threads,
+                                "kind": "port", "sample": desc}
+    if rank == 0:
+        print(json.dumps(line))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main(argv=None):
+    args = parse_args(argv)
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

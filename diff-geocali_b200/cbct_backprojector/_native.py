@@ -1,0 +1,112 @@
+"""ctypes binding of ``libdgc.so`` (the C ABI declared in ``include/dgc.h``).
+
+The library is built in-tree by ``diff-geocali_b200/build.py`` into
+``cbct_backprojector/_lib/libdgc.so``.  There is no fallback: if the library
+is missing or fails to load, every operator raises ``RuntimeError``.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libdgc.so"
+HEADER_PATH = Path(__file__).resolve().parents[2] / "include" / "dgc.h"
+
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_F = ctypes.c_float
+_D = ctypes.c_double
+_S = ctypes.c_size_t
+
+_GEOM = [_P] * 8  # angles, sid, sod, det_u0, det_v0, src_x, src_y, src_z
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "dgc_abi_version": (_I, []),
+    "dgc_last_error": (ctypes.c_char_p, []),
+    "dgc_project_workspace_bytes": (_S, [_I] * 6),
+    "dgc_project": (_I, [_P, _I, _I, _I, *_GEOM, _I, _F, _I, _I, _F, _F, _F, _F, _F, _P, _P, _S, _P]),
+    "dgc_project_sample_counts": (_I, [_I, _I, _I, *_GEOM, _I, _F, _I, _I, _F, _F, _F, _F, _F, _P, _P]),
+    "dgc_project_backward_workspace_bytes": (_S, [_I] * 7),
+    "dgc_project_backward": (_I, [_P, _P, _I, _I, _I, *_GEOM, _I, _F, _I, _I, _F, _F, _I, _F, _F, _F,
+                                  *([_P] * 9), _P, _S, _P]),
+    "dgc_backproject_workspace_bytes": (_S, [_I] * 6),
+    "dgc_backproject": (_I, [_P, _I, _I, _I, *_GEOM, _F, _I, _I, _I, _F, _F, _F, _F, _P, _P, _S, _P]),
+    "dgc_backproject_backward_workspace_bytes": (_S, [_I] * 6),
+    "dgc_backproject_backward": (_I, [_P, _P, _I, _I, _I, *_GEOM, _F, _I, _I, _I, _F, _F, _F, _F,
+                                      *([_P] * 9), _P, _S, _P]),
+    "dgc_fdk_filter_taps": (_I, [_I, _D, _D, ctypes.POINTER(_D)]),
+    "dgc_fdk_filter_workspace_bytes": (_S, [_I] * 3),
+    "dgc_fdk_filter": (_I, [_P, _I, _I, _I, _F, _P, _P, _F, _P, _P, _S, _P]),
+    "dgc_reconstruct_fdk_workspace_bytes": (_S, [_I] * 6),
+    "dgc_reconstruct_fdk": (_I, [_P, _I, _I, _I, *_GEOM, _F, _I, _I, _I, _F, _F, _F, _F, _F, _P, _P,
+                                 _S, _P]),
+    "dgc_trace_enable": (None, [_I]),
+    "dgc_trace_count": (_I, []),
+    "dgc_trace_get": (_I, [_I, ctypes.c_char_p, _I, ctypes.POINTER(_F)]),
+    "dgc_trace_clear": (None, []),
+}
+
+_lib = None
+_lock = threading.Lock()
+
+
+def lib():
+    """Load ``libdgc.so`` once; raise ``RuntimeError`` if it is unavailable."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is None:
+            path = Path(os.environ.get("DGC_LIBRARY", LIB_PATH))
+            if not path.exists():
+                raise RuntimeError(
+                    f"libdgc.so is not built ({path}). Build it with: "
+                    "python diff-geocali_b200/build.py"
+                )
+            handle = ctypes.CDLL(str(path))
+            for name, (res, args) in SIGNATURES.items():
+                fn = getattr(handle, name)
+                fn.restype = res
+                fn.argtypes = args
+            if handle.dgc_abi_version() != 1:
+                raise RuntimeError("libdgc.so ABI version mismatch")
+            _lib = handle
+    return _lib
+
+
+class trace:
+    """Context manager: CUDA-event timing of every libdgc kernel launched inside.
+
+    ``records`` holds ``(kernel_name, milliseconds)`` after exit (the exit
+    waits for the recorded events).
+    """
+
+    def __init__(self):
+        self.records = []
+
+    def __enter__(self):
+        lib().dgc_trace_clear()
+        lib().dgc_trace_enable(1)
+        return self
+
+    def __exit__(self, *exc):
+        L = lib()
+        L.dgc_trace_enable(0)
+        name = ctypes.create_string_buffer(128)
+        ms = ctypes.c_float()
+        for i in range(L.dgc_trace_count()):
+            check(L.dgc_trace_get(i, name, 128, ctypes.byref(ms)))
+            self.records.append((name.value.decode(), float(ms.value)))
+        L.dgc_trace_clear()
+        return False
+
+
+def check(status: int) -> None:
+    """Turn a non-zero status into the reference's exception type (RuntimeError)."""
+    if status != 0:
+        msg = lib().dgc_last_error().decode("utf-8", "replace")
+        raise RuntimeError(msg or f"libdgc call failed with status {status}")

@@ -1,0 +1,274 @@
+"""Tensor-level operators over ``libdgc`` with the reference's native signatures.
+
+The functions below take and return ``torch.Tensor`` objects exactly like the
+reference's pybind11 modules (TomSHINING/diff-geoCali
+``csrc/src_cbct_forwardprojector_cuda.cu:732-758`` and
+``csrc/src_cbct_backprojector_cuda.cu:524-543``): same argument names and
+defaults, same return order, outputs freshly allocated, inputs made
+contiguous, launches on the current PyTorch stream of the input's device, no
+host synchronisation.  Argument checks raise ``RuntimeError`` with the
+reference's messages.  The arithmetic runs in ``libdgc.so`` through the C ABI;
+there is no other code path.
+"""
+
+from __future__ import annotations
+
+import math
+
+import torch
+
+from . import _native
+
+_GEOM_NAMES = ("angles", "sid", "sod", "det_u0", "det_v0", "src_x", "src_y", "src_z")
+_INT_MAX = 2**31 - 1
+
+
+def _require(cond, msg):
+    if not cond:
+        raise RuntimeError(msg)
+
+
+def _workspace(nbytes: int, device) -> torch.Tensor | None:
+    if nbytes == 0:
+        return None
+    return torch.empty(int(nbytes), dtype=torch.uint8, device=device)
+
+
+def _p(t):
+    return None if t is None else t.data_ptr()
+
+
+def _stream(device) -> int:
+    return torch.cuda.current_stream(device).cuda_stream
+
+
+# ------------------------------------------------------------ forward projector
+
+
+def _fp_check_geometry(reference, geometry, expected):
+    # fp.cu:531-563
+    _require(reference.is_cuda, "reference tensor must be CUDA")
+    _require(reference.dtype == torch.float32, "reference tensor must be float32")
+    for name, t in zip(_GEOM_NAMES, geometry):
+        _require(t.is_cuda, f"{name} must be CUDA")
+        _require(t.dtype == torch.float32, f"{name} must be float32")
+        _require(t.device == reference.device,
+                 f"{name} must be on the same CUDA device as the reference tensor")
+        _require(t.numel() == expected, f"{name} must contain A elements")
+
+
+def fp_forward(volume, angles, sid, sod, det_u0_arr, det_v0_arr, src_x_arr, src_y_arr, src_z_arr,
+               pixel_size, U, V, step_size, voxel_size, off_x=0.0, off_y=0.0, off_z=0.0):
+    """Forward projection [A,U,V] (replaces ``src_cbct_forwardprojector_cuda.forward``)."""
+    geometry = (angles, sid, sod, det_u0_arr, det_v0_arr, src_x_arr, src_y_arr, src_z_arr)
+    U, V = int(U), int(V)
+    pixel_size, step_size, voxel_size = float(pixel_size), float(step_size), float(voxel_size)
+    _require(volume.dim() == 3, "volume must have shape [D,H,W]")
+    _require(U > 0 and V > 0, "U and V must be positive")
+    _require(pixel_size > 0.0 and step_size > 0.0 and voxel_size > 0.0,
+             "pixel_size, step_size and voxel_size must be positive")
+    A = angles.numel()
+    _require(A > 0, "angles must contain at least one view")
+    _fp_check_geometry(volume, geometry, A)
+    vol = volume.contiguous()
+    geom = [t.contiguous() for t in geometry]
+    D, H, W = vol.shape
+    _require(D > 0 and H > 0 and W > 0, "every volume dimension must be positive")
+    out = torch.zeros((A, U, V), dtype=torch.float32, device=vol.device)
+    lib = _native.lib()
+    with torch.cuda.device(vol.device):
+        ws = _workspace(lib.dgc_project_workspace_bytes(D, H, W, A, U, V), vol.device)
+        _native.check(lib.dgc_project(
+            vol.data_ptr(), D, H, W, *[g.data_ptr() for g in geom], A, pixel_size, U, V,
+            step_size, voxel_size, float(off_x), float(off_y), float(off_z), out.data_ptr(),
+            _p(ws), 0 if ws is None else ws.numel(), _stream(vol.device)))
+    return out
+
+
+def fp_backward(grad_projection, volume, angles, sid, sod, det_u0_arr, det_v0_arr, src_x_arr,
+                src_y_arr, src_z_arr, pixel_size, step_size, voxel_size, compute_grad_volume=True,
+                off_x=0.0, off_y=0.0, off_z=0.0):
+    """Nine gradients (replaces ``src_cbct_forwardprojector_cuda.backward``)."""
+    geometry = (angles, sid, sod, det_u0_arr, det_v0_arr, src_x_arr, src_y_arr, src_z_arr)
+    pixel_size, step_size, voxel_size = float(pixel_size), float(step_size), float(voxel_size)
+    _require(volume.dim() == 3, "volume must have shape [D,H,W]")
+    _require(grad_projection.dim() == 3, "grad_projection must have shape [A,U,V]")
+    _require(grad_projection.is_cuda and grad_projection.dtype == torch.float32,
+             "grad_projection must be a float32 CUDA tensor")
+    _require(grad_projection.device == volume.device,
+             "grad_projection and volume must be on the same CUDA device")
+    _require(pixel_size > 0.0 and step_size > 0.0 and voxel_size > 0.0,
+             "pixel_size, step_size and voxel_size must be positive")
+    A, U, V = grad_projection.shape
+    _require(A > 0 and U > 0 and V > 0, "every grad_projection dimension must be positive")
+    _fp_check_geometry(volume, geometry, A)
+    gp = grad_projection.contiguous()
+    vol = volume.contiguous()
+    geom = [t.contiguous() for t in geometry]
+    D, H, W = vol.shape
+    _require(D > 0 and H > 0 and W > 0, "every volume dimension must be positive")
+    dev = vol.device
+    compute = bool(compute_grad_volume)
+    grad_volume = torch.zeros_like(vol) if compute else torch.empty(0, dtype=vol.dtype, device=dev)
+    grads = [torch.zeros_like(g) for g in geom]
+    lib = _native.lib()
+    with torch.cuda.device(dev):
+        ws = _workspace(lib.dgc_project_backward_workspace_bytes(D, H, W, A, U, V, int(compute)), dev)
+        _native.check(lib.dgc_project_backward(
+            gp.data_ptr(), vol.data_ptr(), D, H, W, *[g.data_ptr() for g in geom], A, pixel_size,
+            U, V, step_size, voxel_size, int(compute), float(off_x), float(off_y), float(off_z),
+            grad_volume.data_ptr() if compute else None, *[g.data_ptr() for g in grads],
+            _p(ws), 0 if ws is None else ws.numel(), _stream(dev)))
+    return [grad_volume, *grads]
+
+
+# ---------------------------------------------------------------- backprojector
+
+
+def _bp_check_projection(proj):
+    # bp.cu:298-306
+    _require(proj.is_cuda and proj.dtype == torch.float32, "proj must be a CUDA float32 tensor")
+    _require(proj.dim() == 3 and proj.size(0) > 0 and proj.size(1) >= 2 and proj.size(2) >= 2,
+             "proj must have shape [A,U,V] with A >= 1 and U,V >= 2")
+    _require(proj.numel() <= _INT_MAX, "proj exceeds the kernel's 32-bit indexing limit")
+
+
+def _bp_check_geometry(proj, geometry):
+    # bp.cu:308-331
+    _bp_check_projection(proj)
+    for name, t in zip(_GEOM_NAMES, geometry):
+        _require(t.is_cuda and t.dtype == torch.float32 and t.device == proj.device and t.dim() == 1
+                 and t.numel() == proj.size(0),
+                 f"{name} must be CUDA float32 on proj.device with shape [A]")
+
+
+def _bp_check_volume_shape(D, H, W):
+    # bp.cu:333-341
+    _require(0 < D <= _INT_MAX and 0 < H <= _INT_MAX and 0 < W <= _INT_MAX,
+             "D,H,W must be positive and fit in a 32-bit integer")
+    _require(D * H * W <= _INT_MAX, "volume exceeds the kernel's 32-bit indexing limit")
+    _require(D <= 8 * 65535 and H <= 8 * 65535, "D,H exceed the kernel's 3D CUDA grid limits")
+
+
+def _finite(*values):
+    return all(math.isfinite(v) for v in values)
+
+
+def bp_forward(proj, angles, sid, sod, det_u0_arr, det_v0_arr, src_x_arr, src_y_arr, src_z_arr,
+               pixel_size, D, H, W, voxel_size, off_x=0.0, off_y=0.0, off_z=0.0):
+    """Backprojection [D,H,W] (replaces ``src_cbct_backprojector_cuda.forward``)."""
+    geometry = (angles, sid, sod, det_u0_arr, det_v0_arr, src_x_arr, src_y_arr, src_z_arr)
+    pixel_size, voxel_size = float(pixel_size), float(voxel_size)
+    off_x, off_y, off_z = float(off_x), float(off_y), float(off_z)
+    D, H, W = int(D), int(H), int(W)
+    _bp_check_geometry(proj, geometry)
+    _bp_check_volume_shape(D, H, W)
+    _require(_finite(pixel_size, voxel_size, off_x, off_y, off_z),
+             "sizes and ROI offsets must be finite")
+    _require(pixel_size > 0.0 and voxel_size > 0.0, "pixel_size and voxel_size must be positive")
+    p = proj.contiguous()
+    geom = [t.contiguous() for t in geometry]
+    A, U, V = p.shape
+    dev = p.device
+    vol = torch.zeros((D, H, W), dtype=torch.float32, device=dev)
+    lib = _native.lib()
+    with torch.cuda.device(dev):
+        ws = _workspace(lib.dgc_backproject_workspace_bytes(A, U, V, D, H, W), dev)
+        _native.check(lib.dgc_backproject(
+            p.data_ptr(), A, U, V, *[g.data_ptr() for g in geom], pixel_size, D, H, W, voxel_size,
+            off_x, off_y, off_z, vol.data_ptr(), _p(ws), 0 if ws is None else ws.numel(),
+            _stream(dev)))
+    return vol
+
+
+def bp_backward(grad_vol, proj, angles, sid, sod, det_u0_arr, det_v0_arr, src_x_arr, src_y_arr,
+                src_z_arr, pixel_size, voxel_size, off_x=0.0, off_y=0.0, off_z=0.0):
+    """Nine gradients (replaces ``src_cbct_backprojector_cuda.backward``)."""
+    geometry = (angles, sid, sod, det_u0_arr, det_v0_arr, src_x_arr, src_y_arr, src_z_arr)
+    pixel_size, voxel_size = float(pixel_size), float(voxel_size)
+    off_x, off_y, off_z = float(off_x), float(off_y), float(off_z)
+    _bp_check_geometry(proj, geometry)
+    _require(grad_vol.is_cuda and grad_vol.dtype == torch.float32 and grad_vol.device == proj.device
+             and grad_vol.dim() == 3,
+             "grad_vol must be CUDA float32 on proj.device with shape [D,H,W]")
+    _bp_check_volume_shape(*grad_vol.shape)
+    _require(_finite(pixel_size, voxel_size, off_x, off_y, off_z) and pixel_size > 0.0
+             and voxel_size > 0.0,
+             "sizes must be finite and positive; ROI offsets must be finite")
+    gv = grad_vol.contiguous()
+    p = proj.contiguous()
+    geom = [t.contiguous() for t in geometry]
+    A, U, V = p.shape
+    D, H, W = gv.shape
+    dev = p.device
+    grad_proj = torch.zeros_like(p)
+    grads = [torch.zeros_like(g) for g in geom]
+    lib = _native.lib()
+    with torch.cuda.device(dev):
+        ws = _workspace(lib.dgc_backproject_backward_workspace_bytes(A, U, V, D, H, W), dev)
+        _native.check(lib.dgc_backproject_backward(
+            gv.data_ptr(), p.data_ptr(), A, U, V, *[g.data_ptr() for g in geom], pixel_size, D, H,
+            W, voxel_size, off_x, off_y, off_z, grad_proj.data_ptr(),
+            *[g.data_ptr() for g in grads], _p(ws), 0 if ws is None else ws.numel(), _stream(dev)))
+    return [grad_proj, *grads]
+
+
+# ------------------------------------------------------------------------- FDK
+
+
+def fdk_filter(projections, pixel_size, sod, sid, alpha):
+    """Cosine-weighted ramp filter along U; ``sod``/``sid`` are CUDA float32 [A]."""
+    A, U, V = projections.shape
+    p = projections.contiguous()
+    dev = p.device
+    out = torch.empty_like(p)
+    lib = _native.lib()
+    with torch.cuda.device(dev):
+        ws = _workspace(lib.dgc_fdk_filter_workspace_bytes(A, U, V), dev)
+        _native.check(lib.dgc_fdk_filter(
+            p.data_ptr(), A, U, V, float(pixel_size), sod.data_ptr(), sid.data_ptr(), float(alpha),
+            out.data_ptr(), _p(ws), 0 if ws is None else ws.numel(), _stream(dev)))
+    return out
+
+
+def reconstruct_fdk(projections, geometry, pixel_size, volume_shape, voxel_size, volume_offset,
+                    alpha):
+    """Filter + backproject all views, * pi/A, clamp at 0, in two kernels."""
+    p = projections.contiguous()
+    geom = [t.contiguous() for t in geometry]
+    A, U, V = p.shape
+    D, H, W = volume_shape
+    dev = p.device
+    vol = torch.empty((D, H, W), dtype=torch.float32, device=dev)
+    lib = _native.lib()
+    with torch.cuda.device(dev):
+        ws = _workspace(lib.dgc_reconstruct_fdk_workspace_bytes(A, U, V, D, H, W), dev)
+        _native.check(lib.dgc_reconstruct_fdk(
+            p.data_ptr(), A, U, V, *[g.data_ptr() for g in geom], float(pixel_size), D, H, W,
+            float(voxel_size), *map(float, volume_offset), float(alpha), vol.data_ptr(), _p(ws),
+            0 if ws is None else ws.numel(), _stream(dev)))
+    return vol
+
+
+def fdk_filter_taps(U: int, pixel_size: float, alpha: float):
+    """Host-only filter taps h[0..U-1] (FP64), for inspection and tests."""
+    import ctypes
+
+    buf = (ctypes.c_double * int(U))()
+    _native.check(_native.lib().dgc_fdk_filter_taps(int(U), float(pixel_size), float(alpha), buf))
+    return list(buf)
+
+
+def project_sample_counts(volume_shape, geometry, pixel_size, U, V, step_size, voxel_size,
+                          offset=(0.0, 0.0, 0.0)):
+    """int64 [A,U,V] number of trilinear samples per ray (FP32 stepping rule)."""
+    geom = [t.contiguous() for t in geometry]
+    A = geom[0].numel()
+    D, H, W = volume_shape
+    dev = geom[0].device
+    out = torch.empty((A, int(U), int(V)), dtype=torch.int64, device=dev)
+    with torch.cuda.device(dev):
+        _native.check(_native.lib().dgc_project_sample_counts(
+            D, H, W, *[g.data_ptr() for g in geom], A, float(pixel_size), int(U), int(V),
+            float(step_size), float(voxel_size), *map(float, offset), out.data_ptr(), _stream(dev)))
+    return out

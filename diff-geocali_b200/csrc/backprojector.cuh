@@ -1,0 +1,40 @@
+// backprojector.cuh -- launch interface of the backprojector kernels.
+#pragma once
+
+#include "common.cuh"
+
+namespace dgc {
+
+// Per-view terms shared by every voxel of a view (48 bytes).
+struct ViewRow {
+    float c, s;          // cos, sin of the view angle
+    float ds_u, ds_n;    // source offset in the rotating detector frame
+    float ds_v;          // src_z
+    float sod, sid, u0, v0;
+    float pad0, pad1, pad2;
+};
+
+struct BpArgs {
+    const ViewRow* vt;     // [A]
+    const float4* pquads;  // [A][U-1][V-1]
+    int A, U, V, D, H, W;
+    float pixel_size, inv_pixel, voxel_size;
+    float off_x, off_y, off_z;
+    // forward
+    float* volume;     // [D][H][W]
+    float out_scale;   // FDK epilogue scale (pi/A)
+    // backward
+    const float* grad_volume;  // [D][H][W]
+    float* grad_projections;   // [A][U][V], zeroed by the caller
+    double* partials;          // [A][8][blocks]
+};
+
+int bp_view_table(const Geometry& g, int A, ViewRow* vt, cudaStream_t s);
+int build_proj_quads(const float* P, int A, int U, int V, float4* PQ, cudaStream_t s);
+int bp_launch_forward(const BpArgs& p, bool fdk, cudaStream_t s);
+int bp_launch_backward(const BpArgs& p, cudaStream_t s);
+long long bp_backward_blocks(int D, int H, int W);
+int bp_reduce_partials(const double* partials, int A, long long nblocks, const GeometryGrad& out,
+                       cudaStream_t s);
+
+}  // namespace dgc

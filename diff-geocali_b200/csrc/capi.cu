@@ -1,0 +1,463 @@
+// capi.cu -- extern "C" entry points of libdgc (see include/dgc.h).
+//
+// Argument checks reproduce the conditions of the reference's host wrappers
+// (TomSHINING/diff-geoCali csrc/src_cbct_forwardprojector_cuda.cu:531-729 and
+// csrc/src_cbct_backprojector_cuda.cu:298-522) with the same messages; a
+// failed check returns DGC_ERR_INVALID_ARGUMENT, which the Python layer raises
+// as RuntimeError exactly where the reference's TORCH_CHECK would.
+#include <climits>
+#include <cmath>
+#include <cstdlib>
+#include <string>
+
+#include "backprojector.cuh"
+#include "common.cuh"
+#include "fdk.cuh"
+#include "forward_projector.cuh"
+
+namespace dgc {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+void clear_error() { g_last_error.clear(); }
+
+namespace {
+
+Geometry make_geometry(const float* angles, const float* sid, const float* sod,
+                       const float* det_u0, const float* det_v0, const float* src_x,
+                       const float* src_y, const float* src_z) {
+    Geometry g;
+    g.angles = angles;
+    g.sid = sid;
+    g.sod = sod;
+    g.det_u0 = det_u0;
+    g.det_v0 = det_v0;
+    g.src_x = src_x;
+    g.src_y = src_y;
+    g.src_z = src_z;
+    return g;
+}
+
+bool geometry_ok(const Geometry& g) {
+    return g.angles && g.sid && g.sod && g.det_u0 && g.det_v0 && g.src_x && g.src_y && g.src_z;
+}
+
+size_t quad_volume_bytes(int D, int H, int W) {
+    return Workspace::align(sizeof(float4) * (size_t)(D + 2) * (size_t)(H + 1) * (size_t)(W + 1));
+}
+
+size_t padded_volume_bytes(int D, int H, int W) {
+    return Workspace::align(sizeof(float) * (size_t)(D + 2) * (size_t)(H + 2) * (size_t)(W + 2));
+}
+
+// Ray tile of the forward projector: DGC_FP_TILE="tu,wu" overrides the default.
+FpTile forward_tile() {
+    FpTile t{16, 8};
+    if (const char* e = std::getenv("DGC_FP_TILE")) {
+        int tu = 0, wu = 0;
+        if (sscanf(e, "%d,%d", &tu, &wu) == 2) t = FpTile{tu, wu};
+    }
+    return t;
+}
+
+constexpr FpTile kBackwardTile{16, 8};
+
+int check_fp_common(int D, int H, int W, int A, int U, int V, float pixel_size, float step_size,
+                    float voxel_size, const Geometry& g) {
+    DGC_REQUIRE(D > 0 && H > 0 && W > 0, "every volume dimension must be positive");
+    DGC_REQUIRE(U > 0 && V > 0, "U and V must be positive");
+    DGC_REQUIRE(pixel_size > 0.0f && step_size > 0.0f && voxel_size > 0.0f,
+                "pixel_size, step_size and voxel_size must be positive");
+    DGC_REQUIRE(A > 0, "angles must contain at least one view");
+    DGC_REQUIRE(geometry_ok(g), "geometry pointers must be non-null");
+    if ((long long)(D + 2) * (H + 1) * (W + 1) >= (1LL << 31)) {
+        set_error("volume exceeds this build's 2^31 padded-voxel index limit");
+        return DGC_ERR_UNSUPPORTED;
+    }
+    if (fp_tiles_per_view(U, V, 8) * (long long)A >= (1LL << 31)) {
+        set_error("too many rays for one launch");
+        return DGC_ERR_UNSUPPORTED;
+    }
+    return DGC_OK;
+}
+
+int check_bp_common(int A, int U, int V, int D, int H, int W, float pixel_size, float voxel_size,
+                    float off_x, float off_y, float off_z, const Geometry& g) {
+    DGC_REQUIRE(A > 0 && U >= 2 && V >= 2, "proj must have shape [A,U,V] with A >= 1 and U,V >= 2");
+    DGC_REQUIRE((long long)A * U * V <= INT_MAX, "proj exceeds the kernel's 32-bit indexing limit");
+    DGC_REQUIRE(D > 0 && H > 0 && W > 0, "D,H,W must be positive and fit in a 32-bit integer");
+    DGC_REQUIRE((long long)D * H * W <= INT_MAX, "volume exceeds the kernel's 32-bit indexing limit");
+    DGC_REQUIRE(D <= 8 * 65535 && H <= 8 * 65535, "D,H exceed the kernel's 3D CUDA grid limits");
+    DGC_REQUIRE(std::isfinite(pixel_size) && std::isfinite(voxel_size) && std::isfinite(off_x) &&
+                    std::isfinite(off_y) && std::isfinite(off_z),
+                "sizes and ROI offsets must be finite");
+    DGC_REQUIRE(pixel_size > 0.0f && voxel_size > 0.0f, "pixel_size and voxel_size must be positive");
+    DGC_REQUIRE(geometry_ok(g), "geometry pointers must be non-null");
+    return DGC_OK;
+}
+
+size_t bp_table_bytes(int A) { return Workspace::align(sizeof(ViewRow) * (size_t)A); }
+
+size_t bp_quads_bytes(int A, int U, int V) {
+    return Workspace::align(sizeof(float4) * (size_t)A * (size_t)(U - 1) * (size_t)(V - 1));
+}
+
+BpArgs bp_args(const ViewRow* vt, const float4* pq, int A, int U, int V, int D, int H, int W,
+               float pixel_size, float voxel_size, float ox, float oy, float oz) {
+    BpArgs p;
+    memset(&p, 0, sizeof(p));
+    p.vt = vt;
+    p.pquads = pq;
+    p.A = A;
+    p.U = U;
+    p.V = V;
+    p.D = D;
+    p.H = H;
+    p.W = W;
+    p.pixel_size = pixel_size;
+    p.inv_pixel = 1.0f / pixel_size;
+    p.voxel_size = voxel_size;
+    p.off_x = ox;
+    p.off_y = oy;
+    p.off_z = oz;
+    p.out_scale = 1.0f;
+    return p;
+}
+
+}  // namespace
+}  // namespace dgc
+
+using namespace dgc;
+
+extern "C" {
+
+int dgc_abi_version(void) { return DGC_ABI_VERSION; }
+
+const char* dgc_last_error(void) { return g_last_error.c_str(); }
+
+// ----------------------------------------------------------------- forward
+
+size_t dgc_project_workspace_bytes(int D, int H, int W, int A, int U, int V) {
+    (void)A;
+    (void)U;
+    (void)V;
+    if (D <= 0 || H <= 0 || W <= 0) return 0;
+    return quad_volume_bytes(D, H, W);
+}
+
+static int project_impl(const float* volume, int D, int H, int W, const Geometry& g, int A,
+                        float pixel_size, int U, int V, float step_size, float voxel_size,
+                        float off_x, float off_y, float off_z, float* projections,
+                        int64_t* counts, void* workspace, size_t workspace_bytes,
+                        cudaStream_t s) {
+    clear_error();
+    int rc = check_fp_common(D, H, W, A, U, V, pixel_size, step_size, voxel_size, g);
+    if (rc != DGC_OK) return rc;
+    FpArgs p;
+    memset(&p, 0, sizeof(p));
+    p.g = g;
+    p.D = D;
+    p.H = H;
+    p.W = W;
+    p.A = A;
+    p.U = U;
+    p.V = V;
+    p.pixel_size = pixel_size;
+    p.step_size = step_size;
+    p.voxel_size = voxel_size;
+    p.off_x = off_x;
+    p.off_y = off_y;
+    p.off_z = off_z;
+    fp_fill_layout(p);
+    if (counts) return fp_launch_counts(p, counts, s);
+    DGC_REQUIRE(volume && projections, "volume and projections must be non-null");
+    Workspace ws(workspace, workspace_bytes);
+    float4* quads = ws.take<float4>((size_t)(D + 2) * (H + 1) * (W + 1));
+    if (!quads) {
+        set_error("workspace too small: dgc_project needs " +
+                  std::to_string(dgc_project_workspace_bytes(D, H, W, A, U, V)) + " bytes");
+        return DGC_ERR_WORKSPACE;
+    }
+    p.quads = quads;
+    p.projections = projections;
+    rc = build_volume_quads(volume, D, H, W, quads, s);
+    if (rc != DGC_OK) return rc;
+    return fp_launch_forward(p, forward_tile(), s);
+}
+
+int dgc_project(const float* volume, int D, int H, int W, const float* angles, const float* sid,
+                const float* sod, const float* det_u0, const float* det_v0, const float* src_x,
+                const float* src_y, const float* src_z, int A, float pixel_size, int U, int V,
+                float step_size, float voxel_size, float off_x, float off_y, float off_z,
+                float* projections, void* workspace, size_t workspace_bytes, void* stream) {
+    const Geometry g = make_geometry(angles, sid, sod, det_u0, det_v0, src_x, src_y, src_z);
+    return project_impl(volume, D, H, W, g, A, pixel_size, U, V, step_size, voxel_size, off_x,
+                        off_y, off_z, projections, nullptr, workspace, workspace_bytes,
+                        (cudaStream_t)stream);
+}
+
+int dgc_project_sample_counts(int D, int H, int W, const float* angles, const float* sid,
+                              const float* sod, const float* det_u0, const float* det_v0,
+                              const float* src_x, const float* src_y, const float* src_z, int A,
+                              float pixel_size, int U, int V, float step_size, float voxel_size,
+                              float off_x, float off_y, float off_z, int64_t* counts,
+                              void* stream) {
+    if (!counts) {
+        set_error("counts must be non-null");
+        return DGC_ERR_INVALID_ARGUMENT;
+    }
+    const Geometry g = make_geometry(angles, sid, sod, det_u0, det_v0, src_x, src_y, src_z);
+    return project_impl(nullptr, D, H, W, g, A, pixel_size, U, V, step_size, voxel_size, off_x,
+                        off_y, off_z, nullptr, counts, nullptr, 0, (cudaStream_t)stream);
+}
+
+size_t dgc_project_backward_workspace_bytes(int D, int H, int W, int A, int U, int V,
+                                            int compute_grad_volume) {
+    if (D <= 0 || H <= 0 || W <= 0 || A <= 0 || U <= 0 || V <= 0) return 0;
+    size_t n = quad_volume_bytes(D, H, W);
+    if (compute_grad_volume) n += padded_volume_bytes(D, H, W);
+    n += Workspace::align(sizeof(double) * 8 * (size_t)A *
+                          (size_t)fp_tiles_per_view(U, V, kBackwardTile.tu));
+    return n;
+}
+
+int dgc_project_backward(const float* grad_projection, const float* volume, int D, int H, int W,
+                         const float* angles, const float* sid, const float* sod,
+                         const float* det_u0, const float* det_v0, const float* src_x,
+                         const float* src_y, const float* src_z, int A, float pixel_size, int U,
+                         int V, float step_size, float voxel_size, int compute_grad_volume,
+                         float off_x, float off_y, float off_z, float* grad_volume,
+                         float* grad_angles, float* grad_sid, float* grad_sod,
+                         float* grad_det_u0, float* grad_det_v0, float* grad_src_x,
+                         float* grad_src_y, float* grad_src_z, void* workspace,
+                         size_t workspace_bytes, void* stream) {
+    clear_error();
+    cudaStream_t s = (cudaStream_t)stream;
+    const Geometry g = make_geometry(angles, sid, sod, det_u0, det_v0, src_x, src_y, src_z);
+    int rc = check_fp_common(D, H, W, A, U, V, pixel_size, step_size, voxel_size, g);
+    if (rc != DGC_OK) return rc;
+    DGC_REQUIRE(grad_projection && volume, "grad_projection and volume must be non-null");
+    DGC_REQUIRE(!compute_grad_volume || grad_volume, "grad_volume must be non-null");
+    GeometryGrad out{{grad_angles, grad_sid, grad_sod, grad_det_u0, grad_det_v0, grad_src_x,
+                      grad_src_y, grad_src_z}};
+    for (int k = 0; k < 8; ++k) DGC_REQUIRE(out.g[k], "geometry gradient pointers must be non-null");
+    FpArgs p;
+    memset(&p, 0, sizeof(p));
+    p.g = g;
+    p.D = D;
+    p.H = H;
+    p.W = W;
+    p.A = A;
+    p.U = U;
+    p.V = V;
+    p.pixel_size = pixel_size;
+    p.step_size = step_size;
+    p.voxel_size = voxel_size;
+    p.off_x = off_x;
+    p.off_y = off_y;
+    p.off_z = off_z;
+    fp_fill_layout(p);
+    const long long tiles = fp_tiles_per_view(U, V, kBackwardTile.tu);
+    Workspace ws(workspace, workspace_bytes);
+    float4* quads = ws.take<float4>((size_t)(D + 2) * (H + 1) * (W + 1));
+    float* gpad = compute_grad_volume ? ws.take<float>((size_t)(D + 2) * (H + 2) * (W + 2)) : nullptr;
+    double* partials = ws.take<double>((size_t)8 * A * tiles);
+    if (!quads || !partials || (compute_grad_volume && !gpad)) {
+        set_error("workspace too small: dgc_project_backward needs " +
+                  std::to_string(dgc_project_backward_workspace_bytes(D, H, W, A, U, V,
+                                                                      compute_grad_volume)) +
+                  " bytes");
+        return DGC_ERR_WORKSPACE;
+    }
+    p.quads = quads;
+    p.grad_projections = grad_projection;
+    p.grad_pad = gpad;
+    p.partials = partials;
+    rc = build_volume_quads(volume, D, H, W, quads, s);
+    if (rc != DGC_OK) return rc;
+    if (gpad) DGC_CUDA(cudaMemsetAsync(gpad, 0, sizeof(float) * (size_t)(D + 2) * (H + 2) * (W + 2), s));
+    rc = fp_launch_backward(p, kBackwardTile, compute_grad_volume != 0, s);
+    if (rc != DGC_OK) return rc;
+    rc = fp_reduce_partials(partials, A, tiles, out, s);
+    if (rc != DGC_OK) return rc;
+    if (gpad) return fp_fold_gradient(gpad, D, H, W, grad_volume, s);
+    return DGC_OK;
+}
+
+// ----------------------------------------------------------- backprojector
+
+size_t dgc_backproject_workspace_bytes(int A, int U, int V, int D, int H, int W) {
+    (void)D;
+    (void)H;
+    (void)W;
+    if (A <= 0 || U < 2 || V < 2) return 0;
+    return bp_table_bytes(A) + bp_quads_bytes(A, U, V);
+}
+
+int dgc_backproject(const float* projections, int A, int U, int V, const float* angles,
+                    const float* sid, const float* sod, const float* det_u0, const float* det_v0,
+                    const float* src_x, const float* src_y, const float* src_z, float pixel_size,
+                    int D, int H, int W, float voxel_size, float off_x, float off_y, float off_z,
+                    float* volume, void* workspace, size_t workspace_bytes, void* stream) {
+    clear_error();
+    cudaStream_t s = (cudaStream_t)stream;
+    const Geometry g = make_geometry(angles, sid, sod, det_u0, det_v0, src_x, src_y, src_z);
+    int rc = check_bp_common(A, U, V, D, H, W, pixel_size, voxel_size, off_x, off_y, off_z, g);
+    if (rc != DGC_OK) return rc;
+    DGC_REQUIRE(projections && volume, "projections and volume must be non-null");
+    Workspace ws(workspace, workspace_bytes);
+    ViewRow* vt = ws.take<ViewRow>((size_t)A);
+    float4* pq = ws.take<float4>((size_t)A * (U - 1) * (V - 1));
+    if (!vt || !pq) {
+        set_error("workspace too small: dgc_backproject needs " +
+                  std::to_string(dgc_backproject_workspace_bytes(A, U, V, D, H, W)) + " bytes");
+        return DGC_ERR_WORKSPACE;
+    }
+    if ((rc = bp_view_table(g, A, vt, s)) != DGC_OK) return rc;
+    if ((rc = build_proj_quads(projections, A, U, V, pq, s)) != DGC_OK) return rc;
+    BpArgs p = bp_args(vt, pq, A, U, V, D, H, W, pixel_size, voxel_size, off_x, off_y, off_z);
+    p.volume = volume;
+    return bp_launch_forward(p, false, s);
+}
+
+size_t dgc_backproject_backward_workspace_bytes(int A, int U, int V, int D, int H, int W) {
+    if (A <= 0 || U < 2 || V < 2 || D <= 0 || H <= 0 || W <= 0) return 0;
+    return bp_table_bytes(A) + bp_quads_bytes(A, U, V) +
+           Workspace::align(sizeof(double) * 8 * (size_t)A * (size_t)bp_backward_blocks(D, H, W));
+}
+
+int dgc_backproject_backward(const float* grad_volume, const float* projections, int A, int U,
+                             int V, const float* angles, const float* sid, const float* sod,
+                             const float* det_u0, const float* det_v0, const float* src_x,
+                             const float* src_y, const float* src_z, float pixel_size, int D,
+                             int H, int W, float voxel_size, float off_x, float off_y,
+                             float off_z, float* grad_projections, float* grad_angles,
+                             float* grad_sid, float* grad_sod, float* grad_det_u0,
+                             float* grad_det_v0, float* grad_src_x, float* grad_src_y,
+                             float* grad_src_z, void* workspace, size_t workspace_bytes,
+                             void* stream) {
+    clear_error();
+    cudaStream_t s = (cudaStream_t)stream;
+    const Geometry g = make_geometry(angles, sid, sod, det_u0, det_v0, src_x, src_y, src_z);
+    int rc = check_bp_common(A, U, V, D, H, W, pixel_size, voxel_size, off_x, off_y, off_z, g);
+    if (rc != DGC_OK) return rc;
+    DGC_REQUIRE(grad_volume && projections && grad_projections,
+                "grad_vol, proj and grad_proj must be non-null");
+    GeometryGrad out{{grad_angles, grad_sid, grad_sod, grad_det_u0, grad_det_v0, grad_src_x,
+                      grad_src_y, grad_src_z}};
+    for (int k = 0; k < 8; ++k) DGC_REQUIRE(out.g[k], "geometry gradient pointers must be non-null");
+    const long long nblocks = bp_backward_blocks(D, H, W);
+    Workspace ws(workspace, workspace_bytes);
+    ViewRow* vt = ws.take<ViewRow>((size_t)A);
+    float4* pq = ws.take<float4>((size_t)A * (U - 1) * (V - 1));
+    double* partials = ws.take<double>((size_t)8 * A * nblocks);
+    if (!vt || !pq || !partials) {
+        set_error("workspace too small: dgc_backproject_backward needs " +
+                  std::to_string(dgc_backproject_backward_workspace_bytes(A, U, V, D, H, W)) +
+                  " bytes");
+        return DGC_ERR_WORKSPACE;
+    }
+    if ((rc = bp_view_table(g, A, vt, s)) != DGC_OK) return rc;
+    if ((rc = build_proj_quads(projections, A, U, V, pq, s)) != DGC_OK) return rc;
+    DGC_CUDA(cudaMemsetAsync(grad_projections, 0, sizeof(float) * (size_t)A * U * V, s));
+    BpArgs p = bp_args(vt, pq, A, U, V, D, H, W, pixel_size, voxel_size, off_x, off_y, off_z);
+    p.grad_volume = grad_volume;
+    p.grad_projections = grad_projections;
+    p.partials = partials;
+    if ((rc = bp_launch_backward(p, s)) != DGC_OK) return rc;
+    return bp_reduce_partials(partials, A, nblocks, out, s);
+}
+
+// --------------------------------------------------------------------- FDK
+
+int dgc_fdk_filter_taps(int U, double pixel_size, double alpha, double* taps) {
+    clear_error();
+    DGC_REQUIRE(U > 0 && taps, "U must be positive and taps non-null");
+    DGC_REQUIRE(std::isfinite(pixel_size) && pixel_size > 0.0, "pixel_size must be finite and positive");
+    DGC_REQUIRE(std::isfinite(alpha) && alpha > 0.0 && alpha <= 1.0, "alpha must satisfy 0 < alpha <= 1");
+    std::vector<double> h;
+    int rc = fdk_taps_host(U, pixel_size, alpha, h);
+    if (rc != DGC_OK) return rc;
+    for (int i = 0; i < U; ++i) taps[i] = h[i];
+    return DGC_OK;
+}
+
+size_t dgc_fdk_filter_workspace_bytes(int A, int U, int V) {
+    (void)A;
+    (void)V;
+    if (U <= 0) return 0;
+    return Workspace::align(sizeof(float) * (size_t)U);
+}
+
+static int check_fdk(int A, int U, int V, float pixel_size, float alpha) {
+    DGC_REQUIRE(A > 0 && U > 0 && V > 0, "projections must have a nonempty [A, U, V] shape");
+    DGC_REQUIRE(std::isfinite(pixel_size) && pixel_size > 0.0f, "pixel_size must be finite and positive");
+    DGC_REQUIRE(std::isfinite(alpha) && alpha > 0.0f, "alpha must be finite and positive");
+    DGC_REQUIRE(alpha <= 1.0f, "alpha must satisfy 0 < alpha <= 1");
+    return DGC_OK;
+}
+
+int dgc_fdk_filter(const float* projections, int A, int U, int V, float pixel_size,
+                   const float* sod, const float* sid, float alpha, float* filtered,
+                   void* workspace, size_t workspace_bytes, void* stream) {
+    clear_error();
+    cudaStream_t s = (cudaStream_t)stream;
+    int rc = check_fdk(A, U, V, pixel_size, alpha);
+    if (rc != DGC_OK) return rc;
+    DGC_REQUIRE(projections && sod && sid && filtered, "pointers must be non-null");
+    Workspace ws(workspace, workspace_bytes);
+    float* taps = ws.take<float>((size_t)U);
+    if (!taps) {
+        set_error("workspace too small: dgc_fdk_filter needs " +
+                  std::to_string(dgc_fdk_filter_workspace_bytes(A, U, V)) + " bytes");
+        return DGC_ERR_WORKSPACE;
+    }
+    if ((rc = fdk_upload_taps(U, pixel_size, alpha, taps, s)) != DGC_OK) return rc;
+    FdkArgs f{projections, sod, sid, taps, filtered, A, U, V, pixel_size};
+    return fdk_launch_filter(f, s);
+}
+
+size_t dgc_reconstruct_fdk_workspace_bytes(int A, int U, int V, int D, int H, int W) {
+    if (A <= 0 || U < 2 || V < 2) return 0;
+    return dgc_fdk_filter_workspace_bytes(A, U, V) +
+           Workspace::align(sizeof(float) * (size_t)A * U * V) +
+           dgc_backproject_workspace_bytes(A, U, V, D, H, W);
+}
+
+int dgc_reconstruct_fdk(const float* projections, int A, int U, int V, const float* angles,
+                        const float* sid, const float* sod, const float* det_u0,
+                        const float* det_v0, const float* src_x, const float* src_y,
+                        const float* src_z, float pixel_size, int D, int H, int W,
+                        float voxel_size, float off_x, float off_y, float off_z, float alpha,
+                        float* volume, void* workspace, size_t workspace_bytes, void* stream) {
+    clear_error();
+    cudaStream_t s = (cudaStream_t)stream;
+    const Geometry g = make_geometry(angles, sid, sod, det_u0, det_v0, src_x, src_y, src_z);
+    int rc = check_fdk(A, U, V, pixel_size, alpha);
+    if (rc != DGC_OK) return rc;
+    rc = check_bp_common(A, U, V, D, H, W, pixel_size, voxel_size, off_x, off_y, off_z, g);
+    if (rc != DGC_OK) return rc;
+    DGC_REQUIRE(projections && volume, "projections and volume must be non-null");
+    Workspace ws(workspace, workspace_bytes);
+    float* taps = ws.take<float>((size_t)U);
+    float* filtered = ws.take<float>((size_t)A * U * V);
+    ViewRow* vt = ws.take<ViewRow>((size_t)A);
+    float4* pq = ws.take<float4>((size_t)A * (U - 1) * (V - 1));
+    if (!taps || !filtered || !vt || !pq) {
+        set_error("workspace too small: dgc_reconstruct_fdk needs " +
+                  std::to_string(dgc_reconstruct_fdk_workspace_bytes(A, U, V, D, H, W)) + " bytes");
+        return DGC_ERR_WORKSPACE;
+    }
+    if ((rc = fdk_upload_taps(U, pixel_size, alpha, taps, s)) != DGC_OK) return rc;
+    FdkArgs f{projections, sod, sid, taps, filtered, A, U, V, pixel_size};
+    if ((rc = fdk_launch_filter(f, s)) != DGC_OK) return rc;
+    if ((rc = bp_view_table(g, A, vt, s)) != DGC_OK) return rc;
+    if ((rc = build_proj_quads(filtered, A, U, V, pq, s)) != DGC_OK) return rc;
+    BpArgs p = bp_args(vt, pq, A, U, V, D, H, W, pixel_size, voxel_size, off_x, off_y, off_z);
+    p.volume = volume;
+    p.out_scale = (float)(M_PI / (double)A);
+    return bp_launch_forward(p, true, s);
+}
+
+}  // extern "C"

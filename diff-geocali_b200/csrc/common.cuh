@@ -1,0 +1,141 @@
+// common.cuh -- shared device helpers and host plumbing of libdgc (sm_100a).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stddef.h>
+
+#include <cfloat>
+#include <cstring>
+#include <algorithm>
+#include <string>
+
+#include "dgc.h"
+#include "trace.cuh"
+
+namespace dgc {
+
+// ---------------------------------------------------------------------------
+// Host-side status plumbing
+// ---------------------------------------------------------------------------
+
+void set_error(const std::string& msg);
+void clear_error();
+
+struct Fail {
+    int code;
+};
+
+#define DGC_REQUIRE(cond, msg)                                          \
+    do {                                                                \
+        if (!(cond)) {                                                  \
+            ::dgc::set_error(std::string(msg));                         \
+            return DGC_ERR_INVALID_ARGUMENT;                            \
+        }                                                               \
+    } while (0)
+
+#define DGC_CUDA(call)                                                          \
+    do {                                                                        \
+        cudaError_t e__ = (call);                                               \
+        if (e__ != cudaSuccess) {                                               \
+            ::dgc::set_error(std::string(#call) + ": " + cudaGetErrorString(e__)); \
+            return DGC_ERR_CUDA;                                                \
+        }                                                                       \
+    } while (0)
+
+#define DGC_LAUNCH_CHECK(what)                                                   \
+    do {                                                                        \
+        cudaError_t e__ = cudaGetLastError();                                   \
+        if (e__ != cudaSuccess) {                                               \
+            ::dgc::set_error(std::string(what) + " launch failed: " +            \
+                             cudaGetErrorString(e__));                          \
+            return DGC_ERR_CUDA;                                                \
+        }                                                                       \
+    } while (0)
+
+// Bump allocator over a caller-owned workspace (256-byte aligned slices).
+struct Workspace {
+    char* base;
+    size_t size;
+    size_t used;
+    Workspace(void* p, size_t n) : base(static_cast<char*>(p)), size(n), used(0) {}
+    static size_t align(size_t n) { return (n + 255) & ~size_t(255); }
+    template <typename T>
+    T* take(size_t count) {
+        size_t bytes = align(count * sizeof(T));
+        if (base == nullptr || used + bytes > size) return nullptr;
+        T* p = reinterpret_cast<T*>(base + used);
+        used += bytes;
+        return p;
+    }
+};
+
+inline int ceil_div(long long a, long long b) { return static_cast<int>((a + b - 1) / b); }
+
+// Power-of-two test of a positive finite float: for such a value x/v and
+// x*(1/v) are bitwise identical, so the reference's divisions by
+// voxel_size / pixel_size may be executed as multiplications.
+inline bool is_pow2_float(float v) {
+    if (!(v > 0.0f)) return false;
+    uint32_t bits;
+    memcpy(&bits, &v, sizeof(bits));
+    uint32_t exp = (bits >> 23) & 0xffu;
+    return (bits & 0x7fffffu) == 0 && exp > 0 && exp < 254;
+}
+
+// ---------------------------------------------------------------------------
+// Device helpers
+// ---------------------------------------------------------------------------
+
+// floor() of |x| < 2^22 with full-rate FP32 adds: adding 1.5*2^23 with
+// round-toward-minus-infinity leaves floor(x) in the low mantissa bits.
+constexpr float kFloorMagic = 12582912.0f;        // 1.5 * 2^23
+constexpr uint32_t kFloorMagicBits = 0x4B400000u;  // bit pattern of kFloorMagic
+
+struct FloorSplit {
+    uint32_t biased;  // kFloorMagicBits + floor(x) (modular arithmetic)
+    float frac;       // x - floor(x), exact
+};
+
+__device__ __forceinline__ FloorSplit floor_split(float x) {
+    const float f = __fadd_rd(x, kFloorMagic);
+    FloorSplit r;
+    r.biased = __float_as_uint(f);
+    r.frac = __fsub_rn(x, __fsub_rn(f, kFloorMagic));
+    return r;
+}
+
+__device__ __forceinline__ float lerpf(float a, float b, float w) {
+    return fmaf(w, b - a, a);
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Per-view geometry pointers, in the reference's argument order.
+struct Geometry {
+    const float* angles;
+    const float* sid;
+    const float* sod;
+    const float* det_u0;
+    const float* det_v0;
+    const float* src_x;
+    const float* src_y;
+    const float* src_z;
+};
+
+// The eight per-view geometry-gradient outputs.
+struct GeometryGrad {
+    float* g[8];
+};
+
+}  // namespace dgc

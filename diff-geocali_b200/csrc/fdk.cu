@@ -1,0 +1,206 @@
+// fdk.cu -- FDK ramp filtering for sm_100a.
+//
+// The reference (TomSHINING/diff-geoCali, cbct_backprojector/filtering.py:54-104)
+// cosine-weights the projections, zero-pads U to P = 2^bitlen(2U-1), multiplies
+// the FFT along U by Re(FFT(discrete Ram-Lak)) x Hann, inverse-transforms,
+// crops and scales by pixel*sid/sod.  With that padding the circular
+// convolution never wraps onto the data, and the filter response is real and
+// even, so the whole filter is the symmetric Toeplitz product
+//
+//     y[a,u,v] = sum_k h[|u-k|] * w[a,k,v],   u,k in [0,U)
+//
+// i.e. per view a (U x U) * (U x V) matrix product with a Toeplitz left
+// factor.  This file evaluates it as one register-blocked FP32 product per
+// (view, 128x128 output tile): the cosine weight is applied while the input
+// tile is staged into shared memory, the Toeplitz factor is generated from a
+// sliding window of taps, and the pixel*sid/sod scale is applied in the
+// epilogue.  No FFT, no complex temporaries, no padding buffer.
+#include "common.cuh"
+#include "fdk.cuh"
+
+#include <cmath>
+#include <map>
+#include <mutex>
+#include <tuple>
+#include <vector>
+
+namespace dgc {
+
+// ---------------------------------------------------------------------------
+// Filter taps (host, FP64)
+// ---------------------------------------------------------------------------
+
+// h[m], m in [0, U): inverse DFT of H[k] = R[k] * hann[k], with R the DFT of
+// the discrete Ram-Lak kernel r[0] = 1/(4 px^2), r[n odd] = -1/(pi n px)^2
+// (n taken in (-P/2, P/2]), and hann[k] = 0.5 + 0.5 cos(2 pi f_k / alpha) for
+// |f_k| <= alpha/2 (f_k the DFT bin frequency in cycles/sample), else 0.
+// Direct sums over the even symmetry; cached per (U, px, alpha).
+int fdk_taps_host(int U, double px, double alpha, std::vector<double>& out) {
+    static std::mutex mu;
+    static std::map<std::tuple<int, double, double>, std::vector<double>> cache;
+    const auto key = std::make_tuple(U, px, alpha);
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        auto it = cache.find(key);
+        if (it != cache.end()) {
+            out = it->second;
+            return DGC_OK;
+        }
+    }
+    int bl = 0;
+    for (int n = 2 * U - 1; n; n >>= 1) ++bl;
+    const int P = 1 << bl;
+    std::vector<double> cs(P);
+    for (int j = 0; j < P; ++j) cs[j] = std::cos(2.0 * M_PI * (double)j / (double)P);
+    // R[k] for k in [0, P/2] (R is even in k).
+    const int half = P / 2;
+    std::vector<double> Hk(half + 1);
+    for (int k = 0; k <= half; ++k) {
+        double R = 1.0 / (4.0 * px * px);
+        // odd n in (0, P/2) appear twice (n and -n); n = P/2 once when odd.
+        for (int n = 1; n <= half; n += 2) {
+            const double rn = -1.0 / ((M_PI * n * px) * (M_PI * n * px));
+            const double weight = (n == half) ? 1.0 : 2.0;
+            R += weight * rn * cs[((long long)k * n) % P];
+        }
+        const double f = (k == half) ? -0.5 : (double)k / (double)P;
+        const double hann =
+            std::fabs(f) <= alpha * 0.5 ? 0.5 + 0.5 * std::cos(2.0 * M_PI * f / alpha) : 0.0;
+        Hk[k] = R * hann;
+    }
+    out.assign(U, 0.0);
+    for (int m = 0; m < U; ++m) {
+        double acc = Hk[0];
+        for (int k = 1; k < half; ++k) acc += 2.0 * Hk[k] * cs[((long long)k * m) % P];
+        acc += Hk[half] * cs[((long long)half * m) % P];
+        out[m] = acc / P;
+    }
+    std::lock_guard<std::mutex> lock(mu);
+    cache[key] = out;
+    return DGC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Filter kernel
+// ---------------------------------------------------------------------------
+
+constexpr int FBM = 128;  // output rows (U) per CTA
+constexpr int FBN = 128;  // output columns (V) per CTA
+constexpr int FBK = 16;   // reduction slice
+
+__global__ void __launch_bounds__(256) fdk_filter_kernel(FdkArgs p) {
+    __shared__ __align__(16) float ws[FBK][FBN];
+    __shared__ float gw[FBM + FBK];
+    const int a = blockIdx.z;
+    const int m0 = blockIdx.y * FBM;
+    const int n0 = blockIdx.x * FBN;
+    const int tid = threadIdx.x;
+    const int tx = tid & 15, ty = tid >> 4;
+    const float sid = p.sid[a], sod = p.sod[a];
+    const float sid2 = sid * sid;
+    const float* __restrict__ Pa = p.projections + (long long)a * p.U * p.V;
+    const float cu = 0.5f * (p.U - 1), cv = 0.5f * (p.V - 1);
+
+    float acc[8][8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = 0.0f;
+
+    for (int k0 = 0; k0 < p.U; k0 += FBK) {
+        {   // stage the cosine-weighted input slice w[k0..k0+FBK) x [n0..n0+FBN)
+            const int r = tid >> 4;
+            const int k = k0 + r;
+            const int c0 = (tid & 15) * 8;
+            const float uu = ((float)k - cu) * p.pixel_size;
+            float vals[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int v = n0 + c0 + j;
+                float val = 0.0f;
+                if (k < p.U && v < p.V) {
+                    const float vv = ((float)v - cv) * p.pixel_size;
+                    const float dist = sqrtf(sid2 + uu * uu + vv * vv);
+                    val = Pa[(long long)k * p.V + v] * (sid / dist);
+                }
+                vals[j] = val;
+            }
+            *reinterpret_cast<float4*>(&ws[r][c0]) = make_float4(vals[0], vals[1], vals[2], vals[3]);
+            *reinterpret_cast<float4*>(&ws[r][c0 + 4]) = make_float4(vals[4], vals[5], vals[6], vals[7]);
+        }
+        // Toeplitz window: gw[i] = h[|m0 - k0 - (FBK-1) + i|]
+        for (int i = tid; i < FBM + FBK - 1; i += 256) {
+            int d = m0 - k0 - (FBK - 1) + i;
+            d = d < 0 ? -d : d;
+            gw[i] = p.taps[min(d, p.U - 1)];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < FBK; ++kk) {
+            const float4 b0 = *reinterpret_cast<const float4*>(&ws[kk][tx * 8]);
+            const float4 b1 = *reinterpret_cast<const float4*>(&ws[kk][tx * 8 + 4]);
+            const float b[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const float av = gw[ty * 8 + i - kk + FBK - 1];
+#pragma unroll
+                for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(av, b[j], acc[i][j]);
+            }
+        }
+        __syncthreads();
+    }
+    // filtering.py:104: filtered * pixel_size * (sid / sod)
+    const float ratio = sid / sod;
+    float* __restrict__ Oa = p.filtered + (long long)a * p.U * p.V;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const int u = m0 + ty * 8 + i;
+        if (u >= p.U) continue;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const int v = n0 + tx * 8 + j;
+            if (v < p.V) Oa[(long long)u * p.V + v] = (acc[i][j] * p.pixel_size) * ratio;
+        }
+    }
+}
+
+int fdk_launch_filter(const FdkArgs& p, cudaStream_t s) {
+    DGC_TRACE("fdk_filter_kernel", s);
+    if (p.A > 65535) {
+        set_error("fdk filter: more than 65535 views per launch");
+        return DGC_ERR_UNSUPPORTED;
+    }
+    const dim3 grid(ceil_div(p.V, FBN), ceil_div(p.U, FBM), p.A);
+    fdk_filter_kernel<<<grid, 256, 0, s>>>(p);
+    DGC_LAUNCH_CHECK("fdk_filter_kernel");
+    return DGC_OK;
+}
+
+int fdk_upload_taps(int U, float px, float alpha, float* dst, cudaStream_t s) {
+    std::vector<double> h;
+    int rc = fdk_taps_host(U, (double)px, (double)alpha, h);
+    if (rc != DGC_OK) return rc;
+    // Pinned staging buffer owned per thread; the copy is made stream-ordered
+    // and the host waits for it before the buffer is reused.
+    static thread_local float* staging = nullptr;
+    static thread_local size_t staging_n = 0;
+    static thread_local cudaEvent_t done = nullptr;
+    if (staging_n < (size_t)U) {
+        if (staging) {
+            if (done) cudaEventSynchronize(done);
+            cudaFreeHost(staging);
+            staging = nullptr;
+            staging_n = 0;
+        }
+        DGC_CUDA(cudaMallocHost(&staging, sizeof(float) * (size_t)U));
+        staging_n = (size_t)U;
+    }
+    if (!done) DGC_CUDA(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
+    DGC_CUDA(cudaEventSynchronize(done));
+    for (int i = 0; i < U; ++i) staging[i] = (float)h[i];
+    DGC_CUDA(cudaMemcpyAsync(dst, staging, sizeof(float) * (size_t)U, cudaMemcpyHostToDevice, s));
+    DGC_CUDA(cudaEventRecord(done, s));
+    return DGC_OK;
+}
+
+}  // namespace dgc

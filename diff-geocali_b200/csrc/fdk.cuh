@@ -1,0 +1,24 @@
+// fdk.cuh -- launch interface of the FDK filter.
+#pragma once
+
+#include <vector>
+
+#include "common.cuh"
+
+namespace dgc {
+
+struct FdkArgs {
+    const float* projections;  // [A][U][V]
+    const float* sod;          // [A]
+    const float* sid;          // [A]
+    const float* taps;         // [U] filter taps h[0..U-1]
+    float* filtered;           // [A][U][V]
+    int A, U, V;
+    float pixel_size;
+};
+
+int fdk_taps_host(int U, double px, double alpha, std::vector<double>& out);
+int fdk_upload_taps(int U, float px, float alpha, float* dst, cudaStream_t s);
+int fdk_launch_filter(const FdkArgs& p, cudaStream_t s);
+
+}  // namespace dgc

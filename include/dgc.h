@@ -1,0 +1,190 @@
+/*
+ * dgc.h -- C ABI of libdgc, the sm_100a cone-beam CT operators.
+ *
+ * Every entry point takes plain device pointers, sizes and scalars, returns a
+ * status code (DGC_OK == 0) and launches asynchronously on the CUDA stream
+ * passed as `stream` (a cudaStream_t; NULL selects the legacy default stream).
+ * On failure, dgc_last_error() returns a message for the calling thread.
+ *
+ * Memory: all inputs and outputs are caller-owned device buffers, C-contiguous
+ * float32.  Outputs are fully overwritten.  Kernels that need scratch memory
+ * take a caller-owned device `workspace` of at least the size reported by the
+ * matching *_workspace_bytes() query (256-byte aligned); no entry point
+ * allocates device memory.
+ *
+ * Geometry: eight per-view float32 arrays of length A, in the reference's
+ * order: angles [rad], sid (source-detector distance), sod (source-origin
+ * distance), det_u0, det_v0 (detector centre indices, pixels), src_x, src_y,
+ * src_z (world source offsets).  Volumes are [D,H,W] (W fastest), projections
+ * [A,U,V] (V fastest).  Voxel (z,y,x) sits at ((x-W/2)*voxel+off_x,
+ * (y-H/2)*voxel+off_y, (z-D/2)*voxel+off_z).
+ *
+ * Each entry point names the reference interface it replaces (paths within
+ * the TomSHINING/diff-geoCali project).
+ */
+#ifndef DGC_H
+#define DGC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DGC_ABI_VERSION 1
+
+enum dgc_status {
+    DGC_OK = 0,
+    DGC_ERR_INVALID_ARGUMENT = 1, /* the reference raises RuntimeError (TORCH_CHECK) */
+    DGC_ERR_CUDA = 2,             /* a CUDA runtime call or launch failed */
+    DGC_ERR_WORKSPACE = 3,        /* workspace missing, misaligned or too small */
+    DGC_ERR_UNSUPPORTED = 4       /* sizes beyond this build's index limits */
+};
+
+/* ABI version of the loaded library (DGC_ABI_VERSION). */
+int dgc_abi_version(void);
+
+/* Message of the last failure on the calling thread ("" if none). */
+const char* dgc_last_error(void);
+
+/* ---------------------------------------------------------------------- */
+/* Forward projector: p[a,u,v] = step * sum_k trilinear(volume, O + t_k d) */
+/* ---------------------------------------------------------------------- */
+
+/* Scratch of dgc_project / dgc_project_sample_counts (edge-replicated
+ * quad-packed copy of the volume). */
+size_t dgc_project_workspace_bytes(int D, int H, int W, int A, int U, int V);
+
+/* Replaces src_cbct_forwardprojector_cuda.forward
+ * (csrc/src_cbct_forwardprojector_cuda.cu:566-631, kernel 258-339). */
+int dgc_project(const float* volume, int D, int H, int W,
+                const float* angles, const float* sid, const float* sod,
+                const float* det_u0, const float* det_v0,
+                const float* src_x, const float* src_y, const float* src_z, int A,
+                float pixel_size, int U, int V, float step_size, float voxel_size,
+                float off_x, float off_y, float off_z,
+                float* projections,
+                void* workspace, size_t workspace_bytes, void* stream);
+
+/* Number of trilinear samples of every ray under the kernel's FP32 stepping
+ * rule (counts[a,u,v], int64); the algorithmic-work figure of a projection.
+ * No counterpart in the reference (measurement support). */
+int dgc_project_sample_counts(int D, int H, int W,
+                              const float* angles, const float* sid, const float* sod,
+                              const float* det_u0, const float* det_v0,
+                              const float* src_x, const float* src_y, const float* src_z,
+                              int A, float pixel_size, int U, int V, float step_size,
+                              float voxel_size, float off_x, float off_y, float off_z,
+                              int64_t* counts, void* stream);
+
+/* Scratch of dgc_project_backward. */
+size_t dgc_project_backward_workspace_bytes(int D, int H, int W, int A, int U, int V,
+                                            int compute_grad_volume);
+
+/* Replaces src_cbct_forwardprojector_cuda.backward
+ * (csrc/src_cbct_forwardprojector_cuda.cu:634-729, kernel 342-528).
+ * grad_volume [D,H,W] may be NULL when compute_grad_volume == 0.  The eight
+ * geometry gradients [A] are reduced per view in FP64 in a fixed order
+ * (bitwise reproducible); the volume gradient uses float atomics. */
+int dgc_project_backward(const float* grad_projection, const float* volume,
+                         int D, int H, int W,
+                         const float* angles, const float* sid, const float* sod,
+                         const float* det_u0, const float* det_v0,
+                         const float* src_x, const float* src_y, const float* src_z, int A,
+                         float pixel_size, int U, int V, float step_size, float voxel_size,
+                         int compute_grad_volume, float off_x, float off_y, float off_z,
+                         float* grad_volume, float* grad_angles, float* grad_sid,
+                         float* grad_sod, float* grad_det_u0, float* grad_det_v0,
+                         float* grad_src_x, float* grad_src_y, float* grad_src_z,
+                         void* workspace, size_t workspace_bytes, void* stream);
+
+/* ---------------------------------------------------------------------- */
+/* Voxel-driven FDK-weighted backprojector                                  */
+/* ---------------------------------------------------------------------- */
+
+/* Scratch of dgc_backproject (per-view table + quad-packed projections). */
+size_t dgc_backproject_workspace_bytes(int A, int U, int V, int D, int H, int W);
+
+/* Replaces src_cbct_backprojector_cuda.forward
+ * (csrc/src_cbct_backprojector_cuda.cu:344-420, kernel 15-98). */
+int dgc_backproject(const float* projections, int A, int U, int V,
+                    const float* angles, const float* sid, const float* sod,
+                    const float* det_u0, const float* det_v0,
+                    const float* src_x, const float* src_y, const float* src_z,
+                    float pixel_size, int D, int H, int W, float voxel_size,
+                    float off_x, float off_y, float off_z,
+                    float* volume,
+                    void* workspace, size_t workspace_bytes, void* stream);
+
+/* Scratch of dgc_backproject_backward. */
+size_t dgc_backproject_backward_workspace_bytes(int A, int U, int V, int D, int H, int W);
+
+/* Replaces src_cbct_backprojector_cuda.backward
+ * (csrc/src_cbct_backprojector_cuda.cu:423-522, kernel 101-295).
+ * Writes grad_projections [A,U,V] and the eight geometry gradients [A]
+ * (per-view FP64 reductions in a fixed order). */
+int dgc_backproject_backward(const float* grad_volume, const float* projections,
+                             int A, int U, int V,
+                             const float* angles, const float* sid, const float* sod,
+                             const float* det_u0, const float* det_v0,
+                             const float* src_x, const float* src_y, const float* src_z,
+                             float pixel_size, int D, int H, int W, float voxel_size,
+                             float off_x, float off_y, float off_z,
+                             float* grad_projections, float* grad_angles, float* grad_sid,
+                             float* grad_sod, float* grad_det_u0, float* grad_det_v0,
+                             float* grad_src_x, float* grad_src_y, float* grad_src_z,
+                             void* workspace, size_t workspace_bytes, void* stream);
+
+/* ---------------------------------------------------------------------- */
+/* FDK                                                                      */
+/* ---------------------------------------------------------------------- */
+
+/* Host-only: the U filter taps h[0..U-1] of the zero-padded Ram-Lak x Hann
+ * filter (filtering.py:87-103) as a symmetric Toeplitz kernel, FP64. */
+int dgc_fdk_filter_taps(int U, double pixel_size, double alpha, double* taps);
+
+/* Scratch of dgc_fdk_filter. */
+size_t dgc_fdk_filter_workspace_bytes(int A, int U, int V);
+
+/* Replaces cbct_backprojector.filtering.fdk_filter (filtering.py:54-104):
+ * centred cosine preweight, ramp x Hann filter along U, pixel*sid/sod scale.
+ * sod and sid are per-view device arrays [A]. */
+int dgc_fdk_filter(const float* projections, int A, int U, int V, float pixel_size,
+                   const float* sod, const float* sid, float alpha,
+                   float* filtered,
+                   void* workspace, size_t workspace_bytes, void* stream);
+
+/* Scratch of dgc_reconstruct_fdk. */
+size_t dgc_reconstruct_fdk_workspace_bytes(int A, int U, int V, int D, int H, int W);
+
+/* Replaces cbct_backprojector.filtering.reconstruct_fdk (filtering.py:107-198):
+ * filter, backproject all views, * pi/A, clamp at 0 -- one filter launch and
+ * one backprojection launch over all views. */
+int dgc_reconstruct_fdk(const float* projections, int A, int U, int V,
+                        const float* angles, const float* sid, const float* sod,
+                        const float* det_u0, const float* det_v0,
+                        const float* src_x, const float* src_y, const float* src_z,
+                        float pixel_size, int D, int H, int W, float voxel_size,
+                        float off_x, float off_y, float off_z, float alpha,
+                        float* volume,
+                        void* workspace, size_t workspace_bytes, void* stream);
+
+/* ---------------------------------------------------------------------- */
+/* Kernel timing (no counterpart in the reference; measurement support)     */
+/* ---------------------------------------------------------------------- */
+
+/* Enable (1) / disable (0) CUDA-event timing of every kernel launch. */
+void dgc_trace_enable(int on);
+/* Number of launches recorded since the last dgc_trace_clear(). */
+int dgc_trace_count(void);
+/* Name and device duration [ms] of record `index` (waits for its stop event). */
+int dgc_trace_get(int index, char* name, int name_len, float* ms);
+/* Drop all records. */
+void dgc_trace_clear(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DGC_H */

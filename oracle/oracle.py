@@ -1,0 +1,207 @@
+"""ctypes front end of the FP64 CPU oracle (``oracle/dgc_oracle.c``).
+
+TEST INFRASTRUCTURE ONLY: imported by ``tests/``, by ``__graft_entry__.smoke()``
+and by the CPU-baseline leg of ``bench.py`` as the checker.  The product package
+never imports it.
+
+Every function takes numpy arrays (any float dtype; converted to contiguous
+float64) and returns float64 results.  Geometry is given as the reference's
+eight per-view arrays ``(angles, sid, sod, det_u0, det_v0, src_x, src_y, src_z)``.
+The algorithms restate the reference project's kernels and CPU checks; the C
+file cites the reference lines each function follows.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "_lib" / "libdgc_oracle.so"
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_i64p = ctypes.POINTER(ctypes.c_int64)
+_c_int = ctypes.c_int
+_c_long = ctypes.c_long
+_c_d = ctypes.c_double
+
+_lib = None
+
+
+def build(force: bool = False) -> Path:
+    """Compile the oracle with its Makefile (gcc); returns the library path."""
+    src = HERE / "dgc_oracle.c"
+    if force or not LIB_PATH.exists() or LIB_PATH.stat().st_mtime < src.stat().st_mtime:
+        subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    return LIB_PATH
+
+
+def _load():
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            build()
+        lib = ctypes.CDLL(str(LIB_PATH))
+        fp_args = [_c_int, _c_int, _c_int, _dp, _c_int, _c_int, _c_int, _c_d, _c_d, _c_d,
+                   _c_d, _c_d, _c_d, _c_int]
+        lib.oracle_project.argtypes = [_dp] + fp_args + [_dp]
+        lib.oracle_project_rays.argtypes = [_dp] + fp_args + [_i64p, _c_long, _dp]
+        lib.oracle_sample_counts.argtypes = fp_args + [_i64p]
+        lib.oracle_project_backward.argtypes = [_dp, _dp] + fp_args + [_dp, _dp]
+        bp_args = [_c_int, _c_int, _c_int, _dp, _c_d, _c_int, _c_int, _c_int, _c_d, _c_d,
+                   _c_d, _c_d]
+        lib.oracle_backproject.argtypes = [_dp] + bp_args + [_dp]
+        lib.oracle_backproject_backward.argtypes = [_dp, _dp] + bp_args + [_dp, _dp]
+        lib.oracle_fdk_taps.argtypes = [_c_int, _c_d, _c_d, _dp]
+        lib.oracle_fdk_filter.argtypes = [_dp, _c_int, _c_int, _c_int, _c_d, _dp, _dp, _c_d, _dp]
+        lib.oracle_num_threads.restype = _c_int
+        lib.oracle_set_num_threads.argtypes = [_c_int]
+        _lib = lib
+    return _lib
+
+
+def _f64(x):
+    return np.ascontiguousarray(np.asarray(x, dtype=np.float64))
+
+
+def _ptr(a):
+    return a.ctypes.data_as(_dp)
+
+
+def _geom(geometry, A=None):
+    g = np.stack([_f64(np.asarray(x).reshape(-1)) for x in geometry])
+    if g.shape[0] != 8:
+        raise ValueError("geometry must hold 8 per-view arrays")
+    if A is not None and g.shape[1] != A:
+        raise ValueError("geometry arrays must have A entries")
+    return np.ascontiguousarray(g)
+
+
+def num_threads() -> int:
+    return _load().oracle_num_threads()
+
+
+def set_num_threads(n: int) -> None:
+    _load().oracle_set_num_threads(int(n))
+
+
+def project(volume, geometry, pixel_size, U, V, step_size, voxel_size,
+            offset=(0.0, 0.0, 0.0), mode=0):
+    """Forward projection [A,U,V]; ``mode`` 0 = reference CPU rule, 1 = FP32 kernel sample set."""
+    vol = _f64(volume)
+    D, H, W = vol.shape
+    g = _geom(geometry)
+    A = g.shape[1]
+    out = np.empty((A, U, V), np.float64)
+    _load().oracle_project(_ptr(vol), D, H, W, _ptr(g), A, U, V, pixel_size, step_size,
+                           voxel_size, *map(float, offset), int(mode), _ptr(out))
+    return out
+
+
+def project_rays(volume, geometry, pixel_size, U, V, step_size, voxel_size, rays,
+                 offset=(0.0, 0.0, 0.0), mode=0):
+    """Forward projection of selected rays (flat indices ``(a*U+u)*V+v``)."""
+    vol = _f64(volume)
+    D, H, W = vol.shape
+    g = _geom(geometry)
+    A = g.shape[1]
+    r = np.ascontiguousarray(np.asarray(rays, dtype=np.int64))
+    out = np.empty(r.shape[0], np.float64)
+    _load().oracle_project_rays(_ptr(vol), D, H, W, _ptr(g), A, U, V, pixel_size, step_size,
+                                voxel_size, *map(float, offset), int(mode),
+                                r.ctypes.data_as(_i64p), r.shape[0], _ptr(out))
+    return out
+
+
+def sample_counts(volume_shape, geometry, pixel_size, U, V, step_size, voxel_size,
+                  offset=(0.0, 0.0, 0.0), mode=1):
+    D, H, W = volume_shape
+    g = _geom(geometry)
+    A = g.shape[1]
+    out = np.empty((A, U, V), np.int64)
+    _load().oracle_sample_counts(D, H, W, _ptr(g), A, U, V, pixel_size, step_size, voxel_size,
+                                 *map(float, offset), int(mode), out.ctypes.data_as(_i64p))
+    return out
+
+
+def project_backward(grad_projection, volume, geometry, pixel_size, step_size, voxel_size,
+                     offset=(0.0, 0.0, 0.0), mode=0, compute_grad_volume=True):
+    """Analytic gradients: (grad_volume or None, [8, A] geometry gradients)."""
+    gp = _f64(grad_projection)
+    vol = _f64(volume)
+    D, H, W = vol.shape
+    A, U, V = gp.shape
+    g = _geom(geometry, A)
+    gv = np.empty_like(vol) if compute_grad_volume else None
+    gg = np.empty((8, A), np.float64)
+    _load().oracle_project_backward(
+        _ptr(gp), _ptr(vol), D, H, W, _ptr(g), A, U, V, pixel_size, step_size, voxel_size,
+        *map(float, offset), int(mode), _ptr(gv) if gv is not None else None, _ptr(gg))
+    return gv, gg
+
+
+def backproject(projections, geometry, pixel_size, volume_shape, voxel_size,
+                offset=(0.0, 0.0, 0.0)):
+    p = _f64(projections)
+    A, U, V = p.shape
+    g = _geom(geometry, A)
+    D, H, W = volume_shape
+    out = np.empty((D, H, W), np.float64)
+    _load().oracle_backproject(_ptr(p), A, U, V, _ptr(g), pixel_size, D, H, W, voxel_size,
+                               *map(float, offset), _ptr(out))
+    return out
+
+
+def backproject_backward(grad_volume, projections, geometry, pixel_size, voxel_size,
+                         offset=(0.0, 0.0, 0.0)):
+    """Analytic gradients: (grad_projections [A,U,V], [8, A] geometry gradients)."""
+    gv = _f64(grad_volume)
+    p = _f64(projections)
+    A, U, V = p.shape
+    D, H, W = gv.shape
+    g = _geom(geometry, A)
+    gp = np.empty_like(p)
+    gg = np.empty((8, A), np.float64)
+    _load().oracle_backproject_backward(_ptr(gv), _ptr(p), A, U, V, _ptr(g), pixel_size, D, H,
+                                        W, voxel_size, *map(float, offset), _ptr(gp), _ptr(gg))
+    return gp, gg
+
+
+def fdk_taps(U, pixel_size, alpha=0.8):
+    h = np.empty(U, np.float64)
+    _load().oracle_fdk_taps(int(U), float(pixel_size), float(alpha), _ptr(h))
+    return h
+
+
+def fdk_filter(projections, pixel_size, sod, sid, alpha=0.8):
+    p = _f64(projections)
+    A, U, V = p.shape
+    sod = _f64(np.broadcast_to(np.asarray(sod, np.float64).reshape(-1), (A,)))
+    sid = _f64(np.broadcast_to(np.asarray(sid, np.float64).reshape(-1), (A,)))
+    out = np.empty_like(p)
+    _load().oracle_fdk_filter(_ptr(p), A, U, V, float(pixel_size), _ptr(sod), _ptr(sid),
+                              float(alpha), _ptr(out))
+    return out
+
+
+def reconstruct_fdk(projections, geometry, pixel_size, volume_shape, voxel_size,
+                    offset=(0.0, 0.0, 0.0), alpha=0.8):
+    """filtering.py:107-198 in FP64: filter, backproject, * pi/A, clamp >= 0."""
+    g = _geom(geometry)
+    filtered = fdk_filter(projections, pixel_size, g[2], g[1], alpha)
+    vol = backproject(filtered, g, pixel_size, volume_shape, voxel_size, offset)
+    return np.maximum(vol * (np.pi / g.shape[1]), 0.0)
+
+
+__all__ = [
+    "build", "num_threads", "set_num_threads", "project", "project_rays", "sample_counts",
+    "project_backward", "backproject", "backproject_backward", "fdk_taps", "fdk_filter",
+    "reconstruct_fdk",
+]
+
+if os.environ.get("DGC_ORACLE_THREADS"):
+    set_num_threads(int(os.environ["DGC_ORACLE_THREADS"]))

@@ -1,0 +1,97 @@
+"""The C ABI without a GPU: the library loads, exports every symbol that
+include/dgc.h declares, answers workspace queries, computes filter taps on the
+host and rejects invalid arguments with the reference's messages (argument
+checks run before any CUDA call)."""
+
+import ctypes
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+
+def declared_functions():
+    text = (ROOT / "include" / "dgc.h").read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(dgc_[a-z0-9_]+)\s*\(", text)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from cbct_backprojector import _native
+
+    return _native.lib()
+
+
+def test_exports_every_declared_symbol(lib):
+    from cbct_backprojector import _native
+
+    names = declared_functions()
+    assert len(names) >= 15
+    for name in names:
+        assert hasattr(lib, name), name
+        assert name in _native.SIGNATURES, f"{name} has no ctypes signature"
+    assert lib.dgc_abi_version() == 1
+
+
+def test_workspace_queries(lib):
+    a = lib.dgc_project_workspace_bytes(256, 256, 256, 360, 384, 384)
+    assert a == 16 * 258 * 257 * 257 + (-(16 * 258 * 257 * 257) % 256)
+    assert lib.dgc_project_workspace_bytes(0, 1, 1, 1, 1, 1) == 0
+    b0 = lib.dgc_project_backward_workspace_bytes(64, 64, 64, 90, 128, 128, 0)
+    b1 = lib.dgc_project_backward_workspace_bytes(64, 64, 64, 90, 128, 128, 1)
+    assert b1 > b0 > 0
+    assert lib.dgc_backproject_workspace_bytes(360, 384, 384, 256, 256, 256) >= 16 * 360 * 383 * 383
+    assert lib.dgc_reconstruct_fdk_workspace_bytes(360, 384, 384, 256, 256, 256) > \
+        lib.dgc_backproject_workspace_bytes(360, 384, 384, 256, 256, 256)
+    assert lib.dgc_backproject_workspace_bytes(1, 1, 5, 1, 1, 1) == 0
+
+
+def test_filter_taps_on_host(lib, oracle):
+    for U, px, alpha in [(9, 0.9, 0.8), (384, 1.0, 0.8), (768, 1.0, 0.8), (17, 0.75, 1.0)]:
+        buf = (ctypes.c_double * U)()
+        assert lib.dgc_fdk_filter_taps(U, px, alpha, buf) == 0
+        np.testing.assert_allclose(np.array(buf), oracle.fdk_taps(U, px, alpha), rtol=1e-9,
+                                   atol=1e-15)
+    buf = (ctypes.c_double * 4)()
+    assert lib.dgc_fdk_filter_taps(4, 1.0, 1.5, buf) == 1
+    assert b"alpha" in lib.dgc_last_error()
+
+
+def _geom_ptrs():
+    return [ctypes.c_void_p(16)] * 8  # never dereferenced: checks fail first
+
+
+def test_invalid_arguments_return_status(lib):
+    g = _geom_ptrs()
+    # forward projector (fp.cu:585-611)
+    rc = lib.dgc_project(None, 0, 4, 4, *g, 3, 1.0, 4, 4, 0.5, 1.0, 0.0, 0.0, 0.0, None, None, 0,
+                         None)
+    assert rc == 1 and lib.dgc_last_error() == b"every volume dimension must be positive"
+    rc = lib.dgc_project(None, 4, 4, 4, *g, 3, 1.0, 0, 4, 0.5, 1.0, 0.0, 0.0, 0.0, None, None, 0,
+                         None)
+    assert rc == 1 and lib.dgc_last_error() == b"U and V must be positive"
+    rc = lib.dgc_project(None, 4, 4, 4, *g, 3, 1.0, 4, 4, 0.0, 1.0, 0.0, 0.0, 0.0, None, None, 0,
+                         None)
+    assert rc == 1 and b"must be positive" in lib.dgc_last_error()
+    rc = lib.dgc_project(None, 4, 4, 4, *g, 0, 1.0, 4, 4, 0.5, 1.0, 0.0, 0.0, 0.0, None, None, 0,
+                         None)
+    assert rc == 1 and lib.dgc_last_error() == b"angles must contain at least one view"
+    # workspace too small is reported before any launch
+    rc = lib.dgc_project(ctypes.c_void_p(16), 4, 4, 4, *g, 3, 1.0, 4, 4, 0.5, 1.0, 0.0, 0.0, 0.0,
+                         ctypes.c_void_p(16), None, 0, None)
+    assert rc == 3 and b"workspace too small" in lib.dgc_last_error()
+    # backprojector (bp.cu:298-383)
+    rc = lib.dgc_backproject(None, 2, 1, 4, *g, 1.0, 4, 4, 4, 1.0, 0.0, 0.0, 0.0, None, None, 0,
+                             None)
+    assert rc == 1 and b"U,V >= 2" in lib.dgc_last_error()
+    rc = lib.dgc_backproject(None, 2, 4, 4, *g, 1.0, 8 * 65535 + 1, 1, 1, 1.0, 0.0, 0.0, 0.0, None,
+                             None, 0, None)
+    assert rc == 1 and b"grid limits" in lib.dgc_last_error()
+    rc = lib.dgc_backproject(None, 2, 4, 4, *g, 1.0, 4, 4, 4, 1.0, float("nan"), 0.0, 0.0, None,
+                             None, 0, None)
+    assert rc == 1 and lib.dgc_last_error() == b"sizes and ROI offsets must be finite"
+    rc = lib.dgc_fdk_filter(None, 2, 4, 4, -1.0, None, None, 0.8, None, None, 0, None)
+    assert rc == 1 and b"pixel_size" in lib.dgc_last_error()
