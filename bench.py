@@ -52,7 +52,22 @@ def parse_args(argv=None):
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    return ap.parse_args(argv)
+    ap.add_argument("--views", type=int, default=None,
+                    help="override the view count (smaller cases for profiler captures)")
+    ap.add_argument("--volume", type=int, default=None, help="override the cubic volume size")
+    ap.add_argument("--detector", type=int, default=None, help="override the square detector size")
+    args = ap.parse_args(argv)
+    if args.views:
+        WORKLOAD["A"] = args.views
+    if args.volume:
+        WORKLOAD["D"] = WORKLOAD["H"] = WORKLOAD["W"] = args.volume
+    if args.detector:
+        WORKLOAD["U"] = WORKLOAD["V"] = args.detector
+    if args.views or args.volume or args.detector:
+        w = WORKLOAD
+        w["name"] = (f"project {w['D']}^3 -> {w['A']}x{w['U']}^2, then reconstruct_fdk "
+                     f"{w['D']}^3 (profiling size)")
+    return args
 
 
 # ----------------------------------------------------------------- distributed

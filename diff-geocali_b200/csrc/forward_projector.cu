@@ -301,13 +301,15 @@ __global__ void __launch_bounds__(256) fp_backward_kernel(FpArgs p) {
     if (in_range && grad_out != 0.0f) {
         const RaySetup r = setup_ray(vg, u, v, p);
         if (r.ok) {
-            float godx = 0.f, gody = 0.f, godz = 0.f;  // grad wrt origin (direct)
-            float gdx = 0.f, gdy = 0.f, gdz = 0.f;     // grad wrt direction
+            // Gradients wrt the ray origin (direct part) and the target point.
+            float godx = 0.f, gody = 0.f, godz = 0.f;
+            float grx = 0.f, gry = 0.f, grz = 0.f;
             if (r.hit) {
                 const float gs = grad_out * p.step_size;
                 const float hx = p.W * 0.5f, hy = p.H * 0.5f, hz = p.D * 0.5f;
                 const float4* __restrict__ Q = p.quads;
-                // Sums of the voxel-unit spatial gradient and of gradient * t.
+                // s1 = sum of the voxel-unit spatial gradient g over the samples,
+                // s2 = sum of g * (t - t_min).
                 float s1x = 0.f, s1y = 0.f, s1z = 0.f, s2x = 0.f, s2y = 0.f, s2z = 0.f;
                 const int nmax = step_bound(r, p.step_size);
                 float t = r.tmin;
@@ -330,12 +332,13 @@ __global__ void __launch_bounds__(256) fp_backward_kernel(FpArgs p) {
                                            lerpf(q1.z - q1.x, q1.w - q1.y, c.fx), c.fz);
                     const float gz = lerpf(lerpf(q1.x - q0.x, q1.y - q0.y, c.fx),
                                            lerpf(q1.z - q0.z, q1.w - q0.w, c.fx), c.fy);
+                    const float tau = t - r.tmin;
                     s1x += gx;
                     s1y += gy;
                     s1z += gz;
-                    s2x = fmaf(gx, t, s2x);
-                    s2y = fmaf(gy, t, s2y);
-                    s2z = fmaf(gz, t, s2z);
+                    s2x = fmaf(gx, tau, s2x);
+                    s2y = fmaf(gy, tau, s2y);
+                    s2z = fmaf(gz, tau, s2z);
                     if (GRADVOL) {
                         const float mx = 1.0f - c.fx, my = 1.0f - c.fy, mz = 1.0f - c.fz;
                         const float g0 = gs * mz, g1 = gs * c.fz;
@@ -351,32 +354,29 @@ __global__ void __launch_bounds__(256) fp_backward_kernel(FpArgs p) {
                         atomicAdd(gp + p.g_plane + p.g_row + 1, g11 * c.fx);
                     }
                 }
-                const float gw = gs * p.inv_voxel;
-                godx = gw * s1x;
-                gody = gw * s1y;
-                godz = gw * s1z;
-                gdx = gw * s2x;
-                gdy = gw * s2y;
-                gdz = gw * s2z;
-                const float gtmin = godx * r.dx + gody * r.dy + godz * r.dz;
-                // fp.cu:454-467: samples are anchored at the entry slab.
-                if (r.entry_axis == 0) {
-                    godx -= gtmin / r.dx;
-                    gdx -= gtmin * r.tmin / r.dx;
-                } else if (r.entry_axis == 1) {
-                    gody -= gtmin / r.dy;
-                    gdy -= gtmin * r.tmin / r.dy;
-                } else if (r.entry_axis == 2) {
-                    godz -= gtmin / r.dz;
-                    gdz -= gtmin * r.tmin / r.dz;
-                }
+                // fp.cu:441-467 give, with G = gs/voxel,
+                //   grad_origin_direct = G*s1 - (G*(s1.d)/d_e) e_e
+                //   grad_direction     = G*sum g*t - (G*(s1.d) t_min/d_e) e_e
+                // (e = entry axis).  Writing sum g*t = s2 + t_min*s1 and
+                //   q = s1 - ((s1.d)/d_e) e_e   (so q.d = 0)
+                // gives grad_origin_direct = G*q and grad_direction = G*(s2 + t_min*q):
+                // the same values without the large t_min*s1 terms that cancel.
+                float qx = s1x, qy = s1y, qz = s1z;
+                if (r.entry_axis == 0) qx = -(s1y * r.dy + s1z * r.dz) / r.dx;
+                else if (r.entry_axis == 1) qy = -(s1x * r.dx + s1z * r.dz) / r.dy;
+                else if (r.entry_axis == 2) qz = -(s1x * r.dx + s1y * r.dy) / r.dz;
+                const float G = gs * p.inv_voxel;
+                godx = G * qx;
+                gody = G * qy;
+                godz = G * qz;
+                // fp.cu:470-486: chain through direction = normalize(target - origin);
+                // q is orthogonal to d, so only s2 loses its component along d.
+                const float ds2 = r.dx * s2x + r.dy * s2y + r.dz * s2z;
+                const float k = G / r.len;
+                grx = k * (s2x - r.dx * ds2 + r.tmin * qx);
+                gry = k * (s2y - r.dy * ds2 + r.tmin * qy);
+                grz = k * (s2z - r.dz * ds2 + r.tmin * qz);
             }
-            // fp.cu:470-486: chain through direction = normalize(target - origin).
-            const float ddg = r.dx * gdx + r.dy * gdy + r.dz * gdz;
-            const float inv_len = 1.0f / r.len;
-            const float grx = (gdx - r.dx * ddg) * inv_len;
-            const float gry = (gdy - r.dy * ddg) * inv_len;
-            const float grz = (gdz - r.dz * ddg) * inv_len;
             const float gox = godx - grx, goy = gody - gry, goz = godz - grz;
             // fp.cu:488-527: per-view geometry terms.
             const float u_phys = (u - vg.u0) * p.pixel_size;

@@ -386,6 +386,71 @@ void oracle_sample_counts(int D, int H, int W, const double* geom, int A, int U,
 }
 
 /*
+ * Per-ray trace (check_forward_operator.py:145-193 uses the same idea): a hash
+ * of the entry face, the sample count and the interpolation cell of every
+ * sample.  A finite difference that leaves a ray's trace unchanged stays
+ * inside one smooth piece of the piecewise-smooth projector.  The hash is 0
+ * ("ambiguous") when a sample coordinate lies within `margin` of a cell
+ * boundary, where FP32 and FP64 evaluation may pick different cells.
+ */
+typedef struct {
+    FpJob* j;
+    double margin;
+    uint64_t* out;
+} TraceJob;
+
+static inline uint64_t fnv(uint64_t h, int64_t v) {
+    for (int b = 0; b < 8; ++b) {
+        h ^= (uint64_t)((v >> (8 * b)) & 0xff);
+        h *= 1099511628211ULL;
+    }
+    return h;
+}
+
+static void fp_trace_ray(long ray, void* vctx) {
+    TraceJob* tj = (TraceJob*)vctx;
+    const FpJob* j = tj->j;
+    const FpCfg* c = &j->cfg;
+    int V = c->V, U = c->U;
+    int v = (int)(ray % V);
+    int u = (int)((ray / V) % U);
+    int a = (int)(ray / ((long)U * V));
+    Ray r;
+    make_ray(j->g, a, u, v, c->px, c->lo, c->hi, c->lof, c->hif, c->mode, &r);
+    uint64_t h = 1469598103934665603ULL;
+    long n = ray_count(&r, c->step, c->mode);
+    h = fnv(h, r.hit ? r.entry_axis + 2 : 0);
+    h = fnv(h, n);
+    float tf = r.tminf;
+    for (long k = 0; k < n; ++k) {
+        double t = sample_offset(&r, k, c->step, c->mode, &tf);
+        double xyz[3] = {(r.o[0] + t * r.d[0] - c->off[0]) / c->vs + c->W * 0.5,
+                         (r.o[1] + t * r.d[1] - c->off[1]) / c->vs + c->H * 0.5,
+                         (r.o[2] + t * r.d[2] - c->off[2]) / c->vs + c->D * 0.5};
+        for (int q = 0; q < 3; ++q) {
+            double f = floor(xyz[q]);
+            double fr = xyz[q] - f;
+            if (fr < tj->margin || fr > 1.0 - tj->margin) {
+                tj->out[ray] = 0;
+                return;
+            }
+            h = fnv(h, (int64_t)f);
+        }
+        tf += (float)c->step;
+    }
+    tj->out[ray] = h ? h : 1;
+}
+
+void oracle_ray_traces(int D, int H, int W, const double* geom, int A, int U, int V, double px,
+                       double step, double vs, double ox, double oy, double oz, int mode,
+                       double margin, uint64_t* out) {
+    FpJob j;
+    fp_job_init(&j, D, H, W, geom, A, U, V, px, step, vs, ox, oy, oz, mode);
+    TraceJob tj = {&j, margin, out};
+    parallel_for((long)A * U * V, 64, fp_trace_ray, &tj);
+}
+
+/*
  * Analytic backward of the forward projector (fp.cu:342-528) in FP64.
  * Work is split by view: each view owns its geometry sums (deterministic) and,
  * when the volume gradient is requested, a private buffer summed in view

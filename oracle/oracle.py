@@ -51,6 +51,7 @@ def _load():
         lib.oracle_project.argtypes = [_dp] + fp_args + [_dp]
         lib.oracle_project_rays.argtypes = [_dp] + fp_args + [_i64p, _c_long, _dp]
         lib.oracle_sample_counts.argtypes = fp_args + [_i64p]
+        lib.oracle_ray_traces.argtypes = fp_args + [_c_d, _i64p]
         lib.oracle_project_backward.argtypes = [_dp, _dp] + fp_args + [_dp, _dp]
         bp_args = [_c_int, _c_int, _c_int, _dp, _c_d, _c_int, _c_int, _c_int, _c_d, _c_d,
                    _c_d, _c_d]
@@ -128,6 +129,19 @@ def sample_counts(volume_shape, geometry, pixel_size, U, V, step_size, voxel_siz
     return out
 
 
+def ray_traces(volume_shape, geometry, pixel_size, U, V, step_size, voxel_size,
+               offset=(0.0, 0.0, 0.0), mode=1, margin=1e-4):
+    """uint64 [A,U,V] hash of (entry face, sample count, cells); 0 = near a cell boundary."""
+    D, H, W = volume_shape
+    g = _geom(geometry)
+    A = g.shape[1]
+    out = np.empty((A, U, V), np.int64)
+    _load().oracle_ray_traces(D, H, W, _ptr(g), A, U, V, pixel_size, step_size, voxel_size,
+                              *map(float, offset), int(mode), float(margin),
+                              out.ctypes.data_as(_i64p))
+    return out.view(np.uint64)
+
+
 def project_backward(grad_projection, volume, geometry, pixel_size, step_size, voxel_size,
                      offset=(0.0, 0.0, 0.0), mode=0, compute_grad_volume=True):
     """Analytic gradients: (grad_volume or None, [8, A] geometry gradients)."""
@@ -199,7 +213,7 @@ def reconstruct_fdk(projections, geometry, pixel_size, volume_shape, voxel_size,
 
 __all__ = [
     "build", "num_threads", "set_num_threads", "project", "project_rays", "sample_counts",
-    "project_backward", "backproject", "backproject_backward", "fdk_taps", "fdk_filter",
+    "ray_traces", "project_backward", "backproject", "backproject_backward", "fdk_taps", "fdk_filter",
     "reconstruct_fdk",
 ]
 

@@ -73,15 +73,32 @@ def test_reference_check_case(golden):
                                    rtol=3e-4, atol=3e-5, msg=name)
 
 
-def test_config1_against_reference_cpu_oracle(golden):
+def test_config1_against_reference_cpu_oracle(golden, ref_native):
+    """Config-1 backprojection (24 views of 48x40 into 16x20x24).
+
+    The nominal geometry is grid-aligned (voxel centres project exactly onto
+    detector-pixel boundaries at several views), where the bilinear weights'
+    derivatives jump; FP32 and FP64 pick different sides there, so geometry
+    gradients are compared with the FP64 golden loosely and with the
+    reference's CUDA (same FP32 rounding of the mapping) strictly.
+    """
+    _, ref_bp = ref_native
     d = golden("bp_config1.npz")
     case = dict(proj=d["in_data"], geom=golden_geometry(d, np.float32), px=1.0,
                 shape=tuple(int(s) for s in d["volume_shape"]), vs=1.0, off=(0.0, 0.0, 0.0))
     vol, proj, geom = run_bp(case, requires_grad=True)
     assert rel_l2(vol.detach().cpu(), d["output"]) < FWD_RTOL
-    grads = torch.autograd.grad(vol, [proj, *geom], grad_outputs=cuda32(d["upstream"]))
-    for name, g in zip(("data",) + GEOM_NAMES, grads):
-        assert rel_l2(g.cpu(), d["grad_" + name]) < GRAD_RTOL, name
+    up = cuda32(d["upstream"])
+    grads = torch.autograd.grad(vol, [proj, *geom], grad_outputs=up)
+    assert rel_l2(grads[0].cpu(), d["grad_data"]) < GRAD_RTOL
+    for name, g in zip(GEOM_NAMES, grads[1:]):
+        assert rel_l2(g.cpu(), d["grad_" + name]) < 5e-2, name
+    ref = ref_bp.forward(proj.detach(), *[g.detach() for g in geom], 1.0, *case["shape"], 1.0)
+    theirs = ref_bp.backward(up, proj.detach(), *[g.detach() for g in geom], 1.0, 1.0)
+    torch.cuda.synchronize()
+    assert rel_l2(vol.detach().cpu(), ref.cpu()) < FWD_RTOL
+    for k, name in enumerate(("data",) + GEOM_NAMES):
+        assert rel_l2(grads[k].cpu(), theirs[k].cpu()) < GRAD_RTOL, name
 
 
 @pytest.mark.parametrize("seed,px,vs,shape", [(1, 0.9, 0.8, (18, 22, 26)),

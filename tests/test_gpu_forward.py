@@ -91,16 +91,69 @@ def config1_case(d):
                 step=0.5, vs=1.0, off=(0.0, 0.0, 0.0))
 
 
-def test_config1_against_reference_cpu_oracle(golden):
-    """Config 1 (16x20x24, 24 views, 48x40): values and loss=mean(p^2) gradients."""
+def unambiguous_rays(oracle, case, shape):
+    """1.0 for rays whose samples all sit > 1e-4 voxel from a cell boundary."""
+    tr = oracle.ray_traces(shape, case["geom"], case["px"], case["U"], case["V"], case["step"],
+                           case["vs"], case["off"], mode=1)
+    return torch.tensor((tr != 0).astype(np.float32), device="cuda")
+
+
+def test_config1_against_reference_cpu_oracle(golden, oracle):
+    """Config 1 (16x20x24, 24 views, 48x40): values and loss=mean(p^2) gradients.
+
+    The nominal config-1 geometry is grid-aligned: at 0/90/180/270 degrees about
+    5 % of the rays have samples exactly on cell boundaries, where the
+    piecewise-linear interpolant has kinks and FP32 and FP64 legitimately take
+    different one-sided derivatives.  Geometry gradients are therefore checked
+    strictly on the rays away from boundaries (the reference's own finite-
+    difference check guards its ray the same way) and loosely in full.
+    """
     d = golden("fp_config1.npz")
     case = config1_case(d)
     out, vol, geom = run_project(case, requires_grad=True)
     assert rel_l2(out.detach().cpu(), d["output"]) < FWD_RTOL
-    loss = out.double().square().mean()
-    grads = torch.autograd.grad(loss, [vol, *geom])
-    for name, g in zip(("data",) + GEOM_NAMES, grads):
-        assert rel_l2(g.cpu(), d["grad_" + name]) < GRAD_RTOL, name
+    p = out.detach().double()
+    grads = torch.autograd.grad(out, [vol, *geom], grad_outputs=(2 * p / p.numel()).float(),
+                                retain_graph=True)
+    assert rel_l2(grads[0].cpu(), d["grad_data"]) < GRAD_RTOL
+    for name, g in zip(GEOM_NAMES, grads[1:]):
+        assert rel_l2(g.cpu(), d["grad_" + name]) < 5e-2, name
+    mask = unambiguous_rays(oracle, case, d["in_data"].shape)
+    up = (2 * p * mask / p.numel()).float()
+    ours = torch.autograd.grad(out, geom, grad_outputs=up)
+    _, gg = oracle.project_backward(up.cpu().numpy(), case["vol"], case["geom"], 1.0, 0.5, 1.0,
+                                    mode=1, compute_grad_volume=False)
+    for k, name in enumerate(GEOM_NAMES):
+        assert rel_l2(ours[k].cpu(), gg[k]) < GRAD_RTOL, name
+
+
+def test_config1_perturbed_geometry(golden, oracle):
+    """Config 1 sizes with config-3 style per-view perturbations: strict FP64 check."""
+    d = golden("fp_config1.npz")
+    case = config1_case(d)
+    rng = np.random.default_rng(31)
+    A = len(case["geom"][0])
+    g = [x.astype(np.float64) for x in case["geom"]]
+    g[0] = g[0] + np.deg2rad(rng.normal(0, 0.3, A))
+    g[1] = g[1] * (1 + rng.normal(0, 0.005, A))
+    g[2] = g[2] * (1 + rng.normal(0, 0.005, A))
+    g[3] = g[3] + rng.normal(0, 2, A)
+    g[4] = g[4] + rng.normal(0, 2, A)
+    for k in (5, 6, 7):
+        g[k] = g[k] + rng.normal(0, 1.0, A)
+    case["geom"] = [x.astype(np.float32) for x in g]
+    out, vol, geom = run_project(case, requires_grad=True)
+    truth = oracle.project(case["vol"], case["geom"], 1.0, case["U"], case["V"], 0.5, 1.0, mode=1)
+    assert rel_l2(out.detach().cpu(), truth) < FWD_RTOL
+    p = out.detach().double()
+    mask = unambiguous_rays(oracle, case, d["in_data"].shape)
+    up = (2 * p * mask / p.numel()).float()
+    ours = torch.autograd.grad(out, [vol, *geom], grad_outputs=up)
+    gv, gg = oracle.project_backward(up.cpu().numpy(), case["vol"], case["geom"], 1.0, 0.5, 1.0,
+                                     mode=1)
+    assert rel_l2(ours[0].cpu(), gv) < GRAD_RTOL
+    for k, name in enumerate(GEOM_NAMES):
+        assert rel_l2(ours[1 + k].cpu(), gg[k]) < GRAD_RTOL, name
 
 
 # ------------------------------------------------------- reference CUDA parity
@@ -143,36 +196,39 @@ def test_backward_matches_reference_cuda(which, golden, ref_native, oracle):
     torch.cuda.synchronize()
     for name, a, b in zip(("data",) + GEOM_NAMES, ours, ref):
         assert rel_l2(a.cpu(), b.cpu()) < GRAD_RTOL, name
-    gv, gg = oracle.project_backward(gp.cpu().numpy(), case["vol"], case["geom"], case["px"],
+    # FP64 truth on the rays whose samples stay away from cell boundaries
+    mask = unambiguous_rays(oracle, case, case["vol"].shape)
+    gpm = (gp * mask).contiguous()
+    out2, vol2, geom2 = run_project(case, requires_grad=True)
+    ours_m = torch.autograd.grad(out2, [vol2, *geom2], grad_outputs=gpm)
+    gv, gg = oracle.project_backward(gpm.cpu().numpy(), case["vol"], case["geom"], case["px"],
                                      case["step"], case["vs"], case["off"], mode=1)
-    assert rel_l2(ours[0].cpu(), gv) < GRAD_RTOL
+    assert rel_l2(ours_m[0].cpu(), gv) < GRAD_RTOL
     for k, name in enumerate(GEOM_NAMES):
-        assert rel_l2(ours[1 + k].cpu(), gg[k]) < GRAD_RTOL, name
+        assert rel_l2(ours_m[1 + k].cpu(), gg[k]) < GRAD_RTOL, name
 
 
 # ----------------------------------------------------------- finite differences
 
 
-def test_config1_finite_differences(golden):
+def test_config1_finite_differences(golden, oracle):
     """Central differences (eps=1e-3) of L = mean(p^2) for voxels and src_x.
 
-    Geometry differences use only rays whose sample count is unchanged by the
-    perturbation (the count is piecewise constant and not differentiated,
-    fp.cu:454-457).
+    For a geometry parameter the loss runs over the rays whose trace (entry
+    face, sample count, interpolation cells; oracle.ray_traces) is the same at
+    the base point and at +-eps, i.e. the difference stays inside one smooth
+    piece -- the guard of the reference's check_forward_operator.py:178-193.
     """
-    from cbct_backprojector import _ops
-
     d = golden("fp_config1.npz")
     case = config1_case(d)
+    shape = d["in_data"].shape
     out, vol, geom = run_project(case, requires_grad=True)
     p = out.detach().double()
-    loss = p.square().mean()
     gvol = torch.autograd.grad(out, vol, grad_outputs=(2 * p / p.numel()).float(),
                                retain_graph=True)[0]
     eps = 1e-3
     base = vol.detach()
-    idx = torch.topk(gvol.abs().flatten(), 3).indices.tolist()
-    for i in idx:
+    for i in torch.topk(gvol.abs().flatten(), 3).indices.tolist():
         e = torch.zeros_like(base).flatten()
         e[i] = eps
         e = e.view_as(base)
@@ -181,26 +237,27 @@ def test_config1_finite_differences(golden):
         fd = ((lp - lm) / (2 * eps)).item()
         assert math.isclose(gvol.flatten()[i].item(), fd, rel_tol=1e-2, abs_tol=1e-6)
 
-    shape = (vol.shape[0], vol.shape[1], vol.shape[2])
     k_sx = GEOM_NAMES.index("src_x")
-    for a in (0, 5, 13):
+    t0 = oracle.ray_traces(shape, case["geom"], 1.0, case["U"], case["V"], 0.5, 1.0, mode=1)
+    for a in (1, 5, 13, 22):
         gplus = [g.detach().clone() for g in geom]
         gminus = [g.detach().clone() for g in geom]
         gplus[k_sx][a] += eps
         gminus[k_sx][a] -= eps
-        c0 = _ops.project_sample_counts(shape, [g.detach() for g in geom], 1.0, case["U"],
-                                        case["V"], 0.5, 1.0)
-        cp = _ops.project_sample_counts(shape, gplus, 1.0, case["U"], case["V"], 0.5, 1.0)
-        cm = _ops.project_sample_counts(shape, gminus, 1.0, case["U"], case["V"], 0.5, 1.0)
-        mask = ((c0 == cp) & (c0 == cm)).double()
+        tp = oracle.ray_traces(shape, [g.cpu().numpy() for g in gplus], 1.0, case["U"], case["V"],
+                               0.5, 1.0, mode=1)
+        tm = oracle.ray_traces(shape, [g.cpu().numpy() for g in gminus], 1.0, case["U"],
+                               case["V"], 0.5, 1.0, mode=1)
+        keep = (t0 != 0) & (t0 == tp) & (t0 == tm)
+        assert keep[a].mean() > 0.5
+        mask = torch.tensor(keep.astype(np.float64), device="cuda")
         upstream = (2 * p * mask / p.numel()).float()
         g = torch.autograd.grad(out, geom[k_sx], grad_outputs=upstream, retain_graph=True)[0]
         fp_ = (run_project(case, geom=gplus)[0].double().square() * mask).sum() / p.numel()
         fm_ = (run_project(case, geom=gminus)[0].double().square() * mask).sum() / p.numel()
         denom = (gplus[k_sx][a] - gminus[k_sx][a]).item()
         fd = ((fp_ - fm_) / denom).item()
-        assert math.isclose(g[a].item(), fd, rel_tol=2e-2, abs_tol=1e-4), (a, g[a].item(), fd)
-    del loss
+        assert math.isclose(g[a].item(), fd, rel_tol=1e-2, abs_tol=1e-5), (a, g[a].item(), fd)
 
 
 # ------------------------------------------------------------- properties, edges
