@@ -212,12 +212,15 @@ def test_backward_matches_reference_cuda(which, golden, ref_native, oracle):
 
 
 def test_config1_finite_differences(golden, oracle):
-    """Central differences (eps=1e-3) of L = mean(p^2) for voxels and src_x.
+    """Central differences of L = mean(p^2) for voxels (eps=1e-3) and src_x.
 
     For a geometry parameter the loss runs over the rays whose trace (entry
     face, sample count, interpolation cells; oracle.ray_traces) is the same at
     the base point and at +-eps, i.e. the difference stays inside one smooth
     piece -- the guard of the reference's check_forward_operator.py:178-193.
+    The src_x step is 1e-2: sample offsets t_k come from the FP32 recurrence
+    and are quantised to ~1e-5, which at eps=1e-3 is a few percent of the
+    displacement a source shift produces (the FP64 oracle shows the same).
     """
     d = golden("fp_config1.npz")
     case = config1_case(d)
@@ -238,6 +241,7 @@ def test_config1_finite_differences(golden, oracle):
         assert math.isclose(gvol.flatten()[i].item(), fd, rel_tol=1e-2, abs_tol=1e-6)
 
     k_sx = GEOM_NAMES.index("src_x")
+    eps = 1e-2
     t0 = oracle.ray_traces(shape, case["geom"], 1.0, case["U"], case["V"], 0.5, 1.0, mode=1)
     for a in (1, 5, 13, 22):
         gplus = [g.detach().clone() for g in geom]
