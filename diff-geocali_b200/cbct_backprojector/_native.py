@@ -41,6 +41,7 @@ SIGNATURES = {
     "dgc_fdk_filter_taps": (_I, [_I, _D, _D, ctypes.POINTER(_D)]),
     "dgc_fdk_filter_workspace_bytes": (_S, [_I] * 3),
     "dgc_fdk_filter": (_I, [_P, _I, _I, _I, _F, _P, _P, _F, _P, _P, _S, _P]),
+    "dgc_fdk_filter_noalloc": (_I, [_P, _I, _I, _I, _F, _P, _P, _F, _P, _P]),
     "dgc_reconstruct_fdk_workspace_bytes": (_S, [_I] * 6),
     "dgc_reconstruct_fdk": (_I, [_P, _I, _I, _I, *_GEOM, _F, _I, _I, _I, _F, _F, _F, _F, _F, _P, _P,
                                  _S, _P]),

@@ -204,3 +204,70 @@ int fdk_upload_taps(int U, float px, float alpha, float* dst, cudaStream_t s) {
 }
 
 }  // namespace dgc
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant (dgc_fdk_filter_noalloc, see include/dgc.h)
+// ---------------------------------------------------------------------------
+
+// The filter taps of the allocation-free entry point.  Host code must not pass
+// this name to a kernel (on the host it is only a stand-in symbol); its device
+// address is looked up once per device with cudaGetSymbolAddress.
+static __device__ __align__(256) float g_noalloc_taps[DGC_FDK_NOALLOC_MAX_U];
+
+namespace dgc {
+namespace {
+
+std::mutex g_noalloc_mu;
+std::map<int, float*> g_noalloc_taps_by_device;
+
+// Device address of g_noalloc_taps on the current device (first call per
+// device performs the lookup).
+int noalloc_taps_address(float** out) {
+    int dev = 0;
+    DGC_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    auto it = g_noalloc_taps_by_device.find(dev);
+    if (it != g_noalloc_taps_by_device.end()) {
+        *out = it->second;
+        return DGC_OK;
+    }
+    void* p = nullptr;
+    DGC_CUDA(cudaGetSymbolAddress(&p, g_noalloc_taps));
+    g_noalloc_taps_by_device[dev] = static_cast<float*>(p);
+    *out = static_cast<float*>(p);
+    return DGC_OK;
+}
+
+}  // namespace
+}  // namespace dgc
+
+extern "C" int dgc_fdk_filter_noalloc(const float* projections, int A, int U, int V,
+                                      float pixel_size, const float* sod, const float* sid,
+                                      float alpha, float* filtered, void* stream) {
+    using namespace dgc;
+    clear_error();
+    cudaStream_t s = (cudaStream_t)stream;
+    DGC_REQUIRE(A > 0 && U > 0 && V > 0, "projections must have a nonempty [A, U, V] shape");
+    DGC_REQUIRE(std::isfinite(pixel_size) && pixel_size > 0.0f,
+                "pixel_size must be finite and positive");
+    DGC_REQUIRE(std::isfinite(alpha) && alpha > 0.0f, "alpha must be finite and positive");
+    DGC_REQUIRE(alpha <= 1.0f, "alpha must satisfy 0 < alpha <= 1");
+    DGC_REQUIRE(projections && sod && sid && filtered, "pointers must be non-null");
+    if (U > DGC_FDK_NOALLOC_MAX_U) {
+        set_error("dgc_fdk_filter_noalloc: U = " + std::to_string(U) + " exceeds the " +
+                  std::to_string(DGC_FDK_NOALLOC_MAX_U) +
+                  "-tap static scratch; use dgc_fdk_filter with a workspace");
+        return DGC_ERR_UNSUPPORTED;
+    }
+    float* taps = nullptr;
+    int rc = noalloc_taps_address(&taps);
+    if (rc != DGC_OK) return rc;
+    std::vector<double> h;
+    if ((rc = fdk_taps_host(U, (double)pixel_size, (double)alpha, h)) != DGC_OK) return rc;
+    std::vector<float> hf(h.begin(), h.end());
+    // Pageable source: the call returns once the taps are staged, so hf may go.
+    DGC_CUDA(cudaMemcpyAsync(taps, hf.data(), sizeof(float) * (size_t)U, cudaMemcpyHostToDevice, s));
+    FdkArgs f{projections, sod, sid, taps, filtered, A, U, V, pixel_size};
+    return fdk_launch_filter(f, s);
+}
+

@@ -155,6 +155,28 @@ int dgc_fdk_filter(const float* projections, int A, int U, int V, float pixel_si
                    float* filtered,
                    void* workspace, size_t workspace_bytes, void* stream);
 
+/* Maximum detector width U accepted by dgc_fdk_filter_noalloc. */
+#define DGC_FDK_NOALLOC_MAX_U 8192
+
+/* No counterpart in the reference.  dgc_fdk_filter for callers that cannot
+ * allocate device memory: a host application that owns the GPU's memory and
+ * hands each library a fixed budget, a plugin that must not grow the process's
+ * device footprint, or a latency-bound pipeline that keeps cudaMalloc and
+ * cudaFree (which can synchronise the device) out of its steady state.  It
+ * takes no workspace: the only scratch, the filter taps, lives in a static
+ * device array of DGC_FDK_NOALLOC_MAX_U floats (32 KiB) that every GPU loading
+ * the library holds until the process exits; U above that maximum returns
+ * DGC_ERR_UNSUPPORTED.  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress) and caches it; make that first call before
+ * any stream capture.  Every call overwrites taps[0..U-1] before its filter
+ * reads them, so nothing needs to start at zero, but all calls share the one
+ * array: calls that overlap on the GPU (different streams, no ordering
+ * between them) race on it.  Same inputs, outputs and results as
+ * dgc_fdk_filter. */
+int dgc_fdk_filter_noalloc(const float* projections, int A, int U, int V, float pixel_size,
+                           const float* sod, const float* sid, float alpha,
+                           float* filtered, void* stream);
+
 /* Scratch of dgc_reconstruct_fdk. */
 size_t dgc_reconstruct_fdk_workspace_bytes(int A, int U, int V, int D, int H, int W);
 
