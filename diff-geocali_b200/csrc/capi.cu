@@ -53,7 +53,7 @@ size_t padded_volume_bytes(int D, int H, int W) {
 
 // Ray tile of the forward projector: DGC_FP_TILE="tu,wu" overrides the default.
 FpTile forward_tile() {
-    FpTile t{16, 8};
+    FpTile t{8, 1};
     if (const char* e = std::getenv("DGC_FP_TILE")) {
         int tu = 0, wu = 0;
         if (sscanf(e, "%d,%d", &tu, &wu) == 2) t = FpTile{tu, wu};
@@ -61,7 +61,7 @@ FpTile forward_tile() {
     return t;
 }
 
-constexpr FpTile kBackwardTile{16, 8};
+constexpr FpTile kBackwardTile{8, 1};
 
 int check_fp_common(int D, int H, int W, int A, int U, int V, float pixel_size, float step_size,
                     float voxel_size, const Geometry& g) {
@@ -75,7 +75,7 @@ int check_fp_common(int D, int H, int W, int A, int U, int V, float pixel_size, 
         set_error("volume exceeds this build's 2^31 padded-voxel index limit");
         return DGC_ERR_UNSUPPORTED;
     }
-    if (fp_tiles_per_view(U, V, 8) * (long long)A >= (1LL << 31)) {
+    if (fp_tiles_per_view(U, V, 4) * (long long)A >= (1LL << 31)) {
         set_error("too many rays for one launch");
         return DGC_ERR_UNSUPPORTED;
     }

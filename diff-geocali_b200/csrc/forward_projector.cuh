@@ -10,20 +10,20 @@ struct FpArgs {
     int D, H, W, A, U, V;
     float pixel_size, step_size, voxel_size, inv_voxel;
     float off_x, off_y, off_z;
-    // edge-replicated quad-packed volume [(D+2)][(H+1)][(W+1)]
+    // edge-replicated, z-fastest quad-packed volume Q[(yp*(W+1) + xp)*(D+2) + zp]
     const float4* quads;
-    uint32_t q_row, q_plane, q_bias;
+    uint32_t zq_x, zq_y, zq_bias;
     // forward output [A][U][V]
     float* projections;
     // backward
     const float* grad_projections;  // [A][U][V]
-    float* grad_pad;                // [(D+2)][(H+2)][(W+2)] or null
-    uint32_t g_row, g_plane, g_bias;
+    float* grad_pad;                // G[(yp*(W+2) + xp)*(D+2) + zp] or null
+    uint32_t gz_x, gz_y, gz_bias;
     double* partials;  // [A][tiles][8]
 };
 
-// Ray tile of a CTA: TU detector columns x (256/TU) rows; WU lanes of a warp
-// along U.
+// Ray tile of a CTA: TU detector columns x (256/TU) rows; the 32 lanes of a
+// warp run along V (wu = 1).
 struct FpTile {
     int tu;
     int wu;
