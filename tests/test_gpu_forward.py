@@ -222,6 +222,8 @@ def test_config1_finite_differences(golden, oracle):
     and are quantised to ~1e-5, which at eps=1e-3 is a few percent of the
     displacement a source shift produces (the FP64 oracle shows the same).
     """
+    from cbct_backprojector import _ops
+
     d = golden("fp_config1.npz")
     case = config1_case(d)
     shape = d["in_data"].shape
@@ -252,7 +254,12 @@ def test_config1_finite_differences(golden, oracle):
                                0.5, 1.0, mode=1)
         tm = oracle.ray_traces(shape, [g.cpu().numpy() for g in gminus], 1.0, case["U"],
                                case["V"], 0.5, 1.0, mode=1)
-        keep = (t0 != 0) & (t0 == tp) & (t0 == tm)
+        c0 = _ops.project_sample_counts(shape, [g.detach() for g in geom], 1.0, case["U"],
+                                        case["V"], 0.5, 1.0).cpu().numpy()
+        cp = _ops.project_sample_counts(shape, gplus, 1.0, case["U"], case["V"], 0.5, 1.0)
+        cm = _ops.project_sample_counts(shape, gminus, 1.0, case["U"], case["V"], 0.5, 1.0)
+        keep = ((t0 != 0) & (t0 == tp) & (t0 == tm) & (cp.cpu().numpy() == c0) &
+                (cm.cpu().numpy() == c0))
         assert keep[a].mean() > 0.5
         mask = torch.tensor(keep.astype(np.float64), device="cuda")
         upstream = (2 * p * mask / p.numel()).float()
