@@ -45,6 +45,7 @@ SIGNATURES = {
     "dgc_reconstruct_fdk_workspace_bytes": (_S, [_I] * 6),
     "dgc_reconstruct_fdk": (_I, [_P, _I, _I, _I, *_GEOM, _F, _I, _I, _I, _F, _F, _F, _F, _F, _P, _P,
                                  _S, _P]),
+    "dgc_gemm_bf16": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _I, _I, _I, _I, _I, _F, _P, _P]),
     "dgc_trace_enable": (None, [_I]),
     "dgc_trace_count": (_I, []),
     "dgc_trace_get": (_I, [_I, ctypes.c_char_p, _I, ctypes.POINTER(_F)]),

@@ -14,6 +14,7 @@
 #include "common.cuh"
 #include "fdk.cuh"
 #include "forward_projector.cuh"
+#include "tc_gemm.cuh"
 
 namespace dgc {
 
@@ -458,6 +459,26 @@ int dgc_reconstruct_fdk(const float* projections, int A, int U, int V, const flo
     p.volume = volume;
     p.out_scale = (float)(M_PI / (double)A);
     return bp_launch_forward(p, true, s);
+}
+
+// ---------------------------------------------------------- tensor-core GEMM
+
+int dgc_gemm_bf16(const void* A, const void* B, void* C, const float* bias, int M, int N, int K,
+                  int lda, int ldb, int ldc, int c_bf16, int relu, int accumulate, float alpha,
+                  int* error_flag, void* stream) {
+    clear_error();
+    DGC_REQUIRE(A && B && C && error_flag, "A, B, C and error_flag must be non-null");
+    DGC_REQUIRE(M > 0 && N > 0 && K > 0, "M, N, K must be positive");
+    DGC_REQUIRE(K % 8 == 0 && lda % 8 == 0 && ldb % 8 == 0 && lda >= K && ldb >= K,
+                "K, lda and ldb must be multiples of 8 (16-byte rows) with lda, ldb >= K");
+    DGC_REQUIRE(ldc >= N, "ldc must be >= N");
+    DGC_REQUIRE(((uintptr_t)A % 16) == 0 && ((uintptr_t)B % 16) == 0,
+                "A and B must be 16-byte aligned");
+    DGC_REQUIRE(!(accumulate && c_bf16), "accumulate needs an fp32 C");
+    DGC_REQUIRE(ceil_div(M, 128) <= 65535, "M too large for one launch");
+    GemmArgs p{static_cast<const __nv_bfloat16*>(A), static_cast<const __nv_bfloat16*>(B), C, bias,
+               M, N, K, lda, ldb, ldc, c_bf16, relu, accumulate, alpha, error_flag};
+    return tc_gemm(p, (cudaStream_t)stream);
 }
 
 }  // extern "C"

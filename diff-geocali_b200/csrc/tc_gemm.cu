@@ -1,0 +1,285 @@
+// tc_gemm.cu -- BF16 x BF16 -> FP32 GEMM on the sm_100 5th-generation tensor
+// cores (tcgen05.mma, accumulators in tensor memory), for the convolution
+// layers of the warm-start network.  No counterpart in the reference.
+//
+//   C[m, n] (+)= sum_k A[m, k] * B[n, k]  (+ bias[n], optional ReLU)
+//
+// A (M x K) and B (N x K) are row-major bf16 ("K-major"); C is fp32 or bf16.
+//
+// Structure of a CTA (128 threads, one 128 x BN output tile):
+//   * warp 0 allocates BN tensor-memory columns (a 128-lane x BN fp32
+//     accumulator) and frees them at the end;
+//   * all threads stage 128 x 64 tiles of A and BN x 64 tiles of B into shared
+//     memory with cp.async, four stages deep, in the canonical no-swizzle
+//     K-major layout (8-row x 16-byte core matrices: SBO = 128 B between row
+//     groups, LBO = rows*16 B between 8-element K groups);
+//   * one elected thread issues four tcgen05.mma (M=128, N=BN, K=16) per stage
+//     and commits them to the stage's mbarrier, which releases the stage for
+//     the next prefetch and, after the last stage, signals the epilogue;
+//   * the four warps read their 32 accumulator lanes with tcgen05.ld, apply
+//     bias / ReLU / accumulate and store.
+// Every mbarrier wait is bounded; a timeout sets the error word, skips the
+// epilogue and still frees the tensor memory.
+#include "common.cuh"
+#include "tc_gemm.cuh"
+
+namespace dgc {
+namespace {
+
+constexpr int kBM = 128;
+constexpr int kBK = 64;
+constexpr int kStages = 4;
+constexpr long long kWaitLimit = 1LL << 26;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, int src_bytes) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src),
+                 "r"(src_bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
+}
+
+// Bounded wait for the phase with the given parity; false on timeout.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    for (long long i = 0; i < kWaitLimit; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+            " selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+// Shared-memory matrix descriptor, K-major, no swizzle (sm_100 format:
+// start >> 4 in [0,14), LBO >> 4 in [16,30), SBO >> 4 in [32,46), version 1 at
+// bit 46, base offset 0, layout type 0).
+__device__ __forceinline__ uint64_t kmajor_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = 0;
+    d |= static_cast<uint64_t>((saddr >> 4) & 0x3FFFu);
+    d |= static_cast<uint64_t>((lbo >> 4) & 0x3FFFu) << 16;
+    d |= static_cast<uint64_t>((sbo >> 4) & 0x3FFFu) << 32;
+    d |= static_cast<uint64_t>(1) << 46;
+    return d;
+}
+
+// Instruction descriptor of kind::f16 with bf16 A and B, fp32 D, both K-major.
+__host__ __device__ constexpr uint32_t idesc_bf16(int m, int n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(n >> 3) << 17) |
+           (static_cast<uint32_t>(m >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                          uint32_t idesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                     bar)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() {
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_load16(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+        "[%16];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+          "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr)
+        : "memory");
+    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// Stage one K-slice: 'rows' x 64 bf16 of a K-major matrix into the core-matrix
+// layout (16-byte chunk (r, kc) at kc*rows*16 + r*16).  Out-of-range rows or
+// K chunks are zero-filled.
+template <int ROWS>
+__device__ __forceinline__ void stage_tile(uint32_t sbase, const __nv_bfloat16* g, int ld,
+                                           int row0, int nrows, int k0, int K) {
+    constexpr int kChunks = ROWS * (kBK / 8);
+#pragma unroll
+    for (int c = threadIdx.x; c < kChunks; c += 128) {
+        const int r = c % ROWS, kc = c / ROWS;
+        const int row = row0 + r, k = k0 + kc * 8;
+        const bool ok = row < nrows && k < K;
+        const __nv_bfloat16* src = ok ? g + (long long)row * ld + k : g;
+        cp_async16(sbase + static_cast<uint32_t>((kc * ROWS + r) * 16), src, ok ? 16 : 0);
+    }
+}
+
+template <int BN>
+__global__ void __launch_bounds__(128) tc_gemm_kernel(GemmArgs p) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    __shared__ __align__(8) uint64_t bars[kStages + 1];
+    __shared__ uint32_t tmem_slot;
+    constexpr int kABytes = kBM * kBK * 2;
+    constexpr int kBBytes = BN * kBK * 2;
+    constexpr int kStageBytes = kABytes + kBBytes;
+    constexpr uint32_t kIdesc = idesc_bf16(kBM, BN);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m0 = blockIdx.y * kBM, n0 = blockIdx.x * BN;
+    const uint32_t sbase = smem_u32(smem);
+    const int nk = (p.K + kBK - 1) / kBK;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                         smem_u32(&tmem_slot)),
+                     "r"(BN)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+    }
+    if (threadIdx.x == 0) {
+        for (int s = 0; s <= kStages; ++s) mbar_init(smem_u32(&bars[s]), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_slot;
+
+    // prologue: stages 0 .. kStages-2
+#pragma unroll
+    for (int s = 0; s < kStages - 1; ++s) {
+        if (s < nk) {
+            const uint32_t sa = sbase + s * kStageBytes;
+            stage_tile<kBM>(sa, p.A, p.lda, m0, p.M, s * kBK, p.K);
+            stage_tile<BN>(sa + kABytes, p.B, p.ldb, n0, p.N, s * kBK, p.K);
+        }
+        cp_async_commit();
+    }
+
+    bool ok = true;
+    for (int kt = 0; kt < nk; ++kt) {
+        const int s = kt % kStages;
+        cp_async_wait<kStages - 2>();
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        // block-uniform: a timed-out wait anywhere ends the loop for all threads
+        ok = __syncthreads_and(ok);
+        if (!ok) break;
+        if (threadIdx.x == 0) {
+            tc_fence_after();
+            const uint32_t sa = sbase + s * kStageBytes;
+#pragma unroll
+            for (int kk = 0; kk < kBK / 16; ++kk) {
+                // K = 16 per instruction: two 8-element K groups
+                const uint64_t ad = kmajor_desc(sa + kk * 2 * kBM * 16, kBM * 16, 128);
+                const uint64_t bd = kmajor_desc(sa + kABytes + kk * 2 * BN * 16, BN * 16, 128);
+                umma_bf16(tmem, ad, bd, kIdesc, (kt > 0 || kk > 0) ? 1u : 0u);
+            }
+            umma_commit(smem_u32(&bars[s]));
+        }
+        // prefetch tile kt + kStages - 1 into the stage the previous MMAs used
+        const int kn = kt + kStages - 1;
+        if (kn < nk) {
+            const int sn = kn % kStages;
+            if (kt >= 1) ok = mbar_wait(smem_u32(&bars[sn]), ((kt - 1) / kStages) & 1);
+            if (ok) {
+                const uint32_t sa = sbase + sn * kStageBytes;
+                stage_tile<kBM>(sa, p.A, p.lda, m0, p.M, kn * kBK, p.K);
+                stage_tile<BN>(sa + kABytes, p.B, p.ldb, n0, p.N, kn * kBK, p.K);
+            }
+        }
+        cp_async_commit();
+    }
+    cp_async_wait<0>();
+    ok = __syncthreads_and(ok);
+    // the last commit completes after every MMA of the tile
+    if (ok && nk > 0) ok = mbar_wait(smem_u32(&bars[(nk - 1) % kStages]), ((nk - 1) / kStages) & 1);
+    ok = __syncthreads_and(ok);
+    if (!ok && threadIdx.x == 0) atomicExch(p.error, 1);
+    tc_fence_after();
+
+    if (ok) {
+        const int row = m0 + warp * 32 + lane;
+        const uint32_t lane_addr = tmem + (static_cast<uint32_t>(warp * 32) << 16);
+#pragma unroll 1
+        for (int c0 = 0; c0 < BN; c0 += 16) {
+            float v[16];
+            tmem_load16(lane_addr + c0, v);
+            if (row < p.M) {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    const int col = n0 + c0 + j;
+                    if (col >= p.N) break;
+                    float x = (nk > 0) ? v[j] : 0.0f;
+                    x *= p.alpha;
+                    if (p.bias) x += p.bias[col];
+                    if (p.relu) x = fmaxf(x, 0.0f);
+                    const long long off = (long long)row * p.ldc + col;
+                    if (p.c_bf16) {
+                        __nv_bfloat16* C = static_cast<__nv_bfloat16*>(p.C);
+                        C[off] = __float2bfloat16(x);
+                    } else {
+                        float* C = static_cast<float*>(p.C);
+                        C[off] = p.accumulate ? C[off] + x : x;
+                    }
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(BN)
+                     : "memory");
+    }
+}
+
+template <int BN>
+int launch_gemm(const GemmArgs& p, cudaStream_t s) {
+    const int smem = kStages * (kBM * kBK * 2 + BN * kBK * 2);
+    static bool configured = false;
+    if (!configured) {
+        DGC_CUDA(cudaFuncSetAttribute(tc_gemm_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      smem));
+        configured = true;
+    }
+    const dim3 grid(ceil_div(p.N, BN), ceil_div(p.M, kBM));
+    tc_gemm_kernel<BN><<<grid, 128, smem, s>>>(p);
+    DGC_LAUNCH_CHECK("tc_gemm_kernel");
+    return DGC_OK;
+}
+
+}  // namespace
+
+int tc_gemm(const GemmArgs& p, cudaStream_t s) {
+    DGC_TRACE("tc_gemm_kernel", s);
+    if (p.N <= 64) return launch_gemm<64>(p, s);
+    return launch_gemm<128>(p, s);
+}
+
+}  // namespace dgc

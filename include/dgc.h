@@ -193,6 +193,21 @@ int dgc_reconstruct_fdk(const float* projections, int A, int U, int V,
                         void* workspace, size_t workspace_bytes, void* stream);
 
 /* ---------------------------------------------------------------------- */
+/* Tensor-core GEMM of the warm-start network (no counterpart in the        */
+/* reference: its calibration pipeline is not shipped)                      */
+/* ---------------------------------------------------------------------- */
+
+/* C[m,n] = alpha * sum_k A[m,k] B[n,k] (+ bias[n]) (then ReLU if relu != 0),
+ * on the tcgen05 tensor cores with fp32 accumulation in tensor memory.
+ * A [M x K] and B [N x K] are row-major bf16 with 16-byte aligned rows
+ * (lda, ldb multiples of 8, K a multiple of 8); C is bf16 (c_bf16 = 1) or
+ * fp32, row stride ldc; accumulate = 1 adds into an fp32 C.  error_flag is a
+ * device int set to 1 if a pipeline wait of the kernel timed out. */
+int dgc_gemm_bf16(const void* A, const void* B, void* C, const float* bias, int M, int N, int K,
+                  int lda, int ldb, int ldc, int c_bf16, int relu, int accumulate, float alpha,
+                  int* error_flag, void* stream);
+
+/* ---------------------------------------------------------------------- */
 /* Kernel timing (no counterpart in the reference; measurement support)     */
 /* ---------------------------------------------------------------------- */
 
