@@ -56,6 +56,15 @@ def parse_args(argv=None):
                     help="override the view count (smaller cases for profiler captures)")
     ap.add_argument("--volume", type=int, default=None, help="override the cubic volume size")
     ap.add_argument("--detector", type=int, default=None, help="override the square detector size")
+    ap.add_argument("--workload", choices=["fdk256", "batch64", "calib"], default="fdk256",
+                    help="fdk256: the FDK step (default); batch64: 64 uneven project+backward "
+                         "instances, batched vs sequential; calib: calibration wall time to "
+                         "0.1 px, learned warm start vs plain")
+    ap.add_argument("--acq", choices=["half", "eval"], default="half",
+                    help="calib: 256^3/360/384^2 (half) or 512^3/720/768^2 (eval)")
+    ap.add_argument("--max-iterations", type=int, default=600, help="calib: iteration cap")
+    ap.add_argument("--instances", type=int, default=64, help="batch64: number of instances")
+    ap.add_argument("--tune-cache", default=None, help="batch64: autotuner JSON cache path")
     args = ap.parse_args(argv)
     if args.views:
         WORKLOAD["A"] = args.views
@@ -411,10 +420,205 @@ def run_ours(args):
     return 0
 
 
+# ------------------------------------------------------------------ batch64
+
+BATCH64 = dict(name="batch64: uneven instances, project + backward (volume and geometry "
+                    "gradients) each, one persistent launch per pass, CUDA graph",
+               volumes=[(128, 128, 128), (128, 192, 192), (256, 256, 256), (256, 384, 384)],
+               views=[90, 180, 360, 720], detectors=[256, 384, 512], sid=1000.0, sod=600.0,
+               voxel=1.0, step=0.5, seed=4)
+
+
+def make_batch64(device, n, seed):
+    """``n`` problems drawn from the seed: volume shape, views and detector U, V
+    independently; config-3 perturbations of the nominal circular geometry;
+    the pixel size makes the detector cover the magnified volume."""
+    import numpy as np
+
+    from cbct_backprojector.batch import Problem
+    from cbct_backprojector.calibration import perturb_geometry
+    from cbct_backprojector.phantoms import circular_geometry, ellipsoid_phantom
+
+    c = BATCH64
+    rng = np.random.default_rng(seed)
+    problems = []
+    for i in range(n):
+        D, H, W = c["volumes"][rng.integers(len(c["volumes"]))]
+        A = int(c["views"][rng.integers(len(c["views"]))])
+        U = int(c["detectors"][rng.integers(len(c["detectors"]))])
+        V = int(c["detectors"][rng.integers(len(c["detectors"]))])
+        px = 1.2 * max(D, H, W) * c["voxel"] * (c["sid"] / c["sod"]) / min(U, V)
+        vol = ellipsoid_phantom((D, H, W), n=12, seed=seed * 1000 + i, voxel_size=c["voxel"],
+                                device=device)
+        nominal = circular_geometry(A, U, V, c["sid"], c["sod"], px, device=device)
+        true = perturb_geometry(nominal, seed * 1000 + i)
+        problems.append(Problem(vol, true, px, U, V, c["step"], c["voxel"]))
+    return problems
+
+
+def plain_step(problems):
+    """The baseline: one ``project`` call and its autograd backward per instance."""
+    import torch
+
+    import cbct_backprojector as cb
+
+    for pr in problems:
+        vol = pr.volume.detach().requires_grad_()
+        geom = [g.detach().requires_grad_() for g in pr.geometry]
+        p = cb.project(vol, *geom, pr.pixel_size, pr.U, pr.V, step_size=pr.step_size,
+                       voxel_size=pr.voxel_size)
+        torch.autograd.grad(p, [vol, *geom], grad_outputs=p.detach())
+
+
+def run_batch64(args):
+    import torch
+
+    from cbct_backprojector import _native, _ops
+    from cbct_backprojector.autotune import Autotuner
+    from cbct_backprojector.batch import ProjectionBatch
+
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    dist = init_dist(world, "nccl")
+    problems = make_batch64(device, args.instances, BATCH64["seed"] + 1000 * rank)
+    R = sum(pr.rays for pr in problems)
+    S = 0
+    for pr in problems:
+        S += int(_ops.project_sample_counts(tuple(pr.volume.shape), pr.geometry, pr.pixel_size,
+                                            pr.U, pr.V, pr.step_size, pr.voxel_size).sum().item())
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
+    torch.cuda.synchronize(device)
+
+    def timed(fn, steps, warmup):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize(device)
+        if dist is not None:
+            dist.barrier()
+        ms = []
+        for _ in range(steps):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            fn()
+            b.record()
+            b.synchronize()
+            ms.append(a.elapsed_time(b))
+        return max_over_ranks(sum(ms), dist, device) / steps
+
+    t0 = time.perf_counter()
+    tuner = Autotuner(cache_path=args.tune_cache)
+    tuner.choose(problems)
+    tune_s = time.perf_counter() - t0
+    batch = ProjectionBatch(problems)
+    seq_ms = timed(lambda: plain_step(problems), args.steps, max(1, args.warmup // 2))
+    eager_ms = timed(batch.step, args.steps, 1)
+    batch.capture()
+    with ClockSampler(local) as clocks:
+        graph_ms = timed(batch.replay, args.steps, args.warmup)
+    with _native.trace() as tr:
+        batch.step()
+        torch.cuda.synchronize(device)
+    kern = {}
+    for name, ms in tr.records:
+        kern[name] = kern.get(name, 0.0) + ms
+
+    # end to end: volumes from pinned host memory, geometry gradients back
+    host_vols = [pr.volume.cpu().pin_memory() for pr in problems]
+    host_gg = [torch.empty(g.shape, dtype=torch.float32).pin_memory() for g in batch.grad_geometry]
+
+    def e2e_step():
+        for hv, pr in zip(host_vols, problems):
+            pr.volume.copy_(hv, non_blocking=True)
+        batch.replay()
+        for hg, g in zip(host_gg, batch.grad_geometry):
+            hg.copy_(g, non_blocking=True)
+
+    e2e_ms = timed(e2e_step, args.steps, 1)
+    h2d = sum(v.numel() * 4 for v in host_vols)
+    d2h = sum(g.numel() * 4 for g in host_gg)
+    peak, peak_kind = measured_peak_hbm()
+    bwd_ms = kern.get("batch_backward_kernel", float("nan"))
+    alg = 64 * S + 4 * R  # adjoint: 8 gathers + 8 scatters per sample
+    achieved = alg / (bwd_ms * 1e-3) / 1e9
+    value = world * R / (graph_ms * 1e-3) / 1e9
+    line = {
+        "metric": "total Grays/s (forward + backward over all instances)", "value": value,
+        "unit": "Grays/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": graph_ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": BATCH64["name"], "instances": len(problems),
+                   "rays": R, "samples": S, "l2": "flushed between timed steps (256 MiB write)",
+                   "parallelism": f"independent batches x{world}"},
+        "sequential_plain_calls": {"ms_per_step": seq_ms,
+                                   "value": world * R / (seq_ms * 1e-3) / 1e9},
+        "batched_eager": {"ms_per_step": eager_ms, "value": world * R / (eager_ms * 1e-3) / 1e9},
+        "speedup_vs_sequential": seq_ms / graph_ms,
+        "autotune": {"seconds": tune_s, "buckets_measured": len(tuner.measured),
+                     "tiles": sorted({f"{a},{b}" for a, b in (pr.tiles for pr in problems)})},
+        "kernel_ms": kern, "gpu_launches": len(tr.records),
+        "roofline": {"bound": "hbm", "kernel": "batch_backward_kernel", "achieved": achieved,
+                     "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_source": f"{peak_kind} hbm_gbs", "traffic": None,
+                     "algorithmic_bytes": alg, "ms": bwd_ms},
+        "e2e": {"value": world * R / (e2e_ms * 1e-3) / 1e9, "unit": "Grays/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "memory_gb": torch.cuda.max_memory_allocated(device) / 1e9,
+        "clocks": clocks.summary(),
+    }
+    if rank == 0:
+        print(json.dumps(line))
+    del batch
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+# -------------------------------------------------------------------- calib
+
+
+def run_calib(args):
+    """Wall time to 0.1 px RMS reprojection error (and 0.05 deg angle error on
+    the eval acquisition): calibration from the network's warm start vs from
+    nominal, same GPU, same projector; every iteration timed on the host."""
+    import torch
+
+    from cbct_backprojector import warmstart as WS
+
+    torch.cuda.set_device(0)
+    acq = WS.HALF if args.acq == "half" else WS.EVAL
+    net, meta = WS.load(WS.default_checkpoint())
+    target_angle = None if args.acq == "half" else 0.05
+    res = WS.evaluate(net, acq, seed=7, iterations=args.max_iterations, target_mm=0.1 * acq.pixel,
+                      target_angle_deg=target_angle, stop_at_target=True)
+    p, n = res["plain"], res["warm_start"]
+    line = {
+        "metric": "calibration wall time to 0.1 px RMS reprojection error", "unit": "s",
+        "value": n["time_to_target_s"], "higher_is_better": False, "n_gpus": 1,
+        "steps": 1, "warmup": 0, "dtype": "f32 (network bf16/fp32)", "data": "synthetic",
+        "vs_baseline": None,
+        "config": {"workload": f"calibration {acq.volume}^3, {acq.views} views, "
+                               f"{acq.detector}^2 detector, config-3 perturbations, I0=1e5",
+                   "max_iterations": args.max_iterations, "target_px": 0.1,
+                   "target_angle_deg": target_angle,
+                   "network_training_steps": meta.get("steps")},
+        "plain": p, "warm_start": n, "speedup": res["speedup"],
+        "warm_start_accepted": res["warm_start_accepted"], "inference_s": res["inference_s"],
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def main(argv=None):
     args = parse_args(argv)
+    if args.workload == "calib":
+        return run_calib(args)
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "batch64":
+        return run_batch64(args)
     return run_ours(args)
 
 

@@ -23,6 +23,29 @@ _S = ctypes.c_size_t
 
 _GEOM = [_P] * 8  # angles, sid, sod, det_u0, det_v0, src_x, src_y, src_z
 
+
+class FpInstance(ctypes.Structure):
+    """``dgc_fp_instance``: one problem of a batched projection."""
+
+    _fields_ = [("volume", _P), ("D", _I), ("H", _I), ("W", _I),
+                *[(n, _P) for n in ("angles", "sid", "sod", "det_u0", "det_v0", "src_x", "src_y",
+                                    "src_z")],
+                ("A", _I), ("pixel_size", _F), ("U", _I), ("V", _I), ("step_size", _F),
+                ("voxel_size", _F), ("off_x", _F), ("off_y", _F), ("off_z", _F),
+                ("projections", _P), ("grad_projections", _P), ("grad_volume", _P),
+                ("grad_geometry", _P), ("tile_forward", _I), ("tile_backward", _I)]
+
+
+class BatchPlan(ctypes.Structure):
+    """``dgc_batch_plan``: a prepared batch (host-side)."""
+
+    _fields_ = [("workspace", _P), ("n", _I), ("grid_forward", _I), ("grid_backward", _I),
+                ("has_grad_volume", _I), ("backward_ready", _I),
+                *[(n, ctypes.c_longlong) for n in ("items_forward", "items_backward",
+                                                   "quad_blocks", "views", "fold_blocks", "rays")],
+                ("grad_pad_offset", _S), ("grad_pad_bytes", _S), ("tables_bytes", _S)]
+
+
 # name -> (restype, argtypes)
 SIGNATURES = {
     "dgc_abi_version": (_I, []),
@@ -46,6 +69,13 @@ SIGNATURES = {
     "dgc_reconstruct_fdk": (_I, [_P, _I, _I, _I, *_GEOM, _F, _I, _I, _I, _F, _F, _F, _F, _F, _P, _P,
                                  _S, _P]),
     "dgc_gemm_bf16": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _I, _I, _I, _I, _I, _F, _P, _P]),
+    "dgc_im2col_nhwc_bf16": (_I, [_P, _I, _I, _I, _I, _I, _I, _I, _I, _P, _I, _P]),
+    "dgc_col2im_nhwc_f32": (_I, [_P, _I, _I, _I, _I, _I, _I, _I, _I, _I, _P, _P]),
+    "dgc_batch_workspace_bytes": (_S, [ctypes.POINTER(FpInstance), _I]),
+    "dgc_batch_prepare": (_I, [ctypes.POINTER(FpInstance), _I, _P, _S, ctypes.POINTER(BatchPlan),
+                               _P]),
+    "dgc_batch_project": (_I, [ctypes.POINTER(BatchPlan), _P]),
+    "dgc_batch_project_backward": (_I, [ctypes.POINTER(BatchPlan), _I, _P]),
     "dgc_trace_enable": (None, [_I]),
     "dgc_trace_count": (_I, []),
     "dgc_trace_get": (_I, [_I, ctypes.c_char_p, _I, ctypes.POINTER(_F)]),

@@ -158,13 +158,14 @@ def _loss(volume, geometry, measured, scan, mask=None):
 def calibrate(volume, measured, nominal, scan: ScanSetup, iterations=200, lr=None,
               warm_start=None, true_geometry=None, points=None, target_px=0.1,
               target_angle_deg=None, stop_at_target=False, log_every=0, mask=None,
-              final_lr_fraction=1.0):
+              final_lr_fraction=1.0, lr_gamma=1.0, decay_start=0):
     """Adam on per-view geometry offsets; returns a ``CalibrationResult``.
 
     The loss is the mean squared mismatch between ``project(volume, nominal +
     delta)`` and ``measured`` over the rays where ``mask`` is 1 (all rays when
     ``mask`` is None).  Step sizes follow a cosine decay to
-    ``final_lr_fraction`` of their start over ``iterations`` (1.0: constant).
+    ``final_lr_fraction`` of their start over ``iterations`` (1.0: constant),
+    times ``lr_gamma ** max(0, it - decay_start)``.
 
     ``warm_start`` (8 tensors [A], e.g. a network's prediction) is used as the
     initial delta only if it does not raise the projection loss relative to
@@ -194,8 +195,9 @@ def calibrate(volume, measured, nominal, scan: ScanSetup, iterations=200, lr=Non
     opt = torch.optim.Adam([{"params": [d], "lr": lr[name]}
                             for d, name in zip(delta, GEOMETRY_NAMES)], betas=(0.9, 0.99))
     sched = torch.optim.lr_scheduler.LambdaLR(
-        opt, lambda it: final_lr_fraction + (1.0 - final_lr_fraction) * 0.5 *
-        (1.0 + math.cos(math.pi * min(it, iterations) / max(iterations, 1))))
+        opt, lambda it: (final_lr_fraction + (1.0 - final_lr_fraction) * 0.5 *
+                         (1.0 + math.cos(math.pi * min(it, iterations) / max(iterations, 1)))) *
+        lr_gamma ** max(0, it - decay_start))
     if points is None and true_geometry is not None:
         points = lattice_points(volume.shape, scan.voxel_size, scan.volume_offset,
                                 device=volume.device)

@@ -127,6 +127,12 @@ BpArgs bp_args(const ViewRow* vt, const float4* pq, int A, int U, int V, int D, 
 }
 
 }  // namespace
+
+int fp_check_args(int D, int H, int W, int A, int U, int V, float pixel_size, float step_size,
+                  float voxel_size, const Geometry& g) {
+    return check_fp_common(D, H, W, A, U, V, pixel_size, step_size, voxel_size, g);
+}
+
 }  // namespace dgc
 
 using namespace dgc;
@@ -477,7 +483,21 @@ int dgc_gemm_bf16(const void* A, const void* B, void* C, const float* bias, int 
     DGC_REQUIRE(!(accumulate && c_bf16), "accumulate needs an fp32 C");
     DGC_REQUIRE(ceil_div(M, 128) <= 65535, "M too large for one launch");
     GemmArgs p{static_cast<const __nv_bfloat16*>(A), static_cast<const __nv_bfloat16*>(B), C, bias,
-               M, N, K, lda, ldb, ldc, c_bf16, relu, accumulate, alpha, error_flag};
+               M, N, K, lda, ldb, ldc, c_bf16, relu, accumulate, alpha, error_flag, 0};
+    // Long reductions with few output tiles (weight gradients): split K over
+    // CTAs and sum into a zeroed fp32 C with atomics.
+    const long long tiles = (long long)ceil_div(M, 128) * ceil_div(N, N <= 64 ? 64 : 128);
+    const int ktiles = ceil_div(K, 64);
+    if (!c_bf16 && !relu && tiles < 148 && ktiles >= 32) {
+        const int splits = (int)std::min<long long>(std::max<long long>(296 / tiles, 1), ktiles / 8);
+        if (splits > 1) {
+            p.k_tiles_per_split = ceil_div(ktiles, splits);
+            // zero only the M x N window: C may be a column slice of a wider array
+            if (!accumulate)
+                DGC_CUDA(cudaMemset2DAsync(C, sizeof(float) * (size_t)ldc, 0, sizeof(float) * (size_t)N,
+                                           (size_t)M, (cudaStream_t)stream));
+        }
+    }
     return tc_gemm(p, (cudaStream_t)stream);
 }
 

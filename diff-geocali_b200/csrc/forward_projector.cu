@@ -42,14 +42,14 @@ namespace dgc {
 // Volume re-layout: [D][H][W] -> Z-fastest edge-replicated quads
 // ---------------------------------------------------------------------------
 
-// grid: x = ceil((W+1)/32) * (H+1), y = ceil((D+2)/32); block (32, 8)
-__global__ void build_volume_quads_kernel(const float* __restrict__ vol, int D, int H, int W,
-                                          float4* __restrict__ Q) {
-    __shared__ float4 tile[32][33];
+// One 32 x 32 (x, z) tile of the quads at padded row yp: block (32, 8).
+__device__ __forceinline__ void quads_tile(const float* __restrict__ vol, int D, int H, int W,
+                                           float4* __restrict__ Q, int bx, int by,
+                                           float4 (&tile)[32][33]) {
     const int xtiles = (W + 1 + 31) / 32;
-    const int yp = blockIdx.x / xtiles;
-    const int xp0 = (blockIdx.x - yp * xtiles) * 32;
-    const int zp0 = blockIdx.y * 32;
+    const int yp = bx / xtiles;
+    const int xp0 = (bx - yp * xtiles) * 32;
+    const int zp0 = by * 32;
     const int tx = threadIdx.x, ty = threadIdx.y;
     {
         const int xp = xp0 + tx;
@@ -73,6 +73,13 @@ __global__ void build_volume_quads_kernel(const float* __restrict__ vol, int D, 
         if (xp <= W && zp <= D + 1)
             Q[((long long)yp * (W + 1) + xp) * (D + 2) + zp] = tile[tx][xl];
     }
+}
+
+// grid: x = ceil((W+1)/32) * (H+1), y = ceil((D+2)/32); block (32, 8)
+__global__ void build_volume_quads_kernel(const float* __restrict__ vol, int D, int H, int W,
+                                          float4* __restrict__ Q) {
+    __shared__ float4 tile[32][33];
+    quads_tile(vol, D, H, W, Q, blockIdx.x, blockIdx.y, tile);
 }
 
 int build_volume_quads(const float* vol, int D, int H, int W, float4* quads, cudaStream_t s) {
@@ -277,6 +284,10 @@ struct TileCoord {
     int a, tu, tv;
 };
 
+__host__ __device__ __forceinline__ long long fp_tiles_per_view_dev(int U, int V, int tu) {
+    return (long long)((U + tu - 1) / tu) * ((V + 256 / tu - 1) / (256 / tu));
+}
+
 __device__ __forceinline__ TileCoord tile_coord(const FpArgs& p, int tiles_u) {
     int b = blockIdx.x;
     TileCoord tc;
@@ -291,24 +302,22 @@ __device__ __forceinline__ TileCoord tile_coord(const FpArgs& p, int tiles_u) {
 // Forward kernel
 // ---------------------------------------------------------------------------
 
-// A CTA owns TU detector columns x (256/TU) rows of one view; warps run along
-// V (32 consecutive rows of one column).
-template <int TU, bool DIV, bool OFF>
-__global__ void __launch_bounds__(256) fp_forward_kernel(FpArgs p) {
+// Ray of this thread in a TU x (256/TU) tile: warps run along V (32
+// consecutive rows of one column).
+template <int TU>
+__device__ __forceinline__ void tile_ray(const TileCoord& tc, int& u, int& v) {
     constexpr int TV = 256 / TU;
     constexpr int WARPS_V = TV / 32;
     static_assert(TV % 32 == 0, "rows per CTA must be whole warps");
-    __shared__ ViewGeo s_view;
-    const int tiles_u = (p.U + TU - 1) / TU;
-    const TileCoord tc = tile_coord(p, tiles_u);
-    if (threadIdx.x == 0) load_view(p.g, tc.a, s_view);
-    __syncthreads();
-    const ViewGeo vg = s_view;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int u = tc.tu * TU + warp / WARPS_V;
-    const int v = tc.tv * TV + (warp % WARPS_V) * 32 + lane;
-    if (u >= p.U || v >= p.V) return;
+    u = tc.tu * TU + warp / WARPS_V;
+    v = tc.tv * TV + (warp % WARPS_V) * 32 + lane;
+}
 
+// Line integral of one ray, written to p.projections.
+template <bool DIV, bool OFF>
+__device__ __forceinline__ void forward_ray(const FpArgs& p, const ViewGeo& vg, int a, int u,
+                                            int v) {
     const RaySetup r = setup_ray(vg, u, v, p);
     float integral = 0.0f;
     if (r.ok && r.hit) {
@@ -316,7 +325,22 @@ __global__ void __launch_bounds__(256) fp_forward_kernel(FpArgs p) {
                                                  : march_sum<true, DIV, OFF>(r, vg, p);
         integral *= p.step_size;
     }
-    p.projections[((long long)tc.a * p.U + u) * p.V + v] = integral;
+    p.projections[((long long)a * p.U + u) * p.V + v] = integral;
+}
+
+// A CTA owns TU detector columns x (256/TU) rows of one view.
+template <int TU, bool DIV, bool OFF>
+__global__ void __launch_bounds__(256) fp_forward_kernel(FpArgs p) {
+    __shared__ ViewGeo s_view;
+    const int tiles_u = (p.U + TU - 1) / TU;
+    const TileCoord tc = tile_coord(p, tiles_u);
+    if (threadIdx.x == 0) load_view(p.g, tc.a, s_view);
+    __syncthreads();
+    const ViewGeo vg = s_view;
+    int u, v;
+    tile_ray<TU>(tc, u, v);
+    if (u >= p.U || v >= p.V) return;
+    forward_ray<DIV, OFF>(p, vg, tc.a, u, v);
 }
 
 // Sample counts under the same FP32 rule (measurement support).
@@ -405,26 +429,14 @@ __device__ __forceinline__ RayGrad march_grad(const RaySetup& r, const ViewGeo& 
     return rg;
 }
 
-template <int TU, bool GRADVOL>
-__global__ void __launch_bounds__(256) fp_backward_kernel(FpArgs p) {
-    constexpr int TV = 256 / TU;
-    constexpr int WARPS_V = TV / 32;
-    static_assert(TV % 32 == 0, "rows per CTA must be whole warps");
-    __shared__ ViewGeo s_view;
-    __shared__ double s_red[8][8];
-    const int tiles_u = (p.U + TU - 1) / TU;
-    const int tiles = tiles_u * ((p.V + TV - 1) / TV);
-    const TileCoord tc = tile_coord(p, tiles_u);
-    const int a = tc.a;
-    const int tile = tc.tv * tiles_u + tc.tu;
-    if (threadIdx.x == 0) load_view(p.g, a, s_view);
-    __syncthreads();
-    const ViewGeo vg = s_view;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int u = tc.tu * TU + warp / WARPS_V;
-    const int v = tc.tv * TV + (warp % WARPS_V) * 32 + lane;
-
-    float terms[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+// The eight per-view geometry terms of one ray (zero for rays outside the
+// detector or with a zero upstream gradient); with GRADVOL the ray's adjoint
+// samples are scattered into p.grad_pad.
+template <bool GRADVOL>
+__device__ __forceinline__ void backward_ray(const FpArgs& p, const ViewGeo& vg, int a, int u,
+                                             int v, float (&terms)[8]) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) terms[k] = 0.0f;
     const bool in_range = u < p.U && v < p.V;
     const float grad_out =
         in_range ? p.grad_projections[((long long)a * p.U + u) * p.V + v] : 0.0f;
@@ -479,7 +491,14 @@ __global__ void __launch_bounds__(256) fp_backward_kernel(FpArgs p) {
             terms[7] = goz;
         }
     }
-    // Fixed-order FP64 reduction of the eight terms over the CTA.
+}
+
+// Fixed-order FP64 sum of the eight terms over the 256 threads of the CTA,
+// written to partials[(a * tiles + tile) * 8 + k].
+__device__ __forceinline__ void reduce_terms_to_partials(const float (&terms)[8],
+                                                         double (&s_red)[8][8],
+                                                         double* __restrict__ out) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
         const double w = warp_sum((double)terms[k]);
@@ -490,8 +509,28 @@ __global__ void __launch_bounds__(256) fp_backward_kernel(FpArgs p) {
         double acc = 0.0;
 #pragma unroll
         for (int w = 0; w < 8; ++w) acc += s_red[w][threadIdx.x];
-        p.partials[((long long)a * tiles + tile) * 8 + threadIdx.x] = acc;
+        out[threadIdx.x] = acc;
     }
+}
+
+template <int TU, bool GRADVOL>
+__global__ void __launch_bounds__(256) fp_backward_kernel(FpArgs p) {
+    constexpr int TV = 256 / TU;
+    __shared__ ViewGeo s_view;
+    __shared__ double s_red[8][8];
+    const int tiles_u = (p.U + TU - 1) / TU;
+    const int tiles = tiles_u * ((p.V + TV - 1) / TV);
+    const TileCoord tc = tile_coord(p, tiles_u);
+    const int a = tc.a;
+    const int tile = tc.tv * tiles_u + tc.tu;
+    if (threadIdx.x == 0) load_view(p.g, a, s_view);
+    __syncthreads();
+    const ViewGeo vg = s_view;
+    int u, v;
+    tile_ray<TU>(tc, u, v);
+    float terms[8];
+    backward_ray<GRADVOL>(p, vg, a, u, v, terms);
+    reduce_terms_to_partials(terms, s_red, p.partials + ((long long)a * tiles + tile) * 8);
 }
 
 // Per-view sum of the CTA partials, warp k owning gradient k (fixed order).
@@ -507,34 +546,201 @@ __global__ void __launch_bounds__(256) reduce_view_partials_kernel(const double*
 
 // grad_volume[z,y,x] = sum of the padded cells that clamp onto (z,y,x); the
 // padded buffer is z-fastest: G[(yp*(W+2) + xp)*(D+2) + zp].
+__device__ __forceinline__ float fold_voxel(const float* __restrict__ gpad, int D, int H, int W,
+                                            long long i) {
+    const long long PZ = D + 2, PX = W + 2;
+    const int x = (int)(i % W);
+    const long long r = i / W;
+    const int y = (int)(r % H);
+    const int z = (int)(r / H);
+    int xs[3], ys[3], zs[3];
+    int nx = 0, ny = 0, nz = 0;
+    xs[nx++] = x + 1;
+    if (x == 0) xs[nx++] = 0;
+    if (x == W - 1) xs[nx++] = W + 1;
+    ys[ny++] = y + 1;
+    if (y == 0) ys[ny++] = 0;
+    if (y == H - 1) ys[ny++] = H + 1;
+    zs[nz++] = z + 1;
+    if (z == 0) zs[nz++] = 0;
+    if (z == D - 1) zs[nz++] = D + 1;
+    float acc = 0.0f;
+    for (int iy = 0; iy < ny; ++iy)
+        for (int ix = 0; ix < nx; ++ix)
+            for (int iz = 0; iz < nz; ++iz)
+                acc += gpad[((long long)ys[iy] * PX + xs[ix]) * PZ + zs[iz]];
+    return acc;
+}
+
 __global__ void fold_padded_gradient_kernel(const float* __restrict__ gpad, int D, int H, int W,
                                             float* __restrict__ grad) {
-    const long long PZ = D + 2, PX = W + 2;
     const long long total = (long long)D * H * W;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
-         i += (long long)gridDim.x * blockDim.x) {
-        const int x = (int)(i % W);
-        const long long r = i / W;
-        const int y = (int)(r % H);
-        const int z = (int)(r / H);
-        int xs[3], ys[3], zs[3];
-        int nx = 0, ny = 0, nz = 0;
-        xs[nx++] = x + 1;
-        if (x == 0) xs[nx++] = 0;
-        if (x == W - 1) xs[nx++] = W + 1;
-        ys[ny++] = y + 1;
-        if (y == 0) ys[ny++] = 0;
-        if (y == H - 1) ys[ny++] = H + 1;
-        zs[nz++] = z + 1;
-        if (z == 0) zs[nz++] = 0;
-        if (z == D - 1) zs[nz++] = D + 1;
-        float acc = 0.0f;
-        for (int iy = 0; iy < ny; ++iy)
-            for (int ix = 0; ix < nx; ++ix)
-                for (int iz = 0; iz < nz; ++iz)
-                    acc += gpad[((long long)ys[iy] * PX + xs[ix]) * PZ + zs[iz]];
-        grad[i] = acc;
+         i += (long long)gridDim.x * blockDim.x)
+        grad[i] = fold_voxel(gpad, D, H, W, i);
+}
+
+// ---------------------------------------------------------------------------
+// Batched launches: many instances of uneven D/H/W, A, U, V in one launch.
+//
+// A work item is one CTA tile of one instance, numbered instance by instance
+// and inside an instance in the single-instance order (u tile fastest, then
+// view, then row band).  The forward and backward kernels are persistent:
+// each CTA takes the next item from a global counter, loads the instance's
+// arguments and the view geometry into shared memory and runs the same ray
+// code as the single-instance kernels, with the tile shape and the division /
+// offset variants its instance was planned with.  Items are taken in order,
+// so the CTAs in flight work on one or two instances at a time (their
+// volumes stay in L2), and a small instance fills the SMs that a large one
+// leaves idle at its end.  The per-instance set-up kernels (quads, partial
+// reductions, gradient folds) are flattened over instances the same way.
+// ---------------------------------------------------------------------------
+
+// Largest i with starts[i] <= x (starts nondecreasing, starts[0] = 0).
+__device__ __forceinline__ int find_instance(const long long* __restrict__ starts, int n,
+                                             long long x) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(starts + mid) <= x) lo = mid;
+        else hi = mid - 1;
     }
+    return lo;
+}
+
+__device__ __forceinline__ TileCoord item_coord(long long local, int tiles_u, int A) {
+    TileCoord tc;
+    tc.tu = (int)(local % tiles_u);
+    const long long r = local / tiles_u;
+    tc.a = (int)(r % A);
+    tc.tv = (int)(r / A);
+    return tc;
+}
+
+__global__ void __launch_bounds__(256) batch_quads_kernel(BatchTables t) {
+    __shared__ float4 tile[32][33];
+    const int i = find_instance(t.quad_block, t.n, blockIdx.x);
+    const BatchInstance& in = t.inst[i];
+    const long long b = blockIdx.x - t.quad_block[i];
+    quads_tile(in.volume, in.p.D, in.p.H, in.p.W, const_cast<float4*>(in.p.quads),
+               (int)(b % in.quad_gx), (int)(b / in.quad_gx), tile);
+}
+
+// Thread 0 takes the next item of the queue and stages its instance and view.
+__device__ __forceinline__ bool next_item(const BatchTables& t, const long long* __restrict__ starts,
+                                          unsigned long long* counter, bool backward,
+                                          FpArgs& s_p, ViewGeo& s_view, TileCoord& s_tc,
+                                          int& s_tu, int& s_flags, int& s_tile,
+                                          long long& s_item) {
+    if (threadIdx.x == 0) {
+        const long long total = starts[t.n];
+        const long long item = (long long)atomicAdd(counter, 1ULL);
+        s_item = item;
+        if (item < total) {
+            const int i = find_instance(starts, t.n, item);
+            const BatchInstance& in = t.inst[i];
+            const int tu = backward ? in.tile_bwd : in.tile_fwd;
+            const int tiles_u = (in.p.U + tu - 1) / tu;
+            const TileCoord tc = item_coord(item - starts[i], tiles_u, in.p.A);
+            s_p = in.p;
+            s_tu = tu;
+            s_flags = in.flags;
+            s_tc = tc;
+            s_tile = tc.tv * tiles_u + tc.tu;
+            load_view(in.p.g, tc.a, s_view);
+        }
+    }
+    __syncthreads();
+    return s_item < starts[t.n];
+}
+
+template <int TU>
+__device__ __forceinline__ void forward_item(const FpArgs& p, const ViewGeo& vg,
+                                             const TileCoord& tc, int flags) {
+    int u, v;
+    tile_ray<TU>(tc, u, v);
+    if (u >= p.U || v >= p.V) return;
+    switch (flags & (kBatchDiv | kBatchOff)) {
+        case 0: forward_ray<false, false>(p, vg, tc.a, u, v); break;
+        case kBatchOff: forward_ray<false, true>(p, vg, tc.a, u, v); break;
+        case kBatchDiv: forward_ray<true, false>(p, vg, tc.a, u, v); break;
+        default: forward_ray<true, true>(p, vg, tc.a, u, v); break;
+    }
+}
+
+__global__ void __launch_bounds__(256, 6) batch_forward_kernel(BatchTables t) {
+    __shared__ FpArgs s_p;
+    __shared__ ViewGeo s_view;
+    __shared__ TileCoord s_tc;
+    __shared__ int s_tu, s_flags, s_tile;
+    __shared__ long long s_item;
+    while (next_item(t, t.item_fwd, t.counters, false, s_p, s_view, s_tc, s_tu, s_flags, s_tile,
+                     s_item)) {
+        const FpArgs p = s_p;
+        const ViewGeo vg = s_view;
+        const TileCoord tc = s_tc;
+        switch (s_tu) {
+            case 8: forward_item<8>(p, vg, tc, s_flags); break;
+            case 4: forward_item<4>(p, vg, tc, s_flags); break;
+            default: forward_item<2>(p, vg, tc, s_flags); break;
+        }
+        __syncthreads();  // the staged item is read by every thread before the next one
+    }
+}
+
+template <int TU>
+__device__ __forceinline__ void backward_item(const FpArgs& p, const ViewGeo& vg,
+                                              const TileCoord& tc, float (&terms)[8]) {
+    int u, v;
+    tile_ray<TU>(tc, u, v);
+    if (p.grad_pad) backward_ray<true>(p, vg, tc.a, u, v, terms);
+    else backward_ray<false>(p, vg, tc.a, u, v, terms);
+}
+
+__global__ void __launch_bounds__(256) batch_backward_kernel(BatchTables t) {
+    __shared__ FpArgs s_p;
+    __shared__ ViewGeo s_view;
+    __shared__ TileCoord s_tc;
+    __shared__ int s_tu, s_flags, s_tile;
+    __shared__ long long s_item;
+    __shared__ double s_red[8][8];
+    while (next_item(t, t.item_bwd, t.counters + 1, true, s_p, s_view, s_tc, s_tu, s_flags,
+                     s_tile, s_item)) {
+        const FpArgs p = s_p;
+        const ViewGeo vg = s_view;
+        const TileCoord tc = s_tc;
+        float terms[8];
+        if (s_tu == 8) backward_item<8>(p, vg, tc, terms);
+        else backward_item<4>(p, vg, tc, terms);
+        const long long tiles = fp_tiles_per_view_dev(p.U, p.V, s_tu);
+        reduce_terms_to_partials(terms, s_red, p.partials + ((long long)tc.a * tiles + s_tile) * 8);
+        __syncthreads();
+    }
+}
+
+// One block per view of every instance (the order of reduce_view_partials_kernel).
+__global__ void __launch_bounds__(256) batch_reduce_kernel(BatchTables t) {
+    const int i = find_instance(t.view, t.n, blockIdx.x);
+    const BatchInstance& in = t.inst[i];
+    const int a = (int)(blockIdx.x - t.view[i]);
+    const int k = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long long tiles = in.tiles_bwd;
+    const double* __restrict__ partials = in.p.partials;
+    double acc = 0.0;
+    for (long long j = lane; j < tiles; j += 32) acc += partials[((long long)a * tiles + j) * 8 + k];
+    acc = warp_sum(acc);
+    if (lane == 0) in.gout.g[k][a] = (float)acc;
+}
+
+// kFoldChunk voxels of one instance per block.
+__global__ void __launch_bounds__(256) batch_fold_kernel(BatchTables t) {
+    const int i = find_instance(t.fold_block, t.n, blockIdx.x);
+    const BatchInstance& in = t.inst[i];
+    const long long total = (long long)in.p.D * in.p.H * in.p.W;
+    const long long v0 = (blockIdx.x - t.fold_block[i]) * (long long)kFoldChunk;
+    const long long v1 = v0 + kFoldChunk < total ? v0 + kFoldChunk : total;
+    for (long long v = v0 + threadIdx.x; v < v1; v += blockDim.x)
+        in.grad_volume[v] = fold_voxel(in.p.grad_pad, in.p.D, in.p.H, in.p.W, v);
 }
 
 // ---------------------------------------------------------------------------
@@ -596,6 +802,7 @@ int fp_launch_forward(const FpArgs& p, const FpTile& tile, cudaStream_t s) {
     switch (tile.tu) {
         case 8: return launch_forward_tu<8>(p, div, s);
         case 4: return launch_forward_tu<4>(p, div, s);
+        case 2: return launch_forward_tu<2>(p, div, s);
         default:
             set_error("unsupported forward-projector tile");
             return DGC_ERR_INVALID_ARGUMENT;
@@ -606,6 +813,7 @@ int fp_launch_backward(const FpArgs& p, const FpTile& tile, bool gradvol, cudaSt
     switch (tile.tu) {
         case 8: return launch_backward_tu<8>(p, gradvol, s);
         case 4: return launch_backward_tu<4>(p, gradvol, s);
+        case 2: return launch_backward_tu<2>(p, gradvol, s);
         default:
             set_error("unsupported backward tile");
             return DGC_ERR_INVALID_ARGUMENT;
@@ -634,6 +842,56 @@ int fp_fold_gradient(const float* gpad, int D, int H, int W, float* grad, cudaSt
     const int blocks = (int)std::min<long long>((total + 255) / 256, 148LL * 16);
     fold_padded_gradient_kernel<<<blocks, 256, 0, s>>>(gpad, D, H, W, grad);
     DGC_LAUNCH_CHECK("fold_padded_gradient");
+    return DGC_OK;
+}
+
+// ------------------------------------------------------------ batched launches
+
+int batch_launch_quads(const BatchTables& t, long long blocks, cudaStream_t s) {
+    DGC_TRACE("batch_quads", s);
+    batch_quads_kernel<<<(unsigned)blocks, dim3(32, 8), 0, s>>>(t);
+    DGC_LAUNCH_CHECK("batch_quads");
+    return DGC_OK;
+}
+
+int batch_launch_forward(const BatchTables& t, int grid, cudaStream_t s) {
+    DGC_TRACE("batch_forward_kernel", s);
+    DGC_CUDA(cudaMemsetAsync(t.counters, 0, sizeof(unsigned long long), s));
+    batch_forward_kernel<<<grid, 256, 0, s>>>(t);
+    DGC_LAUNCH_CHECK("batch_forward_kernel");
+    return DGC_OK;
+}
+
+int batch_launch_backward(const BatchTables& t, int grid, long long views, long long fold_blocks,
+                          cudaStream_t s) {
+    {
+        DGC_TRACE("batch_backward_kernel", s);
+        DGC_CUDA(cudaMemsetAsync(t.counters + 1, 0, sizeof(unsigned long long), s));
+        batch_backward_kernel<<<grid, 256, 0, s>>>(t);
+        DGC_LAUNCH_CHECK("batch_backward_kernel");
+    }
+    {
+        DGC_TRACE("batch_reduce", s);
+        batch_reduce_kernel<<<(unsigned)views, 256, 0, s>>>(t);
+        DGC_LAUNCH_CHECK("batch_reduce");
+    }
+    if (fold_blocks > 0) {
+        DGC_TRACE("batch_fold", s);
+        batch_fold_kernel<<<(unsigned)fold_blocks, 256, 0, s>>>(t);
+        DGC_LAUNCH_CHECK("batch_fold");
+    }
+    return DGC_OK;
+}
+
+int batch_persistent_grid(bool backward, int* grid) {
+    int dev = 0, sms = 0, per_sm = 0;
+    DGC_CUDA(cudaGetDevice(&dev));
+    DGC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    if (backward)
+        DGC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_backward_kernel, 256, 0));
+    else
+        DGC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_forward_kernel, 256, 0));
+    *grid = std::max(1, per_sm) * sms;
     return DGC_OK;
 }
 

@@ -29,6 +29,43 @@ struct FpTile {
     int wu;
 };
 
+// One instance of a batched launch (an entry of the device-resident table).
+enum : int { kBatchDiv = 1, kBatchOff = 2 };
+constexpr int kFoldChunk = 2048;
+
+struct BatchInstance {
+    FpArgs p;              // arguments with this instance's quads, outputs and workspace slices
+    const float* volume;   // [D][H][W]
+    float* grad_volume;    // [D][H][W]; null: no volume gradient
+    GeometryGrad gout;     // eight [A] outputs
+    int tile_fwd, tile_bwd;  // columns per CTA tile (forward 8/4/2, backward 8/4)
+    int flags;             // kBatchDiv (non power-of-two voxel) | kBatchOff (non-zero ROI offset)
+    int quad_gx;           // blocks along x of the quads build
+    long long tiles_bwd;   // backward tiles per view
+};
+
+// Device pointers of a prepared batch; the prefix arrays have n+1 entries.
+struct BatchTables {
+    const BatchInstance* inst;
+    int n;
+    const long long* item_fwd;     // forward work items
+    const long long* item_bwd;     // backward work items
+    const long long* quad_block;   // quads-build blocks
+    const long long* view;         // views
+    const long long* fold_block;   // gradient-fold blocks
+    unsigned long long* counters;  // [0] forward queue, [1] backward queue
+};
+
+int batch_launch_quads(const BatchTables& t, long long blocks, cudaStream_t s);
+int batch_launch_forward(const BatchTables& t, int grid, cudaStream_t s);
+int batch_launch_backward(const BatchTables& t, int grid, long long views, long long fold_blocks,
+                          cudaStream_t s);
+int batch_persistent_grid(bool backward, int* grid);
+
+// Argument checks of dgc_project (messages as the reference's host wrapper).
+int fp_check_args(int D, int H, int W, int A, int U, int V, float pixel_size, float step_size,
+                  float voxel_size, const Geometry& g);
+
 void fp_fill_layout(FpArgs& p);
 long long fp_tiles_per_view(int U, int V, int tu);
 int build_volume_quads(const float* vol, int D, int H, int W, float4* quads, cudaStream_t s);

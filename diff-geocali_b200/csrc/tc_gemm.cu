@@ -152,7 +152,12 @@ __global__ void __launch_bounds__(128) tc_gemm_kernel(GemmArgs p) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int m0 = blockIdx.y * kBM, n0 = blockIdx.x * BN;
     const uint32_t sbase = smem_u32(smem);
-    const int nk = (p.K + kBK - 1) / kBK;
+    // split-K: this CTA reduces K tiles [kt0, kt0 + nk)
+    const int nk_total = (p.K + kBK - 1) / kBK;
+    const bool split = p.k_tiles_per_split > 0;
+    const int kt0 = split ? blockIdx.z * p.k_tiles_per_split : 0;
+    const int nk = split ? max(0, min(p.k_tiles_per_split, nk_total - kt0)) : nk_total;
+    const int k_base = kt0 * kBK;
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
@@ -175,8 +180,8 @@ __global__ void __launch_bounds__(128) tc_gemm_kernel(GemmArgs p) {
     for (int s = 0; s < kStages - 1; ++s) {
         if (s < nk) {
             const uint32_t sa = sbase + s * kStageBytes;
-            stage_tile<kBM>(sa, p.A, p.lda, m0, p.M, s * kBK, p.K);
-            stage_tile<BN>(sa + kABytes, p.B, p.ldb, n0, p.N, s * kBK, p.K);
+            stage_tile<kBM>(sa, p.A, p.lda, m0, p.M, k_base + s * kBK, p.K);
+            stage_tile<BN>(sa + kABytes, p.B, p.ldb, n0, p.N, k_base + s * kBK, p.K);
         }
         cp_async_commit();
     }
@@ -208,8 +213,8 @@ __global__ void __launch_bounds__(128) tc_gemm_kernel(GemmArgs p) {
             if (kt >= 1) ok = mbar_wait(smem_u32(&bars[sn]), ((kt - 1) / kStages) & 1);
             if (ok) {
                 const uint32_t sa = sbase + sn * kStageBytes;
-                stage_tile<kBM>(sa, p.A, p.lda, m0, p.M, kn * kBK, p.K);
-                stage_tile<BN>(sa + kABytes, p.B, p.ldb, n0, p.N, kn * kBK, p.K);
+                stage_tile<kBM>(sa, p.A, p.lda, m0, p.M, k_base + kn * kBK, p.K);
+                stage_tile<BN>(sa + kABytes, p.B, p.ldb, n0, p.N, k_base + kn * kBK, p.K);
             }
         }
         cp_async_commit();
@@ -236,9 +241,14 @@ __global__ void __launch_bounds__(128) tc_gemm_kernel(GemmArgs p) {
                     if (col >= p.N) break;
                     float x = (nk > 0) ? v[j] : 0.0f;
                     x *= p.alpha;
+                    const long long off = (long long)row * p.ldc + col;
+                    if (split) {  // partial sum of a K range; bias from split 0
+                        if (p.bias && blockIdx.z == 0) x += p.bias[col];
+                        atomicAdd(static_cast<float*>(p.C) + off, x);
+                        continue;
+                    }
                     if (p.bias) x += p.bias[col];
                     if (p.relu) x = fmaxf(x, 0.0f);
-                    const long long off = (long long)row * p.ldc + col;
                     if (p.c_bf16) {
                         __nv_bfloat16* C = static_cast<__nv_bfloat16*>(p.C);
                         C[off] = __float2bfloat16(x);
@@ -268,7 +278,9 @@ int launch_gemm(const GemmArgs& p, cudaStream_t s) {
                                       smem));
         configured = true;
     }
-    const dim3 grid(ceil_div(p.N, BN), ceil_div(p.M, kBM));
+    const int splits = p.k_tiles_per_split > 0
+                           ? ceil_div(ceil_div(p.K, kBK), p.k_tiles_per_split) : 1;
+    const dim3 grid(ceil_div(p.N, BN), ceil_div(p.M, kBM), splits);
     tc_gemm_kernel<BN><<<grid, 128, smem, s>>>(p);
     DGC_LAUNCH_CHECK("tc_gemm_kernel");
     return DGC_OK;

@@ -18,6 +18,7 @@ struct GemmArgs {
     int accumulate;  // fp32 only: C += result
     float alpha;     // result = alpha * A B^T (+ bias)
     int* error;      // device word set to 1 when a pipeline wait times out
+    int k_tiles_per_split;  // > 0: split K over gridDim.z CTAs, fp32 atomic epilogue
 };
 
 int tc_gemm(const GemmArgs& p, cudaStream_t s);

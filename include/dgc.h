@@ -208,6 +208,83 @@ int dgc_gemm_bf16(const void* A, const void* B, void* C, const float* bias, int 
                   int* error_flag, void* stream);
 
 /* ---------------------------------------------------------------------- */
+/* Batched forward projection + backward over uneven instances             */
+/* ---------------------------------------------------------------------- */
+
+/* One projection problem of a batch: the arguments of dgc_project and
+ * dgc_project_backward.  grad_projections may alias projections (the
+ * gradient of 0.5*|p|^2).  grad_volume NULL: no volume gradient.
+ * grad_geometry: [8][A] (angles, sid, sod, det_u0, det_v0, src_x, src_y,
+ * src_z).  tile_forward in {0, 8, 4, 2}, tile_backward in {0, 8, 4}: detector
+ * columns per 256-ray CTA tile (0 = 8), normally chosen by the autotuner. */
+typedef struct dgc_fp_instance {
+    const float* volume;
+    int D, H, W;
+    const float *angles, *sid, *sod, *det_u0, *det_v0, *src_x, *src_y, *src_z;
+    int A;
+    float pixel_size;
+    int U, V;
+    float step_size, voxel_size, off_x, off_y, off_z;
+    float* projections;
+    const float* grad_projections;
+    float* grad_volume;
+    float* grad_geometry;
+    int tile_forward, tile_backward;
+} dgc_fp_instance;
+
+/* A prepared batch: host-side, caller-owned, copyable; it refers to the
+ * device tables that dgc_batch_prepare wrote into the workspace. */
+typedef struct dgc_batch_plan {
+    void* workspace;
+    int n;
+    int grid_forward, grid_backward; /* persistent CTAs */
+    int has_grad_volume;
+    int backward_ready;              /* every instance has grad_projections and grad_geometry */
+    long long items_forward, items_backward, quad_blocks, views, fold_blocks;
+    long long rays;                  /* sum of A*U*V */
+    size_t grad_pad_offset, grad_pad_bytes;
+    size_t tables_bytes;
+} dgc_batch_plan;
+
+/* Workspace of a batch: device tables plus, per instance, the quad-packed
+ * volume, the padded volume gradient (if requested) and the per-tile FP64
+ * partial sums.  No counterpart in the reference (which runs one problem per
+ * call). */
+size_t dgc_batch_workspace_bytes(const dgc_fp_instance* instances, int n);
+
+/* Validates every instance (the checks of dgc_project, with the instance
+ * index in the message), lays out the workspace and copies the device
+ * tables into it on `stream` from host memory.  Call it outside stream
+ * capture; afterwards dgc_batch_project / dgc_batch_project_backward may be
+ * captured into a CUDA graph and replayed while the instances' buffers stay
+ * valid.  No counterpart in the reference. */
+int dgc_batch_prepare(const dgc_fp_instance* instances, int n, void* workspace,
+                      size_t workspace_bytes, dgc_batch_plan* plan, void* stream);
+
+/* Forward projections of every instance: one launch builds all quad-packed
+ * volumes, one persistent launch marches every ray of every instance from an
+ * (instance, view, ray tile) work queue.  Results equal dgc_project's
+ * bitwise.  No counterpart in the reference. */
+int dgc_batch_project(const dgc_batch_plan* plan, void* stream);
+
+/* Backward of every instance (dgc_project_backward's outputs: volume and
+ * geometry gradients).  rebuild_quads = 0 reuses the quad-packed volumes of
+ * the last dgc_batch_project on this plan (the volumes unchanged since).
+ * No counterpart in the reference. */
+int dgc_batch_project_backward(const dgc_batch_plan* plan, int rebuild_quads, void* stream);
+
+/* im2col of an NHWC bf16 image batch x [B,H,W,C] for a kh x kw convolution
+ * (stride, zero padding pad): col [B*Ho*Wo][Kp] with column (ky*kw+kx)*C + c,
+ * zero beyond kh*kw*C.  No counterpart in the reference. */
+int dgc_im2col_nhwc_bf16(const void* x, int B, int H, int W, int C, int kh, int kw, int stride,
+                         int pad, void* col, int Kp, void* stream);
+
+/* Adjoint of dgc_im2col_nhwc_bf16 in fp32: dx [B,H,W,C] = col2im(col).
+ * No counterpart in the reference. */
+int dgc_col2im_nhwc_f32(const float* col, int B, int H, int W, int C, int kh, int kw, int stride,
+                        int pad, int Kp, float* dx, void* stream);
+
+/* ---------------------------------------------------------------------- */
 /* Kernel timing (no counterpart in the reference; measurement support)     */
 /* ---------------------------------------------------------------------- */
 

@@ -1,0 +1,114 @@
+"""Host side of the batched projection without a GPU: the ctypes mirror of
+``dgc_fp_instance`` / ``dgc_batch_plan`` matches the library (the workspace
+query reads the fields it needs), argument checks name the failing instance
+before any CUDA call, and the autotuner's buckets and JSON cache."""
+
+import ctypes
+import math
+from types import SimpleNamespace
+
+import pytest
+
+
+def _instances(specs, grad_volume=True):
+    from cbct_backprojector import _native
+
+    arr = (_native.FpInstance * len(specs))()
+    for inst, (D, H, W, A, U, V, tb) in zip(arr, specs):
+        inst.D, inst.H, inst.W, inst.A, inst.U, inst.V = D, H, W, A, U, V
+        inst.pixel_size = inst.step_size = inst.voxel_size = 1.0
+        for name in ("volume", "angles", "sid", "sod", "det_u0", "det_v0", "src_x", "src_y",
+                     "src_z", "projections", "grad_projections", "grad_geometry"):
+            setattr(inst, name, 256)
+        inst.grad_volume = 256 if grad_volume else None
+        inst.tile_backward = tb
+    return arr
+
+
+def _align(n):
+    return (n + 255) // 256 * 256
+
+
+def test_workspace_bytes_follow_the_layout():
+    from cbct_backprojector import _native
+
+    lib = _native.lib()
+    specs = [(24, 20, 16, 12, 40, 36, 8), (9, 31, 27, 7, 33, 65, 4), (5, 7, 6, 33, 12, 9, 0)]
+    for gv in (True, False):
+        got = lib.dgc_batch_workspace_bytes(_instances(specs, gv), len(specs))
+        per = 0
+        for D, H, W, A, U, V, tb in specs:
+            tu = tb or 8
+            tiles = math.ceil(U / tu) * math.ceil(V / (256 // tu))
+            per += _align(16 * (D + 2) * (H + 1) * (W + 1)) + _align(8 * 8 * A * tiles)
+            if gv:
+                per += _align(4 * (D + 2) * (H + 2) * (W + 2))
+        n = len(specs)
+        table = got - per - 5 * _align(8 * (n + 1)) - _align(16)
+        # the n device-side instance records precede the buffers
+        assert table % 256 == 0 and 64 * n <= table <= 512 * n
+    assert lib.dgc_batch_workspace_bytes(None, 0) == 0
+    bad = _instances([(0, 4, 4, 1, 4, 4, 0)])
+    assert lib.dgc_batch_workspace_bytes(bad, 1) == 0
+
+
+def test_prepare_rejects_bad_instances():
+    from cbct_backprojector import _native
+
+    lib = _native.lib()
+    plan = _native.BatchPlan()
+    arr = _instances([(8, 8, 8, 4, 16, 16, 0), (8, 8, 8, 4, 0, 16, 0)])
+    rc = lib.dgc_batch_prepare(arr, 2, None, 0, ctypes.byref(plan), None)
+    assert rc == 1 and lib.dgc_last_error() == b"instance 1: U and V must be positive"
+    arr = _instances([(8, 8, 8, 4, 16, 16, 0)])
+    arr[0].tile_forward = 16
+    rc = lib.dgc_batch_prepare(arr, 1, None, 0, ctypes.byref(plan), None)
+    assert rc == 1 and b"tile_forward" in lib.dgc_last_error()
+    arr[0].tile_forward = 2
+    arr[0].tile_backward = 2
+    rc = lib.dgc_batch_prepare(arr, 1, None, 0, ctypes.byref(plan), None)
+    assert rc == 1 and b"tile_backward" in lib.dgc_last_error()
+    arr[0].tile_backward = 4
+    rc = lib.dgc_batch_prepare(arr, 1, None, 0, ctypes.byref(plan), None)
+    assert rc == 3 and b"workspace" in lib.dgc_last_error()
+    rc = lib.dgc_batch_prepare(arr, 0, None, 0, ctypes.byref(plan), None)
+    assert rc == 1
+    rc = lib.dgc_batch_project(ctypes.byref(_native.BatchPlan()), None)
+    assert rc == 1 and b"prepared" in lib.dgc_last_error()
+
+
+def _problem(shape, A, U, V, voxel=1.0):
+    return SimpleNamespace(volume=SimpleNamespace(shape=shape),
+                           geometry=[SimpleNamespace(numel=lambda A=A: A)] * 8, U=U, V=V,
+                           voxel_size=voxel, tiles=(0, 0))
+
+
+def test_buckets():
+    from cbct_backprojector.autotune import bucket
+
+    a = bucket(_problem((256, 256, 256), 360, 384, 384))
+    assert a == "vol2^24-U384-V384-mul"
+    assert bucket(_problem((250, 256, 256), 720, 380, 300)) == "vol2^24-U384-V384-mul"
+    assert bucket(_problem((256, 256, 256), 360, 384, 384, voxel=0.75)).endswith("-div")
+    assert bucket(_problem((128, 128, 128), 90, 512, 512)) == "vol2^21-U512-V512-mul"
+
+
+def test_autotuner_picks_fastest_and_caches(tmp_path):
+    from cbct_backprojector.autotune import Autotuner
+
+    calls = []
+
+    def fake(pr, direction, tile):
+        calls.append((direction, tile))
+        best = 4 if direction == "forward" else 8
+        return 1.0 if tile == best else 2.0 + tile
+
+    path = tmp_path / "t.json"
+    tuner = Autotuner(cache_path=path, measure=fake)
+    probs = [_problem((64, 64, 64), 90, 256, 256), _problem((64, 64, 64), 90, 256, 256),
+             _problem((96, 96, 64), 180, 384, 256)]
+    assert tuner.choose(probs) == [(4, 8)] * 3
+    assert len(tuner.measured) == 2 and len(calls) == 2 * (3 + 2)
+    again = Autotuner(cache_path=path, measure=lambda *a: pytest.fail("cache miss"))
+    assert again.choose(probs) == [(4, 8)] * 3
+    assert probs[2].tiles == (4, 8)

@@ -27,8 +27,10 @@ def run(A, B, C, bias=None, relu=False, accumulate=False, alpha=1.0):
 
 
 @pytest.mark.parametrize("M,N,K", [(128, 128, 64), (128, 64, 16), (300, 200, 72), (1000, 64, 256),
-                                   (2048, 256, 2304), (7, 24, 8), (513, 136, 136)])
+                                   (2048, 256, 2304), (7, 24, 8), (513, 136, 136),
+                                   (64, 200, 8192), (32, 96, 4104)])
 def test_gemm_matches_fp32(M, N, K):
+    """The last two shapes take the split-K path (few output tiles, long K)."""
     g = torch.Generator(device="cuda").manual_seed(M * 7 + N)
     A = torch.randn(M, K, device="cuda", generator=g).to(torch.bfloat16)
     B = torch.randn(N, K, device="cuda", generator=g).to(torch.bfloat16)
@@ -57,3 +59,22 @@ def test_gemm_epilogues():
     Bw = torch.randn(N, 48, device="cuda", generator=g).to(torch.bfloat16)[:, :K]
     out2 = run(Aw, Bw, torch.empty(M, N, device="cuda"))
     torch.testing.assert_close(out2, Aw.float() @ Bw.float().t(), rtol=1e-5, atol=1e-4)
+
+
+def test_split_k_into_column_slice():
+    """Split-K zeroes and sums only the M x N window of a strided C: the
+    columns of the wider array around it keep their values."""
+    g = torch.Generator(device="cuda").manual_seed(5)
+    M, N, K = 48, 40, 6144
+    A = torch.randn(M, K, device="cuda", generator=g).to(torch.bfloat16)
+    B = torch.randn(N, K, device="cuda", generator=g).to(torch.bfloat16)
+    wide = torch.full((M, N + 24), 7.0, device="cuda")
+    run(A, B, wide[:, 8:8 + N])
+    want = A.float() @ B.float().t()
+    scale = (A.float().abs() @ B.float().abs().t()).clamp_min(1.0)
+    assert ((wide[:, 8:8 + N] - want).abs() / scale).max().item() < 1e-5
+    assert torch.all(wide[:, :8] == 7.0) and torch.all(wide[:, 8 + N:] == 7.0)
+    # accumulate=True adds the split partial sums to what C holds
+    acc = wide[:, 8:8 + N].clone()
+    run(A, B, acc, accumulate=True, alpha=-1.0)
+    assert (acc.abs() / scale).max().item() < 1e-5
