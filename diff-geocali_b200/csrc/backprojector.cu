@@ -281,10 +281,10 @@ __global__ void __launch_bounds__(256) bp_backward_kernel(BpArgs p) {
                         s_int = fmaf(g, interp, s_int);
                         const float gb = g * w;
                         const float g0 = gb * (1.0f - fu), g1 = gb * fu;
-                        atomicAdd(gp + vi, g0 * (1.0f - fv));
-                        atomicAdd(gp + p.V + vi, g1 * (1.0f - fv));
-                        atomicAdd(gp + vi + 1, g0 * fv);
-                        atomicAdd(gp + p.V + vi + 1, g1 * fv);
+                        red_add_global(gp + vi, g0 * (1.0f - fv));
+                        red_add_global(gp + p.V + vi, g1 * (1.0f - fv));
+                        red_add_global(gp + vi + 1, g0 * fv);
+                        red_add_global(gp + p.V + vi + 1, g1 * fv);
                     }
                 }
                 s_iu = warp_sum(s_iu);

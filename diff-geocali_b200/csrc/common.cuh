@@ -140,6 +140,16 @@ __device__ __forceinline__ f32x2 fma2(f32x2 a, f32x2 b, f32x2 c) {
 // Per-lane lerp of two packed pairs with one weight: a + w*(b-a).
 __device__ __forceinline__ f32x2 lerp2(f32x2 a, f32x2 b, f32x2 w) { return fma2(w, sub2(b, a), a); }
 
+// Float add to global memory whose result is not used (red.global.add.f32,
+// round-to-nearest like atomicAdd).  The asm has no memory clobber, so the
+// compiler need not assume that the add changed other memory: values staged
+// in shared memory (view geometry, batched instance arguments) stay in
+// registers across a scatter loop instead of being re-read after every add.
+// p must point to global memory.
+__device__ __forceinline__ void red_add_global(float* p, float v) {
+    asm volatile("red.global.add.f32 [%0], %1;" ::"l"(__cvta_generic_to_global(p)), "f"(v));
+}
+
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);

@@ -416,14 +416,14 @@ __device__ __forceinline__ RayGrad march_grad(const RaySetup& r, const ViewGeo& 
             const float w00 = gy0 * mx, w01 = gy0 * c.fx, w10 = gy1 * mx, w11 = gy1 * c.fx;
             float* g0 = p.grad_pad + (c.bz + c.bx * p.gz_x + c.by * p.gz_y + p.gz_bias);
             float* g1 = g0 + p.gz_y;
-            atomicAdd(g0, w00 * mz);
-            atomicAdd(g0 + 1, w00 * c.fz);
-            atomicAdd(g0 + p.gz_x, w01 * mz);
-            atomicAdd(g0 + p.gz_x + 1, w01 * c.fz);
-            atomicAdd(g1, w10 * mz);
-            atomicAdd(g1 + 1, w10 * c.fz);
-            atomicAdd(g1 + p.gz_x, w11 * mz);
-            atomicAdd(g1 + p.gz_x + 1, w11 * c.fz);
+            red_add_global(g0, w00 * mz);
+            red_add_global(g0 + 1, w00 * c.fz);
+            red_add_global(g0 + p.gz_x, w01 * mz);
+            red_add_global(g0 + p.gz_x + 1, w01 * c.fz);
+            red_add_global(g1, w10 * mz);
+            red_add_global(g1 + 1, w10 * c.fz);
+            red_add_global(g1 + p.gz_x, w11 * mz);
+            red_add_global(g1 + p.gz_x + 1, w11 * c.fz);
         }
     }
     return rg;
