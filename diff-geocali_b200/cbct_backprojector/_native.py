@@ -56,6 +56,9 @@ SIGNATURES = {
     "dgc_project_backward_workspace_bytes": (_S, [_I] * 7),
     "dgc_project_backward": (_I, [_P, _P, _I, _I, _I, *_GEOM, _I, _F, _I, _I, _F, _F, _I, _F, _F, _F,
                                   *([_P] * 9), _P, _S, _P]),
+    "dgc_project_mse_grad_workspace_bytes": (_S, [_I] * 6),
+    "dgc_project_mse_grad": (_I, [_P, _I, _I, _I, *_GEOM, _I, _F, _I, _I, _F, _F, _F, _F, _F, _P, _P,
+                                  _F, _P, _P, *([_P] * 8), _P, _S, _P]),
     "dgc_backproject_workspace_bytes": (_S, [_I] * 6),
     "dgc_backproject": (_I, [_P, _I, _I, _I, *_GEOM, _F, _I, _I, _I, _F, _F, _F, _F, _P, _P, _S, _P]),
     "dgc_backproject_backward_workspace_bytes": (_S, [_I] * 6),

@@ -122,6 +122,43 @@ def fp_backward(grad_projection, volume, angles, sid, sod, det_u0_arr, det_v0_ar
     return [grad_volume, *grads]
 
 
+def fp_mse_grad(volume, geometry, pixel_size, U, V, step_size, voxel_size, measured, mask=None,
+                scale=1.0, offset=(0.0, 0.0, 0.0), return_projection=False):
+    """One fused calibration step: ``loss = scale * sum(mask * (p - measured)^2)``
+    with ``p = project(volume, geometry)`` and the eight [A] geometry gradients
+    of that loss, from one ray march (no volume gradient).  Returns
+    ``(loss (0-d float64 tensor), [8 gradients], projection or None)``."""
+    pixel_size, step_size, voxel_size = float(pixel_size), float(step_size), float(voxel_size)
+    U, V = int(U), int(V)
+    _require(volume.dim() == 3, "volume must have shape [D,H,W]")
+    A = geometry[0].numel()
+    _require(A > 0, "angles must contain at least one view")
+    _fp_check_geometry(volume, geometry, A)
+    vol = volume.contiguous()
+    geom = [t.contiguous() for t in geometry]
+    dev = vol.device
+    _require(measured.is_cuda and measured.dtype == torch.float32 and measured.device == dev and
+             tuple(measured.shape) == (A, U, V), "measured must be float32 [A,U,V] on the volume's device")
+    meas = measured.contiguous()
+    if mask is not None:
+        _require(mask.is_cuda and mask.dtype == torch.float32 and mask.device == dev and
+                 tuple(mask.shape) == (A, U, V), "mask must be float32 [A,U,V] on the volume's device")
+        mask = mask.contiguous()
+    D, H, W = vol.shape
+    loss = torch.empty((), dtype=torch.float64, device=dev)
+    grads = [torch.empty_like(g) for g in geom]
+    proj = torch.empty((A, U, V), dtype=torch.float32, device=dev) if return_projection else None
+    lib = _native.lib()
+    with torch.cuda.device(dev):
+        ws = _workspace(lib.dgc_project_mse_grad_workspace_bytes(D, H, W, A, U, V), dev)
+        _native.check(lib.dgc_project_mse_grad(
+            vol.data_ptr(), D, H, W, *[g.data_ptr() for g in geom], A, pixel_size, U, V,
+            step_size, voxel_size, *(float(x) for x in offset), meas.data_ptr(), _p(mask),
+            float(scale), _p(proj), loss.data_ptr(), *[g.data_ptr() for g in grads], _p(ws),
+            0 if ws is None else ws.numel(), _stream(dev)))
+    return loss, grads, proj
+
+
 # ---------------------------------------------------------------- backprojector
 
 

@@ -18,7 +18,10 @@ the plain calibration loop on top of this build's operators:
   directions of the per-view parameters (angle vs det_u0 vs src_x, sid vs sod);
 * ``calibrate``: Adam on per-view offsets ``delta`` of the eight geometry
   tensors, minimising ``MSE(project(volume, nominal + delta), measured)``,
-  optionally from a warm start that is rejected if it raises that loss.
+  optionally from a warm start that is rejected if it raises that loss.  By
+  default each step is one fused kernel pass (``dgc_project_mse_grad``:
+  projection, masked squared error and the eight geometry gradients from one
+  ray march) instead of ``project`` + autograd backward (two marches).
 
 All arithmetic on the device; the projector and its geometry gradients run in
 ``libdgc.so``.
@@ -32,6 +35,7 @@ from dataclasses import dataclass, field
 
 import torch
 
+from . import _ops
 from .source_only_forward_projector import project
 
 GEOMETRY_NAMES = ("angles", "sid", "sod", "det_u0", "det_v0", "src_x", "src_y", "src_z")
@@ -155,17 +159,41 @@ def _loss(volume, geometry, measured, scan, mask=None):
     return (r * mask).sum() / mask.sum().clamp_min(1.0)
 
 
+class _FusedMSE(torch.autograd.Function):
+    """Masked MSE of the projection as a function of the eight geometry
+    tensors; value and gradients from one fused kernel pass."""
+
+    @staticmethod
+    def forward(ctx, volume, measured, mask, scale, scan, *geometry):
+        loss, grads, _ = _ops.fp_mse_grad(volume, geometry, scan.pixel_size, scan.U, scan.V,
+                                          scan.step_size, scan.voxel_size, measured, mask, scale,
+                                          scan.volume_offset)
+        ctx.save_for_backward(*grads)
+        return loss.float()
+
+    @staticmethod
+    def backward(ctx, grad_loss):
+        return (None, None, None, None, None, *[g * grad_loss for g in ctx.saved_tensors])
+
+
+def _fused_loss(volume, geometry, measured, scan, mask=None, denom=None):
+    if denom is None:
+        denom = float(measured.numel() if mask is None else mask.sum().clamp_min(1.0))
+    return _FusedMSE.apply(volume, measured, mask, 1.0 / denom, scan, *geometry)
+
+
 def calibrate(volume, measured, nominal, scan: ScanSetup, iterations=200, lr=None,
               warm_start=None, true_geometry=None, points=None, target_px=0.1,
               target_angle_deg=None, stop_at_target=False, log_every=0, mask=None,
-              final_lr_fraction=1.0, lr_gamma=1.0, decay_start=0):
+              final_lr_fraction=1.0, lr_gamma=1.0, decay_start=0, fused=True):
     """Adam on per-view geometry offsets; returns a ``CalibrationResult``.
 
     The loss is the mean squared mismatch between ``project(volume, nominal +
     delta)`` and ``measured`` over the rays where ``mask`` is 1 (all rays when
     ``mask`` is None).  Step sizes follow a cosine decay to
     ``final_lr_fraction`` of their start over ``iterations`` (1.0: constant),
-    times ``lr_gamma ** max(0, it - decay_start)``.
+    times ``lr_gamma ** max(0, it - decay_start)``.  ``fused`` selects the
+    one-pass loss-and-gradient kernel (default) or ``project`` + autograd.
 
     ``warm_start`` (8 tensors [A], e.g. a network's prediction) is used as the
     initial delta only if it does not raise the projection loss relative to
@@ -218,11 +246,15 @@ def calibrate(volume, measured, nominal, scan: ScanSetup, iterations=200, lr=Non
         if log_every and it % log_every == 0:
             print({k: (round(v, 5) if isinstance(v, float) else v) for k, v in entry.items()})
 
+    denom = float(measured.numel() if mask is None else mask.sum().clamp_min(1.0))
     record(0, float("nan"))
     for it in range(1, iterations + 1):
         opt.zero_grad(set_to_none=True)
         geom = [g + d for g, d in zip(nominal, delta)]
-        loss = _loss(volume, geom, measured, scan, mask)
+        if fused:
+            loss = _fused_loss(volume, geom, measured, scan, mask, denom)
+        else:
+            loss = _loss(volume, geom, measured, scan, mask)
         loss.backward()
         opt.step()
         sched.step()

@@ -292,6 +292,74 @@ int dgc_project_backward(const float* grad_projection, const float* volume, int 
     return DGC_OK;
 }
 
+// ------------------------------------------- fused calibration loss + grads
+
+size_t dgc_project_mse_grad_workspace_bytes(int D, int H, int W, int A, int U, int V) {
+    if (D <= 0 || H <= 0 || W <= 0 || A <= 0 || U <= 0 || V <= 0) return 0;
+    const size_t tiles = (size_t)fp_tiles_per_view(U, V, 8) * (size_t)A;
+    return quad_volume_bytes(D, H, W) + Workspace::align(sizeof(double) * 8 * tiles) +
+           Workspace::align(sizeof(double) * tiles);
+}
+
+int dgc_project_mse_grad(const float* volume, int D, int H, int W, const float* angles,
+                         const float* sid, const float* sod, const float* det_u0,
+                         const float* det_v0, const float* src_x, const float* src_y,
+                         const float* src_z, int A, float pixel_size, int U, int V,
+                         float step_size, float voxel_size, float off_x, float off_y, float off_z,
+                         const float* measured, const float* mask, float scale,
+                         float* projections, double* loss, float* grad_angles, float* grad_sid,
+                         float* grad_sod, float* grad_det_u0, float* grad_det_v0,
+                         float* grad_src_x, float* grad_src_y, float* grad_src_z,
+                         void* workspace, size_t workspace_bytes, void* stream) {
+    clear_error();
+    cudaStream_t s = (cudaStream_t)stream;
+    const Geometry g = make_geometry(angles, sid, sod, det_u0, det_v0, src_x, src_y, src_z);
+    int rc = check_fp_common(D, H, W, A, U, V, pixel_size, step_size, voxel_size, g);
+    if (rc != DGC_OK) return rc;
+    DGC_REQUIRE(volume && measured && loss, "volume, measured and loss must be non-null");
+    DGC_REQUIRE(std::isfinite(scale), "scale must be finite");
+    GeometryGrad out{{grad_angles, grad_sid, grad_sod, grad_det_u0, grad_det_v0, grad_src_x,
+                      grad_src_y, grad_src_z}};
+    for (int k = 0; k < 8; ++k) DGC_REQUIRE(out.g[k], "geometry gradient pointers must be non-null");
+    FpArgs p;
+    memset(&p, 0, sizeof(p));
+    p.g = g;
+    p.D = D;
+    p.H = H;
+    p.W = W;
+    p.A = A;
+    p.U = U;
+    p.V = V;
+    p.pixel_size = pixel_size;
+    p.step_size = step_size;
+    p.voxel_size = voxel_size;
+    p.off_x = off_x;
+    p.off_y = off_y;
+    p.off_z = off_z;
+    fp_fill_layout(p);
+    const long long tiles = fp_tiles_per_view(U, V, 8);
+    Workspace ws(workspace, workspace_bytes);
+    float4* quads = ws.take<float4>((size_t)(D + 2) * (H + 1) * (W + 1));
+    double* partials = ws.take<double>((size_t)8 * A * tiles);
+    double* lpart = ws.take<double>((size_t)A * tiles);
+    if (!quads || !partials || !lpart) {
+        set_error("workspace too small: dgc_project_mse_grad needs " +
+                  std::to_string(dgc_project_mse_grad_workspace_bytes(D, H, W, A, U, V)) +
+                  " bytes");
+        return DGC_ERR_WORKSPACE;
+    }
+    p.quads = quads;
+    p.partials = partials;
+    p.projections = projections;
+    rc = build_volume_quads(volume, D, H, W, quads, s);
+    if (rc != DGC_OK) return rc;
+    rc = fp_launch_mse_grad(p, measured, mask, scale, lpart, s);
+    if (rc != DGC_OK) return rc;
+    rc = fp_reduce_partials(partials, A, tiles, out, s);
+    if (rc != DGC_OK) return rc;
+    return fp_sum_partials(lpart, (long long)A * tiles, (double)scale, loss, s);
+}
+
 // ----------------------------------------------------------- backprojector
 
 size_t dgc_backproject_workspace_bytes(int A, int U, int V, int D, int H, int W) {

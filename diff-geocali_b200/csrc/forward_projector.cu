@@ -93,7 +93,11 @@ int build_volume_quads(const float* vol, int D, int H, int W, float4* quads, cud
 // ---------------------------------------------------------------------------
 // Per-view and per-ray set-up (reference arithmetic, kept expression for
 // expression so that t_min / t_max -- and with them the FP32 sample count --
-// agree with the reference kernel)
+// agree with the reference kernel).  Every multiply-add is written out as
+// fmaf / __fmul_rn: left to the compiler, a*b - c*d may be contracted
+// differently in different kernels (depending on which products a kernel
+// reuses), and the forward, backward, fused and batched kernels must march
+// bitwise the same rays.
 // ---------------------------------------------------------------------------
 
 struct ViewGeo {
@@ -108,8 +112,8 @@ __device__ __forceinline__ void load_view(const Geometry& g, int a, ViewGeo& vg)
     vg.dn = vg.sod - g.sid[a];
     vg.u0 = g.det_u0[a];
     vg.v0 = g.det_v0[a];
-    vg.ox = -vg.sod * vg.s + g.src_x[a];
-    vg.oy = vg.sod * vg.c + g.src_y[a];
+    vg.ox = fmaf(-vg.sod, vg.s, g.src_x[a]);
+    vg.oy = fmaf(vg.sod, vg.c, g.src_y[a]);
     vg.oz = g.src_z[a];
 }
 
@@ -145,11 +149,11 @@ __device__ __forceinline__ RaySetup setup_ray(const ViewGeo& vg, int u, int v, c
     RaySetup r;
     const float u_phys = (u - vg.u0) * p.pixel_size;
     const float v_phys = (v - vg.v0) * p.pixel_size;
-    const float tx = u_phys * vg.c - vg.dn * vg.s;
-    const float ty = u_phys * vg.s + vg.dn * vg.c;
+    const float tx = fmaf(u_phys, vg.c, -__fmul_rn(vg.dn, vg.s));
+    const float ty = fmaf(u_phys, vg.s, __fmul_rn(vg.dn, vg.c));
     const float tz = v_phys;
     const float rx = tx - vg.ox, ry = ty - vg.oy, rz = tz - vg.oz;
-    r.len = sqrtf(rx * rx + ry * ry + rz * rz);
+    r.len = sqrtf(fmaf(rz, rz, fmaf(rx, rx, __fmul_rn(ry, ry))));
     r.ok = r.len > 1e-8f;
     r.hit = false;
     r.dx = r.dy = r.dz = 0.0f;
@@ -161,12 +165,13 @@ __device__ __forceinline__ RaySetup setup_ray(const ViewGeo& vg, int u, int v, c
     r.dx = rx * inv_len;
     r.dy = ry * inv_len;
     r.dz = rz * inv_len;
-    const float bxl = (-p.W * 0.5f - 0.5f) * p.voxel_size + p.off_x;
-    const float byl = (-p.H * 0.5f - 0.5f) * p.voxel_size + p.off_y;
-    const float bzl = (-p.D * 0.5f - 0.5f) * p.voxel_size + p.off_z;
-    const float bxh = (p.W * 0.5f - 0.5f) * p.voxel_size + p.off_x;
-    const float byh = (p.H * 0.5f - 0.5f) * p.voxel_size + p.off_y;
-    const float bzh = (p.D * 0.5f - 0.5f) * p.voxel_size + p.off_z;
+    // (-n/2 - 1/2) and (n/2 - 1/2) are exact in FP32 for every n < 2^23
+    const float bxl = fmaf(-p.W * 0.5f - 0.5f, p.voxel_size, p.off_x);
+    const float byl = fmaf(-p.H * 0.5f - 0.5f, p.voxel_size, p.off_y);
+    const float bzl = fmaf(-p.D * 0.5f - 0.5f, p.voxel_size, p.off_z);
+    const float bxh = fmaf(p.W * 0.5f - 0.5f, p.voxel_size, p.off_x);
+    const float byh = fmaf(p.H * 0.5f - 0.5f, p.voxel_size, p.off_y);
+    const float bzh = fmaf(p.D * 0.5f - 0.5f, p.voxel_size, p.off_z);
     float tmin = 0.0f, tmax = FLT_MAX;
     int entry = -1;
     r.hit = slab(vg.ox, r.dx, bxl, bxh, 0, tmin, tmax, entry) &&
@@ -207,12 +212,12 @@ template <bool DIV>
 __device__ __forceinline__ bool ray_inside_pad(const RaySetup& r, const ViewGeo& vg,
                                                const FpArgs& p) {
     const float hx = p.W * 0.5f, hy = p.H * 0.5f, hz = p.D * 0.5f;
-    const float x0 = to_voxel<DIV>(vg.ox + r.tmin * r.dx, p.off_x, p.voxel_size, p.inv_voxel, hx);
-    const float x1 = to_voxel<DIV>(vg.ox + r.tmax * r.dx, p.off_x, p.voxel_size, p.inv_voxel, hx);
-    const float y0 = to_voxel<DIV>(vg.oy + r.tmin * r.dy, p.off_y, p.voxel_size, p.inv_voxel, hy);
-    const float y1 = to_voxel<DIV>(vg.oy + r.tmax * r.dy, p.off_y, p.voxel_size, p.inv_voxel, hy);
-    const float z0 = to_voxel<DIV>(vg.oz + r.tmin * r.dz, p.off_z, p.voxel_size, p.inv_voxel, hz);
-    const float z1 = to_voxel<DIV>(vg.oz + r.tmax * r.dz, p.off_z, p.voxel_size, p.inv_voxel, hz);
+    const float x0 = to_voxel<DIV>(fmaf(r.tmin, r.dx, vg.ox), p.off_x, p.voxel_size, p.inv_voxel, hx);
+    const float x1 = to_voxel<DIV>(fmaf(r.tmax, r.dx, vg.ox), p.off_x, p.voxel_size, p.inv_voxel, hx);
+    const float y0 = to_voxel<DIV>(fmaf(r.tmin, r.dy, vg.oy), p.off_y, p.voxel_size, p.inv_voxel, hy);
+    const float y1 = to_voxel<DIV>(fmaf(r.tmax, r.dy, vg.oy), p.off_y, p.voxel_size, p.inv_voxel, hy);
+    const float z0 = to_voxel<DIV>(fmaf(r.tmin, r.dz, vg.oz), p.off_z, p.voxel_size, p.inv_voxel, hz);
+    const float z1 = to_voxel<DIV>(fmaf(r.tmax, r.dz, vg.oz), p.off_z, p.voxel_size, p.inv_voxel, hz);
     const float lo = -0.95f;
     return fminf(x0, x1) >= lo && fmaxf(x0, x1) <= p.W - 0.05f && fminf(y0, y1) >= lo &&
            fmaxf(y0, y1) <= p.H - 0.05f && fminf(z0, z1) >= lo && fmaxf(z0, z1) <= p.D - 0.05f;
@@ -260,9 +265,9 @@ __device__ __forceinline__ float march_sum(const RaySetup& r, const ViewGeo& vg,
     int n = 0;
 #pragma unroll 1
     for (; t <= r.tmax && n < nmax; t += p.step_size, ++n) {
-        const float px = vg.ox + t * r.dx;
-        const float py = vg.oy + t * r.dy;
-        const float pz = vg.oz + t * r.dz;
+        const float px = fmaf(t, r.dx, vg.ox);
+        const float py = fmaf(t, r.dy, vg.oy);
+        const float pz = fmaf(t, r.dz, vg.oz);
         const Cell c =
             locate<CLAMP>(to_voxel<DIV, OFF>(px, p.off_x, p.voxel_size, p.inv_voxel, hx),
                           to_voxel<DIV, OFF>(py, p.off_y, p.voxel_size, p.inv_voxel, hy),
@@ -385,9 +390,9 @@ __device__ __forceinline__ RayGrad march_grad(const RaySetup& r, const ViewGeo& 
     int n = 0;
 #pragma unroll 1
     for (; t <= r.tmax && n < nmax; t += p.step_size, ++n) {
-        const float px = vg.ox + t * r.dx;
-        const float py = vg.oy + t * r.dy;
-        const float pz = vg.oz + t * r.dz;
+        const float px = fmaf(t, r.dx, vg.ox);
+        const float py = fmaf(t, r.dy, vg.oy);
+        const float pz = fmaf(t, r.dz, vg.oz);
         const Cell c = locate<CLAMP>(to_voxel<false>(px, p.off_x, p.voxel_size, p.inv_voxel, hx),
                                      to_voxel<false>(py, p.off_y, p.voxel_size, p.inv_voxel, hy),
                                      to_voxel<false>(pz, p.off_z, p.voxel_size, p.inv_voxel, hz), p);
@@ -429,9 +434,50 @@ __device__ __forceinline__ RayGrad march_grad(const RaySetup& r, const ViewGeo& 
     return rg;
 }
 
+// The eight per-view geometry terms of a ray that hits the volume, from its
+// march sums and gs = dL/dp * step.
+__device__ __forceinline__ void ray_geometry_terms(const FpArgs& p, const ViewGeo& vg,
+                                                   const RaySetup& r, int u, const RayGrad& rg,
+                                                   float gs, float (&terms)[8]) {
+    // fp.cu:441-467 give, with G = gs/voxel,
+    //   grad_origin_direct = G*s1 - (G*(s1.d)/d_e) e_e
+    //   grad_direction     = G*sum g*t - (G*(s1.d) t_min/d_e) e_e
+    // (e = entry axis).  Writing sum g*t = s2 + t_min*s1 and
+    //   q = s1 - ((s1.d)/d_e) e_e   (so q.d = 0)
+    // gives grad_origin_direct = G*q and grad_direction = G*(s2 + t_min*q):
+    // the same values without the large t_min*s1 terms that cancel.
+    float qx = rg.s1x, qy = rg.s1y, qz = rg.s1z;
+    if (r.entry_axis == 0) qx = -(rg.s1y * r.dy + rg.s1z * r.dz) / r.dx;
+    else if (r.entry_axis == 1) qy = -(rg.s1x * r.dx + rg.s1z * r.dz) / r.dy;
+    else if (r.entry_axis == 2) qz = -(rg.s1x * r.dx + rg.s1y * r.dy) / r.dz;
+    const float G = gs * p.inv_voxel;
+    const float godx = G * qx, gody = G * qy, godz = G * qz;
+    // fp.cu:470-486: chain through direction = normalize(target - origin);
+    // q is orthogonal to d, so only s2 loses its component along d.
+    const float ds2 = r.dx * rg.s2x + r.dy * rg.s2y + r.dz * rg.s2z;
+    const float k = G / r.len;
+    const float grx = k * (rg.s2x - r.dx * ds2 + r.tmin * qx);
+    const float gry = k * (rg.s2y - r.dy * ds2 + r.tmin * qy);
+    const float grz = k * (rg.s2z - r.dz * ds2 + r.tmin * qz);
+    const float gox = godx - grx, goy = gody - gry, goz = godz - grz;
+    // fp.cu:488-527: per-view geometry terms.
+    const float u_phys = (u - vg.u0) * p.pixel_size;
+    const float dOx = -vg.sod * vg.c, dOy = -vg.sod * vg.s;
+    const float dTx = -u_phys * vg.s - vg.dn * vg.c;
+    const float dTy = u_phys * vg.c - vg.dn * vg.s;
+    terms[0] = gox * dOx + goy * dOy + grx * dTx + gry * dTy;
+    terms[1] = grx * vg.s - gry * vg.c;
+    terms[2] = (gox + grx) * (-vg.s) + (goy + gry) * vg.c;
+    terms[3] = -p.pixel_size * (grx * vg.c + gry * vg.s);
+    terms[4] = -p.pixel_size * grz;
+    terms[5] = gox;
+    terms[6] = goy;
+    terms[7] = goz;
+}
+
 // The eight per-view geometry terms of one ray (zero for rays outside the
-// detector or with a zero upstream gradient); with GRADVOL the ray's adjoint
-// samples are scattered into p.grad_pad.
+// detector, missing the volume or with a zero upstream gradient); with
+// GRADVOL the ray's adjoint samples are scattered into p.grad_pad.
 template <bool GRADVOL>
 __device__ __forceinline__ void backward_ray(const FpArgs& p, const ViewGeo& vg, int a, int u,
                                              int v, float (&terms)[8]) {
@@ -443,52 +489,12 @@ __device__ __forceinline__ void backward_ray(const FpArgs& p, const ViewGeo& vg,
     // fp.cu:381 -- rays with a zero upstream gradient contribute nothing.
     if (in_range && grad_out != 0.0f) {
         const RaySetup r = setup_ray(vg, u, v, p);
-        if (r.ok) {
-            // Gradients wrt the ray origin (direct part) and the target point.
-            float godx = 0.f, gody = 0.f, godz = 0.f;
-            float grx = 0.f, gry = 0.f, grz = 0.f;
-            if (r.hit) {
-                const float gs = grad_out * p.step_size;
-                const RayGrad rg = ray_inside_pad<false>(r, vg, p)
-                                       ? march_grad<false, GRADVOL>(r, vg, p, gs)
-                                       : march_grad<true, GRADVOL>(r, vg, p, gs);
-                // fp.cu:441-467 give, with G = gs/voxel,
-                //   grad_origin_direct = G*s1 - (G*(s1.d)/d_e) e_e
-                //   grad_direction     = G*sum g*t - (G*(s1.d) t_min/d_e) e_e
-                // (e = entry axis).  Writing sum g*t = s2 + t_min*s1 and
-                //   q = s1 - ((s1.d)/d_e) e_e   (so q.d = 0)
-                // gives grad_origin_direct = G*q and grad_direction = G*(s2 + t_min*q):
-                // the same values without the large t_min*s1 terms that cancel.
-                float qx = rg.s1x, qy = rg.s1y, qz = rg.s1z;
-                if (r.entry_axis == 0) qx = -(rg.s1y * r.dy + rg.s1z * r.dz) / r.dx;
-                else if (r.entry_axis == 1) qy = -(rg.s1x * r.dx + rg.s1z * r.dz) / r.dy;
-                else if (r.entry_axis == 2) qz = -(rg.s1x * r.dx + rg.s1y * r.dy) / r.dz;
-                const float G = gs * p.inv_voxel;
-                godx = G * qx;
-                gody = G * qy;
-                godz = G * qz;
-                // fp.cu:470-486: chain through direction = normalize(target - origin);
-                // q is orthogonal to d, so only s2 loses its component along d.
-                const float ds2 = r.dx * rg.s2x + r.dy * rg.s2y + r.dz * rg.s2z;
-                const float k = G / r.len;
-                grx = k * (rg.s2x - r.dx * ds2 + r.tmin * qx);
-                gry = k * (rg.s2y - r.dy * ds2 + r.tmin * qy);
-                grz = k * (rg.s2z - r.dz * ds2 + r.tmin * qz);
-            }
-            const float gox = godx - grx, goy = gody - gry, goz = godz - grz;
-            // fp.cu:488-527: per-view geometry terms.
-            const float u_phys = (u - vg.u0) * p.pixel_size;
-            const float dOx = -vg.sod * vg.c, dOy = -vg.sod * vg.s;
-            const float dTx = -u_phys * vg.s - vg.dn * vg.c;
-            const float dTy = u_phys * vg.c - vg.dn * vg.s;
-            terms[0] = gox * dOx + goy * dOy + grx * dTx + gry * dTy;
-            terms[1] = grx * vg.s - gry * vg.c;
-            terms[2] = (gox + grx) * (-vg.s) + (goy + gry) * vg.c;
-            terms[3] = -p.pixel_size * (grx * vg.c + gry * vg.s);
-            terms[4] = -p.pixel_size * grz;
-            terms[5] = gox;
-            terms[6] = goy;
-            terms[7] = goz;
+        if (r.ok && r.hit) {
+            const float gs = grad_out * p.step_size;
+            const RayGrad rg = ray_inside_pad<false>(r, vg, p)
+                                   ? march_grad<false, GRADVOL>(r, vg, p, gs)
+                                   : march_grad<true, GRADVOL>(r, vg, p, gs);
+            ray_geometry_terms(p, vg, r, u, rg, gs, terms);
         }
     }
 }
@@ -531,6 +537,132 @@ __global__ void __launch_bounds__(256) fp_backward_kernel(FpArgs p) {
     float terms[8];
     backward_ray<GRADVOL>(p, vg, a, u, v, terms);
     reduce_terms_to_partials(terms, s_red, p.partials + ((long long)a * tiles + tile) * 8);
+}
+
+// ---------------------------------------------------------------------------
+// Fused projection -> masked MSE -> geometry gradients (calibration step)
+// ---------------------------------------------------------------------------
+
+struct RayValueGrad {
+    float sum;  // sum of the trilinear samples (the forward kernel's arithmetic)
+    RayGrad g;  // s1, s2 of march_grad
+};
+
+// One march that yields both the line-integral sum (bitwise the forward
+// kernel's: same positions, same packed lerps) and the spatial-gradient sums
+// of the backward.  No scatter: the volume is not differentiated here.
+template <bool CLAMP, bool DIV, bool OFF>
+__device__ __forceinline__ RayValueGrad march_value_grad(const RaySetup& r, const ViewGeo& vg,
+                                                         const FpArgs& p) {
+    const float hx = p.W * 0.5f, hy = p.H * 0.5f, hz = p.D * 0.5f;
+    const ulonglong2* __restrict__ Q = reinterpret_cast<const ulonglong2*>(p.quads);
+    RayValueGrad out{0.0f, {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}};
+    const int nmax = step_bound(r, p.step_size);
+    float t = r.tmin;
+    int n = 0;
+#pragma unroll 1
+    for (; t <= r.tmax && n < nmax; t += p.step_size, ++n) {
+        const float px = fmaf(t, r.dx, vg.ox);
+        const float py = fmaf(t, r.dy, vg.oy);
+        const float pz = fmaf(t, r.dz, vg.oz);
+        const Cell c =
+            locate<CLAMP>(to_voxel<DIV, OFF>(px, p.off_x, p.voxel_size, p.inv_voxel, hx),
+                          to_voxel<DIV, OFF>(py, p.off_y, p.voxel_size, p.inv_voxel, hy),
+                          to_voxel<DIV, OFF>(pz, p.off_z, p.voxel_size, p.inv_voxel, hz), p);
+        const uint32_t qi = quad_index(c, p);
+        const ulonglong2 q0 = __ldg(Q + qi);
+        const ulonglong2 q1 = __ldg(Q + qi + 1);
+        const f32x2 wx = pack2(c.fx, c.fx);
+        const f32x2 e0 = lerp2(q0.x, q0.y, wx);
+        const f32x2 e1 = lerp2(q1.x, q1.y, wx);
+        const float2 e = unpack2(lerp2(e0, e1, pack2(c.fz, c.fz)));
+        out.sum += lerpf(e.x, e.y, c.fy);
+        // (x0y0, x0y1), (x1y0, x1y1) at z0 and z1
+        const float2 a0 = unpack2(q0.x), b0 = unpack2(q0.y);
+        const float2 a1 = unpack2(q1.x), b1 = unpack2(q1.y);
+        const float gx = lerpf(lerpf(b0.x - a0.x, b0.y - a0.y, c.fy),
+                               lerpf(b1.x - a1.x, b1.y - a1.y, c.fy), c.fz);
+        const float gy = lerpf(lerpf(a0.y - a0.x, b0.y - b0.x, c.fx),
+                               lerpf(a1.y - a1.x, b1.y - b1.x, c.fx), c.fz);
+        const float gz = lerpf(lerpf(a1.x - a0.x, b1.x - b0.x, c.fx),
+                               lerpf(a1.y - a0.y, b1.y - b0.y, c.fx), c.fy);
+        const float tau = t - r.tmin;
+        out.g.s1x += gx;
+        out.g.s1y += gy;
+        out.g.s1z += gz;
+        out.g.s2x = fmaf(gx, tau, out.g.s2x);
+        out.g.s2y = fmaf(gy, tau, out.g.s2y);
+        out.g.s2z = fmaf(gz, tau, out.g.s2z);
+    }
+    return out;
+}
+
+// Per ray: p = projection, L_ray = mask * (p - measured)^2, dL/dp = 2 * scale *
+// mask * (p - measured); the geometry terms of the backward with that upstream
+// gradient.  Per CTA: FP64 fixed-order sums of the eight terms (partials) and
+// of L_ray (loss_partials).
+template <int TU, bool DIV, bool OFF>
+__global__ void __launch_bounds__(256) fp_mse_grad_kernel(FpArgs p, const float* __restrict__ measured,
+                                                          const float* __restrict__ mask, float scale,
+                                                          double* __restrict__ loss_partials) {
+    constexpr int TV = 256 / TU;
+    __shared__ ViewGeo s_view;
+    __shared__ double s_red[8][8];
+    __shared__ double s_loss[8];
+    const int tiles_u = (p.U + TU - 1) / TU;
+    const int tiles = tiles_u * ((p.V + TV - 1) / TV);
+    const TileCoord tc = tile_coord(p, tiles_u);
+    const int a = tc.a;
+    const int tile = tc.tv * tiles_u + tc.tu;
+    if (threadIdx.x == 0) load_view(p.g, a, s_view);
+    __syncthreads();
+    const ViewGeo vg = s_view;
+    int u, v;
+    tile_ray<TU>(tc, u, v);
+    float terms[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    float lray = 0.0f;
+    if (u < p.U && v < p.V) {
+        const RaySetup r = setup_ray(vg, u, v, p);
+        RayValueGrad m{0.0f, {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}};
+        const bool hit = r.ok && r.hit;
+        if (hit)
+            m = ray_inside_pad<DIV>(r, vg, p) ? march_value_grad<false, DIV, OFF>(r, vg, p)
+                                              : march_value_grad<true, DIV, OFF>(r, vg, p);
+        const float proj = m.sum * p.step_size;
+        const long long idx = ((long long)a * p.U + u) * p.V + v;
+        if (p.projections) p.projections[idx] = proj;
+        const float w = mask ? mask[idx] : 1.0f;
+        const float diff = proj - measured[idx];
+        lray = w * diff * diff;
+        const float g = 2.0f * scale * w * diff;
+        if (hit && g != 0.0f) ray_geometry_terms(p, vg, r, u, m.g, g * p.step_size, terms);
+    }
+    reduce_terms_to_partials(terms, s_red, p.partials + ((long long)a * tiles + tile) * 8);
+    const double l = warp_sum((double)lray);
+    if ((threadIdx.x & 31) == 0) s_loss[threadIdx.x >> 5] = l;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double acc = 0.0;
+#pragma unroll
+        for (int w = 0; w < 8; ++w) acc += s_loss[w];
+        loss_partials[(long long)a * tiles + tile] = acc;
+    }
+}
+
+// Fixed-order sum of n doubles by one block of 256 threads: out[0] = scale * sum.
+__global__ void __launch_bounds__(256) sum_partials_kernel(const double* __restrict__ x, long long n,
+                                                           double scale, double* __restrict__ out) {
+    __shared__ double s[8];
+    double acc = 0.0;
+    for (long long i = threadIdx.x; i < n; i += 256) acc += x[i];
+    acc = warp_sum(acc);
+    if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < 8; ++w) t += s[w];
+        out[0] = scale * t;
+    }
 }
 
 // Per-view sum of the CTA partials, warp k owning gradient k (fixed order).
@@ -818,6 +950,31 @@ int fp_launch_backward(const FpArgs& p, const FpTile& tile, bool gradvol, cudaSt
             set_error("unsupported backward tile");
             return DGC_ERR_INVALID_ARGUMENT;
     }
+}
+
+int fp_launch_mse_grad(const FpArgs& p, const float* measured, const float* mask, float scale,
+                       double* loss_partials, cudaStream_t s) {
+    DGC_TRACE("fp_mse_grad_kernel", s);
+    constexpr int TU = 8;
+    const long long blocks = fp_tiles_per_view(p.U, p.V, TU) * (long long)p.A;
+    const bool div = !is_pow2_float(p.voxel_size);
+    const bool off = p.off_x != 0.0f || p.off_y != 0.0f || p.off_z != 0.0f;
+    if (div) {
+        if (off) fp_mse_grad_kernel<TU, true, true><<<(unsigned)blocks, 256, 0, s>>>(p, measured, mask, scale, loss_partials);
+        else fp_mse_grad_kernel<TU, true, false><<<(unsigned)blocks, 256, 0, s>>>(p, measured, mask, scale, loss_partials);
+    } else {
+        if (off) fp_mse_grad_kernel<TU, false, true><<<(unsigned)blocks, 256, 0, s>>>(p, measured, mask, scale, loss_partials);
+        else fp_mse_grad_kernel<TU, false, false><<<(unsigned)blocks, 256, 0, s>>>(p, measured, mask, scale, loss_partials);
+    }
+    DGC_LAUNCH_CHECK("fp_mse_grad_kernel");
+    return DGC_OK;
+}
+
+int fp_sum_partials(const double* x, long long n, double scale, double* out, cudaStream_t s) {
+    DGC_TRACE("sum_partials", s);
+    sum_partials_kernel<<<1, 256, 0, s>>>(x, n, scale, out);
+    DGC_LAUNCH_CHECK("sum_partials");
+    return DGC_OK;
 }
 
 int fp_launch_counts(const FpArgs& p, int64_t* counts, cudaStream_t s) {

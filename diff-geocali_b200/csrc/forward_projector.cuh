@@ -72,6 +72,11 @@ int build_volume_quads(const float* vol, int D, int H, int W, float4* quads, cud
 int fp_launch_forward(const FpArgs& p, const FpTile& tile, cudaStream_t s);
 int fp_launch_backward(const FpArgs& p, const FpTile& tile, bool gradvol, cudaStream_t s);
 int fp_launch_counts(const FpArgs& p, int64_t* counts, cudaStream_t s);
+// Fused projection -> masked squared error -> geometry-gradient terms (8-column
+// tiles); p.partials [A][tiles][8], loss_partials [A][tiles].
+int fp_launch_mse_grad(const FpArgs& p, const float* measured, const float* mask, float scale,
+                       double* loss_partials, cudaStream_t s);
+int fp_sum_partials(const double* x, long long n, double scale, double* out, cudaStream_t s);
 int fp_reduce_partials(const double* partials, int A, long long tiles, const GeometryGrad& out,
                        cudaStream_t s);
 int fp_fold_gradient(const float* gpad, int D, int H, int W, float* grad, cudaStream_t s);

@@ -207,6 +207,30 @@ int dgc_gemm_bf16(const void* A, const void* B, void* C, const float* bias, int 
                   int lda, int ldb, int ldc, int c_bf16, int relu, int accumulate, float alpha,
                   int* error_flag, void* stream);
 
+/* Scratch of dgc_project_mse_grad. */
+size_t dgc_project_mse_grad_workspace_bytes(int D, int H, int W, int A, int U, int V);
+
+/* One geometry-calibration step fused into one ray march: the projection p of
+ * dgc_project, the loss  *loss = scale * sum(mask * (p - measured)^2)  (FP64,
+ * fixed-order sums) and the eight geometry gradients of that loss (those of
+ * dgc_project_backward with grad_projection = 2*scale*mask*(p - measured)),
+ * without the volume gradient.  mask may be NULL (all ones); projections may
+ * be NULL (not stored).  Replaces the reference's forward + backward pair
+ * (csrc/src_cbct_forwardprojector_cuda.cu:566-729) for a masked MSE loss,
+ * which the reference composes in Python; one march instead of two. */
+int dgc_project_mse_grad(const float* volume, int D, int H, int W,
+                         const float* angles, const float* sid, const float* sod,
+                         const float* det_u0, const float* det_v0,
+                         const float* src_x, const float* src_y, const float* src_z,
+                         int A, float pixel_size, int U, int V, float step_size,
+                         float voxel_size, float off_x, float off_y, float off_z,
+                         const float* measured, const float* mask, float scale,
+                         float* projections, double* loss,
+                         float* grad_angles, float* grad_sid, float* grad_sod,
+                         float* grad_det_u0, float* grad_det_v0,
+                         float* grad_src_x, float* grad_src_y, float* grad_src_z,
+                         void* workspace, size_t workspace_bytes, void* stream);
+
 /* ---------------------------------------------------------------------- */
 /* Batched forward projection + backward over uneven instances             */
 /* ---------------------------------------------------------------------- */

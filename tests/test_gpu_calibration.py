@@ -115,3 +115,41 @@ def test_warm_start_judge():
     # rejected prediction: the run starts from nominal
     assert abs(r_bad.history[0]["reproj_px"] - C.reprojection_error(
         nominal, true, C.lattice_points(vol.shape, device="cuda"), 1.0)) < 1e-9
+
+
+def test_fused_step_matches_project_and_autograd():
+    """dgc_project_mse_grad (one march) against project + masked MSE + autograd
+    (two marches): the projection bitwise (the ray set-up is written with
+    explicit fmaf / __fmul_rn, so both kernels march the same rays), the loss
+    to 1e-5, the eight geometry gradients to 1e-5 (the upstream gradient
+    2*scale*mask*(p - m) is rounded in a different order)."""
+    from cbct_backprojector import _ops, project
+
+    C, vol, nominal, true, scan, meas, mask = setup_case(size=40, A=48, det=72, I0=1e5)
+    geom = [n + 0.5 * (t - n) for t, n in zip(true, nominal)]
+    for m in (mask, None):
+        denom = float(meas.numel() if m is None else m.sum())
+        loss, grads, proj = _ops.fp_mse_grad(vol, geom, 1.0, scan.U, scan.V, 0.5, 1.0, meas, m,
+                                             1.0 / denom, return_projection=True)
+        g = [x.clone().requires_grad_() for x in geom]
+        p = project(vol, *g, 1.0, scan.U, scan.V, step_size=0.5, voxel_size=1.0)
+        r = (p - meas).square()
+        ref = (r if m is None else r * m).sum() / denom
+        want = torch.autograd.grad(ref, g)
+        torch.cuda.synchronize()
+        assert torch.equal(proj, p.detach())
+        assert math.isclose(float(loss), float(ref), rel_tol=1e-5)
+        for k in range(8):
+            a, b = grads[k].double(), want[k].double()
+            assert float((a - b).norm() / b.norm()) < 1e-5, k
+
+
+def test_fused_and_unfused_calibration_agree():
+    C, vol, nominal, true, scan, meas, mask = setup_case(size=40, A=48, det=72, I0=1e5)
+    pts = C.lattice_points(vol.shape, device="cuda")
+    runs = [C.calibrate(vol, meas, nominal, scan, iterations=15, true_geometry=true, points=pts,
+                        mask=mask, fused=f) for f in (True, False)]
+    for a, b in zip(runs[0].history[1:], runs[1].history[1:]):
+        assert math.isclose(a["loss"], b["loss"], rel_tol=1e-4)
+    assert math.isclose(runs[0].history[-1]["reproj_px"], runs[1].history[-1]["reproj_px"],
+                        rel_tol=1e-2)
