@@ -39,9 +39,10 @@ WORKLOAD = dict(name="fdk256: project 256^3 -> 360x384^2, then reconstruct_fdk 2
                 step=0.5, voxel=1.0, ellipsoids=12, alpha=0.8)
 METRIC = "fwd Grays/s, backproj Gvoxel-views/s; calib time to 0.1 px reproj, NN vs plain"
 UNIT = "Grays/s"
-# Per-launch DRAM bytes of fp_forward_kernel from an ncu capture (see
-# profiles/fp_forward_kernel_fdk256.md); None until measured.
-FWD_DRAM_BYTES_PER_LAUNCH = None
+# DRAM bytes (read + write) of one 360-view fp_forward_kernel launch: an ncu
+# capture of the 24-view case (bench.py --workload tour --views 24) measured
+# 351.7 + 17.9 MB, scaled by the view count (x15).
+FWD_DRAM_BYTES_PER_LAUNCH = (351.7e6 + 17.9e6) * 15
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -56,10 +57,11 @@ def parse_args(argv=None):
                     help="override the view count (smaller cases for profiler captures)")
     ap.add_argument("--volume", type=int, default=None, help="override the cubic volume size")
     ap.add_argument("--detector", type=int, default=None, help="override the square detector size")
-    ap.add_argument("--workload", choices=["fdk256", "batch64", "calib"], default="fdk256",
+    ap.add_argument("--workload", choices=["fdk256", "batch64", "calib", "tour"], default="fdk256",
                     help="fdk256: the FDK step (default); batch64: 64 uneven project+backward "
                          "instances, batched vs sequential; calib: calibration wall time to "
-                         "0.1 px, learned warm start vs plain")
+                         "0.1 px, learned warm start vs plain; tour: every kernel once on the "
+                         "fdk256 instance (profiler captures)")
     ap.add_argument("--acq", choices=["half", "eval"], default="half",
                     help="calib: 256^3/360/384^2 (half) or 512^3/720/768^2 (eval)")
     ap.add_argument("--max-iterations", type=int, default=600, help="calib: iteration cap")
@@ -611,8 +613,73 @@ def run_calib(args):
     return 0
 
 
+# --------------------------------------------------------------------- tour
+
+
+def run_tour(args):
+    """Every kernel of the library on the fdk256 instance (honouring --views /
+    --volume / --detector), ``--steps`` times: project, its backward with the
+    volume gradient, the fused calibration step, backproject and its backward,
+    reconstruct_fdk, a two-instance batched step and one warm-start network
+    forward/backward (tensor-core GEMMs).  Prints the per-kernel device times
+    of the last pass; meant for profiler captures of small cases."""
+    import torch
+
+    import cbct_backprojector as cb
+    from cbct_backprojector import _native, _ops
+    from cbct_backprojector import warmstart as WS
+    from cbct_backprojector.batch import Problem, ProjectionBatch
+
+    torch.cuda.set_device(0)
+    device = torch.device("cuda", 0)
+    w = WORKLOAD
+    vol, geom = make_instance(device, instance_seed(0))
+    shape = (w["D"], w["H"], w["W"])
+    meas = cb.project(vol, *geom, w["pixel"], w["U"], w["V"], step_size=w["step"],
+                      voxel_size=w["voxel"]) * 1.01
+    net = WS.WarmStartNet().to(device)
+    x = torch.randn(12, WS.INPUT_SIZE, WS.INPUT_SIZE, 2, device=device).to(torch.bfloat16)
+    problems = [Problem(vol, geom, w["pixel"], w["U"], w["V"], w["step"], w["voxel"]),
+                Problem(vol[: w["D"] // 2].contiguous(), [g[: max(1, w["A"] // 2)] for g in geom],
+                        w["pixel"], w["U"], w["V"], w["step"], w["voxel"])]
+    batch = ProjectionBatch(problems)
+
+    def one_pass():
+        v = vol.detach().requires_grad_()
+        g = [t.detach().requires_grad_() for t in geom]
+        p = cb.project(v, *g, w["pixel"], w["U"], w["V"], step_size=w["step"],
+                       voxel_size=w["voxel"])
+        torch.autograd.grad(p, [v, *g], grad_outputs=p.detach())
+        _ops.fp_mse_grad(vol, geom, w["pixel"], w["U"], w["V"], w["step"], w["voxel"], meas,
+                         None, 1.0 / meas.numel())
+        pr = p.detach().requires_grad_()
+        g2 = [t.detach().requires_grad_() for t in geom]
+        b = cb.backproject(pr, *g2, w["pixel"], shape, w["voxel"])
+        torch.autograd.grad(b, [pr, *g2], grad_outputs=torch.ones_like(b))
+        cb.reconstruct_fdk(p.detach(), *geom, w["pixel"], shape, w["voxel"], alpha=w["alpha"])
+        batch.step()
+        out = net(x)
+        out.square().sum().backward()
+
+    for _ in range(max(0, args.warmup)):
+        one_pass()
+    torch.cuda.synchronize()
+    kern = {}
+    for _ in range(max(1, args.steps)):
+        with _native.trace() as tr:
+            one_pass()
+            torch.cuda.synchronize()
+        kern = {}
+        for name, ms in tr.records:
+            kern[name] = round(kern.get(name, 0.0) + ms, 4)
+    print(json.dumps({"workload": "tour: " + w["name"], "kernel_ms": kern}))
+    return 0
+
+
 def main(argv=None):
     args = parse_args(argv)
+    if args.workload == "tour":
+        return run_tour(args)
     if args.workload == "calib":
         return run_calib(args)
     if args.impl == "reference":
