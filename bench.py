@@ -64,7 +64,7 @@ def parse_args(argv=None):
                          "fdk256 instance (profiler captures)")
     ap.add_argument("--acq", choices=["half", "eval"], default="half",
                     help="calib: 256^3/360/384^2 (half) or 512^3/720/768^2 (eval)")
-    ap.add_argument("--max-iterations", type=int, default=600, help="calib: iteration cap")
+    ap.add_argument("--max-iterations", type=int, default=300, help="calib: iteration cap")
     ap.add_argument("--instances", type=int, default=64, help="batch64: number of instances")
     ap.add_argument("--tune-cache", default=None, help="batch64: autotuner JSON cache path")
     args = ap.parse_args(argv)
@@ -582,9 +582,11 @@ def run_batch64(args):
 
 
 def run_calib(args):
-    """Wall time to 0.1 px RMS reprojection error (and 0.05 deg angle error on
-    the eval acquisition): calibration from the network's warm start vs from
-    nominal, same GPU, same projector; every iteration timed on the host."""
+    """Wall time to 0.1 px RMS reprojection error, and to 0.1 px together with
+    0.05 deg RMS angle error: calibration from the network's warm start vs
+    from nominal, same GPU, same projector, each arm with its own settings;
+    every iteration timed on the host, the warm-start arm's time includes
+    the nominal reprojection and the network inference."""
     import torch
 
     from cbct_backprojector import warmstart as WS
@@ -592,21 +594,23 @@ def run_calib(args):
     torch.cuda.set_device(0)
     acq = WS.HALF if args.acq == "half" else WS.EVAL
     net, meta = WS.load(WS.default_checkpoint())
-    target_angle = None if args.acq == "half" else 0.05
     res = WS.evaluate(net, acq, seed=7, iterations=args.max_iterations, target_mm=0.1 * acq.pixel,
-                      target_angle_deg=target_angle, stop_at_target=True)
+                      target_angle_deg=0.05, stop_at_target=True)
     p, n = res["plain"], res["warm_start"]
     line = {
         "metric": "calibration wall time to 0.1 px RMS reprojection error", "unit": "s",
-        "value": n["time_to_target_s"], "higher_is_better": False, "n_gpus": 1,
+        "value": n["time_to_px_target_s"], "higher_is_better": False, "n_gpus": 1,
         "steps": 1, "warmup": 0, "dtype": "f32 (network bf16/fp32)", "data": "synthetic",
         "vs_baseline": None,
-        "config": {"workload": f"calibration {acq.volume}^3, {acq.views} views, "
-                               f"{acq.detector}^2 detector, config-3 perturbations, I0=1e5",
+        "config": {"workload": f"calibration {acq.volume}^3 x {acq.voxel} mm, {acq.views} views, "
+                               f"{acq.detector}^2 x {acq.pixel} mm detector, config-3 "
+                               "perturbations, Poisson I0=1e5",
                    "max_iterations": args.max_iterations, "target_px": 0.1,
-                   "target_angle_deg": target_angle,
-                   "network_training_steps": meta.get("steps")},
-        "plain": p, "warm_start": n, "speedup": res["speedup"],
+                   "target_angle_deg": 0.05, "network_training_steps": meta.get("steps")},
+        "plain": p, "warm_start": n,
+        "speedup_to_0.1px": res["speedup_px_target"],
+        "speedup_to_0.1px_and_0.05deg": res["speedup"],
+        "stages": res["stages"], "warm_calibration": res["warm_calibration"],
         "warm_start_accepted": res["warm_start_accepted"], "inference_s": res["inference_s"],
     }
     print(json.dumps(line))

@@ -41,11 +41,11 @@ from .source_only_forward_projector import project
 GEOMETRY_NAMES = ("angles", "sid", "sod", "det_u0", "det_v0", "src_x", "src_y", "src_z")
 
 # Adam step sizes per parameter family (radians, length units, pixels): the
-# per-iteration move Adam makes is about this size.  Tuned on the 128^3 / 180
-# view / 256^2 and 256^3 / 360 view / 384^2 calibration cases (0.1 px RMS
-# reprojection error reached in ~120 and ~200 iterations).
-DEFAULT_LR = {"angles": 8e-3, "sid": 2.0, "sod": 2.0, "det_u0": 0.2, "det_v0": 0.2,
-              "src_x": 0.2, "src_y": 0.2, "src_z": 0.2}
+# per-iteration move Adam makes is about this size.  Chosen on held-out
+# stacks of the 128^3 / 180 view / 256^2 acquisition (0.1 px RMS reprojection
+# error in 46-52 iterations) and confirmed on 256^3 / 360 views / 384^2 (71).
+DEFAULT_LR = {"angles": 3e-3, "sid": 3.0, "sod": 3.0, "det_u0": 0.3, "det_v0": 0.3,
+              "src_x": 0.3, "src_y": 0.3, "src_z": 0.3}
 
 
 @dataclass
@@ -185,14 +185,17 @@ def _fused_loss(volume, geometry, measured, scan, mask=None, denom=None):
 def calibrate(volume, measured, nominal, scan: ScanSetup, iterations=200, lr=None,
               warm_start=None, true_geometry=None, points=None, target_px=0.1,
               target_angle_deg=None, stop_at_target=False, log_every=0, mask=None,
-              final_lr_fraction=1.0, lr_gamma=1.0, decay_start=0, fused=True):
+              final_lr_fraction=1.0, lr_gamma=1.0, decay_start=0, fused=True,
+              warmup_iterations=0, betas=(0.9, 0.99)):
     """Adam on per-view geometry offsets; returns a ``CalibrationResult``.
 
     The loss is the mean squared mismatch between ``project(volume, nominal +
     delta)`` and ``measured`` over the rays where ``mask`` is 1 (all rays when
     ``mask`` is None).  Step sizes follow a cosine decay to
     ``final_lr_fraction`` of their start over ``iterations`` (1.0: constant),
-    times ``lr_gamma ** max(0, it - decay_start)``.  ``fused`` selects the
+    times ``lr_gamma ** max(0, it - decay_start)``, ramped up linearly over
+    the first ``warmup_iterations`` (Adam's first steps are ``lr``-sized
+    whatever the gradient, which throws a good start away).  ``fused`` selects the
     one-pass loss-and-gradient kernel (default) or ``project`` + autograd.
 
     ``warm_start`` (8 tensors [A], e.g. a network's prediction) is used as the
@@ -221,11 +224,12 @@ def calibrate(volume, measured, nominal, scan: ScanSetup, iterations=200, lr=Non
     for d in delta:
         d.requires_grad_(True)
     opt = torch.optim.Adam([{"params": [d], "lr": lr[name]}
-                            for d, name in zip(delta, GEOMETRY_NAMES)], betas=(0.9, 0.99))
+                            for d, name in zip(delta, GEOMETRY_NAMES)], betas=tuple(betas))
     sched = torch.optim.lr_scheduler.LambdaLR(
         opt, lambda it: (final_lr_fraction + (1.0 - final_lr_fraction) * 0.5 *
                          (1.0 + math.cos(math.pi * min(it, iterations) / max(iterations, 1)))) *
-        lr_gamma ** max(0, it - decay_start))
+        lr_gamma ** max(0, it - decay_start) *
+        (min(1.0, (it + 1) / warmup_iterations) if warmup_iterations else 1.0))
     if points is None and true_geometry is not None:
         points = lattice_points(volume.shape, scan.voxel_size, scan.volume_offset,
                                 device=volume.device)

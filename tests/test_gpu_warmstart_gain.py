@@ -47,18 +47,25 @@ def test_prediction_beats_nominal(net):
     assert nn_rms < 0.6 * nominal_rms, (nn_rms, nominal_rms)
 
 
-def test_warm_started_calibration_ends_closer(net):
+def test_warm_started_calibration_reaches_target_faster(net):
+    """From the network's two-stage start with its calibration settings, the
+    0.1 px target comes in fewer than half the iterations of calibration from
+    nominal (46-52 vs 12-15 on held-out stacks when the settings were chosen)."""
     from cbct_backprojector import warmstart as WS
     from cbct_backprojector.calibration import calibrate, lattice_points
 
     acq = WS.TRAIN
-    st = WS.make_stack(acq, 7)
+    st = WS.make_stack(acq, 42)
     pts = lattice_points(st["volume"].shape, acq.voxel, device="cuda")
-    kw = dict(iterations=40, true_geometry=st["true"], points=pts, mask=st["mask"])
+    kw = dict(iterations=120, true_geometry=st["true"], points=pts, mask=st["mask"],
+              target_px=0.1, stop_at_target=True)
     plain = calibrate(st["volume"], st["measured"], st["nominal"], acq.scan, **kw)
     warm = WS.predict(net, st["measured"], st["nominal_projection"], st["mask"], st["nominal"],
-                      acq)
-    nn = calibrate(st["volume"], st["measured"], st["nominal"], acq.scan, warm_start=warm, **kw)
+                      acq, volume=st["volume"], stages=WS.WARM_STAGES)
+    nn = calibrate(st["volume"], st["measured"], st["nominal"], acq.scan, warm_start=warm,
+                   **dict(kw, **WS.WARM_CALIBRATION))
     assert nn.warm_start_accepted
-    assert nn.history[0]["reproj_px"] < plain.history[0]["reproj_px"]
-    assert nn.history[-1]["reproj_px"] < plain.history[-1]["reproj_px"]
+    assert nn.history[0]["reproj_px"] < 0.3 * plain.history[0]["reproj_px"]
+    assert plain.iterations_to_target is not None and nn.iterations_to_target is not None
+    assert 2 * nn.iterations_to_target < plain.iterations_to_target, (
+        nn.iterations_to_target, plain.iterations_to_target)
