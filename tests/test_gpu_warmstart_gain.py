@@ -48,9 +48,9 @@ def test_prediction_beats_nominal(net):
 
 
 def test_warm_started_calibration_reaches_target_faster(net):
-    """From the network's two-stage start with its calibration settings, the
+    """From the network's multi-stage start with its calibration settings, the
     0.1 px target comes in fewer than half the iterations of calibration from
-    nominal (46-52 vs 12-15 on held-out stacks when the settings were chosen)."""
+    nominal (46-52 vs 7-12 on held-out stacks when the settings were chosen)."""
     from cbct_backprojector import warmstart as WS
     from cbct_backprojector.calibration import calibrate, lattice_points
 
