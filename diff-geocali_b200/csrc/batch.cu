@@ -174,7 +174,8 @@ int dgc_batch_prepare(const dgc_fp_instance* instances, int n, void* workspace,
         b.tile_fwd = tile_fwd(in);
         b.tile_bwd = tile_bwd(in);
         b.flags = (is_pow2_float(in.voxel_size) ? 0 : kBatchDiv) |
-                  ((in.off_x != 0.0f || in.off_y != 0.0f || in.off_z != 0.0f) ? kBatchOff : 0);
+                  ((in.off_x != 0.0f || in.off_y != 0.0f || in.off_z != 0.0f) ? kBatchOff : 0) |
+                  (fp_merge_scatter(in.U, in.V, in.H, in.W) ? kBatchMerge : 0);
         b.quad_gx = ceil_div(in.W + 1, 32) * (in.H + 1);
         b.tiles_bwd = fp_tiles_per_view(in.U, in.V, b.tile_bwd);
         host[i] = b;

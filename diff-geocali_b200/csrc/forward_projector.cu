@@ -33,6 +33,9 @@
 //     (consecutive lanes hit consecutive addresses) and folded back onto the
 //     clamped edge voxels afterwards (the sums of the reference's clamped-index
 //     atomics).
+#include <cstdlib>
+#include <cstring>
+
 #include "common.cuh"
 #include "forward_projector.cuh"
 
@@ -379,7 +382,61 @@ struct RayGrad {
     float s1x, s1y, s1z, s2x, s2y, s2z;
 };
 
-template <bool CLAMP, bool GRADVOL>
+// Scatter of one trilinear sample's eight weights into the padded gradient,
+// merged across lane pairs first.  The lanes of a warp march 32 consecutive
+// detector rows of one column, so at a given instruction two neighbouring
+// lanes usually sample the same (x, y) cell column at the same or adjacent z:
+// the odd lane then adds its partner's weights that land on its own eight
+// addresses (all eight for the same cell, four for a cell one z above or
+// below) and the even lane leaves those reductions out.  Sums are unchanged
+// (up to float reassociation, as with any atomics); the L2 sees up to half
+// the reductions.  Lanes whose partner is not converged here scatter alone.
+__device__ __forceinline__ void scatter_cell_pairwise(const FpArgs& p, uint32_t gi, float (&lo)[4],
+                                                      float (&hi)[4]) {
+    const unsigned mask = __activemask();
+    const int lane = threadIdx.x & 31;
+    const int partner = lane ^ 1;
+    const bool odd = lane & 1;
+    const uint32_t gpart = __shfl_sync(mask, gi, partner);
+    float plo[4], phi[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        plo[k] = __shfl_sync(mask, lo[k], partner);
+        phi[k] = __shfl_sync(mask, hi[k], partner);
+    }
+    // cell of the odd lane minus cell of the even lane; 0 or +-1 means the
+    // same (x, y) column (z differs by at most D+1 < the x stride D+2)
+    const int d = (int)(odd ? gi - gpart : gpart - gi);
+    const int mode = !((mask >> partner) & 1u) ? 0 : d == 0 ? 1 : d == 1 ? 2 : d == -1 ? 3 : 0;
+    bool emit_lo = true, emit_hi = true;
+    if (odd) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (mode == 1) {
+                lo[k] += plo[k];
+                hi[k] += phi[k];
+            } else if (mode == 2) {
+                lo[k] += phi[k];  // even lane's z+1 level is this lane's z level
+            } else if (mode == 3) {
+                hi[k] += plo[k];  // even lane's z level is this lane's z+1 level
+            }
+        }
+    } else {
+        emit_lo = mode == 0 || mode == 2;
+        emit_hi = mode == 0 || mode == 3;
+    }
+    float* g = p.grad_pad + gi;
+    const uint32_t off[4] = {0u, p.gz_x, p.gz_y, p.gz_y + p.gz_x};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        if (emit_lo) red_add_global(g + off[k], lo[k]);
+        if (emit_hi) red_add_global(g + off[k] + 1, hi[k]);
+    }
+}
+
+// GV: 0 = no volume gradient, 1 = scatter every sample's eight weights,
+// 2 = merge them across lane pairs first (scatter_cell_pairwise).
+template <bool CLAMP, int GV>
 __device__ __forceinline__ RayGrad march_grad(const RaySetup& r, const ViewGeo& vg,
                                               const FpArgs& p, float gs) {
     const float hx = p.W * 0.5f, hy = p.H * 0.5f, hz = p.D * 0.5f;
@@ -414,21 +471,26 @@ __device__ __forceinline__ RayGrad march_grad(const RaySetup& r, const ViewGeo& 
         rg.s2x = fmaf(gx, tau, rg.s2x);
         rg.s2y = fmaf(gy, tau, rg.s2y);
         rg.s2z = fmaf(gz, tau, rg.s2z);
-        if (GRADVOL) {
+        if (GV != 0) {
             // adjoint of the trilinear sample (fp.cu:231-240), padded z-fastest buffer
             const float mx = 1.0f - c.fx, my = 1.0f - c.fy, mz = 1.0f - c.fz;
             const float gy0 = gs * my, gy1 = gs * c.fy;
             const float w00 = gy0 * mx, w01 = gy0 * c.fx, w10 = gy1 * mx, w11 = gy1 * c.fx;
-            float* g0 = p.grad_pad + (c.bz + c.bx * p.gz_x + c.by * p.gz_y + p.gz_bias);
-            float* g1 = g0 + p.gz_y;
-            red_add_global(g0, w00 * mz);
-            red_add_global(g0 + 1, w00 * c.fz);
-            red_add_global(g0 + p.gz_x, w01 * mz);
-            red_add_global(g0 + p.gz_x + 1, w01 * c.fz);
-            red_add_global(g1, w10 * mz);
-            red_add_global(g1 + 1, w10 * c.fz);
-            red_add_global(g1 + p.gz_x, w11 * mz);
-            red_add_global(g1 + p.gz_x + 1, w11 * c.fz);
+            // (x, y) corner columns 00, 10, 01, 11 at the cell's z (lo) and z+1 (hi)
+            float lo[4] = {w00 * mz, w01 * mz, w10 * mz, w11 * mz};
+            float hi[4] = {w00 * c.fz, w01 * c.fz, w10 * c.fz, w11 * c.fz};
+            const uint32_t gi = c.bz + c.bx * p.gz_x + c.by * p.gz_y + p.gz_bias;
+            if (GV == 2) {
+                scatter_cell_pairwise(p, gi, lo, hi);
+            } else {
+                float* g = p.grad_pad + gi;
+                const uint32_t off[4] = {0u, p.gz_x, p.gz_y, p.gz_y + p.gz_x};
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    red_add_global(g + off[k], lo[k]);
+                    red_add_global(g + off[k] + 1, hi[k]);
+                }
+            }
         }
     }
     return rg;
@@ -446,29 +508,31 @@ __device__ __forceinline__ void ray_geometry_terms(const FpArgs& p, const ViewGe
     //   q = s1 - ((s1.d)/d_e) e_e   (so q.d = 0)
     // gives grad_origin_direct = G*q and grad_direction = G*(s2 + t_min*q):
     // the same values without the large t_min*s1 terms that cancel.
+    // (the multiply-adds are explicit, as in the ray set-up, so that every
+    // kernel that inlines this produces bitwise the same terms)
     float qx = rg.s1x, qy = rg.s1y, qz = rg.s1z;
-    if (r.entry_axis == 0) qx = -(rg.s1y * r.dy + rg.s1z * r.dz) / r.dx;
-    else if (r.entry_axis == 1) qy = -(rg.s1x * r.dx + rg.s1z * r.dz) / r.dy;
-    else if (r.entry_axis == 2) qz = -(rg.s1x * r.dx + rg.s1y * r.dy) / r.dz;
+    if (r.entry_axis == 0) qx = -fmaf(rg.s1y, r.dy, __fmul_rn(rg.s1z, r.dz)) / r.dx;
+    else if (r.entry_axis == 1) qy = -fmaf(rg.s1x, r.dx, __fmul_rn(rg.s1z, r.dz)) / r.dy;
+    else if (r.entry_axis == 2) qz = -fmaf(rg.s1x, r.dx, __fmul_rn(rg.s1y, r.dy)) / r.dz;
     const float G = gs * p.inv_voxel;
     const float godx = G * qx, gody = G * qy, godz = G * qz;
     // fp.cu:470-486: chain through direction = normalize(target - origin);
     // q is orthogonal to d, so only s2 loses its component along d.
-    const float ds2 = r.dx * rg.s2x + r.dy * rg.s2y + r.dz * rg.s2z;
+    const float ds2 = fmaf(r.dz, rg.s2z, fmaf(r.dx, rg.s2x, __fmul_rn(r.dy, rg.s2y)));
     const float k = G / r.len;
-    const float grx = k * (rg.s2x - r.dx * ds2 + r.tmin * qx);
-    const float gry = k * (rg.s2y - r.dy * ds2 + r.tmin * qy);
-    const float grz = k * (rg.s2z - r.dz * ds2 + r.tmin * qz);
+    const float grx = k * fmaf(r.tmin, qx, fmaf(-r.dx, ds2, rg.s2x));
+    const float gry = k * fmaf(r.tmin, qy, fmaf(-r.dy, ds2, rg.s2y));
+    const float grz = k * fmaf(r.tmin, qz, fmaf(-r.dz, ds2, rg.s2z));
     const float gox = godx - grx, goy = gody - gry, goz = godz - grz;
     // fp.cu:488-527: per-view geometry terms.
     const float u_phys = (u - vg.u0) * p.pixel_size;
     const float dOx = -vg.sod * vg.c, dOy = -vg.sod * vg.s;
-    const float dTx = -u_phys * vg.s - vg.dn * vg.c;
-    const float dTy = u_phys * vg.c - vg.dn * vg.s;
-    terms[0] = gox * dOx + goy * dOy + grx * dTx + gry * dTy;
-    terms[1] = grx * vg.s - gry * vg.c;
-    terms[2] = (gox + grx) * (-vg.s) + (goy + gry) * vg.c;
-    terms[3] = -p.pixel_size * (grx * vg.c + gry * vg.s);
+    const float dTx = fmaf(-u_phys, vg.s, -__fmul_rn(vg.dn, vg.c));
+    const float dTy = fmaf(u_phys, vg.c, -__fmul_rn(vg.dn, vg.s));
+    terms[0] = fmaf(gry, dTy, fmaf(grx, dTx, fmaf(goy, dOy, __fmul_rn(gox, dOx))));
+    terms[1] = fmaf(grx, vg.s, -__fmul_rn(gry, vg.c));
+    terms[2] = fmaf(goy + gry, vg.c, -__fmul_rn(gox + grx, vg.s));
+    terms[3] = -p.pixel_size * fmaf(grx, vg.c, __fmul_rn(gry, vg.s));
     terms[4] = -p.pixel_size * grz;
     terms[5] = gox;
     terms[6] = goy;
@@ -476,9 +540,9 @@ __device__ __forceinline__ void ray_geometry_terms(const FpArgs& p, const ViewGe
 }
 
 // The eight per-view geometry terms of one ray (zero for rays outside the
-// detector, missing the volume or with a zero upstream gradient); with
-// GRADVOL the ray's adjoint samples are scattered into p.grad_pad.
-template <bool GRADVOL>
+// detector, missing the volume or with a zero upstream gradient); with GV
+// (march_grad) the ray's adjoint samples are scattered into p.grad_pad.
+template <int GV>
 __device__ __forceinline__ void backward_ray(const FpArgs& p, const ViewGeo& vg, int a, int u,
                                              int v, float (&terms)[8]) {
 #pragma unroll
@@ -492,8 +556,8 @@ __device__ __forceinline__ void backward_ray(const FpArgs& p, const ViewGeo& vg,
         if (r.ok && r.hit) {
             const float gs = grad_out * p.step_size;
             const RayGrad rg = ray_inside_pad<false>(r, vg, p)
-                                   ? march_grad<false, GRADVOL>(r, vg, p, gs)
-                                   : march_grad<true, GRADVOL>(r, vg, p, gs);
+                                   ? march_grad<false, GV>(r, vg, p, gs)
+                                   : march_grad<true, GV>(r, vg, p, gs);
             ray_geometry_terms(p, vg, r, u, rg, gs, terms);
         }
     }
@@ -519,7 +583,7 @@ __device__ __forceinline__ void reduce_terms_to_partials(const float (&terms)[8]
     }
 }
 
-template <int TU, bool GRADVOL>
+template <int TU, int GV>
 __global__ void __launch_bounds__(256) fp_backward_kernel(FpArgs p) {
     constexpr int TV = 256 / TU;
     __shared__ ViewGeo s_view;
@@ -535,7 +599,7 @@ __global__ void __launch_bounds__(256) fp_backward_kernel(FpArgs p) {
     int u, v;
     tile_ray<TU>(tc, u, v);
     float terms[8];
-    backward_ray<GRADVOL>(p, vg, a, u, v, terms);
+    backward_ray<GV>(p, vg, a, u, v, terms);
     reduce_terms_to_partials(terms, s_red, p.partials + ((long long)a * tiles + tile) * 8);
 }
 
@@ -822,11 +886,12 @@ __global__ void __launch_bounds__(256, 6) batch_forward_kernel(BatchTables t) {
 
 template <int TU>
 __device__ __forceinline__ void backward_item(const FpArgs& p, const ViewGeo& vg,
-                                              const TileCoord& tc, float (&terms)[8]) {
+                                              const TileCoord& tc, int flags, float (&terms)[8]) {
     int u, v;
     tile_ray<TU>(tc, u, v);
-    if (p.grad_pad) backward_ray<true>(p, vg, tc.a, u, v, terms);
-    else backward_ray<false>(p, vg, tc.a, u, v, terms);
+    if (!p.grad_pad) backward_ray<0>(p, vg, tc.a, u, v, terms);
+    else if (flags & kBatchMerge) backward_ray<2>(p, vg, tc.a, u, v, terms);
+    else backward_ray<1>(p, vg, tc.a, u, v, terms);
 }
 
 __global__ void __launch_bounds__(256) batch_backward_kernel(BatchTables t) {
@@ -842,8 +907,8 @@ __global__ void __launch_bounds__(256) batch_backward_kernel(BatchTables t) {
         const ViewGeo vg = s_view;
         const TileCoord tc = s_tc;
         float terms[8];
-        if (s_tu == 8) backward_item<8>(p, vg, tc, terms);
-        else backward_item<4>(p, vg, tc, terms);
+        if (s_tu == 8) backward_item<8>(p, vg, tc, s_flags, terms);
+        else backward_item<4>(p, vg, tc, s_flags, terms);
         const long long tiles = fp_tiles_per_view_dev(p.U, p.V, s_tu);
         reduce_terms_to_partials(terms, s_red, p.partials + ((long long)tc.a * tiles + s_tile) * 8);
         __syncthreads();
@@ -901,15 +966,26 @@ template <int TU>
 int launch_backward_tu(const FpArgs& p, bool gradvol, cudaStream_t s) {
     DGC_TRACE(gradvol ? "fp_backward_kernel<gradvol>" : "fp_backward_kernel", s);
     const long long blocks = fp_tiles_per_view(p.U, p.V, TU) * (long long)p.A;
-    if (gradvol)
-        fp_backward_kernel<TU, true><<<(unsigned)blocks, 256, 0, s>>>(p);
+    if (!gradvol)
+        fp_backward_kernel<TU, 0><<<(unsigned)blocks, 256, 0, s>>>(p);
+    else if (fp_merge_scatter(p.U, p.V, p.H, p.W))
+        fp_backward_kernel<TU, 2><<<(unsigned)blocks, 256, 0, s>>>(p);
     else
-        fp_backward_kernel<TU, false><<<(unsigned)blocks, 256, 0, s>>>(p);
+        fp_backward_kernel<TU, 1><<<(unsigned)blocks, 256, 0, s>>>(p);
     DGC_LAUNCH_CHECK("fp_backward_kernel");
     return DGC_OK;
 }
 
 }  // namespace
+
+bool fp_merge_scatter(int U, int V, int H, int W) {
+    // DGC_SCATTER=plain|pairs overrides the choice (tests of both variants)
+    if (const char* e = std::getenv("DGC_SCATTER")) {
+        if (std::strcmp(e, "pairs") == 0) return true;
+        if (std::strcmp(e, "plain") == 0) return false;
+    }
+    return (long long)U * V >= 4LL * H * W;
+}
 
 long long fp_tiles_per_view(int U, int V, int tu) {
     const int tv = 256 / tu;

@@ -30,7 +30,7 @@ struct FpTile {
 };
 
 // One instance of a batched launch (an entry of the device-resident table).
-enum : int { kBatchDiv = 1, kBatchOff = 2 };
+enum : int { kBatchDiv = 1, kBatchOff = 2, kBatchMerge = 4 };
 constexpr int kFoldChunk = 2048;
 
 struct BatchInstance {
@@ -39,7 +39,8 @@ struct BatchInstance {
     float* grad_volume;    // [D][H][W]; null: no volume gradient
     GeometryGrad gout;     // eight [A] outputs
     int tile_fwd, tile_bwd;  // columns per CTA tile (forward 8/4/2, backward 8/4)
-    int flags;             // kBatchDiv (non power-of-two voxel) | kBatchOff (non-zero ROI offset)
+    int flags;             // kBatchDiv (non power-of-two voxel) | kBatchOff (non-zero ROI
+                           // offset) | kBatchMerge (lane-pair merged scatter)
     int quad_gx;           // blocks along x of the quads build
     long long tiles_bwd;   // backward tiles per view
 };
@@ -68,6 +69,10 @@ int fp_check_args(int D, int H, int W, int A, int U, int V, float pixel_size, fl
 
 void fp_fill_layout(FpArgs& p);
 long long fp_tiles_per_view(int U, int V, int tu);
+// Whether the volume-gradient scatter merges lane pairs first: it pays where
+// many rays cross each (x, y) column (U*V >= 4*H*W); elsewhere the shuffles
+// cost more than the reductions they save.
+bool fp_merge_scatter(int U, int V, int H, int W);
 int build_volume_quads(const float* vol, int D, int H, int W, float4* quads, cudaStream_t s);
 int fp_launch_forward(const FpArgs& p, const FpTile& tile, cudaStream_t s);
 int fp_launch_backward(const FpArgs& p, const FpTile& tile, bool gradvol, cudaStream_t s);
