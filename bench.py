@@ -57,15 +57,20 @@ def parse_args(argv=None):
                     help="override the view count (smaller cases for profiler captures)")
     ap.add_argument("--volume", type=int, default=None, help="override the cubic volume size")
     ap.add_argument("--detector", type=int, default=None, help="override the square detector size")
-    ap.add_argument("--workload", choices=["fdk256", "batch64", "calib", "tour"], default="fdk256",
+    ap.add_argument("--workload", choices=["fdk256", "batch64", "calib", "tour", "gemm"],
+                    default="fdk256",
                     help="fdk256: the FDK step (default); batch64: 64 uneven project+backward "
                          "instances, batched vs sequential; calib: calibration wall time to "
                          "0.1 px, learned warm start vs plain; tour: every kernel once on the "
-                         "fdk256 instance (profiler captures)")
+                         "fdk256 instance (profiler captures); gemm: the tcgen05 GEMM at "
+                         "8192^3 and at the network's largest layer shapes")
     ap.add_argument("--acq", choices=["half", "eval"], default="half",
                     help="calib: 256^3/360/384^2 (half) or 512^3/720/768^2 (eval)")
     ap.add_argument("--max-iterations", type=int, default=300, help="calib: iteration cap")
     ap.add_argument("--instances", type=int, default=64, help="batch64: number of instances")
+    ap.add_argument("--batch-set", choices=["config4", "small"], default="config4",
+                    help="batch64 shape sets: config4 (128^3..384x384x256, 90-720 views, "
+                         "256-512 detectors) or small (48^3..64x96x96, 30-90 views, 96-160)")
     ap.add_argument("--tune-cache", default=None, help="batch64: autotuner JSON cache path")
     args = ap.parse_args(argv)
     if args.views:
@@ -429,19 +434,24 @@ BATCH64 = dict(name="batch64: uneven instances, project + backward (volume and g
                volumes=[(128, 128, 128), (128, 192, 192), (256, 256, 256), (256, 384, 384)],
                views=[90, 180, 360, 720], detectors=[256, 384, 512], sid=1000.0, sod=600.0,
                voxel=1.0, step=0.5, seed=4)
+BATCH_SMALL = dict(BATCH64, name="batch64 small: many small uneven instances (hypotheses on "
+                                 "downsampled data), project + backward each",
+                   volumes=[(48, 48, 48), (64, 64, 64), (64, 96, 96)], views=[30, 60, 90],
+                   detectors=[96, 128, 160])
 
 
-def make_batch64(device, n, seed):
+def make_batch64(device, n, seed, c=None):
     """``n`` problems drawn from the seed: volume shape, views and detector U, V
-    independently; config-3 perturbations of the nominal circular geometry;
-    the pixel size makes the detector cover the magnified volume."""
+    independently from the shape set ``c`` (default BATCH64); config-3
+    perturbations of the nominal circular geometry; the pixel size makes the
+    detector cover the magnified volume."""
     import numpy as np
 
     from cbct_backprojector.batch import Problem
     from cbct_backprojector.calibration import perturb_geometry
     from cbct_backprojector.phantoms import circular_geometry, ellipsoid_phantom
 
-    c = BATCH64
+    c = BATCH64 if c is None else c
     rng = np.random.default_rng(seed)
     problems = []
     for i in range(n):
@@ -483,7 +493,8 @@ def run_batch64(args):
     torch.cuda.set_device(local)
     device = torch.device("cuda", local)
     dist = init_dist(world, "nccl")
-    problems = make_batch64(device, args.instances, BATCH64["seed"] + 1000 * rank)
+    shapes = BATCH64 if args.batch_set == "config4" else BATCH_SMALL
+    problems = make_batch64(device, args.instances, shapes["seed"] + 1000 * rank, shapes)
     R = sum(pr.rays for pr in problems)
     S = 0
     for pr in problems:
@@ -550,7 +561,7 @@ def run_batch64(args):
         "unit": "Grays/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": graph_ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": BATCH64["name"], "instances": len(problems),
+        "config": {"workload": shapes["name"], "instances": len(problems),
                    "rays": R, "samples": S, "l2": "flushed between timed steps (256 MiB write)",
                    "parallelism": f"independent batches x{world}"},
         "sequential_plain_calls": {"ms_per_step": seq_ms,
@@ -680,8 +691,60 @@ def run_tour(args):
     return 0
 
 
+# --------------------------------------------------------------------- gemm
+
+
+def run_gemm(args):
+    """TFLOP/s of the tcgen05 BF16 GEMM (fp32 out) against the measured cuBLAS
+    bf16 peak: 8192^3, and the forward / weight-gradient products of the
+    network's widest layer on 360 views (M = 360*6*6, N = 256, K = 9*256;
+    M = 256, N = 2304, K = 360*6*6)."""
+    import torch
+
+    from cbct_backprojector import _native
+    from cbct_backprojector.warmstart import gemm
+
+    torch.cuda.set_device(0)
+    peak = None
+    try:
+        peak = float(json.loads((ROOT / "MEASURED_PEAKS.json").read_text())["bf16_tflops"])
+    except Exception:
+        pass
+    shapes = [(8192, 8192, 8192), (360 * 36, 256, 2304), (256, 2304, 360 * 36)]
+    out = {}
+    g = torch.Generator(device="cuda").manual_seed(0)
+    for M, N, K in shapes:
+        A = torch.randn(M, K, device="cuda", generator=g).to(torch.bfloat16)
+        B = torch.randn(N, K, device="cuda", generator=g).to(torch.bfloat16)
+        C = torch.empty(M, N, device="cuda")
+        for _ in range(max(1, args.warmup)):
+            gemm(A, B, out=C)
+        torch.cuda.synchronize()
+        times = []
+        for _ in range(max(1, args.steps)):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            gemm(A, B, out=C)
+            b.record()
+            b.synchronize()
+            times.append(a.elapsed_time(b))
+        ms = sorted(times)[len(times) // 2]
+        with _native.trace() as tr:
+            gemm(A, B, out=C)
+            torch.cuda.synchronize()
+        tf = 2.0 * M * N * K / (ms * 1e-3) / 1e12
+        err = float(((C - A.float() @ B.float().t()).abs().max()).item())
+        out[f"{M}x{N}x{K}"] = {"ms": ms, "tflops": tf, "kernels": sorted({n for n, _ in tr.records}),
+                               "frac_of_measured_peak":
+                               None if peak is None else tf / peak, "max_abs_err": err}
+    print(json.dumps({"workload": "tcgen05 bf16 GEMM", "peak_bf16_tflops": peak, "shapes": out}))
+    return 0
+
+
 def main(argv=None):
     args = parse_args(argv)
+    if args.workload == "gemm":
+        return run_gemm(args)
     if args.workload == "tour":
         return run_tour(args)
     if args.workload == "calib":

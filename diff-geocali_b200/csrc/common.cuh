@@ -137,6 +137,19 @@ __device__ __forceinline__ f32x2 fma2(f32x2 a, f32x2 b, f32x2 c) {
     return r;
 }
 
+// Per-lane a + b rounded toward minus infinity (the packed __fadd_rd).
+__device__ __forceinline__ f32x2 add2_rd(f32x2 a, f32x2 b) {
+    f32x2 r;
+    asm("add.rm.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+
+__device__ __forceinline__ uint2 unpack2_bits(f32x2 v) {
+    uint2 r;
+    asm("mov.b64 {%0, %1}, %2;" : "=r"(r.x), "=r"(r.y) : "l"(v));
+    return r;
+}
+
 // Per-lane lerp of two packed pairs with one weight: a + w*(b-a).
 __device__ __forceinline__ f32x2 lerp2(f32x2 a, f32x2 b, f32x2 w) { return fma2(w, sub2(b, a), a); }
 

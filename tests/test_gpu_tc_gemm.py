@@ -1,6 +1,7 @@
 """The tcgen05 BF16 GEMM (dgc_gemm_bf16) against an FP32 matmul of the same
-bf16 inputs: ragged M/N/K, both tile widths, bias + ReLU, bf16 output,
-accumulation into fp32."""
+bf16 inputs: ragged M/N/K, all three tile widths, bias + ReLU, bf16 output,
+accumulation into fp32, split-K; the TMA pipeline (default) and the cp.async
+pipeline (DGC_GEMM=cpasync)."""
 
 import pytest
 import torch
@@ -28,15 +29,24 @@ def run(A, B, C, bias=None, relu=False, accumulate=False, alpha=1.0):
 
 @pytest.mark.parametrize("M,N,K", [(128, 128, 64), (128, 64, 16), (300, 200, 72), (1000, 64, 256),
                                    (2048, 256, 2304), (7, 24, 8), (513, 136, 136),
-                                   (64, 200, 8192), (32, 96, 4104)])
-def test_gemm_matches_fp32(M, N, K):
-    """The last two shapes take the split-K path (few output tiles, long K)."""
+                                   (64, 200, 8192), (32, 96, 4104), (18944, 264, 72)])
+@pytest.mark.parametrize("pipeline", ["tma", "cpasync"])
+def test_gemm_matches_fp32(M, N, K, pipeline, monkeypatch):
+    """(64, 200, 8192) and (32, 96, 4104) take the split-K path (few output
+    tiles, long K); (18944, 264, 72) the 256-column tiles."""
+    if pipeline == "cpasync":
+        monkeypatch.setenv("DGC_GEMM", "cpasync")
     g = torch.Generator(device="cuda").manual_seed(M * 7 + N)
     A = torch.randn(M, K, device="cuda", generator=g).to(torch.bfloat16)
     B = torch.randn(N, K, device="cuda", generator=g).to(torch.bfloat16)
     want = A.float() @ B.float().t()
     C = torch.full((M, N), float("nan"), device="cuda")
-    got = run(A, B, C)
+    from cbct_backprojector import _native
+
+    with _native.trace() as tr:
+        got = run(A, B, C)
+    want_kernel = "tc_gemm_tma_kernel" if pipeline == "tma" else "tc_gemm_kernel"
+    assert {n for n, _ in tr.records} == {want_kernel}
     scale = (A.float().abs() @ B.float().abs().t()).clamp_min(1.0)
     assert ((got - want).abs() / scale).max().item() < 1e-5
 
