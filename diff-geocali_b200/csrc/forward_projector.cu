@@ -765,6 +765,240 @@ __global__ void __launch_bounds__(256) sum_partials_kernel(const double* __restr
     }
 }
 
+// ---------------------------------------------------------------------------
+// Backward with the volume gradient accumulated in shared-memory bricks
+// ---------------------------------------------------------------------------
+//
+// The 256 rays of a CTA (one view, 8 detector columns x 32 rows) form a thin,
+// nearly parallel bundle.  Their march is cut into slabs of kBrickL voxel
+// cells along the main horizontal axis of the bundle (x or y, whichever the
+// rays run along more); all threads process one slab at a time, in the
+// direction of travel, each continuing its own t recurrence.  The trilinear
+// weights of a slab's samples are added into a shared-memory brick that
+// covers the slab's part of the bundle (bounded from the four corner rays of
+// the tile, which hold the extreme cross-axis positions), and after a barrier
+// the brick is flushed to the padded gradient with one reduction per
+// non-zero cell.  A sample whose cell falls outside the brick (only through
+// rounding at its edge, or when the bundle is too wide for the buffer) is
+// scattered to global memory directly.  The samples, their order within a
+// ray and the geometry sums are those of fp_backward_kernel; only the order
+// of the float additions into the volume gradient differs.
+
+constexpr int kBrickL = 8;         // cells per slab along the main axis
+constexpr int kBrickCap = 12288;   // floats of the brick buffer (48 KiB)
+
+struct BrickSlab {
+    int m_lo, c_lo, z_lo;  // padded indices of the brick's first cell
+    int bc, bz;            // extents along the cross axis and z (main: kBrickL + 1)
+    int ok;                // the brick fits the buffer
+};
+
+// Padded-voxel cross-axis and z ranges that the corner rays cover between
+// main-axis coordinates xm0 and xm1 (voxel units), with one cell of margin.
+__device__ __forceinline__ void corner_extent(const float (&dir)[4][3], const ViewGeo& vg,
+                                              const FpArgs& p, int axis, float xm0, float xm1,
+                                              BrickSlab& b) {
+    const int n_m = axis == 0 ? p.W : p.H, n_c = axis == 0 ? p.H : p.W;
+    const float off_m = axis == 0 ? p.off_x : p.off_y, off_c = axis == 0 ? p.off_y : p.off_x;
+    const float o_m = axis == 0 ? vg.ox : vg.oy, o_c = axis == 0 ? vg.oy : vg.ox;
+    float cmin = FLT_MAX, cmax = -FLT_MAX, zmin = FLT_MAX, zmax = -FLT_MAX;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const float dm = axis == 0 ? dir[i][0] : dir[i][1];
+        const float dc = axis == 0 ? dir[i][1] : dir[i][0];
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            const float xm = e ? xm1 : xm0;
+            const float pm = (xm - n_m * 0.5f) * p.voxel_size + off_m;
+            const float t = (pm - o_m) / dm;
+            const float xc = (o_c + t * dc - off_c) / p.voxel_size + n_c * 0.5f;
+            const float xz = (vg.oz + t * dir[i][2] - p.off_z) / p.voxel_size + p.D * 0.5f;
+            cmin = fminf(cmin, xc);
+            cmax = fmaxf(cmax, xc);
+            zmin = fminf(zmin, xz);
+            zmax = fmaxf(zmax, xz);
+        }
+    }
+    // cell floors, one cell of margin, clamped like the samples ([-1, n-1])
+    const int fc0 = max(-1, min(n_c - 1, (int)floorf(cmin) - 1));
+    const int fc1 = max(-1, min(n_c - 1, (int)floorf(cmax) + 1));
+    const int fz0 = max(-1, min(p.D - 1, (int)floorf(zmin) - 1));
+    const int fz1 = max(-1, min(p.D - 1, (int)floorf(zmax) + 1));
+    b.c_lo = fc0 + 1;
+    b.z_lo = fz0 + 1;
+    b.bc = fc1 - fc0 + 2;  // corners of cells fc0..fc1
+    b.bz = fz1 - fz0 + 2;
+    const long long cells = (long long)(kBrickL + 1) * b.bc * b.bz;
+    b.ok = (isfinite(cmin) && isfinite(cmax) && isfinite(zmin) && isfinite(zmax) &&
+            cells <= kBrickCap) ? 1 : 0;
+}
+
+// Samples of one ray inside main-axis floors [f_lo, f_hi] (in travel order),
+// continuing (t, n); stops at the first sample of a later slab.
+template <bool CLAMP>
+__device__ __forceinline__ void march_grad_slab(const RaySetup& r, const ViewGeo& vg,
+                                                const FpArgs& p, const XYPacks& k, float gs,
+                                                int axis, int dir, int f_lo, int f_hi,
+                                                const BrickSlab& b, float* brick, float& t,
+                                                int& n, int nmax, RayGrad& rg) {
+    const float4* __restrict__ Q = p.quads;
+#pragma unroll 1
+    for (; t <= r.tmax && n < nmax; t += p.step_size, ++n) {
+        const Cell c = sample_cell<CLAMP, false, true, false>(t, r, vg, p, k);
+        const int fx = (int)(c.bx - kFloorMagicBits), fy = (int)(c.by - kFloorMagicBits);
+        const int fz = (int)(c.bz - kFloorMagicBits);
+        const int fm = axis == 0 ? fx : fy, fcr = axis == 0 ? fy : fx;
+        if (dir > 0 ? fm > f_hi : fm < f_lo) break;  // belongs to a later slab
+        const uint32_t qi = quad_index(c, p);
+        const float4 q0 = __ldg(Q + qi);
+        const float4 q1 = __ldg(Q + qi + 1);
+        const float gx = lerpf(lerpf(q0.z - q0.x, q0.w - q0.y, c.fy),
+                               lerpf(q1.z - q1.x, q1.w - q1.y, c.fy), c.fz);
+        const float gy = lerpf(lerpf(q0.y - q0.x, q0.w - q0.z, c.fx),
+                               lerpf(q1.y - q1.x, q1.w - q1.z, c.fx), c.fz);
+        const float gz = lerpf(lerpf(q1.x - q0.x, q1.z - q0.z, c.fx),
+                               lerpf(q1.y - q0.y, q1.w - q0.w, c.fx), c.fy);
+        const float tau = t - r.tmin;
+        rg.s1x += gx;
+        rg.s1y += gy;
+        rg.s1z += gz;
+        rg.s2x = fmaf(gx, tau, rg.s2x);
+        rg.s2y = fmaf(gy, tau, rg.s2y);
+        rg.s2z = fmaf(gz, tau, rg.s2z);
+        // adjoint of the trilinear sample (fp.cu:231-240)
+        const float mx = 1.0f - c.fx, my = 1.0f - c.fy, mz = 1.0f - c.fz;
+        const float gy0 = gs * my, gy1 = gs * c.fy;
+        const float w00 = gy0 * mx, w01 = gy0 * c.fx, w10 = gy1 * mx, w11 = gy1 * c.fx;
+        const int im = fm + 1 - b.m_lo, ic = fcr + 1 - b.c_lo, iz = fz + 1 - b.z_lo;
+        if (b.ok && im >= 0 && im < kBrickL && ic >= 0 && ic <= b.bc - 2 && iz >= 0 &&
+            iz <= b.bz - 2) {
+            // brick cell (im, ic, iz) at (im * bc + ic) * bz + iz; x/y map to m/c
+            const int sm = b.bc * b.bz, sc = b.bz;
+            const int sx = axis == 0 ? sm : sc, sy = axis == 0 ? sc : sm;
+            float* g = brick + (im * b.bc + ic) * b.bz + iz;
+            atomicAdd(g, w00 * mz);
+            atomicAdd(g + 1, w00 * c.fz);
+            atomicAdd(g + sx, w01 * mz);
+            atomicAdd(g + sx + 1, w01 * c.fz);
+            atomicAdd(g + sy, w10 * mz);
+            atomicAdd(g + sy + 1, w10 * c.fz);
+            atomicAdd(g + sx + sy, w11 * mz);
+            atomicAdd(g + sx + sy + 1, w11 * c.fz);
+        } else {
+            float* g0 = p.grad_pad + (c.bz + c.bx * p.gz_x + c.by * p.gz_y + p.gz_bias);
+            float* g1 = g0 + p.gz_y;
+            red_add_global(g0, w00 * mz);
+            red_add_global(g0 + 1, w00 * c.fz);
+            red_add_global(g0 + p.gz_x, w01 * mz);
+            red_add_global(g0 + p.gz_x + 1, w01 * c.fz);
+            red_add_global(g1, w10 * mz);
+            red_add_global(g1 + 1, w10 * c.fz);
+            red_add_global(g1 + p.gz_x, w11 * mz);
+            red_add_global(g1 + p.gz_x + 1, w11 * c.fz);
+        }
+    }
+}
+
+template <int TU>
+__global__ void __launch_bounds__(256) fp_backward_brick_kernel(FpArgs p) {
+    constexpr int TV = 256 / TU;
+    extern __shared__ float brick[];  // kBrickCap floats
+    __shared__ ViewGeo s_view;
+    __shared__ double s_red[8][8];
+    __shared__ float s_dir[4][3];
+    __shared__ int s_axis, s_dirsign, s_nslab;
+    __shared__ BrickSlab s_slab;
+    const int tiles_u = (p.U + TU - 1) / TU;
+    const int tiles = tiles_u * ((p.V + TV - 1) / TV);
+    const TileCoord tc = tile_coord(p, tiles_u);
+    const int a = tc.a;
+    const int tile = tc.tv * tiles_u + tc.tu;
+    if (threadIdx.x == 0) load_view(p.g, a, s_view);
+    for (int i = threadIdx.x; i < kBrickCap; i += 256) brick[i] = 0.0f;
+    __syncthreads();
+    const ViewGeo vg = s_view;
+    if (threadIdx.x == 0) {
+        // corner rays of the tile (clamped to the detector) and the main axis
+        const int u0 = tc.tu * TU, u1 = min(p.U - 1, u0 + TU - 1);
+        const int v0 = tc.tv * TV, v1 = min(p.V - 1, v0 + TV - 1);
+        float sx = 0.0f, sy = 0.0f;
+        for (int i = 0; i < 4; ++i) {
+            const RaySetup cr = setup_ray(vg, (i & 1) ? u1 : u0, (i & 2) ? v1 : v0, p);
+            s_dir[i][0] = cr.dx;
+            s_dir[i][1] = cr.dy;
+            s_dir[i][2] = cr.dz;
+            sx += cr.dx;
+            sy += cr.dy;
+        }
+        const int axis = fabsf(sx) >= fabsf(sy) ? 0 : 1;
+        s_axis = axis;
+        s_dirsign = (axis == 0 ? sx : sy) >= 0.0f ? 1 : -1;
+        s_nslab = ((axis == 0 ? p.W : p.H) + 1 + kBrickL - 1) / kBrickL;
+    }
+    __syncthreads();
+    const int axis = s_axis, dir = s_dirsign, nslab = s_nslab;
+    int u, v;
+    tile_ray<TU>(tc, u, v);
+
+    float terms[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    const bool in_range = u < p.U && v < p.V;
+    const float grad_out =
+        in_range ? p.grad_projections[((long long)a * p.U + u) * p.V + v] : 0.0f;
+    RaySetup r = setup_ray(vg, in_range ? u : 0, in_range ? v : 0, p);
+    // fp.cu:381 -- rays with a zero upstream gradient contribute nothing.
+    const bool active = in_range && grad_out != 0.0f && r.ok && r.hit;
+    const bool inside = active && ray_inside_pad<false>(r, vg, p);
+    const XYPacks k = make_xy_packs(r, vg, p);
+    const float gs = grad_out * p.step_size;
+    const int nmax = active ? step_bound(r, p.step_size) : 0;
+    float t = r.tmin;
+    int n = 0;
+    RayGrad rg{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+
+    for (int si = 0; si < nslab; ++si) {
+        const int sl = dir > 0 ? si : nslab - 1 - si;
+        const int f_lo = -1 + sl * kBrickL, f_hi = f_lo + kBrickL - 1;
+        if (threadIdx.x == 0) {
+            BrickSlab b;
+            b.m_lo = f_lo + 1;
+            corner_extent(s_dir, vg, p, axis, (float)f_lo, (float)(f_hi + 1), b);
+            s_slab = b;
+        }
+        __syncthreads();
+        const BrickSlab b = s_slab;
+        if (active) {
+            if (inside)
+                march_grad_slab<false>(r, vg, p, k, gs, axis, dir, f_lo, f_hi, b, brick, t, n,
+                                       nmax, rg);
+            else
+                march_grad_slab<true>(r, vg, p, k, gs, axis, dir, f_lo, f_hi, b, brick, t, n,
+                                      nmax, rg);
+        }
+        __syncthreads();
+        if (b.ok) {
+            // flush: one reduction per non-zero brick cell, z fastest (coalesced)
+            const int cells = (kBrickL + 1) * b.bc * b.bz;
+            for (int i = threadIdx.x; i < cells; i += 256) {
+                const float val = brick[i];
+                if (val != 0.0f) {
+                    brick[i] = 0.0f;
+                    const int iz = i % b.bz;
+                    const int rest = i / b.bz;
+                    const int ic = rest % b.bc, im = rest / b.bc;
+                    const int pm = b.m_lo + im, pc = b.c_lo + ic, pz = b.z_lo + iz;
+                    const int xp = axis == 0 ? pm : pc, yp = axis == 0 ? pc : pm;
+                    if (xp <= p.W + 1 && yp <= p.H + 1 && pz <= p.D + 1)
+                        red_add_global(p.grad_pad + ((long long)yp * (p.W + 2) + xp) * (p.D + 2) + pz,
+                                       val);
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if (active) ray_geometry_terms(p, vg, r, u, rg, gs, terms);
+    reduce_terms_to_partials(terms, s_red, p.partials + ((long long)a * tiles + tile) * 8);
+}
+
 // Per-view sum of the CTA partials, warp k owning gradient k (fixed order).
 __global__ void __launch_bounds__(256) reduce_view_partials_kernel(const double* __restrict__ partials,
                                                                    int tiles, GeometryGrad out) {
@@ -1002,7 +1236,23 @@ template <int TU>
 int launch_backward_tu(const FpArgs& p, bool gradvol, cudaStream_t s) {
     DGC_TRACE(gradvol ? "fp_backward_kernel<gradvol>" : "fp_backward_kernel", s);
     const long long blocks = fp_tiles_per_view(p.U, p.V, TU) * (long long)p.A;
-    if (!gradvol)
+    // DGC_SCATTER=brick selects the shared-memory brick adjoint.  It is not
+    // the default: measured 1.7-2.1x slower than the direct scatter
+    // (204 vs 117 ms at 256^3 / 360 x 384^2): the slab barriers hold the
+    // bundle's fastest rays back, and the shared-memory additions cost about
+    // what the L2 reductions they replace cost.
+    const char* e = std::getenv("DGC_SCATTER");
+    const bool brick = gradvol && e && std::strcmp(e, "brick") == 0;
+    if (brick) {
+        constexpr int smem = kBrickCap * (int)sizeof(float);
+        static bool configured = false;
+        if (!configured) {
+            DGC_CUDA(cudaFuncSetAttribute(fp_backward_brick_kernel<TU>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+            configured = true;
+        }
+        fp_backward_brick_kernel<TU><<<(unsigned)blocks, 256, smem, s>>>(p);
+    } else if (!gradvol)
         fp_backward_kernel<TU, 0><<<(unsigned)blocks, 256, 0, s>>>(p);
     else if (fp_merge_scatter(p.U, p.V, p.H, p.W))
         fp_backward_kernel<TU, 2><<<(unsigned)blocks, 256, 0, s>>>(p);
@@ -1015,7 +1265,7 @@ int launch_backward_tu(const FpArgs& p, bool gradvol, cudaStream_t s) {
 }  // namespace
 
 bool fp_merge_scatter(int U, int V, int H, int W) {
-    // DGC_SCATTER=plain|pairs overrides the choice (tests of both variants)
+    // DGC_SCATTER=plain|pairs overrides the choice (tests of the variants)
     if (const char* e = std::getenv("DGC_SCATTER")) {
         if (std::strcmp(e, "pairs") == 0) return true;
         if (std::strcmp(e, "plain") == 0) return false;
