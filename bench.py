@@ -224,13 +224,15 @@ def measured_peak_hbm():
 # ------------------------------------------------------------- CPU baseline
 
 
-def cpu_baseline_sample(vol_np, geom_np, threads=None):
+def cpu_baseline_sample(vol_np, geom_np, threads=None, fwd_rays=None, filt_views=1, slab=4,
+                        bp_views=None):
     """Time the FP64 oracle (a port of the reference's CPU checks) on a bounded sample.
 
-    Sample: the forward projection of 2 full views (2 x 384^2 rays), the FDK
-    filter of 2 views, and the backprojection of an 8-slice z-slab over all 360
-    views.  Each part is scaled to the full step by its share of the work.
-    Returns (seconds per full step, threads used, description).
+    Sample: the forward projection of the first ``fwd_rays`` rays of view 0
+    (default one full view), the FDK filter of ``filt_views`` views, and the
+    backprojection of a ``slab``-slice z-slab over the first ``bp_views``
+    views (default all).  Each part is scaled to the full step by its share of
+    the work.  Returns (seconds per full step, threads used, description).
     """
     import numpy as np
 
@@ -240,25 +242,26 @@ def cpu_baseline_sample(vol_np, geom_np, threads=None):
         oracle.set_num_threads(threads)
     w = WORKLOAD
     A, U, V = w["A"], w["U"], w["V"]
-    nv = 2
+    fwd_rays = U * V if fwd_rays is None else int(fwd_rays)
+    bp_views = A if bp_views is None else int(bp_views)
     t0 = time.perf_counter()
-    rays = np.arange(0, nv * U * V, dtype=np.int64)
+    rays = np.arange(0, fwd_rays, dtype=np.int64)
     oracle.project_rays(vol_np, geom_np, w["pixel"], U, V, w["step"], w["voxel"], rays, mode=1)
-    t_fwd = (time.perf_counter() - t0) * (A / nv)
-    proj_part = np.ones((nv, U, V), np.float32)
+    t_fwd = (time.perf_counter() - t0) * (A * U * V / fwd_rays)
+    proj_part = np.ones((filt_views, U, V), np.float32)
     t0 = time.perf_counter()
-    filt = oracle.fdk_filter(proj_part, w["pixel"], geom_np[2][:nv], geom_np[1][:nv], w["alpha"])
-    t_filt = (time.perf_counter() - t0) * (A / nv)
-    slab = 8
-    proj_all = np.broadcast_to(filt[:1], (A, U, V))
+    filt = oracle.fdk_filter(proj_part, w["pixel"], geom_np[2][:filt_views],
+                             geom_np[1][:filt_views], w["alpha"])
+    t_filt = (time.perf_counter() - t0) * (A / filt_views)
+    proj_all = np.broadcast_to(filt[:1], (bp_views, U, V))
     t0 = time.perf_counter()
     # the central slab: slab voxel z' sits where full-volume voxel D/2 - slab/2 + z' does
-    oracle.backproject(proj_all, geom_np, w["pixel"], (slab, w["H"], w["W"]), w["voxel"],
-                       offset=(0.0, 0.0, 0.0))
-    t_bp = (time.perf_counter() - t0) * (w["D"] / slab)
-    desc = (f"FP64 oracle on {oracle.num_threads()} threads: forward of {nv} full views, "
-            f"filter of {nv} views, backprojection of a {slab}-slice slab over {A} views; "
-            "each scaled to the full step")
+    oracle.backproject(proj_all, [g[:bp_views] for g in geom_np], w["pixel"],
+                       (slab, w["H"], w["W"]), w["voxel"], offset=(0.0, 0.0, 0.0))
+    t_bp = (time.perf_counter() - t0) * (w["D"] / slab) * (A / bp_views)
+    desc = (f"FP64 oracle on {oracle.num_threads()} threads: forward of {fwd_rays} rays of one "
+            f"view, filter of {filt_views} view(s), backprojection of a {slab}-slice slab over "
+            f"{bp_views} views; each scaled to the full step")
     return t_fwd + t_filt + t_bp, oracle.num_threads(), desc
 
 
@@ -283,12 +286,15 @@ def run_reference(args):
                             voxel_size=w["voxel"], device="cpu").numpy()
     geom = [g.numpy().astype(np.float64) for g in
             circular_geometry(w["A"], w["U"], w["V"], w["sid"], w["sod"], w["pixel"], device="cpu")]
+    # a small sample per step (about 2-3 s of host work), so that the driver's
+    # --steps/--warmup run ends within minutes
+    sample = dict(fwd_rays=w["U"] * w["V"] // 8, filt_views=1, slab=1, bp_views=w["A"] // 4)
     for _ in range(args.warmup):
-        cpu_baseline_sample(vol, geom)
+        cpu_baseline_sample(vol, geom, **sample)
     times = []
     threads, desc = 1, ""
     for _ in range(args.steps):
-        t, threads, desc = cpu_baseline_sample(vol, geom)
+        t, threads, desc = cpu_baseline_sample(vol, geom, **sample)
         times.append(t)
     t_step = sum(times) / len(times)
     rays = w["A"] * w["U"] * w["V"]

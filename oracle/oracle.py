@@ -61,6 +61,8 @@ def _load():
         lib.oracle_fdk_filter.argtypes = [_dp, _c_int, _c_int, _c_int, _c_d, _dp, _dp, _c_d, _dp]
         lib.oracle_num_threads.restype = _c_int
         lib.oracle_set_num_threads.argtypes = [_c_int]
+        env = os.environ.get("DGC_ORACLE_THREADS")
+        lib.oracle_set_num_threads(int(env) if env else usable_cpus())
         _lib = lib
     return _lib
 
@@ -214,8 +216,23 @@ def reconstruct_fdk(projections, geometry, pixel_size, volume_shape, voxel_size,
 __all__ = [
     "build", "num_threads", "set_num_threads", "project", "project_rays", "sample_counts",
     "ray_traces", "project_backward", "backproject", "backproject_backward", "fdk_taps", "fdk_filter",
-    "reconstruct_fdk",
+    "reconstruct_fdk", "usable_cpus",
 ]
 
-if os.environ.get("DGC_ORACLE_THREADS"):
-    set_num_threads(int(os.environ["DGC_ORACLE_THREADS"]))
+
+def usable_cpus() -> int:
+    """CPUs this process may use: its affinity set, capped by a cgroup-v2 CPU
+    quota (cpu.max) when one is set -- the count of online processors can be
+    far larger inside a container."""
+    try:
+        n = len(os.sched_getaffinity(0))
+    except (AttributeError, OSError):
+        n = os.cpu_count() or 1
+    try:
+        quota, period = open("/sys/fs/cgroup/cpu.max").read().split()[:2]
+        if quota != "max":
+            n = min(n, max(1, -(-int(quota) // int(period))))
+    except (OSError, ValueError):
+        pass
+    return max(1, n)
+
