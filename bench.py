@@ -286,9 +286,9 @@ def run_reference(args):
                             voxel_size=w["voxel"], device="cpu").numpy()
     geom = [g.numpy().astype(np.float64) for g in
             circular_geometry(w["A"], w["U"], w["V"], w["sid"], w["sod"], w["pixel"], device="cpu")]
-    # a small sample per step (about 2-3 s of host work), so that the driver's
-    # --steps/--warmup run ends within minutes
-    sample = dict(fwd_rays=w["U"] * w["V"] // 8, filt_views=1, slab=1, bp_views=w["A"] // 4)
+    # a small sample per step (a few seconds of host work), so that the
+    # driver's --steps/--warmup run ends within minutes
+    sample = dict(fwd_rays=w["U"] * w["V"] // 2, filt_views=1, slab=2, bp_views=w["A"] // 2)
     for _ in range(args.warmup):
         cpu_baseline_sample(vol, geom, **sample)
     times = []
