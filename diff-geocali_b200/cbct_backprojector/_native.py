@@ -74,6 +74,7 @@ SIGNATURES = {
     "dgc_gemm_bf16": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _I, _I, _I, _I, _I, _F, _P, _P]),
     "dgc_im2col_nhwc_bf16": (_I, [_P, _I, _I, _I, _I, _I, _I, _I, _I, _P, _I, _P]),
     "dgc_col2im_nhwc_f32": (_I, [_P, _I, _I, _I, _I, _I, _I, _I, _I, _I, _P, _P]),
+    "dgc_preprocess": (_I, [_P, _P, _P, _I, _I, _I, _I, _F, _P, _P]),
     "dgc_batch_workspace_bytes": (_S, [ctypes.POINTER(FpInstance), _I]),
     "dgc_batch_prepare": (_I, [ctypes.POINTER(FpInstance), _I, _P, _S, ctypes.POINTER(BatchPlan),
                                _P]),

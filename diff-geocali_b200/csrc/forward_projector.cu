@@ -486,7 +486,7 @@ __device__ __forceinline__ void scatter_cell_pairwise(const FpArgs& p, uint32_t 
 template <bool CLAMP, int GV>
 __device__ __forceinline__ RayGrad march_grad(const RaySetup& r, const ViewGeo& vg,
                                               const FpArgs& p, float gs) {
-    const float4* __restrict__ Q = p.quads;
+    const ulonglong2* __restrict__ Q = reinterpret_cast<const ulonglong2*>(p.quads);
     const XYPacks k = make_xy_packs(r, vg, p);
     RayGrad rg{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     const int nmax = step_bound(r, p.step_size);
@@ -496,16 +496,20 @@ __device__ __forceinline__ RayGrad march_grad(const RaySetup& r, const ViewGeo& 
     for (; t <= r.tmax && n < nmax; t += p.step_size, ++n) {
         const Cell c = sample_cell<CLAMP, false, true, false>(t, r, vg, p, k);
         const uint32_t qi = quad_index(c, p);
-        const float4 q0 = __ldg(Q + qi);
-        const float4 q1 = __ldg(Q + qi + 1);
-        // d/dx, d/dy, d/dz of the trilinear interpolant (voxel units); quad
-        // components are (x0y0, x0y1, x1y0, x1y1)
-        const float gx = lerpf(lerpf(q0.z - q0.x, q0.w - q0.y, c.fy),
-                               lerpf(q1.z - q1.x, q1.w - q1.y, c.fy), c.fz);
-        const float gy = lerpf(lerpf(q0.y - q0.x, q0.w - q0.z, c.fx),
-                               lerpf(q1.y - q1.x, q1.w - q1.z, c.fx), c.fz);
-        const float gz = lerpf(lerpf(q1.x - q0.x, q1.z - q0.z, c.fx),
-                               lerpf(q1.y - q0.y, q1.w - q0.w, c.fx), c.fy);
+        const ulonglong2 q0 = __ldg(Q + qi);
+        const ulonglong2 q1 = __ldg(Q + qi + 1);
+        // d/dx, d/dy, d/dz of the trilinear interpolant (voxel units), from
+        // packed (y0, y1) pairs: .x of a quad is x0, .y is x1
+        const f32x2 wx = pack2(c.fx, c.fx), wz = pack2(c.fz, c.fz);
+        const f32x2 d0 = sub2(q0.y, q0.x), d1 = sub2(q1.y, q1.x);  // x1 - x0
+        const f32x2 e0 = fma2(wx, d0, q0.x), e1 = fma2(wx, d1, q1.x);
+        const f32x2 ez = sub2(e1, e0);
+        const float2 e = unpack2(fma2(wz, ez, e0));
+        const float2 dx = unpack2(fma2(wz, sub2(d1, d0), d0));
+        const float2 dz = unpack2(ez);
+        const float gx = lerpf(dx.x, dx.y, c.fy);
+        const float gy = e.y - e.x;
+        const float gz = lerpf(dz.x, dz.y, c.fy);
         const float tau = t - r.tmin;
         rg.s1x += gx;
         rg.s1y += gy;
@@ -672,20 +676,24 @@ __device__ __forceinline__ RayValueGrad march_value_grad(const RaySetup& r, cons
         const uint32_t qi = quad_index(c, p);
         const ulonglong2 q0 = __ldg(Q + qi);
         const ulonglong2 q1 = __ldg(Q + qi + 1);
-        const f32x2 wx = pack2(c.fx, c.fx);
-        const f32x2 e0 = lerp2(q0.x, q0.y, wx);
-        const f32x2 e1 = lerp2(q1.x, q1.y, wx);
-        const float2 e = unpack2(lerp2(e0, e1, pack2(c.fz, c.fz)));
+        // value: exactly the forward kernel's packed lerps (lerp2(a, b, w) =
+        // fma2(w, b - a, a)), keeping the intermediate pairs
+        const f32x2 wx = pack2(c.fx, c.fx), wz = pack2(c.fz, c.fz);
+        const f32x2 d0 = sub2(q0.y, q0.x);  // x1 - x0 at (y0, y1), z0
+        const f32x2 d1 = sub2(q1.y, q1.x);  // x1 - x0 at (y0, y1), z1
+        const f32x2 e0 = fma2(wx, d0, q0.x);
+        const f32x2 e1 = fma2(wx, d1, q1.x);
+        const f32x2 ez = sub2(e1, e0);
+        const float2 e = unpack2(fma2(wz, ez, e0));
         out.sum += lerpf(e.x, e.y, c.fy);
-        // (x0y0, x0y1), (x1y0, x1y1) at z0 and z1
-        const float2 a0 = unpack2(q0.x), b0 = unpack2(q0.y);
-        const float2 a1 = unpack2(q1.x), b1 = unpack2(q1.y);
-        const float gx = lerpf(lerpf(b0.x - a0.x, b0.y - a0.y, c.fy),
-                               lerpf(b1.x - a1.x, b1.y - a1.y, c.fy), c.fz);
-        const float gy = lerpf(lerpf(a0.y - a0.x, b0.y - b0.x, c.fx),
-                               lerpf(a1.y - a1.x, b1.y - b1.x, c.fx), c.fz);
-        const float gz = lerpf(lerpf(a1.x - a0.x, b1.x - b0.x, c.fx),
-                               lerpf(a1.y - a0.y, b1.y - b0.y, c.fx), c.fy);
+        // spatial gradient from the same pairs (the trilinear interpolant is
+        // linear along each axis): d/dx = lerp_y(lerp_z(x1 - x0)),
+        // d/dy = Y1 - Y0, d/dz = lerp_y(lerp_x(z1) - lerp_x(z0))
+        const float2 dx = unpack2(fma2(wz, sub2(d1, d0), d0));
+        const float2 dz = unpack2(ez);
+        const float gx = lerpf(dx.x, dx.y, c.fy);
+        const float gy = e.y - e.x;
+        const float gz = lerpf(dz.x, dz.y, c.fy);
         const float tau = t - r.tmin;
         out.g.s1x += gx;
         out.g.s1y += gy;

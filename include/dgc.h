@@ -232,6 +232,20 @@ int dgc_project_mse_grad(const float* volume, int D, int H, int W,
                          void* workspace, size_t workspace_bytes, void* stream);
 
 /* ---------------------------------------------------------------------- */
+/* Raw frames to line integrals                                             */
+/* ---------------------------------------------------------------------- */
+
+/* out[a,u,v] = -log(max((raw - dark) / (flat - dark), min_ratio)), the
+ * dark/flat-field correction and negative log the reference requires
+ * upstream of its operators (README.md:108), fused with the transpose of
+ * frames stored [A,V,U] (layout_avu = 1; U fastest) into the operators'
+ * [A,U,V] (docs/USAGE.md:247-251).  raw: [A,V,U] or [A,U,V]; dark, flat: one
+ * frame in the same layout, or NULL for 0 and 1.  No counterpart in the
+ * reference's code. */
+int dgc_preprocess(const float* raw, const float* dark, const float* flat, int A, int U, int V,
+                   int layout_avu, float min_ratio, float* out, void* stream);
+
+/* ---------------------------------------------------------------------- */
 /* Batched forward projection + backward over uneven instances             */
 /* ---------------------------------------------------------------------- */
 

@@ -95,3 +95,14 @@ def test_invalid_arguments_return_status(lib):
     assert rc == 1 and lib.dgc_last_error() == b"sizes and ROI offsets must be finite"
     rc = lib.dgc_fdk_filter(None, 2, 4, 4, -1.0, None, None, 0.8, None, None, 0, None)
     assert rc == 1 and b"pixel_size" in lib.dgc_last_error()
+
+
+def test_preprocess_argument_checks(lib):
+    p = ctypes.c_void_p(256)
+    assert lib.dgc_preprocess(None, None, None, 1, 4, 4, 1, 1e-6, p, None) == 1
+    assert b"non-null" in lib.dgc_last_error()
+    assert lib.dgc_preprocess(p, None, None, 1, 0, 4, 1, 1e-6, ctypes.c_void_p(512), None) == 1
+    assert lib.dgc_preprocess(p, None, None, 1, 4, 4, 1, 0.0, ctypes.c_void_p(512), None) == 1
+    assert b"min_ratio" in lib.dgc_last_error()
+    assert lib.dgc_preprocess(p, None, None, 1, 4, 4, 1, 1e-6, p, None) == 1
+    assert b"alias" in lib.dgc_last_error()
