@@ -194,6 +194,14 @@ __device__ __forceinline__ int step_bound(const RaySetup& r, float step) {
     return n < 1.0e9f ? 2 * (int)n + 16 : 2000000000;
 }
 
+// True when every t of the ray's recurrence satisfies |t| < 2^22 * step: then
+// ulp(t) < step, each t += step advances t by more than step/2 and the loop
+// ends by itself, so it may run without the iteration counter.
+__device__ __forceinline__ bool steps_advance(const RaySetup& r, float step) {
+    const float lim = 4194304.0f * step;
+    return fabsf(r.tmin) < lim && fabsf(r.tmax) + step < lim;
+}
+
 // Voxel coordinate of a world position along one axis.
 //   forward (fp.cu:326-328): (p - off) / voxel + n/2
 //   backward (fp.cu:425-427): (p - off) * (1/voxel) + n/2
@@ -311,7 +319,7 @@ __device__ __forceinline__ uint32_t quad_index(const Cell& c, const FpArgs& p) {
 // Sum of the trilinear samples along the ray (fp.cu:321-335).  The quads
 // hold the y-pairs of x0 and x1 as 64-bit halves, so the interpolation runs
 // as packed pairs: along x for (y0, y1) at z0 and z1, along z, then along y.
-template <bool CLAMP, bool DIV, bool OFF>
+template <bool CLAMP, bool DIV, bool OFF, bool GUARD = true>
 __device__ __forceinline__ float march_sum(const RaySetup& r, const ViewGeo& vg, const FpArgs& p) {
     const ulonglong2* __restrict__ Q = reinterpret_cast<const ulonglong2*>(p.quads);
     const XYPacks k = make_xy_packs(r, vg, p);
@@ -320,7 +328,7 @@ __device__ __forceinline__ float march_sum(const RaySetup& r, const ViewGeo& vg,
     float t = r.tmin;
     int n = 0;
 #pragma unroll 1
-    for (; t <= r.tmax && n < nmax; t += p.step_size, ++n) {
+    for (; t <= r.tmax && (!GUARD || n < nmax); t += p.step_size, n += GUARD ? 1 : 0) {
         const Cell c = sample_cell<CLAMP, DIV, OFF, true>(t, r, vg, p, k);
         const uint32_t qi = quad_index(c, p);
         const ulonglong2 q0 = __ldg(Q + qi);
@@ -376,8 +384,13 @@ __device__ __forceinline__ void forward_ray(const FpArgs& p, const ViewGeo& vg, 
     const RaySetup r = setup_ray(vg, u, v, p);
     float integral = 0.0f;
     if (r.ok && r.hit) {
-        integral = ray_inside_pad<DIV>(r, vg, p) ? march_sum<false, DIV, OFF>(r, vg, p)
-                                                 : march_sum<true, DIV, OFF>(r, vg, p);
+        const bool inside = ray_inside_pad<DIV>(r, vg, p);
+        if (steps_advance(r, p.step_size))
+            integral = inside ? march_sum<false, DIV, OFF, false>(r, vg, p)
+                              : march_sum<true, DIV, OFF, false>(r, vg, p);
+        else
+            integral = inside ? march_sum<false, DIV, OFF>(r, vg, p)
+                              : march_sum<true, DIV, OFF>(r, vg, p);
         integral *= p.step_size;
     }
     p.projections[((long long)a * p.U + u) * p.V + v] = integral;
@@ -661,7 +674,7 @@ struct RayValueGrad {
 // One march that yields both the line-integral sum (bitwise the forward
 // kernel's: same positions, same packed lerps) and the spatial-gradient sums
 // of the backward.  No scatter: the volume is not differentiated here.
-template <bool CLAMP, bool DIV, bool OFF>
+template <bool CLAMP, bool DIV, bool OFF, bool GUARD = true>
 __device__ __forceinline__ RayValueGrad march_value_grad(const RaySetup& r, const ViewGeo& vg,
                                                          const FpArgs& p) {
     const ulonglong2* __restrict__ Q = reinterpret_cast<const ulonglong2*>(p.quads);
@@ -671,7 +684,7 @@ __device__ __forceinline__ RayValueGrad march_value_grad(const RaySetup& r, cons
     float t = r.tmin;
     int n = 0;
 #pragma unroll 1
-    for (; t <= r.tmax && n < nmax; t += p.step_size, ++n) {
+    for (; t <= r.tmax && (!GUARD || n < nmax); t += p.step_size, n += GUARD ? 1 : 0) {
         const Cell c = sample_cell<CLAMP, DIV, OFF, false>(t, r, vg, p, k);
         const uint32_t qi = quad_index(c, p);
         const ulonglong2 q0 = __ldg(Q + qi);
@@ -733,9 +746,15 @@ __global__ void __launch_bounds__(256) fp_mse_grad_kernel(FpArgs p, const float*
         const RaySetup r = setup_ray(vg, u, v, p);
         RayValueGrad m{0.0f, {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}};
         const bool hit = r.ok && r.hit;
-        if (hit)
-            m = ray_inside_pad<DIV>(r, vg, p) ? march_value_grad<false, DIV, OFF>(r, vg, p)
-                                              : march_value_grad<true, DIV, OFF>(r, vg, p);
+        if (hit) {
+            const bool inside = ray_inside_pad<DIV>(r, vg, p);
+            if (steps_advance(r, p.step_size))
+                m = inside ? march_value_grad<false, DIV, OFF, false>(r, vg, p)
+                           : march_value_grad<true, DIV, OFF, false>(r, vg, p);
+            else
+                m = inside ? march_value_grad<false, DIV, OFF>(r, vg, p)
+                           : march_value_grad<true, DIV, OFF>(r, vg, p);
+        }
         const float proj = m.sum * p.step_size;
         const long long idx = ((long long)a * p.U + u) * p.V + v;
         if (p.projections) p.projections[idx] = proj;
