@@ -287,6 +287,41 @@ def reconstruct_fdk(projections, geometry, pixel_size, volume_shape, voxel_size,
     return vol
 
 
+def parker_weights(angles, sid, U, pixel_size):
+    """float32 [A,U] Parker short-scan weights of the scan ``angles`` (dgc_parker_weights)."""
+    a = angles.contiguous()
+    d = sid.contiguous()
+    A = a.numel()
+    out = torch.empty((A, int(U)), dtype=torch.float32, device=a.device)
+    with torch.cuda.device(a.device):
+        _native.check(_native.lib().dgc_parker_weights(a.data_ptr(), d.data_ptr(), A, int(U),
+                                                       float(pixel_size), out.data_ptr(),
+                                                       _stream(a.device)))
+    return out
+
+
+def reconstruct_fdk_weighted(projections, geometry, pixel_size, volume_shape, voxel_size,
+                             volume_offset, alpha, uweights, angle_scale):
+    """reconstruct_fdk with per-(view, column) weights and angular factor
+    ``angle_scale`` in place of pi/A (short scans)."""
+    p = projections.contiguous()
+    geom = [t.contiguous() for t in geometry]
+    w = None if uweights is None else uweights.contiguous()
+    A, U, V = p.shape
+    D, H, W = volume_shape
+    dev = p.device
+    vol = torch.empty((D, H, W), dtype=torch.float32, device=dev)
+    lib = _native.lib()
+    with torch.cuda.device(dev):
+        ws = _workspace(lib.dgc_reconstruct_fdk_workspace_bytes(A, U, V, D, H, W), dev)
+        _native.check(lib.dgc_reconstruct_fdk_weighted(
+            p.data_ptr(), A, U, V, *[g.data_ptr() for g in geom], float(pixel_size), D, H, W,
+            float(voxel_size), *map(float, volume_offset), float(alpha), _p(w),
+            float(angle_scale), vol.data_ptr(), _p(ws), 0 if ws is None else ws.numel(),
+            _stream(dev)))
+    return vol
+
+
 def fdk_filter_taps(U: int, pixel_size: float, alpha: float):
     """Host-only filter taps h[0..U-1] (FP64), for inspection and tests."""
     import ctypes

@@ -99,6 +99,7 @@ def reconstruct_fdk(
     volume_offset=(0.0, 0.0, 0.0),
     alpha=0.8,
     angle_chunk_size=32,
+    short_scan=False,
 ):
     """FDK reconstruction: filter, backproject, multiply by ``pi / A``, clamp at 0.
 
@@ -107,6 +108,11 @@ def reconstruct_fdk(
     centres).  ``volume_shape`` is ``(D, H, W)``; ``volume_offset`` follows
     ``backproject``.  Uniform angular weights assume a complete, uniformly
     sampled circular scan; the cosine preweight is centred.
+
+    ``short_scan=True`` (an addition to the reference's signature) treats the
+    views as a uniformly spaced short scan over ``angles[0] .. angles[-1]``
+    (monotone, covering pi plus twice the largest fan angle): Parker weights
+    multiply the cosine preweight and the view spacing replaces ``pi / A``.
     """
     _check_projections(projections)
     if not projections.is_cuda:
@@ -148,5 +154,20 @@ def reconstruct_fdk(
     offset = tuple(float(v) for v in volume_offset)
     if len(offset) != 3 or not all(math.isfinite(v) for v in offset):
         raise ValueError("volume_offset must contain three finite values")
+    if short_scan:
+        a0, a1 = float(angles[0]), float(angles[-1])
+        span = abs(a1 - a0)
+        fan = math.atan(((projections.shape[1] - 1) / 2 * pixel_size) / float(sid.min()))
+        if views < 2 or span < math.pi + 2 * fan - 1e-6:
+            raise ValueError("a short scan must cover pi plus twice the largest fan angle "
+                             f"({math.degrees(math.pi + 2 * fan):.2f} deg); got "
+                             f"{math.degrees(span):.2f} deg")
+        steps = torch.diff(angles.double()) * (1.0 if a1 >= a0 else -1.0)
+        if bool((steps <= 0).any()):
+            raise ValueError("short-scan angles must be strictly monotone")
+        weights = _ops.parker_weights(angles, sid, projections.shape[1], pixel_size)
+        return _ops.reconstruct_fdk_weighted(projections, geometry, pixel_size, volume_shape,
+                                             voxel_size, offset, alpha, weights,
+                                             span / (views - 1))
     return _ops.reconstruct_fdk(projections, geometry, pixel_size, volume_shape, voxel_size,
                                 offset, alpha)

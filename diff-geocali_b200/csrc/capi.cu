@@ -500,12 +500,14 @@ size_t dgc_reconstruct_fdk_workspace_bytes(int A, int U, int V, int D, int H, in
            dgc_backproject_workspace_bytes(A, U, V, D, H, W);
 }
 
-int dgc_reconstruct_fdk(const float* projections, int A, int U, int V, const float* angles,
-                        const float* sid, const float* sod, const float* det_u0,
-                        const float* det_v0, const float* src_x, const float* src_y,
-                        const float* src_z, float pixel_size, int D, int H, int W,
-                        float voxel_size, float off_x, float off_y, float off_z, float alpha,
-                        float* volume, void* workspace, size_t workspace_bytes, void* stream) {
+static int reconstruct_fdk_impl(const float* projections, int A, int U, int V,
+                                const float* angles, const float* sid, const float* sod,
+                                const float* det_u0, const float* det_v0, const float* src_x,
+                                const float* src_y, const float* src_z, float pixel_size, int D,
+                                int H, int W, float voxel_size, float off_x, float off_y,
+                                float off_z, float alpha, const float* uweights,
+                                float angle_scale, float* volume, void* workspace,
+                                size_t workspace_bytes, void* stream) {
     clear_error();
     cudaStream_t s = (cudaStream_t)stream;
     const Geometry g = make_geometry(angles, sid, sod, det_u0, det_v0, src_x, src_y, src_z);
@@ -525,14 +527,53 @@ int dgc_reconstruct_fdk(const float* projections, int A, int U, int V, const flo
         return DGC_ERR_WORKSPACE;
     }
     if ((rc = fdk_upload_taps(U, pixel_size, alpha, taps, s)) != DGC_OK) return rc;
-    FdkArgs f{projections, sod, sid, taps, filtered, A, U, V, pixel_size};
+    FdkArgs f{projections, sod, sid, taps, filtered, A, U, V, pixel_size, uweights};
     if ((rc = fdk_launch_filter(f, s)) != DGC_OK) return rc;
     if ((rc = bp_view_table(g, A, vt, s)) != DGC_OK) return rc;
     if ((rc = build_proj_quads(filtered, A, U, V, pq, s)) != DGC_OK) return rc;
     BpArgs p = bp_args(vt, pq, A, U, V, D, H, W, pixel_size, voxel_size, off_x, off_y, off_z);
     p.volume = volume;
-    p.out_scale = (float)(M_PI / (double)A);
+    p.out_scale = angle_scale;
     return bp_launch_forward(p, true, s);
+}
+
+int dgc_reconstruct_fdk(const float* projections, int A, int U, int V, const float* angles,
+                        const float* sid, const float* sod, const float* det_u0,
+                        const float* det_v0, const float* src_x, const float* src_y,
+                        const float* src_z, float pixel_size, int D, int H, int W,
+                        float voxel_size, float off_x, float off_y, float off_z, float alpha,
+                        float* volume, void* workspace, size_t workspace_bytes, void* stream) {
+    return reconstruct_fdk_impl(projections, A, U, V, angles, sid, sod, det_u0, det_v0, src_x,
+                                src_y, src_z, pixel_size, D, H, W, voxel_size, off_x, off_y, off_z,
+                                alpha, nullptr, (float)(M_PI / (double)A), volume, workspace,
+                                workspace_bytes, stream);
+}
+
+int dgc_reconstruct_fdk_weighted(const float* projections, int A, int U, int V,
+                                 const float* angles, const float* sid, const float* sod,
+                                 const float* det_u0, const float* det_v0, const float* src_x,
+                                 const float* src_y, const float* src_z, float pixel_size, int D,
+                                 int H, int W, float voxel_size, float off_x, float off_y,
+                                 float off_z, float alpha, const float* uweights,
+                                 float angle_scale, float* volume, void* workspace,
+                                 size_t workspace_bytes, void* stream) {
+    clear_error();
+    DGC_REQUIRE(std::isfinite(angle_scale) && angle_scale > 0.0f,
+                "angle_scale must be positive and finite");
+    return reconstruct_fdk_impl(projections, A, U, V, angles, sid, sod, det_u0, det_v0, src_x,
+                                src_y, src_z, pixel_size, D, H, W, voxel_size, off_x, off_y, off_z,
+                                alpha, uweights, angle_scale, volume, workspace, workspace_bytes,
+                                stream);
+}
+
+int dgc_parker_weights(const float* angles, const float* sid, int A, int U, float pixel_size,
+                       float* weights, void* stream) {
+    clear_error();
+    DGC_REQUIRE(angles && sid && weights, "angles, sid and weights must be non-null");
+    DGC_REQUIRE(A >= 2 && U >= 1, "a short scan needs A >= 2 views and U >= 1");
+    DGC_REQUIRE((long long)A * U <= INT_MAX, "A*U exceeds the 32-bit launch limit");
+    DGC_REQUIRE(std::isfinite(pixel_size) && pixel_size > 0.0f, "pixel_size must be positive");
+    return fdk_parker_weights(angles, sid, A, U, pixel_size, weights, (cudaStream_t)stream);
 }
 
 // ---------------------------------------------------------- tensor-core GEMM

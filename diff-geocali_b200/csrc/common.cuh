@@ -5,6 +5,7 @@
 #include <stdint.h>
 #include <stddef.h>
 
+#include <atomic>
 #include <cfloat>
 #include <cstring>
 #include <algorithm>
@@ -52,6 +53,20 @@ struct Fail {
             return DGC_ERR_CUDA;                                                \
         }                                                                       \
     } while (0)
+
+// Runs set() (returning a DGC status) once per device: kernel attributes such
+// as the dynamic shared-memory limit belong to a device's context, so a
+// process that drives several GPUs must set them on each.
+template <typename F>
+int once_per_device(std::atomic<unsigned long long>& done, F set) {
+    int dev = 0;
+    DGC_CUDA(cudaGetDevice(&dev));
+    const unsigned long long bit = dev < 64 ? (1ull << dev) : 0ull;
+    if (bit && (done.load() & bit)) return DGC_OK;
+    const int rc = set();
+    if (rc == DGC_OK && bit) done.fetch_or(bit);
+    return rc;
+}
 
 // Bump allocator over a caller-owned workspace (256-byte aligned slices).
 struct Workspace {

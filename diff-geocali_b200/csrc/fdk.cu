@@ -113,6 +113,7 @@ __global__ void __launch_bounds__(256) fdk_filter_kernel(FdkArgs p) {
             const int k = k0 + r;
             const int c0 = (tid & 15) * 8;
             const float uu = ((float)k - cu) * p.pixel_size;
+            const float wk = (p.uweight && k < p.U) ? p.uweight[(long long)a * p.U + k] : 1.0f;
             float vals[8];
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
@@ -121,7 +122,7 @@ __global__ void __launch_bounds__(256) fdk_filter_kernel(FdkArgs p) {
                 if (k < p.U && v < p.V) {
                     const float vv = ((float)v - cv) * p.pixel_size;
                     const float dist = sqrtf(sid2 + uu * uu + vv * vv);
-                    val = Pa[(long long)k * p.V + v] * (sid / dist);
+                    val = Pa[(long long)k * p.V + v] * (sid / dist) * wk;
                 }
                 vals[j] = val;
             }
@@ -162,6 +163,53 @@ __global__ void __launch_bounds__(256) fdk_filter_kernel(FdkArgs p) {
             if (v < p.V) Oa[(long long)u * p.V + v] = (acc[i][j] * p.pixel_size) * ratio;
         }
     }
+}
+
+// Parker's short-scan weights (D. L. Parker, Med. Phys. 9(2), 1982): for a
+// scan over beta in [0, pi + 2*Gamma] and the fan angle gamma = atan(u_c/sid)
+// of detector column u (u_c centred as in the cosine preweight),
+//   w = sin^2(pi/4 * beta / (Gamma - gamma))                 beta <  2(Gamma - gamma)
+//   w = 1                                                   beta <= pi - 2 gamma
+//   w = sin^2(pi/4 * (pi + 2 Gamma - beta) / (Gamma + gamma)) beta <= pi + 2 Gamma
+// and 0 beyond, so that every ray and its conjugate (beta + pi + 2 gamma,
+// -gamma) weigh 1 together.  Gamma is taken from the scan's own range,
+// (range - pi) / 2, which must be at least the largest fan angle (Parker
+// weights with a wider Gamma are the usual over-scan form).  beta runs from
+// angles[0] in the direction of the scan; for a decreasing scan gamma flips
+// sign with it.  FP64 (a table of A*U values).
+__global__ void parker_weights_kernel(const float* __restrict__ angles,
+                                      const float* __restrict__ sid, int A, int U, float px,
+                                      float* __restrict__ out) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= (long long)A * U) return;
+    const int a = (int)(i / U), u = (int)(i - (long long)a * U);
+    const double b0 = angles[0], bl = angles[A - 1];
+    const double dir = bl >= b0 ? 1.0 : -1.0;
+    const double beta = dir * ((double)angles[a] - b0);
+    const double Gam = 0.5 * (dir * (bl - b0) - M_PI);
+    const double uc = ((double)u - 0.5 * (U - 1)) * (double)px;
+    const double gam = dir * atan(uc / (double)sid[a]);
+    double w = 0.0;
+    if (beta >= 0.0 && beta < 2.0 * (Gam - gam)) {
+        const double sw = sin(0.25 * M_PI * beta / (Gam - gam));
+        w = sw * sw;
+    } else if (beta >= 0.0 && beta <= M_PI - 2.0 * gam) {
+        w = 1.0;
+    } else if (beta > M_PI - 2.0 * gam && beta <= M_PI + 2.0 * Gam) {
+        const double sw = sin(0.25 * M_PI * (M_PI + 2.0 * Gam - beta) / (Gam + gam));
+        w = sw * sw;
+    }
+    out[i] = (float)w;
+}
+
+int fdk_parker_weights(const float* angles, const float* sid, int A, int U, float pixel_size,
+                       float* weights, cudaStream_t s) {
+    DGC_TRACE("parker_weights", s);
+    const long long n = (long long)A * U;
+    parker_weights_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(angles, sid, A, U, pixel_size,
+                                                                       weights);
+    DGC_LAUNCH_CHECK("parker_weights");
+    return DGC_OK;
 }
 
 int fdk_launch_filter(const FdkArgs& p, cudaStream_t s) {

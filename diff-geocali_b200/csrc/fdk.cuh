@@ -15,10 +15,14 @@ struct FdkArgs {
     float* filtered;           // [A][U][V]
     int A, U, V;
     float pixel_size;
+    const float* uweight;      // [A][U] extra per-column weight (short-scan), or null
 };
 
 int fdk_taps_host(int U, double px, double alpha, std::vector<double>& out);
 int fdk_upload_taps(int U, float px, float alpha, float* dst, cudaStream_t s);
 int fdk_launch_filter(const FdkArgs& p, cudaStream_t s);
+// Parker short-scan weights w[a][u] of a scan over angles[0] .. angles[A-1].
+int fdk_parker_weights(const float* angles, const float* sid, int A, int U, float pixel_size,
+                       float* weights, cudaStream_t s);
 
 }  // namespace dgc

@@ -1272,12 +1272,13 @@ int launch_backward_tu(const FpArgs& p, bool gradvol, cudaStream_t s) {
     const bool brick = gradvol && e && std::strcmp(e, "brick") == 0;
     if (brick) {
         constexpr int smem = kBrickCap * (int)sizeof(float);
-        static bool configured = false;
-        if (!configured) {
+        static std::atomic<unsigned long long> configured{0};
+        const int rc = once_per_device(configured, []() -> int {
             DGC_CUDA(cudaFuncSetAttribute(fp_backward_brick_kernel<TU>,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-            configured = true;
-        }
+            return DGC_OK;
+        });
+        if (rc != DGC_OK) return rc;
         fp_backward_brick_kernel<TU><<<(unsigned)blocks, 256, smem, s>>>(p);
     } else if (!gradvol)
         fp_backward_kernel<TU, 0><<<(unsigned)blocks, 256, 0, s>>>(p);

@@ -474,12 +474,13 @@ int launch_gemm_tma(const GemmArgs& p, cudaStream_t s, bool* used) {
         !make_kmajor_map(&tb, p.B, p.N, p.K, p.ldb, BN))
         return DGC_OK;
     const int smem = TmaStages<BN>::value * TmaStages<BN>::kStageBytes + 1024;
-    static bool configured = false;
-    if (!configured) {
+    static std::atomic<unsigned long long> configured{0};
+    const int rc = once_per_device(configured, [smem]() -> int {
         DGC_CUDA(cudaFuncSetAttribute(tc_gemm_tma_kernel<BN>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-        configured = true;
-    }
+        return DGC_OK;
+    });
+    if (rc != DGC_OK) return rc;
     const int splits = p.k_tiles_per_split > 0
                            ? ceil_div(ceil_div(p.K, kBK), p.k_tiles_per_split) : 1;
     const dim3 grid(ceil_div(p.N, BN), ceil_div(p.M, kBM), splits);
@@ -493,12 +494,13 @@ int launch_gemm_tma(const GemmArgs& p, cudaStream_t s, bool* used) {
 template <int BN>
 int launch_gemm(const GemmArgs& p, cudaStream_t s) {
     const int smem = kStages * (kBM * kBK * 2 + BN * kBK * 2) + 1024;
-    static bool configured = false;
-    if (!configured) {
+    static std::atomic<unsigned long long> configured{0};
+    const int rc = once_per_device(configured, [smem]() -> int {
         DGC_CUDA(cudaFuncSetAttribute(tc_gemm_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       smem));
-        configured = true;
-    }
+        return DGC_OK;
+    });
+    if (rc != DGC_OK) return rc;
     const int splits = p.k_tiles_per_split > 0
                            ? ceil_div(ceil_div(p.K, kBK), p.k_tiles_per_split) : 1;
     const dim3 grid(ceil_div(p.N, BN), ceil_div(p.M, kBM), splits);

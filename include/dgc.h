@@ -192,6 +192,29 @@ int dgc_reconstruct_fdk(const float* projections, int A, int U, int V,
                         float* volume,
                         void* workspace, size_t workspace_bytes, void* stream);
 
+/* Parker short-scan weights w[a][u] (Parker, Med. Phys. 9(2), 1982) of a scan
+ * over angles[0] .. angles[A-1] (monotone, range pi + 2*Gamma with Gamma at
+ * least the largest fan angle atan(((U-1)/2 * pixel_size) / sid)): each ray
+ * and its conjugate weigh 1 together.  The reference's FDK assumes a full
+ * circle (README.md:115, filtering.py:1-8); no counterpart there. */
+int dgc_parker_weights(const float* angles, const float* sid, int A, int U, float pixel_size,
+                       float* weights, void* stream);
+
+/* dgc_reconstruct_fdk with a per-(view, column) weight multiplied into the
+ * cosine preweight (uweights [A][U], e.g. dgc_parker_weights; NULL for none)
+ * and the angular factor angle_scale in place of pi/A (the view spacing for
+ * a Parker-weighted short scan).  Same workspace as dgc_reconstruct_fdk.
+ * Extends filtering.py:107-198 to short scans; no counterpart in the
+ * reference. */
+int dgc_reconstruct_fdk_weighted(const float* projections, int A, int U, int V,
+                                 const float* angles, const float* sid, const float* sod,
+                                 const float* det_u0, const float* det_v0,
+                                 const float* src_x, const float* src_y, const float* src_z,
+                                 float pixel_size, int D, int H, int W, float voxel_size,
+                                 float off_x, float off_y, float off_z, float alpha,
+                                 const float* uweights, float angle_scale, float* volume,
+                                 void* workspace, size_t workspace_bytes, void* stream);
+
 /* ---------------------------------------------------------------------- */
 /* Tensor-core GEMM of the warm-start network (no counterpart in the        */
 /* reference: its calibration pipeline is not shipped)                      */

@@ -204,6 +204,32 @@ def fdk_filter(projections, pixel_size, sod, sid, alpha=0.8):
     return out
 
 
+def parker_weights(angles, sid, U, pixel_size):
+    """FP64 [A,U] short-scan weights (Parker, Med. Phys. 9(2), 1982), as
+    dgc_parker_weights defines them: beta from angles[0] in the scan's
+    direction, Gamma = (range - pi) / 2, gamma = atan(u_c / sid) with the
+    centred u_c of filtering.py's cosine preweight, gamma's sign following the
+    scan direction."""
+    a = np.asarray(angles, np.float64)
+    d = np.broadcast_to(np.asarray(sid, np.float64), a.shape)
+    direction = 1.0 if a[-1] >= a[0] else -1.0
+    beta = (direction * (a - a[0]))[:, None]
+    gam_max = 0.5 * (direction * (a[-1] - a[0]) - np.pi)
+    uc = (np.arange(U) - 0.5 * (U - 1)) * pixel_size
+    gam = direction * np.arctan(uc[None, :] / d[:, None])
+    w = np.zeros((a.size, U))
+    with np.errstate(divide="ignore", invalid="ignore"):
+        rise = np.sin(0.25 * np.pi * beta / (gam_max - gam)) ** 2
+        fall = np.sin(0.25 * np.pi * (np.pi + 2 * gam_max - beta) / (gam_max + gam)) ** 2
+    r1 = (beta >= 0) & (beta < 2 * (gam_max - gam))
+    r2 = ~r1 & (beta >= 0) & (beta <= np.pi - 2 * gam)
+    r3 = (beta > np.pi - 2 * gam) & (beta <= np.pi + 2 * gam_max)
+    w = np.where(r1, rise, w)
+    w = np.where(r2, 1.0, w)
+    w = np.where(r3 & ~r1 & ~r2, fall, w)
+    return w
+
+
 def reconstruct_fdk(projections, geometry, pixel_size, volume_shape, voxel_size,
                     offset=(0.0, 0.0, 0.0), alpha=0.8):
     """filtering.py:107-198 in FP64: filter, backproject, * pi/A, clamp >= 0."""
@@ -216,7 +242,7 @@ def reconstruct_fdk(projections, geometry, pixel_size, volume_shape, voxel_size,
 __all__ = [
     "build", "num_threads", "set_num_threads", "project", "project_rays", "sample_counts",
     "ray_traces", "project_backward", "backproject", "backproject_backward", "fdk_taps", "fdk_filter",
-    "reconstruct_fdk", "usable_cpus",
+    "reconstruct_fdk", "parker_weights", "usable_cpus",
 ]
 
 
