@@ -16,7 +16,11 @@ pi/A, and the Shannon entropy of the normalised absolute intensities is
 minimised with Adam.  Stage 1 fits one offset per geometry family shared by
 all views (the well-determined, strongly blurring errors: a detector or
 source shift common to the scan); stage 2 then fits per-view offsets.  The
-parameter families of each stage are a choice of the caller.
+parameter families of each stage are a choice of the caller; the default,
+the detector centre in both stages, is what the entropy determines well --
+a shared sid or per-view angles moved the estimate away from the truth in
+the tests that chose it (the reconstruction's sharpness does not pin the
+magnification), and per-view fits drift again after ~40 iterations.
 """
 
 from __future__ import annotations
@@ -52,9 +56,9 @@ DEFAULT_STEP = {"angles": 1e-3, "sid": 1.0, "sod": 1.0, "det_u0": 0.1, "det_v0":
 
 
 def entropy_calibrate(projections, nominal, pixel_size, volume_shape, voxel_size,
-                      volume_offset=(0.0, 0.0, 0.0), stages=(("det_u0",), ("det_u0",)),
-                      iterations=(60, 60), lr=None, alpha=0.8, true_geometry=None, points=None,
-                      log_every=0):
+                      volume_offset=(0.0, 0.0, 0.0),
+                      stages=(("det_u0", "det_v0"), ("det_u0", "det_v0")), iterations=(40, 40),
+                      lr=None, alpha=0.8, true_geometry=None, points=None, log_every=0):
     """Two-stage entropy self-calibration; returns a ``SelfCalibrationResult``.
 
     ``stages[0]`` lists the families fitted with one offset shared by all

@@ -27,6 +27,7 @@ def test_entropy_recovers_detector_shift():
     pts = lattice_points((N, N, N), device="cuda")
     res = entropy_calibrate(proj, nominal, px, (N, N, N), 1.0, stages=(("det_u0",), ("det_u0",)),
                             iterations=(40, 40), true_geometry=true, points=pts)
+    # measured when written: 2.54 px -> 0.45 after the shared stage -> 0.07
     start = reprojection_error(nominal, true, pts, px)
     after1 = [h for h in res.history if h["stage"] == 0][-1]["reproj_px"]
     final = reprojection_error(res.geometry, true, pts, px)
