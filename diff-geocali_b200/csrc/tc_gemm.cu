@@ -319,19 +319,23 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map
         : "memory");
 }
 
-template <int BN>
+// MSUB 128-row sub-tiles of A per CTA (1 or 2): with 2, a CTA computes a
+// 256 x BN tile as two M = 128 accumulators that share every staged B tile,
+// which cuts the operand bytes moved per FLOP by a third at BN = 256.
+template <int BN, int MSUB = 1>
 struct TmaStages {
-    static constexpr int kStageBytes = kBM * kBK * 2 + BN * kBK * 2;
+    static constexpr int kStageBytes = MSUB * kBM * kBK * 2 + BN * kBK * 2;
     static constexpr int value = (196608 / kStageBytes) < 8 ? (196608 / kStageBytes) : 8;
 };
 
-template <int BN>
+template <int BN, int MSUB>
 __global__ void __launch_bounds__(128) tc_gemm_tma_kernel(const __grid_constant__ CUtensorMap tmA,
                                                           const __grid_constant__ CUtensorMap tmB,
                                                           GemmArgs p) {
-    constexpr int S = TmaStages<BN>::value;
-    constexpr int kABytes = kBM * kBK * 2;
-    constexpr int kStageBytes = TmaStages<BN>::kStageBytes;
+    constexpr int S = TmaStages<BN, MSUB>::value;
+    constexpr int kABytes = MSUB * kBM * kBK * 2;
+    constexpr int kStageBytes = TmaStages<BN, MSUB>::kStageBytes;
+    constexpr int kCols = MSUB * BN;  // tensor-memory columns of the accumulators
     constexpr uint32_t kIdesc = idesc_bf16(kBM, BN);
     extern __shared__ __align__(1024) uint8_t smem[];
     __shared__ __align__(8) uint64_t full[S];
@@ -341,7 +345,7 @@ __global__ void __launch_bounds__(128) tc_gemm_tma_kernel(const __grid_constant_
     __shared__ int s_err, s_consumed;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int m0 = blockIdx.y * kBM, n0 = blockIdx.x * BN;
+    const int m0 = blockIdx.y * kBM * MSUB, n0 = blockIdx.x * BN;
     const uint32_t sbase = (smem_u32(smem) + 1023u) & ~1023u;
     const int nk_total = (p.K + kBK - 1) / kBK;
     const bool split = p.k_tiles_per_split > 0;
@@ -351,7 +355,7 @@ __global__ void __launch_bounds__(128) tc_gemm_tma_kernel(const __grid_constant_
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
                          smem_u32(&tmem_slot)),
-                     "r"(BN)
+                     "r"(kCols)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
     }
@@ -399,9 +403,13 @@ __global__ void __launch_bounds__(128) tc_gemm_tma_kernel(const __grid_constant_
             const uint32_t sa = sbase + s * kStageBytes;
 #pragma unroll
             for (int kk = 0; kk < kBK / 16; ++kk) {
-                const uint64_t ad = kmajor_sw128_desc(sa + kk * 32);
                 const uint64_t bd = kmajor_sw128_desc(sa + kABytes + kk * 32);
-                umma_bf16(tmem, ad, bd, kIdesc, (kt > 0 || kk > 0) ? 1u : 0u);
+#pragma unroll
+                for (int m = 0; m < MSUB; ++m) {
+                    // sub-tile m: rows 128m.. of the staged A (128 B per row)
+                    const uint64_t ad = kmajor_sw128_desc(sa + m * kBM * 128 + kk * 32);
+                    umma_bf16(tmem + m * BN, ad, bd, kIdesc, (kt > 0 || kk > 0) ? 1u : 0u);
+                }
             }
             umma_commit(smem_u32(&empty[s]));
         }
@@ -421,12 +429,16 @@ __global__ void __launch_bounds__(128) tc_gemm_tma_kernel(const __grid_constant_
     __syncwarp();
     if (!ok && threadIdx.x == 0) atomicExch(p.error, 1);
     tc_fence_after();
-    if (ok) gemm_epilogue<BN>(p, tmem, m0, n0, nk > 0, split);
+    if (ok) {
+#pragma unroll
+        for (int m = 0; m < MSUB; ++m)
+            gemm_epilogue<BN>(p, tmem + m * BN, m0 + m * kBM, n0, nk > 0, split);
+    }
     tc_fence_before();
     __syncthreads();
     if (warp == 0) {
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(BN)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(kCols)
                      : "memory");
     }
 }
@@ -466,26 +478,26 @@ bool make_kmajor_map(CUtensorMap* map, const void* base, int rows, int cols, int
               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-template <int BN>
+template <int BN, int MSUB>
 int launch_gemm_tma(const GemmArgs& p, cudaStream_t s, bool* used) {
     *used = false;
     CUtensorMap ta, tb;
-    if (!make_kmajor_map(&ta, p.A, p.M, p.K, p.lda, kBM) ||
+    if (!make_kmajor_map(&ta, p.A, p.M, p.K, p.lda, kBM * MSUB) ||
         !make_kmajor_map(&tb, p.B, p.N, p.K, p.ldb, BN))
         return DGC_OK;
-    const int smem = TmaStages<BN>::value * TmaStages<BN>::kStageBytes + 1024;
+    const int smem = TmaStages<BN, MSUB>::value * TmaStages<BN, MSUB>::kStageBytes + 1024;
     static std::atomic<unsigned long long> configured{0};
     const int rc = once_per_device(configured, [smem]() -> int {
-        DGC_CUDA(cudaFuncSetAttribute(tc_gemm_tma_kernel<BN>,
+        DGC_CUDA(cudaFuncSetAttribute(tc_gemm_tma_kernel<BN, MSUB>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
         return DGC_OK;
     });
     if (rc != DGC_OK) return rc;
     const int splits = p.k_tiles_per_split > 0
                            ? ceil_div(ceil_div(p.K, kBK), p.k_tiles_per_split) : 1;
-    const dim3 grid(ceil_div(p.N, BN), ceil_div(p.M, kBM), splits);
+    const dim3 grid(ceil_div(p.N, BN), ceil_div(p.M, kBM * MSUB), splits);
     DGC_TRACE("tc_gemm_tma_kernel", s);
-    tc_gemm_tma_kernel<BN><<<grid, 128, smem, s>>>(ta, tb, p);
+    tc_gemm_tma_kernel<BN, MSUB><<<grid, 128, smem, s>>>(ta, tb, p);
     DGC_LAUNCH_CHECK("tc_gemm_tma_kernel");
     *used = true;
     return DGC_OK;
@@ -524,10 +536,14 @@ int tc_gemm(const GemmArgs& p, cudaStream_t s) {
     // the driver cannot encode tensor maps)
     const char* e = std::getenv("DGC_GEMM");
     if (!(e && std::strcmp(e, "cpasync") == 0)) {
+        // 256 x 256 tiles (two accumulators) where they still give every SM a tile
+        const bool two = bn == 256 &&
+                         (long long)ceil_div(p.M, 2 * kBM) * ceil_div(p.N, 256) * splits >= 148;
         bool used = false;
-        int rc = bn == 64 ? launch_gemm_tma<64>(p, s, &used)
-                 : bn == 256 ? launch_gemm_tma<256>(p, s, &used)
-                             : launch_gemm_tma<128>(p, s, &used);
+        int rc = bn == 64    ? launch_gemm_tma<64, 1>(p, s, &used)
+                 : two       ? launch_gemm_tma<256, 2>(p, s, &used)
+                 : bn == 256 ? launch_gemm_tma<256, 1>(p, s, &used)
+                             : launch_gemm_tma<128, 1>(p, s, &used);
         if (rc != DGC_OK || used) return rc;
     }
     if (bn == 64) return launch_gemm<64>(p, s);

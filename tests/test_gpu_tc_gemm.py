@@ -29,11 +29,13 @@ def run(A, B, C, bias=None, relu=False, accumulate=False, alpha=1.0):
 
 @pytest.mark.parametrize("M,N,K", [(128, 128, 64), (128, 64, 16), (300, 200, 72), (1000, 64, 256),
                                    (2048, 256, 2304), (7, 24, 8), (513, 136, 136),
-                                   (64, 200, 8192), (32, 96, 4104), (18944, 264, 72)])
+                                   (64, 200, 8192), (32, 96, 4104), (18944, 264, 72),
+                                   (9000, 520, 136), (9400, 1000, 200)])
 @pytest.mark.parametrize("pipeline", ["tma", "cpasync"])
 def test_gemm_matches_fp32(M, N, K, pipeline, monkeypatch):
     """(64, 200, 8192) and (32, 96, 4104) take the split-K path (few output
-    tiles, long K); (18944, 264, 72) the 256-column tiles."""
+    tiles, long K); (9000, 520, 136) the 128 x 256 tiles; (18944, 264, 72)
+    and (9400, 1000, 200) the 256 x 256 tiles of two accumulators."""
     if pipeline == "cpasync":
         monkeypatch.setenv("DGC_GEMM", "cpasync")
     g = torch.Generator(device="cuda").manual_seed(M * 7 + N)
