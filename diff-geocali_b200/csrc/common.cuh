@@ -178,6 +178,14 @@ __device__ __forceinline__ void red_add_global(float* p, float v) {
     asm volatile("red.global.add.f32 [%0], %1;" ::"l"(__cvta_generic_to_global(p)), "f"(v));
 }
 
+// Four float adds to 16-byte-aligned global memory as one vector reduction
+// (red.global.add.v4.f32; each element is added atomically), without a
+// memory clobber like red_add_global.
+__device__ __forceinline__ void red_add4_global(float* p, float a, float b, float c, float d) {
+    asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(__cvta_generic_to_global(p)),
+                 "f"(a), "f"(b), "f"(c), "f"(d));
+}
+
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);

@@ -494,8 +494,61 @@ __device__ __forceinline__ void scatter_cell_pairwise(const FpArgs& p, uint32_t 
     }
 }
 
+// The eight weights of a sample into the cell-major buffer: record ci (32
+// bytes) holds the weights of the corners ci + (dz, dy, dx) at k = dz*4 + dy*2
+// + dx, and fold_cell_gradient_kernel sums the records onto the voxels.  Lane
+// pairs merge first, as in scatter_cell_pairwise: the same cell gives one
+// 16-byte reduction per lane (even lane the z level, odd lane z+1), cells
+// adjacent in z give three (the corners the two share go into the upper cell's
+// z-level record), other pairs four.  The z stride of the records is D+2, so
+// a cell index difference of +-1 always means the same (x, y) column.
+__device__ __forceinline__ void scatter_cell_records(const FpArgs& p, uint32_t ci, float (&lo)[4],
+                                                     float (&hi)[4]) {
+    const unsigned mask = __activemask();
+    const int lane = threadIdx.x & 31;
+    const int partner = lane ^ 1;
+    const bool odd = lane & 1;
+    const uint32_t cpart = __shfl_sync(mask, ci, partner);
+    float plo[4], phi[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        plo[k] = __shfl_sync(mask, lo[k], partner);
+        phi[k] = __shfl_sync(mask, hi[k], partner);
+    }
+    // cell of the odd lane minus cell of the even lane
+    const int d = (int)(odd ? ci - cpart : cpart - ci);
+    const int mode = !((mask >> partner) & 1u) ? 0 : d == 0 ? 1 : d == 1 ? 2 : d == -1 ? 3 : 0;
+    float* o = p.grad_pad + 8ull * ci;
+    if (mode == 1) {
+        if (odd)
+            red_add4_global(o + 4, hi[0] + phi[0], hi[1] + phi[1], hi[2] + phi[2], hi[3] + phi[3]);
+        else
+            red_add4_global(o, lo[0] + plo[0], lo[1] + plo[1], lo[2] + plo[2], lo[3] + plo[3]);
+    } else if (mode == 2) {
+        // odd cell = even cell + 1: the even lane's z+1 corners are the odd lane's z level
+        if (odd) {
+            red_add4_global(o, lo[0] + phi[0], lo[1] + phi[1], lo[2] + phi[2], lo[3] + phi[3]);
+            red_add4_global(o + 4, hi[0], hi[1], hi[2], hi[3]);
+        } else {
+            red_add4_global(o, lo[0], lo[1], lo[2], lo[3]);
+        }
+    } else if (mode == 3) {
+        // even cell = odd cell + 1: the odd lane's z+1 corners are the even lane's z level
+        if (odd) {
+            red_add4_global(o, lo[0], lo[1], lo[2], lo[3]);
+        } else {
+            red_add4_global(o, lo[0] + phi[0], lo[1] + phi[1], lo[2] + phi[2], lo[3] + phi[3]);
+            red_add4_global(o + 4, hi[0], hi[1], hi[2], hi[3]);
+        }
+    } else {
+        red_add4_global(o, lo[0], lo[1], lo[2], lo[3]);
+        red_add4_global(o + 4, hi[0], hi[1], hi[2], hi[3]);
+    }
+}
+
 // GV: 0 = no volume gradient, 1 = scatter every sample's eight weights,
-// 2 = merge them across lane pairs first (scatter_cell_pairwise).
+// 2 = merge them across lane pairs first (scatter_cell_pairwise), 3 = merge
+// lane pairs into per-cell 32-byte records (scatter_cell_records).
 template <bool CLAMP, int GV>
 __device__ __forceinline__ RayGrad march_grad(const RaySetup& r, const ViewGeo& vg,
                                               const FpArgs& p, float gs) {
@@ -539,7 +592,9 @@ __device__ __forceinline__ RayGrad march_grad(const RaySetup& r, const ViewGeo& 
             float lo[4] = {w00 * mz, w01 * mz, w10 * mz, w11 * mz};
             float hi[4] = {w00 * c.fz, w01 * c.fz, w10 * c.fz, w11 * c.fz};
             const uint32_t gi = c.bz + c.bx * p.gz_x + c.by * p.gz_y + p.gz_bias;
-            if (GV == 2) {
+            if (GV == 3) {
+                scatter_cell_records(p, gi, lo, hi);
+            } else if (GV == 2) {
                 scatter_cell_pairwise(p, gi, lo, hi);
             } else {
                 float* g = p.grad_pad + gi;
@@ -1073,6 +1128,53 @@ __global__ void fold_padded_gradient_kernel(const float* __restrict__ gpad, int 
         grad[i] = fold_voxel(gpad, D, H, W, i);
 }
 
+// Volume gradient from the cell-major buffer O[((cy*(W+1) + cx)*(D+2) + cz)*8 + k]
+// (cells at padded index floor+1 in [0, n], z stride D+2 with the record at
+// cz = D+1 unused; record k = dz*4 + dy*2 + dx the weight of corner (dz, dy,
+// dx)): a padded corner P gets record P - d of every cell with P - d in range,
+// and padded corners fold onto clamped voxels as in fold_padded_gradient_kernel.
+__device__ __forceinline__ float fold_cell_voxel(const float* __restrict__ O, int D, int H, int W,
+                                                 long long i) {
+    const long long CZ = D + 2, CX = W + 1;
+    {
+        const int x = (int)(i % W);
+        const long long r = i / W;
+        const int y = (int)(r % H);
+        const int z = (int)(r / H);
+        int xs[3], ys[3], zs[3];
+        int nx = 0, ny = 0, nz = 0;
+        xs[nx++] = x + 1;
+        if (x == 0) xs[nx++] = 0;
+        if (x == W - 1) xs[nx++] = W + 1;
+        ys[ny++] = y + 1;
+        if (y == 0) ys[ny++] = 0;
+        if (y == H - 1) ys[ny++] = H + 1;
+        zs[nz++] = z + 1;
+        if (z == 0) zs[nz++] = 0;
+        if (z == D - 1) zs[nz++] = D + 1;
+        float acc = 0.0f;
+        for (int iy = 0; iy < ny; ++iy)
+            for (int ix = 0; ix < nx; ++ix)
+                for (int iz = 0; iz < nz; ++iz)
+#pragma unroll
+                    for (int k = 0; k < 8; ++k) {
+                        const int dz = k >> 2, dy = (k >> 1) & 1, dx = k & 1;
+                        const int cz = zs[iz] - dz, cy = ys[iy] - dy, cx = xs[ix] - dx;
+                        if (cz < 0 || cz > D || cy < 0 || cy > H || cx < 0 || cx > W) continue;
+                        acc += O[((cy * CX + cx) * CZ + cz) * 8 + k];
+                    }
+        return acc;
+    }
+}
+
+__global__ void fold_cell_gradient_kernel(const float* __restrict__ O, int D, int H, int W,
+                                          float* __restrict__ grad) {
+    const long long total = (long long)D * H * W;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x)
+        grad[i] = fold_cell_voxel(O, D, H, W, i);
+}
+
 // ---------------------------------------------------------------------------
 // Batched launches: many instances of uneven D/H/W, A, U, V in one launch.
 //
@@ -1187,6 +1289,7 @@ __device__ __forceinline__ void backward_item(const FpArgs& p, const ViewGeo& vg
     int u, v;
     tile_ray<TU>(tc, u, v);
     if (!p.grad_pad) backward_ray<0>(p, vg, tc.a, u, v, terms);
+    else if (flags & kBatchCells) backward_ray<3>(p, vg, tc.a, u, v, terms);
     else if (flags & kBatchMerge) backward_ray<2>(p, vg, tc.a, u, v, terms);
     else backward_ray<1>(p, vg, tc.a, u, v, terms);
 }
@@ -1233,8 +1336,13 @@ __global__ void __launch_bounds__(256) batch_fold_kernel(BatchTables t) {
     const long long total = (long long)in.p.D * in.p.H * in.p.W;
     const long long v0 = (blockIdx.x - t.fold_block[i]) * (long long)kFoldChunk;
     const long long v1 = v0 + kFoldChunk < total ? v0 + kFoldChunk : total;
-    for (long long v = v0 + threadIdx.x; v < v1; v += blockDim.x)
-        in.grad_volume[v] = fold_voxel(in.p.grad_pad, in.p.D, in.p.H, in.p.W, v);
+    if (in.flags & kBatchCells) {
+        for (long long v = v0 + threadIdx.x; v < v1; v += blockDim.x)
+            in.grad_volume[v] = fold_cell_voxel(in.p.grad_pad, in.p.D, in.p.H, in.p.W, v);
+    } else {
+        for (long long v = v0 + threadIdx.x; v < v1; v += blockDim.x)
+            in.grad_volume[v] = fold_voxel(in.p.grad_pad, in.p.D, in.p.H, in.p.W, v);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -1268,8 +1376,7 @@ int launch_backward_tu(const FpArgs& p, bool gradvol, cudaStream_t s) {
     // (204 vs 117 ms at 256^3 / 360 x 384^2): the slab barriers hold the
     // bundle's fastest rays back, and the shared-memory additions cost about
     // what the L2 reductions they replace cost.
-    const char* e = std::getenv("DGC_SCATTER");
-    const bool brick = gradvol && e && std::strcmp(e, "brick") == 0;
+    const bool brick = gradvol && fp_volume_scatter() == kScatterBrick;
     if (brick) {
         constexpr int smem = kBrickCap * (int)sizeof(float);
         static std::atomic<unsigned long long> configured{0};
@@ -1280,25 +1387,52 @@ int launch_backward_tu(const FpArgs& p, bool gradvol, cudaStream_t s) {
         });
         if (rc != DGC_OK) return rc;
         fp_backward_brick_kernel<TU><<<(unsigned)blocks, 256, smem, s>>>(p);
-    } else if (!gradvol)
+    } else if (!gradvol) {
         fp_backward_kernel<TU, 0><<<(unsigned)blocks, 256, 0, s>>>(p);
-    else if (fp_merge_scatter(p.U, p.V, p.H, p.W))
-        fp_backward_kernel<TU, 2><<<(unsigned)blocks, 256, 0, s>>>(p);
-    else
-        fp_backward_kernel<TU, 1><<<(unsigned)blocks, 256, 0, s>>>(p);
+    } else {
+        switch (fp_volume_scatter()) {
+            case kScatterCells: fp_backward_kernel<TU, 3><<<(unsigned)blocks, 256, 0, s>>>(p); break;
+            case kScatterPairs: fp_backward_kernel<TU, 2><<<(unsigned)blocks, 256, 0, s>>>(p); break;
+            default: fp_backward_kernel<TU, 1><<<(unsigned)blocks, 256, 0, s>>>(p); break;
+        }
+    }
     DGC_LAUNCH_CHECK("fp_backward_kernel");
     return DGC_OK;
 }
 
 }  // namespace
 
-bool fp_merge_scatter(int U, int V, int H, int W) {
-    // DGC_SCATTER=plain|pairs overrides the choice (tests of the variants)
+VolumeScatter fp_volume_scatter() {
+    // Cell records by default: at 256^3 / 360 x 384^2, 128^3 / 180 x 256^2 and
+    // 256^3 / 90 x 192^2 the backward took 452 / 46 / 31 ms with them against
+    // 554 / 58 / 36 ms with lane pairs merged into the padded buffer and
+    // 682 / 81 / 45 ms with every sample alone.
     if (const char* e = std::getenv("DGC_SCATTER")) {
-        if (std::strcmp(e, "pairs") == 0) return true;
-        if (std::strcmp(e, "plain") == 0) return false;
+        if (std::strcmp(e, "pairs") == 0) return kScatterPairs;
+        if (std::strcmp(e, "plain") == 0) return kScatterPlain;
+        if (std::strcmp(e, "brick") == 0) return kScatterBrick;
     }
-    return (long long)U * V >= 4LL * H * W;
+    return kScatterCells;
+}
+
+size_t fp_cell_floats(int D, int H, int W) {
+    return (size_t)8 * (size_t)(D + 2) * (size_t)(H + 1) * (size_t)(W + 1);
+}
+
+void fp_fill_cell_layout(FpArgs& p) {
+    // cell record index of padded cell (floor+1) from the biased floors
+    p.gz_x = (uint32_t)(p.D + 2);
+    p.gz_y = (uint32_t)(p.W + 1) * (uint32_t)(p.D + 2);
+    p.gz_bias = (1u + p.gz_x + p.gz_y) - kFloorMagicBits * (1u + p.gz_x + p.gz_y);
+}
+
+int fp_fold_cells(const float* cells, int D, int H, int W, float* grad, cudaStream_t s) {
+    DGC_TRACE("fold_cell_gradient", s);
+    const long long total = (long long)D * H * W;
+    const int blocks = (int)std::min<long long>((total + 255) / 256, 148LL * 16);
+    fold_cell_gradient_kernel<<<blocks, 256, 0, s>>>(cells, D, H, W, grad);
+    DGC_LAUNCH_CHECK("fold_cell_gradient");
+    return DGC_OK;
 }
 
 long long fp_tiles_per_view(int U, int V, int tu) {

@@ -29,9 +29,16 @@ def _align(n):
     return (n + 255) // 256 * 256
 
 
-def test_workspace_bytes_follow_the_layout():
+@pytest.mark.parametrize("scatter", [None, "pairs"])
+def test_workspace_bytes_follow_the_layout(scatter, monkeypatch):
+    """Volume-gradient buffers: 32-byte cell records over (D+2)(H+1)(W+1)
+    cells by default, the padded volume with DGC_SCATTER=pairs."""
     from cbct_backprojector import _native
 
+    if scatter:
+        monkeypatch.setenv("DGC_SCATTER", scatter)
+    else:
+        monkeypatch.delenv("DGC_SCATTER", raising=False)
     lib = _native.lib()
     specs = [(24, 20, 16, 12, 40, 36, 8), (9, 31, 27, 7, 33, 65, 4), (5, 7, 6, 33, 12, 9, 0)]
     for gv in (True, False):
@@ -41,7 +48,9 @@ def test_workspace_bytes_follow_the_layout():
             tu = tb or 8
             tiles = math.ceil(U / tu) * math.ceil(V / (256 // tu))
             per += _align(16 * (D + 2) * (H + 1) * (W + 1)) + _align(8 * 8 * A * tiles)
-            if gv:
+            if gv and scatter is None:
+                per += _align(32 * (D + 2) * (H + 1) * (W + 1))
+            elif gv:
                 per += _align(4 * (D + 2) * (H + 2) * (W + 2))
         n = len(specs)
         table = got - per - 5 * _align(8 * (n + 1)) - _align(16)

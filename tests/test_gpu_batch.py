@@ -56,9 +56,12 @@ def plain(pr):
     return p.detach(), grads[0], torch.stack(grads[1:])
 
 
-def test_batch_matches_plain_calls():
+@pytest.mark.parametrize("scatter", ["cells", "pairs", "plain"])
+def test_batch_matches_plain_calls(scatter, monkeypatch):
+    """Every volume-gradient scatter: batched launches against per-problem calls."""
     from cbct_backprojector.batch import ProjectionBatch
 
+    monkeypatch.setenv("DGC_SCATTER", scatter)
     problems = make_problems()
     batch = ProjectionBatch(problems)
     batch.step()
