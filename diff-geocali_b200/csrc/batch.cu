@@ -27,8 +27,9 @@ size_t quads_bytes(const dgc_fp_instance& in) {
 
 // volume-gradient buffer: cell records or the padded volume (fp_volume_scatter)
 size_t gpad_bytes(const dgc_fp_instance& in) {
-    if (fp_volume_scatter() == kScatterCells)
-        return align256(sizeof(float) * fp_cell_floats(in.D, in.H, in.W));
+    const VolumeScatter scatter = fp_volume_scatter();
+    if (fp_record_floats(scatter) > 0)
+        return align256(sizeof(float) * fp_record_buffer_floats(scatter, in.D, in.H, in.W));
     return align256(sizeof(float) * (size_t)(in.D + 2) * (size_t)(in.H + 2) * (size_t)(in.W + 2));
 }
 
@@ -171,7 +172,7 @@ int dgc_batch_prepare(const dgc_fp_instance* instances, int n, void* workspace,
         if (in.grad_volume) {
             p.grad_pad = reinterpret_cast<float*>(base + gpad_off + gpad_total);
             gpad_total += gpad_bytes(in);
-            if (scatter == kScatterCells) fp_fill_cell_layout(p);
+            if (fp_record_floats(scatter) > 0) fp_fill_cell_layout(p);
         }
         b.volume = in.volume;
         b.grad_volume = in.grad_volume;
@@ -182,7 +183,8 @@ int dgc_batch_prepare(const dgc_fp_instance* instances, int n, void* workspace,
         b.flags = (is_pow2_float(in.voxel_size) ? 0 : kBatchDiv) |
                   ((in.off_x != 0.0f || in.off_y != 0.0f || in.off_z != 0.0f) ? kBatchOff : 0) |
                   (scatter == kScatterPairs ? kBatchMerge : 0) |
-                  (scatter == kScatterCells ? kBatchCells : 0);
+                  (scatter == kScatterCells ? kBatchCells : 0) |
+                  (scatter == kScatterLevels ? kBatchLevels : 0);
         b.quad_gx = ceil_div(in.W + 1, 32) * (in.H + 1);
         b.tiles_bwd = fp_tiles_per_view(in.U, in.V, b.tile_bwd);
         host[i] = b;

@@ -52,8 +52,12 @@ size_t padded_volume_bytes(int D, int H, int W) {
     return Workspace::align(sizeof(float) * (size_t)(D + 2) * (size_t)(H + 2) * (size_t)(W + 2));
 }
 
-size_t cell_volume_bytes(int D, int H, int W) {
-    return Workspace::align(sizeof(float) * fp_cell_floats(D, H, W));
+// volume-gradient buffer of the selected scatter (fp_volume_scatter)
+size_t gradient_buffer_bytes(int D, int H, int W) {
+    const VolumeScatter scatter = fp_volume_scatter();
+    if (fp_record_floats(scatter) > 0)
+        return Workspace::align(sizeof(float) * fp_record_buffer_floats(scatter, D, H, W));
+    return padded_volume_bytes(D, H, W);
 }
 
 // Ray tile of the forward projector: DGC_FP_TILE="tu,wu" overrides the default.
@@ -227,7 +231,7 @@ size_t dgc_project_backward_workspace_bytes(int D, int H, int W, int A, int U, i
                                             int compute_grad_volume) {
     if (D <= 0 || H <= 0 || W <= 0 || A <= 0 || U <= 0 || V <= 0) return 0;
     size_t n = quad_volume_bytes(D, H, W);
-    if (compute_grad_volume) n += std::max(padded_volume_bytes(D, H, W), cell_volume_bytes(D, H, W));
+    if (compute_grad_volume) n += gradient_buffer_bytes(D, H, W);
     n += Workspace::align(sizeof(double) * 8 * (size_t)A *
                           (size_t)fp_tiles_per_view(U, V, kBackwardTile.tu));
     return n;
@@ -272,8 +276,10 @@ int dgc_project_backward(const float* grad_projection, const float* volume, int 
     const long long tiles = fp_tiles_per_view(U, V, kBackwardTile.tu);
     Workspace ws(workspace, workspace_bytes);
     float4* quads = ws.take<float4>((size_t)(D + 2) * (H + 1) * (W + 1));
-    const bool cells = compute_grad_volume && fp_volume_scatter() == kScatterCells;
-    const size_t gfloats = cells ? fp_cell_floats(D, H, W) : (size_t)(D + 2) * (H + 2) * (W + 2);
+    const VolumeScatter scatter = fp_volume_scatter();
+    const bool records = compute_grad_volume && fp_record_floats(scatter) > 0;
+    const size_t gfloats = records ? fp_record_buffer_floats(scatter, D, H, W)
+                                   : (size_t)(D + 2) * (H + 2) * (W + 2);
     float* gpad = compute_grad_volume ? ws.take<float>(gfloats) : nullptr;
     double* partials = ws.take<double>((size_t)8 * A * tiles);
     if (!quads || !partials || (compute_grad_volume && !gpad)) {
@@ -289,14 +295,14 @@ int dgc_project_backward(const float* grad_projection, const float* volume, int 
     p.partials = partials;
     rc = build_volume_quads(volume, D, H, W, quads, s);
     if (rc != DGC_OK) return rc;
-    if (cells) fp_fill_cell_layout(p);
+    if (records) fp_fill_cell_layout(p);
     if (gpad) DGC_CUDA(cudaMemsetAsync(gpad, 0, sizeof(float) * gfloats, s));
     rc = fp_launch_backward(p, kBackwardTile, compute_grad_volume != 0, s);
     if (rc != DGC_OK) return rc;
     rc = fp_reduce_partials(partials, A, tiles, out, s);
     if (rc != DGC_OK) return rc;
-    if (gpad) return cells ? fp_fold_cells(gpad, D, H, W, grad_volume, s)
-                           : fp_fold_gradient(gpad, D, H, W, grad_volume, s);
+    if (gpad) return records ? fp_fold_records(scatter, gpad, D, H, W, grad_volume, s)
+                             : fp_fold_gradient(gpad, D, H, W, grad_volume, s);
     return DGC_OK;
 }
 

@@ -494,16 +494,23 @@ __device__ __forceinline__ void scatter_cell_pairwise(const FpArgs& p, uint32_t 
     }
 }
 
-// The eight weights of a sample into the cell-major buffer: record ci (32
-// bytes) holds the weights of the corners ci + (dz, dy, dx) at k = dz*4 + dy*2
-// + dx, and fold_cell_gradient_kernel sums the records onto the voxels.  Lane
-// pairs merge first, as in scatter_cell_pairwise: the same cell gives one
-// 16-byte reduction per lane (even lane the z level, odd lane z+1), cells
-// adjacent in z give three (the corners the two share go into the upper cell's
-// z-level record), other pairs four.  The z stride of the records is D+2, so
-// a cell index difference of +-1 always means the same (x, y) column.
+// The eight weights of a sample into a cell-major buffer of records, RS
+// floats per cell at cell index ci (z stride D+2, so a cell-index difference
+// of +-1 always means the same (x, y) column):
+//   RS = 8 (cells): record ci holds the weights of the corners ci + (dz, dy,
+//     dx) at k = dz*4 + dy*2 + dx -- the sample's z level at o[0..3], its
+//     z+1 level at o[4..7];
+//   RS = 4 (levels): record ci holds the corners ci + (0, dy, dx) at k = dy*2
+//     + dx, so the sample's z+1 level is the next record, again at o[4..7].
+// fold_record_voxel sums the records onto the voxels.  Lane pairs merge first,
+// as in scatter_cell_pairwise: the same cell gives one 16-byte reduction per
+// lane (even lane the z level, odd lane z+1), cells adjacent in z give three
+// (the corners the two share go to the upper cell's z level, o[0..3] of its
+// record), other pairs four.
+template <int RS>
 __device__ __forceinline__ void scatter_cell_records(const FpArgs& p, uint32_t ci, float (&lo)[4],
                                                      float (&hi)[4]) {
+    static_assert(RS == 8 || RS == 4, "records of 8 (cells) or 4 (levels) floats");
     const unsigned mask = __activemask();
     const int lane = threadIdx.x & 31;
     const int partner = lane ^ 1;
@@ -518,7 +525,7 @@ __device__ __forceinline__ void scatter_cell_records(const FpArgs& p, uint32_t c
     // cell of the odd lane minus cell of the even lane
     const int d = (int)(odd ? ci - cpart : cpart - ci);
     const int mode = !((mask >> partner) & 1u) ? 0 : d == 0 ? 1 : d == 1 ? 2 : d == -1 ? 3 : 0;
-    float* o = p.grad_pad + 8ull * ci;
+    float* o = p.grad_pad + (unsigned long long)RS * ci;
     if (mode == 1) {
         if (odd)
             red_add4_global(o + 4, hi[0] + phi[0], hi[1] + phi[1], hi[2] + phi[2], hi[3] + phi[3]);
@@ -547,8 +554,8 @@ __device__ __forceinline__ void scatter_cell_records(const FpArgs& p, uint32_t c
 }
 
 // GV: 0 = no volume gradient, 1 = scatter every sample's eight weights,
-// 2 = merge them across lane pairs first (scatter_cell_pairwise), 3 = merge
-// lane pairs into per-cell 32-byte records (scatter_cell_records).
+// 2 = merge them across lane pairs first (scatter_cell_pairwise), 3 / 4 =
+// merge lane pairs into per-cell records of 8 / 4 floats (scatter_cell_records).
 template <bool CLAMP, int GV>
 __device__ __forceinline__ RayGrad march_grad(const RaySetup& r, const ViewGeo& vg,
                                               const FpArgs& p, float gs) {
@@ -593,7 +600,9 @@ __device__ __forceinline__ RayGrad march_grad(const RaySetup& r, const ViewGeo& 
             float hi[4] = {w00 * c.fz, w01 * c.fz, w10 * c.fz, w11 * c.fz};
             const uint32_t gi = c.bz + c.bx * p.gz_x + c.by * p.gz_y + p.gz_bias;
             if (GV == 3) {
-                scatter_cell_records(p, gi, lo, hi);
+                scatter_cell_records<8>(p, gi, lo, hi);
+            } else if (GV == 4) {
+                scatter_cell_records<4>(p, gi, lo, hi);
             } else if (GV == 2) {
                 scatter_cell_pairwise(p, gi, lo, hi);
             } else {
@@ -1128,51 +1137,52 @@ __global__ void fold_padded_gradient_kernel(const float* __restrict__ gpad, int 
         grad[i] = fold_voxel(gpad, D, H, W, i);
 }
 
-// Volume gradient from the cell-major buffer O[((cy*(W+1) + cx)*(D+2) + cz)*8 + k]
-// (cells at padded index floor+1 in [0, n], z stride D+2 with the record at
-// cz = D+1 unused; record k = dz*4 + dy*2 + dx the weight of corner (dz, dy,
-// dx)): a padded corner P gets record P - d of every cell with P - d in range,
-// and padded corners fold onto clamped voxels as in fold_padded_gradient_kernel.
-__device__ __forceinline__ float fold_cell_voxel(const float* __restrict__ O, int D, int H, int W,
-                                                 long long i) {
+// Volume gradient from a cell-major record buffer O[((cy*(W+1) + cx)*(D+2) + cz)*RS + k]
+// (scatter_cell_records; cells at padded index floor+1 in [0, n]): a padded
+// corner P gets entry k of record P - (dz, dy, dx) for every record in range
+// (cells: cz <= D, dz = k >> 2; levels: cz <= D+1, dz = 0), and padded corners
+// fold onto clamped voxels as in fold_padded_gradient_kernel.
+template <int RS>
+__device__ __forceinline__ float fold_record_voxel(const float* __restrict__ O, int D, int H, int W,
+                                                   long long i) {
     const long long CZ = D + 2, CX = W + 1;
-    {
-        const int x = (int)(i % W);
-        const long long r = i / W;
-        const int y = (int)(r % H);
-        const int z = (int)(r / H);
-        int xs[3], ys[3], zs[3];
-        int nx = 0, ny = 0, nz = 0;
-        xs[nx++] = x + 1;
-        if (x == 0) xs[nx++] = 0;
-        if (x == W - 1) xs[nx++] = W + 1;
-        ys[ny++] = y + 1;
-        if (y == 0) ys[ny++] = 0;
-        if (y == H - 1) ys[ny++] = H + 1;
-        zs[nz++] = z + 1;
-        if (z == 0) zs[nz++] = 0;
-        if (z == D - 1) zs[nz++] = D + 1;
-        float acc = 0.0f;
-        for (int iy = 0; iy < ny; ++iy)
-            for (int ix = 0; ix < nx; ++ix)
-                for (int iz = 0; iz < nz; ++iz)
+    const int zmax = RS == 8 ? D : D + 1;
+    const int x = (int)(i % W);
+    const long long r = i / W;
+    const int y = (int)(r % H);
+    const int z = (int)(r / H);
+    int xs[3], ys[3], zs[3];
+    int nx = 0, ny = 0, nz = 0;
+    xs[nx++] = x + 1;
+    if (x == 0) xs[nx++] = 0;
+    if (x == W - 1) xs[nx++] = W + 1;
+    ys[ny++] = y + 1;
+    if (y == 0) ys[ny++] = 0;
+    if (y == H - 1) ys[ny++] = H + 1;
+    zs[nz++] = z + 1;
+    if (z == 0) zs[nz++] = 0;
+    if (z == D - 1) zs[nz++] = D + 1;
+    float acc = 0.0f;
+    for (int iy = 0; iy < ny; ++iy)
+        for (int ix = 0; ix < nx; ++ix)
+            for (int iz = 0; iz < nz; ++iz)
 #pragma unroll
-                    for (int k = 0; k < 8; ++k) {
-                        const int dz = k >> 2, dy = (k >> 1) & 1, dx = k & 1;
-                        const int cz = zs[iz] - dz, cy = ys[iy] - dy, cx = xs[ix] - dx;
-                        if (cz < 0 || cz > D || cy < 0 || cy > H || cx < 0 || cx > W) continue;
-                        acc += O[((cy * CX + cx) * CZ + cz) * 8 + k];
-                    }
-        return acc;
-    }
+                for (int k = 0; k < RS; ++k) {
+                    const int dz = k >> 2, dy = (k >> 1) & 1, dx = k & 1;
+                    const int cz = zs[iz] - dz, cy = ys[iy] - dy, cx = xs[ix] - dx;
+                    if (cz < 0 || cz > zmax || cy < 0 || cy > H || cx < 0 || cx > W) continue;
+                    acc += O[((cy * CX + cx) * CZ + cz) * RS + k];
+                }
+    return acc;
 }
 
-__global__ void fold_cell_gradient_kernel(const float* __restrict__ O, int D, int H, int W,
-                                          float* __restrict__ grad) {
+template <int RS>
+__global__ void fold_record_gradient_kernel(const float* __restrict__ O, int D, int H, int W,
+                                            float* __restrict__ grad) {
     const long long total = (long long)D * H * W;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
          i += (long long)gridDim.x * blockDim.x)
-        grad[i] = fold_cell_voxel(O, D, H, W, i);
+        grad[i] = fold_record_voxel<RS>(O, D, H, W, i);
 }
 
 // ---------------------------------------------------------------------------
@@ -1290,6 +1300,7 @@ __device__ __forceinline__ void backward_item(const FpArgs& p, const ViewGeo& vg
     tile_ray<TU>(tc, u, v);
     if (!p.grad_pad) backward_ray<0>(p, vg, tc.a, u, v, terms);
     else if (flags & kBatchCells) backward_ray<3>(p, vg, tc.a, u, v, terms);
+    else if (flags & kBatchLevels) backward_ray<4>(p, vg, tc.a, u, v, terms);
     else if (flags & kBatchMerge) backward_ray<2>(p, vg, tc.a, u, v, terms);
     else backward_ray<1>(p, vg, tc.a, u, v, terms);
 }
@@ -1338,7 +1349,10 @@ __global__ void __launch_bounds__(256) batch_fold_kernel(BatchTables t) {
     const long long v1 = v0 + kFoldChunk < total ? v0 + kFoldChunk : total;
     if (in.flags & kBatchCells) {
         for (long long v = v0 + threadIdx.x; v < v1; v += blockDim.x)
-            in.grad_volume[v] = fold_cell_voxel(in.p.grad_pad, in.p.D, in.p.H, in.p.W, v);
+            in.grad_volume[v] = fold_record_voxel<8>(in.p.grad_pad, in.p.D, in.p.H, in.p.W, v);
+    } else if (in.flags & kBatchLevels) {
+        for (long long v = v0 + threadIdx.x; v < v1; v += blockDim.x)
+            in.grad_volume[v] = fold_record_voxel<4>(in.p.grad_pad, in.p.D, in.p.H, in.p.W, v);
     } else {
         for (long long v = v0 + threadIdx.x; v < v1; v += blockDim.x)
             in.grad_volume[v] = fold_voxel(in.p.grad_pad, in.p.D, in.p.H, in.p.W, v);
@@ -1392,6 +1406,7 @@ int launch_backward_tu(const FpArgs& p, bool gradvol, cudaStream_t s) {
     } else {
         switch (fp_volume_scatter()) {
             case kScatterCells: fp_backward_kernel<TU, 3><<<(unsigned)blocks, 256, 0, s>>>(p); break;
+            case kScatterLevels: fp_backward_kernel<TU, 4><<<(unsigned)blocks, 256, 0, s>>>(p); break;
             case kScatterPairs: fp_backward_kernel<TU, 2><<<(unsigned)blocks, 256, 0, s>>>(p); break;
             default: fp_backward_kernel<TU, 1><<<(unsigned)blocks, 256, 0, s>>>(p); break;
         }
@@ -1403,20 +1418,27 @@ int launch_backward_tu(const FpArgs& p, bool gradvol, cudaStream_t s) {
 }  // namespace
 
 VolumeScatter fp_volume_scatter() {
-    // Cell records by default: at 256^3 / 360 x 384^2, 128^3 / 180 x 256^2 and
-    // 256^3 / 90 x 192^2 the backward took 452 / 46 / 31 ms with them against
-    // 554 / 58 / 36 ms with lane pairs merged into the padded buffer and
-    // 682 / 81 / 45 ms with every sample alone.
+    // Level records by default: the backward (sid 1000, sod 600, step 0.5) at
+    // 256^3 / 360 x 384^2, 128^3 / 180 x 256^2 and 512^3 / 90 x 512^2 took
+    // 163 / 15.3 / 181 ms with them, 170 / 15.7 / 201 ms with cell records,
+    // 206 / 19.1 / 221 ms with lane pairs merged into the padded buffer and
+    // 215 / 18.5 / 273 ms with every sample alone.
     if (const char* e = std::getenv("DGC_SCATTER")) {
         if (std::strcmp(e, "pairs") == 0) return kScatterPairs;
         if (std::strcmp(e, "plain") == 0) return kScatterPlain;
         if (std::strcmp(e, "brick") == 0) return kScatterBrick;
+        if (std::strcmp(e, "cells") == 0) return kScatterCells;
+        if (std::strcmp(e, "levels") == 0) return kScatterLevels;
     }
-    return kScatterCells;
+    return kScatterLevels;
 }
 
-size_t fp_cell_floats(int D, int H, int W) {
-    return (size_t)8 * (size_t)(D + 2) * (size_t)(H + 1) * (size_t)(W + 1);
+int fp_record_floats(VolumeScatter scatter) {
+    return scatter == kScatterCells ? 8 : scatter == kScatterLevels ? 4 : 0;
+}
+
+size_t fp_record_buffer_floats(VolumeScatter scatter, int D, int H, int W) {
+    return (size_t)fp_record_floats(scatter) * (size_t)(D + 2) * (size_t)(H + 1) * (size_t)(W + 1);
 }
 
 void fp_fill_cell_layout(FpArgs& p) {
@@ -1426,12 +1448,16 @@ void fp_fill_cell_layout(FpArgs& p) {
     p.gz_bias = (1u + p.gz_x + p.gz_y) - kFloorMagicBits * (1u + p.gz_x + p.gz_y);
 }
 
-int fp_fold_cells(const float* cells, int D, int H, int W, float* grad, cudaStream_t s) {
-    DGC_TRACE("fold_cell_gradient", s);
+int fp_fold_records(VolumeScatter scatter, const float* records, int D, int H, int W, float* grad,
+                    cudaStream_t s) {
+    DGC_TRACE("fold_record_gradient", s);
     const long long total = (long long)D * H * W;
     const int blocks = (int)std::min<long long>((total + 255) / 256, 148LL * 16);
-    fold_cell_gradient_kernel<<<blocks, 256, 0, s>>>(cells, D, H, W, grad);
-    DGC_LAUNCH_CHECK("fold_cell_gradient");
+    if (scatter == kScatterCells)
+        fold_record_gradient_kernel<8><<<blocks, 256, 0, s>>>(records, D, H, W, grad);
+    else
+        fold_record_gradient_kernel<4><<<blocks, 256, 0, s>>>(records, D, H, W, grad);
+    DGC_LAUNCH_CHECK("fold_record_gradient");
     return DGC_OK;
 }
 

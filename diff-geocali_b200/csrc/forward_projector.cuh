@@ -30,7 +30,7 @@ struct FpTile {
 };
 
 // One instance of a batched launch (an entry of the device-resident table).
-enum : int { kBatchDiv = 1, kBatchOff = 2, kBatchMerge = 4, kBatchCells = 8 };
+enum : int { kBatchDiv = 1, kBatchOff = 2, kBatchMerge = 4, kBatchCells = 8, kBatchLevels = 16 };
 constexpr int kFoldChunk = 2048;
 
 struct BatchInstance {
@@ -41,7 +41,8 @@ struct BatchInstance {
     int tile_fwd, tile_bwd;  // columns per CTA tile (forward 8/4/2, backward 8/4)
     int flags;             // kBatchDiv (non power-of-two voxel) | kBatchOff (non-zero ROI
                            // offset) | kBatchMerge (lane-pair merged scatter) |
-                           // kBatchCells (lane pairs merged into cell records)
+                           // kBatchCells / kBatchLevels (lane pairs merged into
+                           // cell records of 8 / 4 floats)
     int quad_gx;           // blocks along x of the quads build
     long long tiles_bwd;   // backward tiles per view
 };
@@ -70,18 +71,24 @@ int fp_check_args(int D, int H, int W, int A, int U, int V, float pixel_size, fl
 
 void fp_fill_layout(FpArgs& p);
 long long fp_tiles_per_view(int U, int V, int tu);
-// Volume-gradient scatter of the backward.  kScatterCells (the default) adds
-// lane-pair-merged weights as 16-byte vector reductions into a cell-major
-// buffer of 32-byte records (fp_fill_cell_layout, fp_fold_cells); kScatterPlain
-// and kScatterPairs add single floats into the padded buffer (every sample
-// alone, lane pairs merged first); kScatterBrick accumulates shared-memory
-// bricks flushed into the padded buffer (single-problem backward only; the
-// batched one scatters plain).  DGC_SCATTER=plain|pairs|cells|brick overrides.
-enum VolumeScatter : int { kScatterPlain = 1, kScatterPairs = 2, kScatterCells = 3, kScatterBrick = 4 };
+// Volume-gradient scatter of the backward.  kScatterLevels (the default) and
+// kScatterCells add lane-pair-merged weights as 16-byte vector reductions into
+// a cell-major buffer of records, 4 / 8 floats per cell (fp_fill_cell_layout,
+// fp_record_buffer_floats, fp_fold_records); kScatterPlain and kScatterPairs
+// add single floats into the padded buffer (every sample alone, lane pairs
+// merged first); kScatterBrick accumulates shared-memory bricks flushed into
+// the padded buffer (single-problem backward only; the batched one scatters
+// plain).  DGC_SCATTER=plain|pairs|cells|levels|brick overrides.
+enum VolumeScatter : int {
+    kScatterPlain = 1, kScatterPairs = 2, kScatterCells = 3, kScatterBrick = 4, kScatterLevels = 5
+};
 VolumeScatter fp_volume_scatter();
+// floats per cell record: 8 (cells), 4 (levels), 0 (padded-buffer scatters)
+int fp_record_floats(VolumeScatter scatter);
+size_t fp_record_buffer_floats(VolumeScatter scatter, int D, int H, int W);
 void fp_fill_cell_layout(FpArgs& p);
-size_t fp_cell_floats(int D, int H, int W);
-int fp_fold_cells(const float* cells, int D, int H, int W, float* grad, cudaStream_t s);
+int fp_fold_records(VolumeScatter scatter, const float* records, int D, int H, int W, float* grad,
+                    cudaStream_t s);
 int build_volume_quads(const float* vol, int D, int H, int W, float4* quads, cudaStream_t s);
 int fp_launch_forward(const FpArgs& p, const FpTile& tile, cudaStream_t s);
 int fp_launch_backward(const FpArgs& p, const FpTile& tile, bool gradvol, cudaStream_t s);

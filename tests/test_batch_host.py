@@ -31,7 +31,7 @@ def _align(n):
 
 @pytest.mark.parametrize("scatter", [None, "pairs"])
 def test_workspace_bytes_follow_the_layout(scatter, monkeypatch):
-    """Volume-gradient buffers: 32-byte cell records over (D+2)(H+1)(W+1)
+    """Volume-gradient buffers: 16-byte level records over (D+2)(H+1)(W+1)
     cells by default, the padded volume with DGC_SCATTER=pairs."""
     from cbct_backprojector import _native
 
@@ -49,7 +49,7 @@ def test_workspace_bytes_follow_the_layout(scatter, monkeypatch):
             tiles = math.ceil(U / tu) * math.ceil(V / (256 // tu))
             per += _align(16 * (D + 2) * (H + 1) * (W + 1)) + _align(8 * 8 * A * tiles)
             if gv and scatter is None:
-                per += _align(32 * (D + 2) * (H + 1) * (W + 1))
+                per += _align(16 * (D + 2) * (H + 1) * (W + 1))
             elif gv:
                 per += _align(4 * (D + 2) * (H + 2) * (W + 2))
         n = len(specs)

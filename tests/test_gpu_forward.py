@@ -184,12 +184,12 @@ def test_forward_matches_reference_cuda(which, golden, ref_native, oracle):
     assert rel_l2(ours.cpu(), truth) < FWD_RTOL
 
 
-@pytest.mark.parametrize("scatter", ["brick", "plain", "pairs", "cells"])
+@pytest.mark.parametrize("scatter", ["brick", "plain", "pairs", "cells", "levels"])
 @pytest.mark.parametrize("which", ["config1", "random_nonpow2"])
 def test_backward_matches_reference_cuda(which, scatter, golden, ref_native, oracle, monkeypatch):
-    """All four volume-gradient scatters: shared-memory bricks flushed once per
-    slab, every sample alone, lane pairs merged first, per-cell 32-byte
-    records folded afterwards."""
+    """Every volume-gradient scatter: shared-memory bricks flushed once per
+    slab, every sample alone, lane pairs merged first, lane pairs merged into
+    per-cell records of 8 or 4 floats folded afterwards."""
     monkeypatch.setenv("DGC_SCATTER", scatter)
     ref_fp, _ = ref_native
     case = config1_case(golden("fp_config1.npz")) if which == "config1" else random_case(5)
