@@ -322,6 +322,39 @@ def reconstruct_fdk_weighted(projections, geometry, pixel_size, volume_shape, vo
     return vol
 
 
+def reconstruct_fdk_partial(projections, geometry, pixel_size, volume_shape, voxel_size,
+                            volume_offset, alpha, uweights, angle_scale):
+    """This rank's unclamped share of a view-sharded reconstruction
+    (dgc_reconstruct_fdk_partial): filter + backproject its views, times
+    ``angle_scale``."""
+    p = projections.contiguous()
+    geom = [t.contiguous() for t in geometry]
+    w = None if uweights is None else uweights.contiguous()
+    A, U, V = p.shape
+    D, H, W = volume_shape
+    dev = p.device
+    vol = torch.empty((D, H, W), dtype=torch.float32, device=dev)
+    lib = _native.lib()
+    with torch.cuda.device(dev):
+        ws = _workspace(lib.dgc_reconstruct_fdk_workspace_bytes(A, U, V, D, H, W), dev)
+        _native.check(lib.dgc_reconstruct_fdk_partial(
+            p.data_ptr(), A, U, V, *[g.data_ptr() for g in geom], float(pixel_size), D, H, W,
+            float(voxel_size), *map(float, volume_offset), float(alpha), _p(w),
+            float(angle_scale), vol.data_ptr(), _p(ws), 0 if ws is None else ws.numel(),
+            _stream(dev)))
+    return vol
+
+
+def clamp_volume(volume):
+    """In-place clamp at zero (dgc_clamp_volume) of a contiguous float32 CUDA volume."""
+    _require(volume.is_cuda and volume.dtype == torch.float32 and volume.is_contiguous(),
+             "volume must be a contiguous float32 CUDA tensor")
+    with torch.cuda.device(volume.device):
+        _native.check(_native.lib().dgc_clamp_volume(volume.data_ptr(), volume.numel(),
+                                                     _stream(volume.device)))
+    return volume
+
+
 def fdk_filter_taps(U: int, pixel_size: float, alpha: float):
     """Host-only filter taps h[0..U-1] (FP64), for inspection and tests."""
     import ctypes

@@ -82,6 +82,52 @@ def fdk_filter(projections, pixel_size, sod, sid, alpha=0.8):
     return _ops.fdk_filter(projections, pixel_size, sod, sid, alpha)
 
 
+def _fdk_arguments(projections, geometry, pixel_size, volume_shape, voxel_size, volume_offset,
+                   alpha, angle_chunk_size):
+    """The argument checks of the reference's reconstruct_fdk
+    (filtering.py:107-198) on one rank's views; returns (pixel_size,
+    volume_shape, voxel_size, offset, alpha)."""
+    _check_projections(projections)
+    sid, sod = geometry[1], geometry[2]
+    if min(projections.shape[1:]) < 2:
+        raise ValueError("reconstruct_fdk requires detector dimensions U and V >= 2")
+    views = projections.shape[0]
+    names = ("angles", "sid", "sod", "det_u0", "det_v0", "src_x", "src_y", "src_z")
+    for name, t in zip(names, geometry):
+        if not isinstance(t, torch.Tensor):
+            raise TypeError(f"{name} must be a torch.Tensor of shape [A]")
+        if t.ndim != 1 or t.numel() != views:
+            raise ValueError(f"{name} must have shape [{views}]")
+        if t.dtype != projections.dtype or t.device != projections.device:
+            raise ValueError(f"{name} must match the projections' dtype and device")
+    if not bool(torch.isfinite(torch.stack(geometry)).all()):
+        raise ValueError("geometry must contain only finite values")
+    if bool((sid <= 0).any()) or bool((sod <= 0).any()):
+        raise ValueError("sid and sod must contain positive distances")
+    pixel_size = _positive_scalar("pixel_size", pixel_size)
+    voxel_size = _positive_scalar("voxel_size", voxel_size)
+    alpha = _check_alpha(alpha)
+    try:
+        angle_chunk_size = operator.index(angle_chunk_size)
+        volume_shape = tuple(operator.index(s) for s in volume_shape)
+    except TypeError as error:
+        raise TypeError("angle_chunk_size and volume dimensions must be integers") from error
+    if angle_chunk_size < 1:
+        raise ValueError("angle_chunk_size must be at least 1")
+    if len(volume_shape) != 3 or min(volume_shape) < 1:
+        raise ValueError("volume_shape must contain three positive dimensions (D, H, W)")
+    if math.prod(volume_shape) > 2**31 - 1:
+        raise ValueError("volume exceeds the backprojector's 32-bit indexing limit")
+    if max(volume_shape[:2]) > 8 * 65535:
+        raise ValueError("D,H exceed the backprojector's 3D CUDA grid limits")
+    if min(views, angle_chunk_size) * math.prod(projections.shape[1:]) > 2**31 - 1:
+        raise ValueError("Reduce angle_chunk_size to fit the backprojector's 32-bit indexing limit")
+    offset = tuple(float(v) for v in volume_offset)
+    if len(offset) != 3 or not all(math.isfinite(v) for v in offset):
+        raise ValueError("volume_offset must contain three finite values")
+    return pixel_size, volume_shape, voxel_size, offset, alpha
+
+
 @torch.no_grad()
 def reconstruct_fdk(
     projections,
@@ -117,43 +163,11 @@ def reconstruct_fdk(
     _check_projections(projections)
     if not projections.is_cuda:
         raise ValueError("reconstruct_fdk requires CUDA projections")
-    if min(projections.shape[1:]) < 2:
-        raise ValueError("reconstruct_fdk requires detector dimensions U and V >= 2")
-    views = projections.shape[0]
     geometry = (angles, sid, sod, det_u0, det_v0, src_x, src_y, src_z)
-    names = ("angles", "sid", "sod", "det_u0", "det_v0", "src_x", "src_y", "src_z")
-    for name, t in zip(names, geometry):
-        if not isinstance(t, torch.Tensor):
-            raise TypeError(f"{name} must be a torch.Tensor of shape [A]")
-        if t.ndim != 1 or t.numel() != views:
-            raise ValueError(f"{name} must have shape [{views}]")
-        if t.dtype != projections.dtype or t.device != projections.device:
-            raise ValueError(f"{name} must match the projections' dtype and device")
-    if not bool(torch.isfinite(torch.stack(geometry)).all()):
-        raise ValueError("geometry must contain only finite values")
-    if bool((sid <= 0).any()) or bool((sod <= 0).any()):
-        raise ValueError("sid and sod must contain positive distances")
-    pixel_size = _positive_scalar("pixel_size", pixel_size)
-    voxel_size = _positive_scalar("voxel_size", voxel_size)
-    alpha = _check_alpha(alpha)
-    try:
-        angle_chunk_size = operator.index(angle_chunk_size)
-        volume_shape = tuple(operator.index(s) for s in volume_shape)
-    except TypeError as error:
-        raise TypeError("angle_chunk_size and volume dimensions must be integers") from error
-    if angle_chunk_size < 1:
-        raise ValueError("angle_chunk_size must be at least 1")
-    if len(volume_shape) != 3 or min(volume_shape) < 1:
-        raise ValueError("volume_shape must contain three positive dimensions (D, H, W)")
-    if math.prod(volume_shape) > 2**31 - 1:
-        raise ValueError("volume exceeds the backprojector's 32-bit indexing limit")
-    if max(volume_shape[:2]) > 8 * 65535:
-        raise ValueError("D,H exceed the backprojector's 3D CUDA grid limits")
-    if min(views, angle_chunk_size) * math.prod(projections.shape[1:]) > 2**31 - 1:
-        raise ValueError("Reduce angle_chunk_size to fit the backprojector's 32-bit indexing limit")
-    offset = tuple(float(v) for v in volume_offset)
-    if len(offset) != 3 or not all(math.isfinite(v) for v in offset):
-        raise ValueError("volume_offset must contain three finite values")
+    pixel_size, volume_shape, voxel_size, offset, alpha = _fdk_arguments(
+        projections, geometry, pixel_size, volume_shape, voxel_size, volume_offset, alpha,
+        angle_chunk_size)
+    views = projections.shape[0]
     if short_scan:
         a0, a1 = float(angles[0]), float(angles[-1])
         span = abs(a1 - a0)

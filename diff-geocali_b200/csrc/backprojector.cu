@@ -189,7 +189,7 @@ __global__ void __launch_bounds__(256) bp_forward_kernel(BpArgs p) {
         float val = acc[k];
         if (FDK) {
             val *= p.out_scale;
-            val = val < 0.0f ? 0.0f : val;  // clamp_min(0); NaN propagates
+            if (p.clamp) val = val < 0.0f ? 0.0f : val;  // clamp_min(0); NaN propagates
         }
         s_out[lane + 32 * k][warp] = val;
     }
@@ -412,6 +412,22 @@ int bp_launch_backward(const BpArgs& p, cudaStream_t s) {
         default: bp_backward_kernel<8><<<grid, 256, 0, s>>>(p); break;
     }
     DGC_LAUNCH_CHECK("bp_backward_kernel");
+    return DGC_OK;
+}
+
+__global__ void clamp_volume_kernel(float* __restrict__ v, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const float x = v[i];
+        v[i] = x < 0.0f ? 0.0f : x;  // as the FDK epilogue: NaN propagates
+    }
+}
+
+int bp_clamp_volume(float* volume, long long n, cudaStream_t s) {
+    DGC_TRACE("clamp_volume", s);
+    const int blocks = (int)std::min<long long>((n + 255) / 256, 148LL * 16);
+    clamp_volume_kernel<<<blocks, 256, 0, s>>>(volume, n);
+    DGC_LAUNCH_CHECK("clamp_volume");
     return DGC_OK;
 }
 

@@ -23,6 +23,7 @@ struct BpArgs {
     // forward
     float* volume;     // [D][H][W]
     float out_scale;   // FDK epilogue scale (pi/A)
+    int clamp;         // FDK epilogue: clamp at 0 (0 for a view-sharded partial volume)
     // backward
     const float* grad_volume;  // [D][H][W]
     float* grad_projections;   // [A][U][V], zeroed by the caller
@@ -33,6 +34,7 @@ int bp_view_table(const Geometry& g, int A, ViewRow* vt, cudaStream_t s);
 int build_proj_quads(const float* P, int A, int U, int V, float4* PQ, cudaStream_t s);
 int bp_launch_forward(const BpArgs& p, bool fdk, cudaStream_t s);
 int bp_launch_backward(const BpArgs& p, cudaStream_t s);
+int bp_clamp_volume(float* volume, long long n, cudaStream_t s);
 long long bp_backward_blocks(int D, int H, int W);
 int bp_reduce_partials(const double* partials, int A, long long nblocks, const GeometryGrad& out,
                        cudaStream_t s);

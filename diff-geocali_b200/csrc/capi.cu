@@ -131,6 +131,7 @@ BpArgs bp_args(const ViewRow* vt, const float4* pq, int A, int U, int V, int D, 
     p.off_y = oy;
     p.off_z = oz;
     p.out_scale = 1.0f;
+    p.clamp = 1;
     return p;
 }
 
@@ -520,7 +521,7 @@ static int reconstruct_fdk_impl(const float* projections, int A, int U, int V,
                                 const float* src_y, const float* src_z, float pixel_size, int D,
                                 int H, int W, float voxel_size, float off_x, float off_y,
                                 float off_z, float alpha, const float* uweights,
-                                float angle_scale, float* volume, void* workspace,
+                                float angle_scale, bool clamp, float* volume, void* workspace,
                                 size_t workspace_bytes, void* stream) {
     clear_error();
     cudaStream_t s = (cudaStream_t)stream;
@@ -548,6 +549,7 @@ static int reconstruct_fdk_impl(const float* projections, int A, int U, int V,
     BpArgs p = bp_args(vt, pq, A, U, V, D, H, W, pixel_size, voxel_size, off_x, off_y, off_z);
     p.volume = volume;
     p.out_scale = angle_scale;
+    p.clamp = clamp ? 1 : 0;
     return bp_launch_forward(p, true, s);
 }
 
@@ -559,8 +561,8 @@ int dgc_reconstruct_fdk(const float* projections, int A, int U, int V, const flo
                         float* volume, void* workspace, size_t workspace_bytes, void* stream) {
     return reconstruct_fdk_impl(projections, A, U, V, angles, sid, sod, det_u0, det_v0, src_x,
                                 src_y, src_z, pixel_size, D, H, W, voxel_size, off_x, off_y, off_z,
-                                alpha, nullptr, (float)(M_PI / (double)A), volume, workspace,
-                                workspace_bytes, stream);
+                                alpha, nullptr, (float)(M_PI / (double)A), true, volume,
+                                workspace, workspace_bytes, stream);
 }
 
 int dgc_reconstruct_fdk_weighted(const float* projections, int A, int U, int V,
@@ -576,8 +578,33 @@ int dgc_reconstruct_fdk_weighted(const float* projections, int A, int U, int V,
                 "angle_scale must be positive and finite");
     return reconstruct_fdk_impl(projections, A, U, V, angles, sid, sod, det_u0, det_v0, src_x,
                                 src_y, src_z, pixel_size, D, H, W, voxel_size, off_x, off_y, off_z,
-                                alpha, uweights, angle_scale, volume, workspace, workspace_bytes,
-                                stream);
+                                alpha, uweights, angle_scale, true, volume, workspace,
+                                workspace_bytes, stream);
+}
+
+int dgc_reconstruct_fdk_partial(const float* projections, int A, int U, int V,
+                                const float* angles, const float* sid, const float* sod,
+                                const float* det_u0, const float* det_v0, const float* src_x,
+                                const float* src_y, const float* src_z, float pixel_size, int D,
+                                int H, int W, float voxel_size, float off_x, float off_y,
+                                float off_z, float alpha, const float* uweights,
+                                float angle_scale, float* volume, void* workspace,
+                                size_t workspace_bytes, void* stream) {
+    clear_error();
+    DGC_REQUIRE(std::isfinite(angle_scale) && angle_scale > 0.0f,
+                "angle_scale must be positive and finite");
+    return reconstruct_fdk_impl(projections, A, U, V, angles, sid, sod, det_u0, det_v0, src_x,
+                                src_y, src_z, pixel_size, D, H, W, voxel_size, off_x, off_y, off_z,
+                                alpha, uweights, angle_scale, false, volume, workspace,
+                                workspace_bytes, stream);
+}
+
+int dgc_clamp_volume(float* volume, long long n, void* stream) {
+    clear_error();
+    DGC_REQUIRE(n >= 0, "n must be non-negative");
+    DGC_REQUIRE(volume || n == 0, "volume must be non-null");
+    if (n == 0) return DGC_OK;
+    return bp_clamp_volume(volume, n, (cudaStream_t)stream);
 }
 
 int dgc_parker_weights(const float* angles, const float* sid, int A, int U, float pixel_size,

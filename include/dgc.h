@@ -215,6 +215,26 @@ int dgc_reconstruct_fdk_weighted(const float* projections, int A, int U, int V,
                                  const float* uweights, float angle_scale, float* volume,
                                  void* workspace, size_t workspace_bytes, void* stream);
 
+/* One rank's share of a view-sharded FDK reconstruction: dgc_reconstruct_fdk_weighted
+ * over this rank's views without the final clamp, so that the partial volumes
+ * of all ranks can be summed (an all-reduce) before dgc_clamp_volume.
+ * angle_scale is pi / (views over all ranks) for a full scan.  Same workspace
+ * as dgc_reconstruct_fdk.  The reference reconstructs on one device
+ * (filtering.py:107-198); no counterpart there. */
+int dgc_reconstruct_fdk_partial(const float* projections, int A, int U, int V,
+                                const float* angles, const float* sid, const float* sod,
+                                const float* det_u0, const float* det_v0,
+                                const float* src_x, const float* src_y, const float* src_z,
+                                float pixel_size, int D, int H, int W, float voxel_size,
+                                float off_x, float off_y, float off_z, float alpha,
+                                const float* uweights, float angle_scale, float* volume,
+                                void* workspace, size_t workspace_bytes, void* stream);
+
+/* volume[i] = max(volume[i], 0) in place (NaN stays NaN): the clamp that ends
+ * an FDK reconstruction (filtering.py:197), after the partial volumes of a
+ * view-sharded reconstruction have been summed. */
+int dgc_clamp_volume(float* volume, long long n, void* stream);
+
 /* ---------------------------------------------------------------------- */
 /* Tensor-core GEMM of the warm-start network (no counterpart in the        */
 /* reference: its calibration pipeline is not shipped)                      */

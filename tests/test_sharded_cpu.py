@@ -1,0 +1,125 @@
+"""View-sharded operators on the CPU: two ``gloo`` ranks (the process-group
+calls an NCCL run makes).  Each rank's local operator is replaced by a CPU
+stand-in -- the FP64 oracle's filter and backprojection for the FDK
+reconstruction, fixed random linear maps for ``project`` / ``backproject`` --
+so what is checked is the sharding: the view ranges, the sum of the partial
+volumes before the clamp, the pi / (views of the whole scan) factor, and
+where autograd sums gradients over the ranks."""
+
+import os
+import socket
+from datetime import timedelta
+
+import pytest
+import torch.multiprocessing as mp
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def test_view_shard_ranges():
+    from cbct_backprojector.sharded import view_shard
+
+    for views in (0, 1, 7, 360):
+        for world in (1, 2, 3, 8):
+            got = [view_shard(views, world, r) for r in range(world)]
+            assert [v for r in got for v in r] == list(range(views))
+            assert max(map(len, got)) - min(map(len, got)) <= 1
+    with pytest.raises(ValueError):
+        view_shard(4, 2, 2)
+
+
+def _rank(rank, world, port, out):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank),
+                      WORLD_SIZE=str(world), LOCAL_RANK=str(rank))
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from cbct_backprojector import sharded
+    from oracle import oracle as O
+
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
+    try:
+        res = {}
+        A, U, V, shape, px, vox, off, alpha = 11, 12, 10, (6, 7, 8), 1.0, 1.0, (0.3, -0.2, 0.1), 0.8
+        rng = np.random.default_rng(3)  # the same scan on every rank
+        proj = (rng.random((A, U, V)) * 4).astype(np.float32)
+        angles = np.arange(A) * (2 * np.pi / A)
+        cols = [angles, np.full(A, 300.0), np.full(A, 180.0), np.full(A, (U - 1) / 2),
+                np.full(A, (V - 1) / 2), rng.normal(0, 1, A), rng.normal(0, 1, A),
+                rng.normal(0, 1, A)]
+        geom = np.stack(cols).astype(np.float32)
+        mine = sharded.view_shard(A, world, rank)
+        res["views"] = (mine.start, mine.stop)
+        res["total"] = sharded.total_views(len(mine), "cpu")
+
+        # FDK: oracle filter + backprojection as the rank's partial volume
+        def partial(p, geometry, pixel, vshape, voxel, offset, a, scale):
+            g = np.stack([t.numpy() for t in geometry])
+            f = O.fdk_filter(p.numpy(), pixel, g[2], g[1], a)
+            return torch.from_numpy(O.backproject(f, g, pixel, vshape, voxel, offset) * scale)
+
+        sharded._partial_volume = partial
+        sharded._clamp = lambda v: v.clamp_min_(0.0)
+        local = [torch.from_numpy(geom[k, mine.start:mine.stop].copy()) for k in range(8)]
+        vol = sharded.reconstruct_fdk_sharded(
+            torch.from_numpy(proj[mine.start:mine.stop].copy()), *local, px, shape, vox,
+            volume_offset=off, alpha=alpha)
+        truth = O.reconstruct_fdk(proj, geom, px, shape, vox, off, alpha)
+        res["fdk_err"] = float(np.linalg.norm(vol.numpy() - truth) / np.linalg.norm(truth))
+        res["fdk_negative_clamped"] = bool((vol >= 0).all())
+
+        # project: linear stand-in p_a = M_a vol; loss = 0.5 sum over this rank's p^2
+        n = shape[0] * shape[1] * shape[2]
+        M = torch.from_numpy(rng.standard_normal((A, U * V, n)))
+        v0 = torch.from_numpy(rng.standard_normal(shape))
+        sharded.project = lambda volume, *rest: torch.einsum(
+            "apk,k->ap", M[mine.start:mine.stop], volume.reshape(-1)).reshape(-1, U, V)
+        v = v0.clone().requires_grad_()
+        p = sharded.project_sharded(v, *local, px, U, V, group=None)
+        (0.5 * p.square().sum()).backward()
+        vf = v0.clone().requires_grad_()
+        (0.5 * torch.einsum("apk,k->ap", M, vf.reshape(-1)).square().sum()).backward()
+        res["project_grad_err"] = float((v.grad - vf.grad).norm() / vf.grad.norm())
+
+        # backproject: linear stand-in vol = sum_a M_a^T p_a; loss = <vol, c>
+        c = torch.from_numpy(rng.standard_normal(n))
+        pr = torch.from_numpy(rng.standard_normal((A, U, V)))
+        sharded.backproject = lambda q, *rest: torch.einsum(
+            "apk,ap->k", M[mine.start:mine.stop], q.reshape(q.shape[0], -1)).reshape(shape)
+        q = pr[mine.start:mine.stop].clone().requires_grad_()
+        b = sharded.backproject_sharded(q, *local, px, shape, vox)
+        (b.reshape(-1) * c).sum().backward()
+        full = torch.einsum("apk,ap->k", M, pr.reshape(A, -1))
+        res["bp_value_err"] = float((b.detach().reshape(-1) - full).norm() / full.norm())
+        gfull = torch.einsum("apk,k->ap", M, c).reshape(A, U, V)[mine.start:mine.stop]
+        res["bp_grad_err"] = float((q.grad - gfull).norm() / gfull.norm())
+        out.put((rank, res))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.timeout(180)
+def test_two_gloo_ranks_sharded_views():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(150)
+    assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
+    got = dict(q.get(timeout=5) for _ in range(2))
+    assert got[0]["views"] == (0, 6) and got[1]["views"] == (6, 11)
+    for r in (0, 1):
+        res = got[r]
+        assert res["total"] == 11
+        assert res["fdk_err"] < 1e-6 and res["fdk_negative_clamped"], res
+        assert res["project_grad_err"] < 1e-12, res
+        assert res["bp_value_err"] < 1e-12 and res["bp_grad_err"] < 1e-12, res
