@@ -219,8 +219,11 @@ def bp_forward(proj, angles, sid, sod, det_u0_arr, det_v0_arr, src_x_arr, src_y_
 
 
 def bp_backward(grad_vol, proj, angles, sid, sod, det_u0_arr, det_v0_arr, src_x_arr, src_y_arr,
-                src_z_arr, pixel_size, voxel_size, off_x=0.0, off_y=0.0, off_z=0.0):
-    """Nine gradients (replaces ``src_cbct_backprojector_cuda.backward``)."""
+                src_z_arr, pixel_size, voxel_size, off_x=0.0, off_y=0.0, off_z=0.0,
+                compute_grad_proj=True):
+    """Nine gradients (replaces ``src_cbct_backprojector_cuda.backward``);
+    with ``compute_grad_proj=False`` the first is ``None`` and its scatter is
+    skipped."""
     geometry = (angles, sid, sod, det_u0_arr, det_v0_arr, src_x_arr, src_y_arr, src_z_arr)
     pixel_size, voxel_size = float(pixel_size), float(voxel_size)
     off_x, off_y, off_z = float(off_x), float(off_y), float(off_z)
@@ -238,14 +241,14 @@ def bp_backward(grad_vol, proj, angles, sid, sod, det_u0_arr, det_v0_arr, src_x_
     A, U, V = p.shape
     D, H, W = gv.shape
     dev = p.device
-    grad_proj = torch.zeros_like(p)
+    grad_proj = torch.empty_like(p) if compute_grad_proj else None
     grads = [torch.zeros_like(g) for g in geom]
     lib = _native.lib()
     with torch.cuda.device(dev):
         ws = _workspace(lib.dgc_backproject_backward_workspace_bytes(A, U, V, D, H, W), dev)
         _native.check(lib.dgc_backproject_backward(
             gv.data_ptr(), p.data_ptr(), A, U, V, *[g.data_ptr() for g in geom], pixel_size, D, H,
-            W, voxel_size, off_x, off_y, off_z, grad_proj.data_ptr(),
+            W, voxel_size, off_x, off_y, off_z, _p(grad_proj),
             *[g.data_ptr() for g in grads], _p(ws), 0 if ws is None else ws.numel(), _stream(dev)))
     return [grad_proj, *grads]
 

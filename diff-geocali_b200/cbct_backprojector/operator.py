@@ -63,9 +63,9 @@ class _Backproject(torch.autograd.Function):
     @once_differentiable
     def backward(ctx, grad_volume):
         pixel_size, voxel_size, offset = ctx.settings
-        grads = _ops.bp_backward(grad_volume.contiguous(), *ctx.saved_tensors,
-                                 pixel_size, voxel_size, *offset)
         wanted = ctx.needs_input_grad[:9]
+        grads = _ops.bp_backward(grad_volume.contiguous(), *ctx.saved_tensors,
+                                 pixel_size, voxel_size, *offset, compute_grad_proj=wanted[0])
         return tuple(g if need else None for g, need in zip(grads, wanted)) + (None,) * 4
 
 

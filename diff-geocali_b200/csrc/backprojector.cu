@@ -205,7 +205,9 @@ __global__ void __launch_bounds__(256) bp_forward_kernel(BpArgs p) {
 // Backward kernel
 // ---------------------------------------------------------------------------
 
-template <int KZ>
+// GP: projection gradient 0 = not computed (p.grad_projections null), 1 = four
+// float reductions per voxel-view into grad_projections.
+template <int KZ, int GP>
 __global__ void __launch_bounds__(256) bp_backward_kernel(BpArgs p) {
     __shared__ double s_terms[8][32][8];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -260,7 +262,8 @@ __global__ void __launch_bounds__(256) bp_backward_kernel(BpArgs p) {
             if (ok) {  // warp-uniform
                 float s_iu = 0.f, s_iv = 0.f, s_ivdv = 0.f, s_int = 0.f;
                 const float4* __restrict__ rq = p.pquads + (a * (p.U - 1) + ui) * (p.V - 1);
-                float* __restrict__ gp = p.grad_projections + ((long long)a * p.U + ui) * p.V;
+                float* __restrict__ gp = GP ? p.grad_projections + ((long long)a * p.U + ui) * p.V
+                                            : nullptr;
 #pragma unroll
                 for (int k = 0; k < KZ; ++k) {
                     const float dv = pz[k] - r.ds_v;
@@ -279,12 +282,14 @@ __global__ void __launch_bounds__(256) bp_backward_kernel(BpArgs p) {
                         s_iv = fmaf(g, iv, s_iv);
                         s_ivdv = fmaf(g * iv, dv, s_ivdv);
                         s_int = fmaf(g, interp, s_int);
-                        const float gb = g * w;
-                        const float g0 = gb * (1.0f - fu), g1 = gb * fu;
-                        red_add_global(gp + vi, g0 * (1.0f - fv));
-                        red_add_global(gp + p.V + vi, g1 * (1.0f - fv));
-                        red_add_global(gp + vi + 1, g0 * fv);
-                        red_add_global(gp + p.V + vi + 1, g1 * fv);
+                        if (GP) {
+                            const float gb = g * w;
+                            const float g0 = gb * (1.0f - fu), g1 = gb * fu;
+                            red_add_global(gp + vi, g0 * (1.0f - fv));
+                            red_add_global(gp + p.V + vi, g1 * (1.0f - fv));
+                            red_add_global(gp + vi + 1, g0 * fv);
+                            red_add_global(gp + p.V + vi + 1, g1 * fv);
+                        }
                     }
                 }
                 s_iu = warp_sum(s_iu);
@@ -382,6 +387,14 @@ int launch_bp_forward_kz(const BpArgs& p, bool pixdiv, bool fdk, dim3 grid, cuda
     DGC_LAUNCH_CHECK("bp_forward_kernel");
     return DGC_OK;
 }
+
+template <int KZ>
+int launch_bp_backward_kz(const BpArgs& p, int gp, dim3 grid, cudaStream_t s) {
+    if (gp) bp_backward_kernel<KZ, 1><<<grid, 256, 0, s>>>(p);
+    else bp_backward_kernel<KZ, 0><<<grid, 256, 0, s>>>(p);
+    DGC_LAUNCH_CHECK("bp_backward_kernel");
+    return DGC_OK;
+}
 }  // namespace
 
 int bp_launch_forward(const BpArgs& p, bool fdk, cudaStream_t s) {
@@ -405,14 +418,13 @@ int bp_launch_backward(const BpArgs& p, cudaStream_t s) {
     unsigned gx, gy;
     bp_grid(p.D, p.H, p.W, kz, gx, gy);
     const dim3 grid(gx, gy);
+    const int gp = p.grad_projections ? 1 : 0;
     switch (kz) {
-        case 1: bp_backward_kernel<1><<<grid, 256, 0, s>>>(p); break;
-        case 2: bp_backward_kernel<2><<<grid, 256, 0, s>>>(p); break;
-        case 4: bp_backward_kernel<4><<<grid, 256, 0, s>>>(p); break;
-        default: bp_backward_kernel<8><<<grid, 256, 0, s>>>(p); break;
+        case 1: return launch_bp_backward_kz<1>(p, gp, grid, s);
+        case 2: return launch_bp_backward_kz<2>(p, gp, grid, s);
+        case 4: return launch_bp_backward_kz<4>(p, gp, grid, s);
+        default: return launch_bp_backward_kz<8>(p, gp, grid, s);
     }
-    DGC_LAUNCH_CHECK("bp_backward_kernel");
-    return DGC_OK;
 }
 
 __global__ void clamp_volume_kernel(float* __restrict__ v, long long n) {

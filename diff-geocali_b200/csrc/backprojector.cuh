@@ -26,7 +26,7 @@ struct BpArgs {
     int clamp;         // FDK epilogue: clamp at 0 (0 for a view-sharded partial volume)
     // backward
     const float* grad_volume;  // [D][H][W]
-    float* grad_projections;   // [A][U][V], zeroed by the caller
+    float* grad_projections;   // [A][U][V], zeroed by the caller; null: not computed
     double* partials;          // [A][8][blocks]
 };
 

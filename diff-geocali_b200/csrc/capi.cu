@@ -432,8 +432,7 @@ int dgc_backproject_backward(const float* grad_volume, const float* projections,
     const Geometry g = make_geometry(angles, sid, sod, det_u0, det_v0, src_x, src_y, src_z);
     int rc = check_bp_common(A, U, V, D, H, W, pixel_size, voxel_size, off_x, off_y, off_z, g);
     if (rc != DGC_OK) return rc;
-    DGC_REQUIRE(grad_volume && projections && grad_projections,
-                "grad_vol, proj and grad_proj must be non-null");
+    DGC_REQUIRE(grad_volume && projections, "grad_vol and proj must be non-null");
     GeometryGrad out{{grad_angles, grad_sid, grad_sod, grad_det_u0, grad_det_v0, grad_src_x,
                       grad_src_y, grad_src_z}};
     for (int k = 0; k < 8; ++k) DGC_REQUIRE(out.g[k], "geometry gradient pointers must be non-null");
@@ -450,10 +449,12 @@ int dgc_backproject_backward(const float* grad_volume, const float* projections,
     }
     if ((rc = bp_view_table(g, A, vt, s)) != DGC_OK) return rc;
     if ((rc = build_proj_quads(projections, A, U, V, pq, s)) != DGC_OK) return rc;
-    DGC_CUDA(cudaMemsetAsync(grad_projections, 0, sizeof(float) * (size_t)A * U * V, s));
     BpArgs p = bp_args(vt, pq, A, U, V, D, H, W, pixel_size, voxel_size, off_x, off_y, off_z);
+    if (grad_projections) {
+        DGC_CUDA(cudaMemsetAsync(grad_projections, 0, sizeof(float) * (size_t)A * U * V, s));
+        p.grad_projections = grad_projections;
+    }
     p.grad_volume = grad_volume;
-    p.grad_projections = grad_projections;
     p.partials = partials;
     if ((rc = bp_launch_backward(p, s)) != DGC_OK) return rc;
     return bp_reduce_partials(partials, A, nblocks, out, s);

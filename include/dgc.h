@@ -123,7 +123,9 @@ size_t dgc_backproject_backward_workspace_bytes(int A, int U, int V, int D, int 
 /* Replaces src_cbct_backprojector_cuda.backward
  * (csrc/src_cbct_backprojector_cuda.cu:423-522, kernel 101-295).
  * Writes grad_projections [A,U,V] and the eight geometry gradients [A]
- * (per-view FP64 reductions in a fixed order). */
+ * (per-view FP64 reductions in a fixed order).  grad_projections may be NULL:
+ * the projection gradient (the bilinear scatter) is then skipped, which the
+ * reference always computes. */
 int dgc_backproject_backward(const float* grad_volume, const float* projections,
                              int A, int U, int V,
                              const float* angles, const float* sid, const float* sod,

@@ -149,3 +149,28 @@ def test_determinism_and_edges():
     # voxel at (-0.05, -0.05, -0.05): weight ((sod)/(sod+0.05))^2, bilinear of ones = 1
     q = 10.0 + 0.05
     assert math.isclose(v.item(), (10.0 / q) ** 2, rel_tol=1e-5)
+
+
+def test_geometry_only_backward_skips_the_projection_gradient():
+    """With projections that need no gradient the scatter is skipped
+    (grad_projections NULL in the C ABI); the geometry gradients are bitwise
+    those of the full backward."""
+    from cbct_backprojector import _ops
+
+    case = random_case(5)
+    vol, proj, geom = run_bp(case, requires_grad=True)
+    up = torch.linspace(-0.7, 1.3, vol.numel(), device="cuda").view_as(vol)
+    full = torch.autograd.grad(vol, [proj, *geom], grad_outputs=up)
+    from cbct_backprojector import backproject
+
+    geom2 = [cuda32(g).requires_grad_() for g in case["geom"]]
+    vol2 = backproject(cuda32(case["proj"]), *geom2, case["px"], case["shape"], case["vs"],
+                       volume_offset=case["off"])
+    part = torch.autograd.grad(vol2, geom2, grad_outputs=up)
+    for a, b in zip(full[1:], part):
+        assert torch.equal(a, b)
+    grads = _ops.bp_backward(up, proj.detach(), *[g.detach() for g in geom], case["px"], case["vs"],
+                             *case["off"], compute_grad_proj=False)
+    assert grads[0] is None
+    for a, b in zip(full[1:], grads[1:]):
+        assert torch.equal(a, b)
