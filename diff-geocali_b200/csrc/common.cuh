@@ -186,6 +186,16 @@ __device__ __forceinline__ void red_add4_global(float* p, float a, float b, floa
                  "f"(a), "f"(b), "f"(c), "f"(d));
 }
 
+// red_add4_global under a predicate inside the asm (a predicated
+// instruction, not a branch around it).
+__device__ __forceinline__ void red_add4_global_if(bool on, float* p, float a, float b, float c,
+                                                   float d) {
+    asm volatile(
+        "{\n\t.reg .pred q;\n\tsetp.ne.b32 q, %5, 0;\n\t"
+        "@q red.global.add.v4.f32 [%0], {%1, %2, %3, %4};\n\t}"
+        ::"l"(__cvta_generic_to_global(p)), "f"(a), "f"(b), "f"(c), "f"(d), "r"((int)on));
+}
+
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
