@@ -508,44 +508,42 @@ __device__ __forceinline__ void scatter_cell_pairwise(const FpArgs& p, uint32_t 
 // (the corners the two share go to the upper cell's z level, o[0..3] of its
 // record), other pairs four.
 template <int RS>
-__device__ __forceinline__ void scatter_cell_records(const FpArgs& p, uint32_t ci, float (&lo)[4],
-                                                     float (&hi)[4]) {
+__device__ __forceinline__ void scatter_cell_records(const FpArgs& p, uint32_t ci, f32x2 (&lo)[2],
+                                                     f32x2 (&hi)[2]) {
     static_assert(RS == 8 || RS == 4, "records of 8 (cells) or 4 (levels) floats");
     const unsigned mask = __activemask();
     const int lane = threadIdx.x & 31;
     const int partner = lane ^ 1;
     const bool odd = lane & 1;
     const uint32_t cpart = __shfl_sync(mask, ci, partner);
-    float plo[4], phi[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        plo[k] = __shfl_sync(mask, lo[k], partner);
-        phi[k] = __shfl_sync(mask, hi[k], partner);
-    }
     // cell of the odd lane minus cell of the even lane
     const int d = (int)(odd ? ci - cpart : cpart - ci);
     const int mode = !((mask >> partner) & 1u) ? 0 : d == 0 ? 1 : d == 1 ? 2 : d == -1 ? 3 : 0;
-    float* o = p.grad_pad + (unsigned long long)RS * ci;
-    // Branch-free: each lane adds at most one partner level into its z-level
-    // record and emits each of its two records or not, as predicated
-    // reductions.  mode 1 (same cell): the even lane emits both z levels, the
-    // odd lane both z+1 levels; mode 2 (odd = even + 1) / 3 (even = odd + 1):
-    // the upper lane's z-level record takes the lower lane's z+1 level, which
-    // the lower lane then does not emit.
     const bool m1 = mode == 1, m2 = mode == 2, m3 = mode == 3;
-    const bool add_plo = m1 && !odd;
-    const bool add_phi = (m2 && odd) || (m3 && !odd);
-    const bool emit_lo = !(m1 && odd);
-    const bool emit_hi = m1 ? odd : m2 ? odd : m3 ? !odd : true;
-    const bool hi_phi = m1 && odd;
-    float vlo[4], vhi[4];
+    // Each lane needs at most one level of its partner, so each sends one:
+    // mode 1 (same cell): the even lane emits both z levels, the odd lane both
+    // z+1 levels; mode 2 (odd = even + 1) / 3 (even = odd + 1): the upper
+    // lane's z-level record takes the lower lane's z+1 level, which the lower
+    // lane then does not emit.  Branch-free: selects, then the two records as
+    // predicated reductions.
+    const bool lo_add = odd ? m2 : (m1 || m3);
+    const bool hi_add = odd && m1;
+    const bool emit_lo = !(odd && m1);
+    const bool emit_hi = odd ? !m3 : !(m1 || m2);
+    const f32x2 zero = pack2(0.0f, 0.0f);
+    f32x2 vlo[2], vhi[2];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        vlo[k] = lo[k] + (add_plo ? plo[k] : add_phi ? phi[k] : 0.0f);
-        vhi[k] = hi[k] + (hi_phi ? phi[k] : 0.0f);
+    for (int k = 0; k < 2; ++k) {
+        const f32x2 snd = (odd && m1) ? lo[k] : hi[k];
+        const f32x2 rcv = __shfl_sync(mask, snd, partner);
+        vlo[k] = add2(lo[k], lo_add ? rcv : zero);
+        vhi[k] = add2(hi[k], hi_add ? rcv : zero);
     }
-    red_add4_global_if(emit_lo, o, vlo[0], vlo[1], vlo[2], vlo[3]);
-    red_add4_global_if(emit_hi, o + 4, vhi[0], vhi[1], vhi[2], vhi[3]);
+    float* o = p.grad_pad + (unsigned long long)RS * ci;
+    const float2 a0 = unpack2(vlo[0]), a1 = unpack2(vlo[1]);
+    const float2 b0 = unpack2(vhi[0]), b1 = unpack2(vhi[1]);
+    red_add4_global_if(emit_lo, o, a0.x, a0.y, a1.x, a1.y);
+    red_add4_global_if(emit_hi, o + 4, b0.x, b0.y, b1.x, b1.y);
 }
 
 // GV: 0 = no volume gradient, 1 = scatter every sample's eight weights,
@@ -589,15 +587,23 @@ __device__ __forceinline__ RayGrad march_grad(const RaySetup& r, const ViewGeo& 
             // adjoint of the trilinear sample (fp.cu:231-240), padded z-fastest buffer
             const float mx = 1.0f - c.fx, my = 1.0f - c.fy, mz = 1.0f - c.fz;
             const float gy0 = gs * my, gy1 = gs * c.fy;
-            const float w00 = gy0 * mx, w01 = gy0 * c.fx, w10 = gy1 * mx, w11 = gy1 * c.fx;
-            // (x, y) corner columns 00, 10, 01, 11 at the cell's z (lo) and z+1 (hi)
-            float lo[4] = {w00 * mz, w01 * mz, w10 * mz, w11 * mz};
-            float hi[4] = {w00 * c.fz, w01 * c.fz, w10 * c.fz, w11 * c.fz};
+            // (x, y) corner columns 00, 10, 01, 11 at the cell's z (lo) and z+1
+            // (hi) as packed pairs: w0 = (w00, w01), w1 = (w10, w11), the
+            // products lane by lane those of the scalar form
+            const f32x2 wxs = pack2(mx, c.fx);
+            const f32x2 w0 = mul2(pack2(gy0, gy0), wxs), w1 = mul2(pack2(gy1, gy1), wxs);
+            const f32x2 zl = pack2(mz, mz), zh = pack2(c.fz, c.fz);
+            f32x2 lo2[2] = {mul2(w0, zl), mul2(w1, zl)};
+            f32x2 hi2[2] = {mul2(w0, zh), mul2(w1, zh)};
             const uint32_t gi = c.bz + c.bx * p.gz_x + c.by * p.gz_y + p.gz_bias;
+            const float2 l0 = unpack2(lo2[0]), l1 = unpack2(lo2[1]);
+            const float2 h0 = unpack2(hi2[0]), h1 = unpack2(hi2[1]);
+            float lo[4] = {l0.x, l0.y, l1.x, l1.y};
+            float hi[4] = {h0.x, h0.y, h1.x, h1.y};
             if (GV == 3) {
-                scatter_cell_records<8>(p, gi, lo, hi);
+                scatter_cell_records<8>(p, gi, lo2, hi2);
             } else if (GV == 4) {
-                scatter_cell_records<4>(p, gi, lo, hi);
+                scatter_cell_records<4>(p, gi, lo2, hi2);
             } else if (GV == 2) {
                 scatter_cell_pairwise(p, gi, lo, hi);
             } else {
