@@ -184,7 +184,8 @@ int dgc_batch_prepare(const dgc_fp_instance* instances, int n, void* workspace,
                   ((in.off_x != 0.0f || in.off_y != 0.0f || in.off_z != 0.0f) ? kBatchOff : 0) |
                   (scatter == kScatterPairs ? kBatchMerge : 0) |
                   (scatter == kScatterCells ? kBatchCells : 0) |
-                  (scatter == kScatterLevels ? kBatchLevels : 0);
+                  (scatter == kScatterLevels ? kBatchLevels : 0) |
+                  (scatter == kScatterRuns ? kBatchRuns : 0);
         b.quad_gx = ceil_div(in.W + 1, 32) * (in.H + 1);
         b.tiles_bwd = fp_tiles_per_view(in.U, in.V, b.tile_bwd);
         host[i] = b;

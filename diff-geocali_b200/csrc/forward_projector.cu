@@ -548,7 +548,8 @@ __device__ __forceinline__ void scatter_cell_records(const FpArgs& p, uint32_t c
 
 // GV: 0 = no volume gradient, 1 = scatter every sample's eight weights,
 // 2 = merge them across lane pairs first (scatter_cell_pairwise), 3 / 4 =
-// merge lane pairs into per-cell records of 8 / 4 floats (scatter_cell_records).
+// merge lane pairs into per-cell records of 8 / 4 floats (scatter_cell_records),
+// 5 = merge a lane's consecutive samples of one cell into level records.
 template <bool CLAMP, int GV>
 __device__ __forceinline__ RayGrad march_grad(const RaySetup& r, const ViewGeo& vg,
                                               const FpArgs& p, float gs) {
@@ -556,6 +557,12 @@ __device__ __forceinline__ RayGrad march_grad(const RaySetup& r, const ViewGeo& 
     const XYPacks k = make_xy_packs(r, vg, p);
     RayGrad rg{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     const int nmax = step_bound(r, p.step_size);
+    // GV == 5: this lane's pending level records (cell run_ci: its z level and
+    // z+1 level), flushed when the ray leaves the cell
+    const f32x2 zero = pack2(0.0f, 0.0f);
+    uint32_t run_ci = 0u;
+    bool run_have = false;
+    f32x2 run_lo[2] = {zero, zero}, run_hi[2] = {zero, zero};
     float t = r.tmin;
     int n = 0;
 #pragma unroll 1
@@ -600,7 +607,30 @@ __device__ __forceinline__ RayGrad march_grad(const RaySetup& r, const ViewGeo& 
             const float2 h0 = unpack2(hi2[0]), h1 = unpack2(hi2[1]);
             float lo[4] = {l0.x, l0.y, l1.x, l1.y};
             float hi[4] = {h0.x, h0.y, h1.x, h1.y};
-            if (GV == 3) {
+            if (GV == 5) {
+                // Consecutive samples of the ray mostly share a cell: add them
+                // in registers and emit a cell's two level records when the
+                // ray moves on.  A move to the cell above (below) in z shares a
+                // level, which stays pending.  Branch-free: predicated
+                // reductions of the pending records, then selects.
+                const int d = (int)(gi - run_ci);
+                const bool same = run_have && d == 0, up = run_have && d == 1,
+                           down = run_have && d == -1;
+                float* o = p.grad_pad + 4ull * run_ci;
+                const float2 a0 = unpack2(run_lo[0]), a1 = unpack2(run_lo[1]);
+                const float2 b0 = unpack2(run_hi[0]), b1 = unpack2(run_hi[1]);
+                red_add4_global_if(run_have && !same && !down, o, a0.x, a0.y, a1.x, a1.y);
+                red_add4_global_if(run_have && !same && !up, o + 4, b0.x, b0.y, b1.x, b1.y);
+#pragma unroll
+                for (int j = 0; j < 2; ++j) {
+                    const f32x2 base_lo = same ? run_lo[j] : up ? run_hi[j] : zero;
+                    const f32x2 base_hi = same ? run_hi[j] : down ? run_lo[j] : zero;
+                    run_lo[j] = add2(base_lo, lo2[j]);
+                    run_hi[j] = add2(base_hi, hi2[j]);
+                }
+                run_ci = gi;
+                run_have = true;
+            } else if (GV == 3) {
                 scatter_cell_records<8>(p, gi, lo2, hi2);
             } else if (GV == 4) {
                 scatter_cell_records<4>(p, gi, lo2, hi2);
@@ -616,6 +646,13 @@ __device__ __forceinline__ RayGrad march_grad(const RaySetup& r, const ViewGeo& 
                 }
             }
         }
+    }
+    if (GV == 5 && run_have) {
+        float* o = p.grad_pad + 4ull * run_ci;
+        const float2 a0 = unpack2(run_lo[0]), a1 = unpack2(run_lo[1]);
+        const float2 b0 = unpack2(run_hi[0]), b1 = unpack2(run_hi[1]);
+        red_add4_global(o, a0.x, a0.y, a1.x, a1.y);
+        red_add4_global(o + 4, b0.x, b0.y, b1.x, b1.y);
     }
     return rg;
 }
@@ -1302,6 +1339,7 @@ __device__ __forceinline__ void backward_item(const FpArgs& p, const ViewGeo& vg
     if (!p.grad_pad) backward_ray<0>(p, vg, tc.a, u, v, terms);
     else if (flags & kBatchCells) backward_ray<3>(p, vg, tc.a, u, v, terms);
     else if (flags & kBatchLevels) backward_ray<4>(p, vg, tc.a, u, v, terms);
+    else if (flags & kBatchRuns) backward_ray<5>(p, vg, tc.a, u, v, terms);
     else if (flags & kBatchMerge) backward_ray<2>(p, vg, tc.a, u, v, terms);
     else backward_ray<1>(p, vg, tc.a, u, v, terms);
 }
@@ -1351,7 +1389,7 @@ __global__ void __launch_bounds__(256) batch_fold_kernel(BatchTables t) {
     if (in.flags & kBatchCells) {
         for (long long v = v0 + threadIdx.x; v < v1; v += blockDim.x)
             in.grad_volume[v] = fold_record_voxel<8>(in.p.grad_pad, in.p.D, in.p.H, in.p.W, v);
-    } else if (in.flags & kBatchLevels) {
+    } else if (in.flags & (kBatchLevels | kBatchRuns)) {
         for (long long v = v0 + threadIdx.x; v < v1; v += blockDim.x)
             in.grad_volume[v] = fold_record_voxel<4>(in.p.grad_pad, in.p.D, in.p.H, in.p.W, v);
     } else {
@@ -1408,6 +1446,7 @@ int launch_backward_tu(const FpArgs& p, bool gradvol, cudaStream_t s) {
         switch (fp_volume_scatter()) {
             case kScatterCells: fp_backward_kernel<TU, 3><<<(unsigned)blocks, 256, 0, s>>>(p); break;
             case kScatterLevels: fp_backward_kernel<TU, 4><<<(unsigned)blocks, 256, 0, s>>>(p); break;
+            case kScatterRuns: fp_backward_kernel<TU, 5><<<(unsigned)blocks, 256, 0, s>>>(p); break;
             case kScatterPairs: fp_backward_kernel<TU, 2><<<(unsigned)blocks, 256, 0, s>>>(p); break;
             default: fp_backward_kernel<TU, 1><<<(unsigned)blocks, 256, 0, s>>>(p); break;
         }
@@ -1419,23 +1458,25 @@ int launch_backward_tu(const FpArgs& p, bool gradvol, cudaStream_t s) {
 }  // namespace
 
 VolumeScatter fp_volume_scatter() {
-    // Level records by default: the backward (sid 1000, sod 600, step 0.5) at
-    // 256^3 / 360 x 384^2, 128^3 / 180 x 256^2 and 512^3 / 90 x 512^2 took
-    // 129 / 12.1 / 145 ms with them, 170 / 15.7 / 201 ms with cell records,
-    // 206 / 19.1 / 221 ms with lane pairs merged into the padded buffer and
-    // 215 / 18.5 / 273 ms with every sample alone.
+    // Level records with a lane's consecutive samples of a cell merged first
+    // by default: the backward (sid 1000, sod 600, step 0.5) at 256^3 / 360 x
+    // 384^2, 128^3 / 180 x 256^2 and 512^3 / 90 x 512^2 took 109 / 10.1 /
+    // 125 ms with them, 130 / 12.2 / 147 ms with lane pairs merged into level
+    // records, 214 / 18.5 / 273 ms with every sample alone (and 262 / 319 /
+    // 549 ms at 256^3, step 0.2).
     if (const char* e = std::getenv("DGC_SCATTER")) {
         if (std::strcmp(e, "pairs") == 0) return kScatterPairs;
         if (std::strcmp(e, "plain") == 0) return kScatterPlain;
         if (std::strcmp(e, "brick") == 0) return kScatterBrick;
         if (std::strcmp(e, "cells") == 0) return kScatterCells;
         if (std::strcmp(e, "levels") == 0) return kScatterLevels;
+        if (std::strcmp(e, "runs") == 0) return kScatterRuns;
     }
-    return kScatterLevels;
+    return kScatterRuns;
 }
 
 int fp_record_floats(VolumeScatter scatter) {
-    return scatter == kScatterCells ? 8 : scatter == kScatterLevels ? 4 : 0;
+    return scatter == kScatterCells ? 8 : (scatter == kScatterLevels || scatter == kScatterRuns) ? 4 : 0;
 }
 
 size_t fp_record_buffer_floats(VolumeScatter scatter, int D, int H, int W) {

@@ -30,7 +30,9 @@ struct FpTile {
 };
 
 // One instance of a batched launch (an entry of the device-resident table).
-enum : int { kBatchDiv = 1, kBatchOff = 2, kBatchMerge = 4, kBatchCells = 8, kBatchLevels = 16 };
+enum : int {
+    kBatchDiv = 1, kBatchOff = 2, kBatchMerge = 4, kBatchCells = 8, kBatchLevels = 16, kBatchRuns = 32
+};
 constexpr int kFoldChunk = 2048;
 
 struct BatchInstance {
@@ -71,16 +73,19 @@ int fp_check_args(int D, int H, int W, int A, int U, int V, float pixel_size, fl
 
 void fp_fill_layout(FpArgs& p);
 long long fp_tiles_per_view(int U, int V, int tu);
-// Volume-gradient scatter of the backward.  kScatterLevels (the default) and
-// kScatterCells add lane-pair-merged weights as 16-byte vector reductions into
-// a cell-major buffer of records, 4 / 8 floats per cell (fp_fill_cell_layout,
+// Volume-gradient scatter of the backward.  kScatterRuns (the default) adds
+// the weights of a lane's consecutive samples in one cell in registers and
+// emits them as 16-byte vector reductions into a cell-major buffer of level
+// records (4 floats per cell); kScatterLevels and kScatterCells merge lane
+// pairs into records of 4 / 8 floats instead (fp_fill_cell_layout,
 // fp_record_buffer_floats, fp_fold_records); kScatterPlain and kScatterPairs
 // add single floats into the padded buffer (every sample alone, lane pairs
 // merged first); kScatterBrick accumulates shared-memory bricks flushed into
 // the padded buffer (single-problem backward only; the batched one scatters
-// plain).  DGC_SCATTER=plain|pairs|cells|levels|brick overrides.
+// plain).  DGC_SCATTER=runs|levels|cells|plain|pairs|brick overrides.
 enum VolumeScatter : int {
-    kScatterPlain = 1, kScatterPairs = 2, kScatterCells = 3, kScatterBrick = 4, kScatterLevels = 5
+    kScatterPlain = 1, kScatterPairs = 2, kScatterCells = 3, kScatterBrick = 4, kScatterLevels = 5,
+    kScatterRuns = 6  // level records, a lane's consecutive samples of a cell merged first
 };
 VolumeScatter fp_volume_scatter();
 // floats per cell record: 8 (cells), 4 (levels), 0 (padded-buffer scatters)

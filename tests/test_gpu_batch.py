@@ -56,7 +56,7 @@ def plain(pr):
     return p.detach(), grads[0], torch.stack(grads[1:])
 
 
-@pytest.mark.parametrize("scatter", ["cells", "levels", "pairs", "plain"])
+@pytest.mark.parametrize("scatter", ["cells", "levels", "runs", "pairs", "plain"])
 def test_batch_matches_plain_calls(scatter, monkeypatch):
     """Every volume-gradient scatter: batched launches against per-problem calls."""
     from cbct_backprojector.batch import ProjectionBatch

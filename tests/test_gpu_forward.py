@@ -184,7 +184,7 @@ def test_forward_matches_reference_cuda(which, golden, ref_native, oracle):
     assert rel_l2(ours.cpu(), truth) < FWD_RTOL
 
 
-@pytest.mark.parametrize("scatter", ["brick", "plain", "pairs", "cells", "levels"])
+@pytest.mark.parametrize("scatter", ["brick", "plain", "pairs", "cells", "levels", "runs"])
 @pytest.mark.parametrize("which", ["config1", "random_nonpow2"])
 def test_backward_matches_reference_cuda(which, scatter, golden, ref_native, oracle, monkeypatch):
     """Every volume-gradient scatter: shared-memory bricks flushed once per
