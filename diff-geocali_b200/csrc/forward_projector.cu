@@ -1344,7 +1344,7 @@ __device__ __forceinline__ void backward_item(const FpArgs& p, const ViewGeo& vg
     else backward_ray<1>(p, vg, tc.a, u, v, terms);
 }
 
-__global__ void __launch_bounds__(256) batch_backward_kernel(BatchTables t) {
+__global__ void __launch_bounds__(256, 4) batch_backward_kernel(BatchTables t) {
     __shared__ FpArgs s_p;
     __shared__ ViewGeo s_view;
     __shared__ TileCoord s_tc;
