@@ -21,6 +21,8 @@
 //   * The backward sums the per-voxel terms over Z in four accumulators and
 //     applies the (column, view) chain-rule coefficients once per warp; the
 //     eight per-view gradients are reduced in FP64 in a fixed order.
+#include <cstdio>
+
 #include "common.cuh"
 #include "backprojector.cuh"
 
@@ -128,14 +130,17 @@ __device__ __forceinline__ ColumnView column_view(const ViewRow& r, int a, float
 // Forward (backprojection) kernel
 // ---------------------------------------------------------------------------
 
+// A CTA owns a cta_x x cta_y patch of (x, y) columns, one warp per column
+// (at most kBpMaxWarps warps), and 32*KZ voxels of each along z.
 template <int KZ, bool PIXDIV, bool FDK>
-__global__ void __launch_bounds__(256) bp_forward_kernel(BpArgs p) {
-    __shared__ float s_out[32 * KZ][9];
+__global__ void __launch_bounds__(32 * kBpMaxWarps) bp_forward_kernel(BpArgs p) {
+    __shared__ float s_out[32 * KZ][kBpMaxWarps + 1];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int cols_x = (p.W + 7) >> 3;
-    const int y = blockIdx.x / cols_x;
-    const int xb = (blockIdx.x - y * cols_x) * 8;
-    const int x = xb + warp;
+    const int cx = p.cta_x, cy = p.cta_y, nw = cx * cy;
+    const int tiles_x = (p.W + cx - 1) / cx;
+    const int ty = blockIdx.x / tiles_x;
+    const int xb = (blockIdx.x - ty * tiles_x) * cx, yb = ty * cy;
+    const int x = xb + warp % cx, y = yb + warp / cx;
     const int zbase = blockIdx.y * 32 * KZ;
     const unsigned FULL = 0xffffffffu;
 
@@ -147,7 +152,7 @@ __global__ void __launch_bounds__(256) bp_forward_kernel(BpArgs p) {
         const int z = zbase + lane + 32 * k;
         pz[k] = (z - p.D * 0.5f) * p.voxel_size + p.off_z;
     }
-    if (x < p.W) {
+    if (x < p.W && y < p.H) {
         const float vx = (x - p.W * 0.5f) * p.voxel_size + p.off_x;
         const float vy = (y - p.H * 0.5f) * p.voxel_size + p.off_y;
         const float vlim = p.V - 1.0f;
@@ -194,10 +199,11 @@ __global__ void __launch_bounds__(256) bp_forward_kernel(BpArgs p) {
         s_out[lane + 32 * k][warp] = val;
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < 32 * KZ * 8; i += 256) {
-        const int zl = i >> 3, xl = i & 7;
-        const int z = zbase + zl, xx = xb + xl;
-        if (z < p.D && xx < p.W) p.volume[((long long)z * p.H + y) * p.W + xx] = s_out[zl][xl];
+    for (int i = threadIdx.x; i < 32 * KZ * nw; i += 32 * nw) {
+        const int zl = i / nw, w = i - zl * nw;
+        const int z = zbase + zl, xx = xb + w % cx, yy = yb + w / cx;
+        if (z < p.D && xx < p.W && yy < p.H)
+            p.volume[((long long)z * p.H + yy) * p.W + xx] = s_out[zl][w];
     }
 }
 
@@ -384,6 +390,20 @@ int bp_kz_forward(int D) {
     return D <= 32 ? 1 : 2;
 }
 
+// Column patch of a forward CTA; DGC_BP_CTA="cx,cy" (cx*cy <= kBpMaxWarps)
+// overrides (tuning experiments).
+void bp_forward_cta(int& cx, int& cy) {
+    cx = 8;
+    cy = 1;
+    if (const char* e = std::getenv("DGC_BP_CTA")) {
+        int a = 0, b = 0;
+        if (std::sscanf(e, "%d,%d", &a, &b) == 2 && a >= 1 && b >= 1 && a * b <= kBpMaxWarps) {
+            cx = a;
+            cy = b;
+        }
+    }
+}
+
 int bp_kz_backward(int D) {
     if (const int k = bp_kz_override()) return k;
     return D <= 32 ? 1 : D <= 64 ? 2 : 4;
@@ -403,12 +423,13 @@ long long bp_backward_blocks(int D, int H, int W) {
 namespace {
 template <int KZ>
 int launch_bp_forward_kz(const BpArgs& p, bool pixdiv, bool fdk, dim3 grid, cudaStream_t s) {
+    const unsigned threads = 32u * (unsigned)(p.cta_x * p.cta_y);
     if (fdk) {
-        if (pixdiv) bp_forward_kernel<KZ, true, true><<<grid, 256, 0, s>>>(p);
-        else bp_forward_kernel<KZ, false, true><<<grid, 256, 0, s>>>(p);
+        if (pixdiv) bp_forward_kernel<KZ, true, true><<<grid, threads, 0, s>>>(p);
+        else bp_forward_kernel<KZ, false, true><<<grid, threads, 0, s>>>(p);
     } else {
-        if (pixdiv) bp_forward_kernel<KZ, true, false><<<grid, 256, 0, s>>>(p);
-        else bp_forward_kernel<KZ, false, false><<<grid, 256, 0, s>>>(p);
+        if (pixdiv) bp_forward_kernel<KZ, true, false><<<grid, threads, 0, s>>>(p);
+        else bp_forward_kernel<KZ, false, false><<<grid, threads, 0, s>>>(p);
     }
     DGC_LAUNCH_CHECK("bp_forward_kernel");
     return DGC_OK;
@@ -423,13 +444,14 @@ int launch_bp_backward_kz(const BpArgs& p, int gp, dim3 grid, cudaStream_t s) {
 }
 }  // namespace
 
-int bp_launch_forward(const BpArgs& p, bool fdk, cudaStream_t s) {
+int bp_launch_forward(const BpArgs& args, bool fdk, cudaStream_t s) {
     DGC_TRACE(fdk ? "bp_forward_kernel<fdk>" : "bp_forward_kernel", s);
+    BpArgs p = args;
+    bp_forward_cta(p.cta_x, p.cta_y);
     const bool pixdiv = !is_pow2_float(p.pixel_size);
     const int kz = bp_kz_forward(p.D);
-    unsigned gx, gy;
-    bp_grid(p.D, p.H, p.W, kz, gx, gy);
-    const dim3 grid(gx, gy);
+    const dim3 grid((unsigned)(ceil_div(p.W, p.cta_x) * (long long)ceil_div(p.H, p.cta_y)),
+                    (unsigned)ceil_div(p.D, 32 * kz));
     switch (kz) {
         case 1: return launch_bp_forward_kz<1>(p, pixdiv, fdk, grid, s);
         case 2: return launch_bp_forward_kz<2>(p, pixdiv, fdk, grid, s);

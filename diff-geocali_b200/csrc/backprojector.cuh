@@ -5,6 +5,9 @@
 
 namespace dgc {
 
+// Most warps (columns) in one CTA of the backprojection.
+constexpr int kBpMaxWarps = 16;
+
 // Per-view terms shared by every voxel of a view (48 bytes).
 struct ViewRow {
     float c, s;          // cos, sin of the view angle
@@ -22,6 +25,7 @@ struct BpArgs {
     float off_x, off_y, off_z;
     // forward
     float* volume;     // [D][H][W]
+    int cta_x, cta_y;  // forward: columns per CTA along x and y (cta_x*cta_y <= kBpMaxWarps)
     float out_scale;   // FDK epilogue scale (pi/A)
     int clamp;         // FDK epilogue: clamp at 0 (0 for a view-sharded partial volume)
     // backward

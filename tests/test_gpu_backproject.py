@@ -194,3 +194,21 @@ def test_every_z_blocking_matches_the_oracle(kz, oracle, monkeypatch):
     for k, name in enumerate(GEOM_NAMES):
         assert rel_l2(ours[1 + k].cpu(), gg[k]) < GRAD_RTOL, name
 
+
+@pytest.mark.parametrize("cta", ["4,2", "2,4", "4,4", "16,1", "3,5"])
+def test_column_patch_shapes_are_bitwise(cta, monkeypatch):
+    """DGC_BP_CTA: the forward's CTA as a cx x cy patch of columns gives the
+    default's volume bit for bit (each voxel sums its views in one order),
+    W and H not multiples of the patch included."""
+    from cbct_backprojector import backproject
+
+    case = random_case(6, px=1.0, vs=1.0, shape=(45, 23, 19))
+    proj = cuda32(case["proj"])
+    geom = [cuda32(g) for g in case["geom"]]
+    monkeypatch.delenv("DGC_BP_CTA", raising=False)
+    a = backproject(proj, *geom, 1.0, case["shape"], 1.0, volume_offset=case["off"])
+    monkeypatch.setenv("DGC_BP_CTA", cta)
+    b = backproject(proj, *geom, 1.0, case["shape"], 1.0, volume_offset=case["off"])
+    torch.cuda.synchronize()
+    assert torch.equal(a, b)
+
