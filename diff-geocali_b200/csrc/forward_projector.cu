@@ -1425,7 +1425,7 @@ int launch_backward_tu(const FpArgs& p, bool gradvol, cudaStream_t s) {
     DGC_TRACE(gradvol ? "fp_backward_kernel<gradvol>" : "fp_backward_kernel", s);
     const long long blocks = fp_tiles_per_view(p.U, p.V, TU) * (long long)p.A;
     // DGC_SCATTER=brick selects the shared-memory brick adjoint.  It is not
-    // the default: measured 1.7-2.1x slower than the direct scatter
+    // the default: measured 1.7-2.1x slower than the plain direct scatter
     // (204 vs 117 ms at 256^3 / 360 x 384^2): the slab barriers hold the
     // bundle's fastest rays back, and the shared-memory additions cost about
     // what the L2 reductions they replace cost.
