@@ -77,6 +77,9 @@ SIGNATURES = {
     "dgc_reconstruct_fdk_partial": (_I, [_P, _I, _I, _I, *_GEOM, _F, _I, _I, _I, _F, _F, _F, _F, _F,
                                          _P, _F, _P, _P, _S, _P]),
     "dgc_clamp_volume": (_I, [_P, ctypes.c_longlong, _P]),
+    "dgc_bp_add_tile_rule": (_I, [_I] * 6),
+    "dgc_bp_clear_tile_rules": (_I, []),
+    "dgc_bp_tiles": (_I, [_I, _I] + [ctypes.POINTER(ctypes.c_int)] * 4),
     "dgc_gemm_bf16": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _I, _I, _I, _I, _I, _F, _P, _P]),
     "dgc_im2col_nhwc_bf16": (_I, [_P, _I, _I, _I, _I, _I, _I, _I, _I, _P, _I, _P]),
     "dgc_col2im_nhwc_f32": (_I, [_P, _I, _I, _I, _I, _I, _I, _I, _I, _I, _P, _P]),

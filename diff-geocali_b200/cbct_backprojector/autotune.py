@@ -12,7 +12,13 @@ Buckets: volume size class (log2 of the voxel count, rounded), detector U and
 V rounded up to a multiple of 128, and whether the voxel size is a power of
 two (division or multiplication variant).  The view count only scales the
 number of tiles, so it is not part of the key, and a bucket is timed on its
-first ``TUNE_VIEWS`` views.  No counterpart in the reference.
+first ``TUNE_VIEWS`` views.
+
+The backprojector is tuned the same way (``tune_backprojector``): the Z
+blocking of its forward and backward (32*KZ voxels of a column per warp) and
+the forward's patch of columns per CTA, per bucket of volume depth and view
+count (each rounded up to a power of two), registered in the library as tile
+rules (``dgc_bp_add_tile_rule``).  No counterpart in the reference.
 """
 
 from __future__ import annotations
@@ -25,6 +31,10 @@ from pathlib import Path
 FORWARD_TILES = (8, 4, 2)
 BACKWARD_TILES = (8, 4)
 TUNE_VIEWS = 48
+BP_KZ_FORWARD = (1, 2, 4, 8)
+BP_KZ_BACKWARD = (2, 4, 8)
+BP_CTAS = ((8, 1), (4, 2))
+BP_TUNE_VIEWS = 360
 
 
 def _pow2(x: float) -> bool:
@@ -76,15 +86,69 @@ def time_problem(problem, direction: str, tile: int, grad_volume=True, warmup=1,
     return sorted(times)[len(times) // 2]
 
 
+def bp_bucket(volume_shape, views):
+    """(d_max, a_max) of a backprojection: depth and view count rounded up to powers of two."""
+    D, A = int(volume_shape[0]), int(views)
+    return 1 << max(0, (D - 1).bit_length()), 1 << max(0, (A - 1).bit_length())
+
+
+def time_backprojector(projections, geometry, pixel_size, volume_shape, voxel_size,
+                       volume_offset, direction, kz, cta=(8, 1), warmup=1, repeats=3):
+    """Median device time [ms] of the backprojection (``direction`` "forward")
+    or of its backward without the projection gradient ("backward") with Z
+    blocking ``kz`` and forward column patch ``cta``, on the first
+    ``BP_TUNE_VIEWS`` views (set through DGC_BP_KZ / DGC_BP_CTA for the
+    measurement, restored afterwards)."""
+    import torch
+
+    from . import _ops
+
+    views = min(int(geometry[0].numel()), BP_TUNE_VIEWS)
+    proj = projections[:views].contiguous()
+    geom = [g[:views].contiguous() for g in geometry]
+    D, H, W = (int(x) for x in volume_shape)
+    saved = {k: os.environ.get(k) for k in ("DGC_BP_KZ", "DGC_BP_CTA")}
+    os.environ["DGC_BP_KZ"] = str(int(kz))
+    os.environ["DGC_BP_CTA"] = f"{int(cta[0])},{int(cta[1])}"
+    try:
+        if direction == "forward":
+            def run():
+                _ops.bp_forward(proj, *geom, pixel_size, D, H, W, voxel_size, *volume_offset)
+        else:
+            gv = torch.ones((D, H, W), dtype=torch.float32, device=proj.device)
+
+            def run():
+                _ops.bp_backward(gv, proj, *geom, pixel_size, voxel_size, *volume_offset,
+                                 compute_grad_proj=False)
+        for _ in range(warmup):
+            run()
+        times = []
+        for _ in range(repeats):
+            start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            start.record()
+            run()
+            stop.record()
+            stop.synchronize()
+            times.append(start.elapsed_time(stop))
+    finally:
+        for k, v in saved.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
+    return sorted(times)[len(times) // 2]
+
+
 class Autotuner:
     """Chooses (forward, backward) tiles per shape bucket; caches them as JSON.
 
     ``measure(problem, direction, tile) -> ms`` defaults to ``time_problem``.
     """
 
-    def __init__(self, cache_path=None, measure=None, grad_volume=True):
+    def __init__(self, cache_path=None, measure=None, grad_volume=True, measure_bp=None):
         self.cache_path = Path(cache_path) if cache_path else default_cache_path()
         self.measure = measure or (lambda pr, d, t: time_problem(pr, d, t, grad_volume))
+        self.measure_bp = measure_bp or time_backprojector
         self.table = {}
         if self.cache_path.exists():
             try:
@@ -113,6 +177,50 @@ class Autotuner:
         self._save()
         return entry
 
+    def tune_backprojector(self, projections, geometry, pixel_size, volume_shape, voxel_size,
+                           volume_offset=(0.0, 0.0, 0.0)):
+        """Z blocking and column patch of the backprojector for the bucket of
+        ``volume_shape`` and the view count; measured once, cached, and
+        registered in the library (``apply_backprojector_rules``).
+
+        ``measure_bp(projections, geometry, pixel_size, volume_shape,
+        voxel_size, volume_offset, direction, kz, cta) -> ms`` defaults to
+        ``time_backprojector``."""
+        d_max, a_max = bp_bucket(volume_shape, int(geometry[0].numel()))
+        key = f"bp:D{d_max}-A{a_max}"
+        if key not in self.table:
+            args = (projections, geometry, pixel_size, volume_shape, voxel_size,
+                    tuple(float(x) for x in volume_offset))
+            fwd = {f"{kz}/{cx}x{cy}": float(self.measure_bp(*args, "forward", kz, (cx, cy)))
+                   for kz in BP_KZ_FORWARD for cx, cy in BP_CTAS}
+            bwd = {str(kz): float(self.measure_bp(*args, "backward", kz, (8, 1)))
+                   for kz in BP_KZ_BACKWARD}
+            best = min(fwd, key=fwd.get)
+            kz_f, patch = best.split("/")
+            cx, cy = (int(x) for x in patch.split("x"))
+            self.table[key] = {"d_max": d_max, "a_max": a_max, "kz_forward": int(kz_f),
+                               "kz_backward": int(min(bwd, key=bwd.get)), "cta": [cx, cy],
+                               "forward_ms": fwd, "backward_ms": bwd}
+            self.measured.append(key)
+            self._save()
+        self.apply_backprojector_rules()
+        return self.table[key]
+
+    def apply_backprojector_rules(self):
+        """Register every cached backprojector bucket as a library tile rule,
+        tightest bucket first."""
+        from . import _native
+
+        lib = _native.lib()
+        _native.check(lib.dgc_bp_clear_tile_rules())
+        rules = sorted((e for k, e in self.table.items() if k.startswith("bp:")),
+                       key=lambda e: (e["d_max"], e["a_max"]))
+        for e in rules[:16]:
+            _native.check(lib.dgc_bp_add_tile_rule(int(e["d_max"]), int(e["a_max"]),
+                                                   int(e["kz_forward"]), int(e["kz_backward"]),
+                                                   int(e["cta"][0]), int(e["cta"][1])))
+        return len(rules[:16])
+
     def choose(self, problems):
         """Set ``problem.tiles`` of every problem from its bucket's choice."""
         out = []
@@ -123,4 +231,17 @@ class Autotuner:
         return out
 
 
-__all__ = ["Autotuner", "bucket", "time_problem", "FORWARD_TILES", "BACKWARD_TILES"]
+def backprojector_tiles(D, A):
+    """(kz_forward, kz_backward, (cta_x, cta_y)) a backprojection of depth D
+    over A views uses (dgc_bp_tiles)."""
+    import ctypes
+
+    from . import _native
+
+    out = [ctypes.c_int() for _ in range(4)]
+    _native.check(_native.lib().dgc_bp_tiles(int(D), int(A), *[ctypes.byref(x) for x in out]))
+    return out[0].value, out[1].value, (out[2].value, out[3].value)
+
+
+__all__ = ["Autotuner", "bucket", "bp_bucket", "time_problem", "time_backprojector",
+           "backprojector_tiles", "FORWARD_TILES", "BACKWARD_TILES"]

@@ -22,6 +22,7 @@
 //     applies the (column, view) chain-rule coefficients once per warp; the
 //     eight per-view gradients are reduced in FP64 in a fixed order.
 #include <cstdio>
+#include <mutex>
 
 #include "common.cuh"
 #include "backprojector.cuh"
@@ -385,28 +386,83 @@ static int bp_kz_override() {
     return 0;
 }
 
-int bp_kz_forward(int D) {
-    if (const int k = bp_kz_override()) return k;
-    return D <= 32 ? 1 : 2;
-}
-
-// Column patch of a forward CTA; DGC_BP_CTA="cx,cy" (cx*cy <= kBpMaxWarps)
-// overrides (tuning experiments).
-void bp_forward_cta(int& cx, int& cy) {
-    cx = 8;
-    cy = 1;
+static bool bp_cta_override(int& cx, int& cy) {
     if (const char* e = std::getenv("DGC_BP_CTA")) {
         int a = 0, b = 0;
         if (std::sscanf(e, "%d,%d", &a, &b) == 2 && a >= 1 && b >= 1 && a * b <= kBpMaxWarps) {
             cx = a;
             cy = b;
+            return true;
         }
     }
+    return false;
 }
 
-int bp_kz_backward(int D) {
+// Tile rules registered by the autotuner (dgc_bp_add_tile_rule): the first
+// rule with D <= d_max and A <= a_max applies; a zero field keeps the
+// built-in choice.  Precedence: DGC_BP_KZ / DGC_BP_CTA, then the rules, then
+// the built-in choice.
+namespace {
+struct BpTileRule {
+    int d_max, a_max, kz_forward, kz_backward, cta_x, cta_y;
+};
+std::mutex g_rule_mutex;
+BpTileRule g_rules[kBpMaxTileRules];
+int g_rule_count = 0;
+
+bool bp_rule(int D, int A, BpTileRule& out) {
+    std::lock_guard<std::mutex> lock(g_rule_mutex);
+    for (int i = 0; i < g_rule_count; ++i)
+        if (D <= g_rules[i].d_max && A <= g_rules[i].a_max) {
+            out = g_rules[i];
+            return true;
+        }
+    return false;
+}
+
+bool valid_kz(int k) { return k == 0 || k == 1 || k == 2 || k == 4 || k == 8; }
+}  // namespace
+
+int bp_add_tile_rule(int d_max, int a_max, int kz_forward, int kz_backward, int cta_x, int cta_y) {
+    if (d_max < 1 || a_max < 1 || !valid_kz(kz_forward) || !valid_kz(kz_backward)) return -1;
+    const bool cta_default = cta_x == 0 && cta_y == 0;
+    if (!cta_default && (cta_x < 1 || cta_y < 1 || cta_x * cta_y > kBpMaxWarps)) return -1;
+    std::lock_guard<std::mutex> lock(g_rule_mutex);
+    if (g_rule_count >= kBpMaxTileRules) return -2;
+    g_rules[g_rule_count++] = BpTileRule{d_max, a_max, kz_forward, kz_backward, cta_x, cta_y};
+    return 0;
+}
+
+void bp_clear_tile_rules() {
+    std::lock_guard<std::mutex> lock(g_rule_mutex);
+    g_rule_count = 0;
+}
+
+int bp_kz_forward(int D, int A) {
     if (const int k = bp_kz_override()) return k;
+    BpTileRule r;
+    if (bp_rule(D, A, r) && r.kz_forward) return r.kz_forward;
+    return D <= 32 ? 1 : 2;
+}
+
+int bp_kz_backward(int D, int A) {
+    if (const int k = bp_kz_override()) return k;
+    BpTileRule r;
+    if (bp_rule(D, A, r) && r.kz_backward) return r.kz_backward;
     return D <= 32 ? 1 : D <= 64 ? 2 : 4;
+}
+
+// Column patch of a forward CTA (cx*cy <= kBpMaxWarps); 8 x 1 built in.
+void bp_forward_cta(int D, int A, int& cx, int& cy) {
+    if (bp_cta_override(cx, cy)) return;
+    BpTileRule r;
+    if (bp_rule(D, A, r) && r.cta_x) {
+        cx = r.cta_x;
+        cy = r.cta_y;
+        return;
+    }
+    cx = 8;
+    cy = 1;
 }
 
 void bp_grid(int D, int H, int W, int kz, unsigned& gx, unsigned& gy) {
@@ -414,9 +470,9 @@ void bp_grid(int D, int H, int W, int kz, unsigned& gx, unsigned& gy) {
     gy = (unsigned)ceil_div(D, 32 * kz);
 }
 
-long long bp_backward_blocks(int D, int H, int W) {
+long long bp_backward_blocks(int D, int H, int W, int A) {
     unsigned gx, gy;
-    bp_grid(D, H, W, bp_kz_backward(D), gx, gy);
+    bp_grid(D, H, W, bp_kz_backward(D, A), gx, gy);
     return (long long)gx * gy;
 }
 
@@ -447,9 +503,9 @@ int launch_bp_backward_kz(const BpArgs& p, int gp, dim3 grid, cudaStream_t s) {
 int bp_launch_forward(const BpArgs& args, bool fdk, cudaStream_t s) {
     DGC_TRACE(fdk ? "bp_forward_kernel<fdk>" : "bp_forward_kernel", s);
     BpArgs p = args;
-    bp_forward_cta(p.cta_x, p.cta_y);
+    bp_forward_cta(p.D, p.A, p.cta_x, p.cta_y);
     const bool pixdiv = !is_pow2_float(p.pixel_size);
-    const int kz = bp_kz_forward(p.D);
+    const int kz = bp_kz_forward(p.D, p.A);
     const dim3 grid((unsigned)(ceil_div(p.W, p.cta_x) * (long long)ceil_div(p.H, p.cta_y)),
                     (unsigned)ceil_div(p.D, 32 * kz));
     switch (kz) {
@@ -462,7 +518,7 @@ int bp_launch_forward(const BpArgs& args, bool fdk, cudaStream_t s) {
 
 int bp_launch_backward(const BpArgs& p, cudaStream_t s) {
     DGC_TRACE("bp_backward_kernel", s);
-    const int kz = bp_kz_backward(p.D);
+    const int kz = bp_kz_backward(p.D, p.A);
     unsigned gx, gy;
     bp_grid(p.D, p.H, p.W, kz, gx, gy);
     const dim3 grid(gx, gy);

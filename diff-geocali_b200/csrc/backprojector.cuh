@@ -5,8 +5,9 @@
 
 namespace dgc {
 
-// Most warps (columns) in one CTA of the backprojection.
+// Most warps (columns) in one CTA of the backprojection; most tile rules.
 constexpr int kBpMaxWarps = 16;
+constexpr int kBpMaxTileRules = 16;
 
 // Per-view terms shared by every voxel of a view (48 bytes).
 struct ViewRow {
@@ -39,7 +40,15 @@ int build_proj_quads(const float* P, int A, int U, int V, float4* PQ, cudaStream
 int bp_launch_forward(const BpArgs& p, bool fdk, cudaStream_t s);
 int bp_launch_backward(const BpArgs& p, cudaStream_t s);
 int bp_clamp_volume(float* volume, long long n, cudaStream_t s);
-long long bp_backward_blocks(int D, int H, int W);
+long long bp_backward_blocks(int D, int H, int W, int A);
+// Tiles of a call with volume depth D and A views (rules, overrides, built-in
+// choice) and the rule table behind dgc_bp_add_tile_rule (0 ok, -1 invalid,
+// -2 table full).
+int bp_kz_forward(int D, int A);
+int bp_kz_backward(int D, int A);
+void bp_forward_cta(int D, int A, int& cx, int& cy);
+int bp_add_tile_rule(int d_max, int a_max, int kz_forward, int kz_backward, int cta_x, int cta_y);
+void bp_clear_tile_rules();
 int bp_reduce_partials(const double* partials, int A, long long nblocks, const GeometryGrad& out,
                        cudaStream_t s);
 

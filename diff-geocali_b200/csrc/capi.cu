@@ -414,7 +414,7 @@ int dgc_backproject(const float* projections, int A, int U, int V, const float* 
 size_t dgc_backproject_backward_workspace_bytes(int A, int U, int V, int D, int H, int W) {
     if (A <= 0 || U < 2 || V < 2 || D <= 0 || H <= 0 || W <= 0) return 0;
     return bp_table_bytes(A) + bp_quads_bytes(A, U, V) +
-           Workspace::align(sizeof(double) * 8 * (size_t)A * (size_t)bp_backward_blocks(D, H, W));
+           Workspace::align(sizeof(double) * 8 * (size_t)A * (size_t)bp_backward_blocks(D, H, W, A));
 }
 
 int dgc_backproject_backward(const float* grad_volume, const float* projections, int A, int U,
@@ -436,7 +436,7 @@ int dgc_backproject_backward(const float* grad_volume, const float* projections,
     GeometryGrad out{{grad_angles, grad_sid, grad_sod, grad_det_u0, grad_det_v0, grad_src_x,
                       grad_src_y, grad_src_z}};
     for (int k = 0; k < 8; ++k) DGC_REQUIRE(out.g[k], "geometry gradient pointers must be non-null");
-    const long long nblocks = bp_backward_blocks(D, H, W);
+    const long long nblocks = bp_backward_blocks(D, H, W, A);
     Workspace ws(workspace, workspace_bytes);
     ViewRow* vt = ws.take<ViewRow>((size_t)A);
     float4* pq = ws.take<float4>((size_t)A * (U - 1) * (V - 1));
@@ -598,6 +598,35 @@ int dgc_reconstruct_fdk_partial(const float* projections, int A, int U, int V,
                                 src_y, src_z, pixel_size, D, H, W, voxel_size, off_x, off_y, off_z,
                                 alpha, uweights, angle_scale, false, volume, workspace,
                                 workspace_bytes, stream);
+}
+
+int dgc_bp_add_tile_rule(int d_max, int a_max, int kz_forward, int kz_backward, int cta_x,
+                         int cta_y) {
+    clear_error();
+    const int rc = bp_add_tile_rule(d_max, a_max, kz_forward, kz_backward, cta_x, cta_y);
+    if (rc == -2) {
+        set_error("dgc_bp_add_tile_rule: the rule table is full");
+        return DGC_ERR_INVALID_ARGUMENT;
+    }
+    DGC_REQUIRE(rc == 0, "dgc_bp_add_tile_rule: need d_max, a_max >= 1, kz in {0,1,2,4,8} and "
+                         "cta_x = cta_y = 0 or cta_x, cta_y >= 1 with cta_x*cta_y <= 16");
+    return DGC_OK;
+}
+
+int dgc_bp_clear_tile_rules(void) {
+    clear_error();
+    bp_clear_tile_rules();
+    return DGC_OK;
+}
+
+int dgc_bp_tiles(int D, int A, int* kz_forward, int* kz_backward, int* cta_x, int* cta_y) {
+    clear_error();
+    DGC_REQUIRE(D >= 1 && A >= 1, "D and A must be positive");
+    DGC_REQUIRE(kz_forward && kz_backward && cta_x && cta_y, "output pointers must be non-null");
+    *kz_forward = bp_kz_forward(D, A);
+    *kz_backward = bp_kz_backward(D, A);
+    bp_forward_cta(D, A, *cta_x, *cta_y);
+    return DGC_OK;
 }
 
 int dgc_clamp_volume(float* volume, long long n, void* stream) {

@@ -232,6 +232,21 @@ int dgc_reconstruct_fdk_partial(const float* projections, int A, int U, int V,
                                 const float* uweights, float angle_scale, float* volume,
                                 void* workspace, size_t workspace_bytes, void* stream);
 
+/* Backprojector tile rules (what the autotuner chose per shape bucket): a
+ * call with volume depth D <= d_max and A <= a_max views uses Z blocking
+ * kz_forward / kz_backward (32*kz voxels of a column per warp; 1, 2, 4 or 8,
+ * 0 = built-in choice) and a cta_x x cta_y patch of columns per CTA in the
+ * forward (both 0 = built-in 8 x 1; cta_x*cta_y <= 16).  Rules are tried in
+ * the order they were added (at most 16); the environment variables
+ * DGC_BP_KZ / DGC_BP_CTA take precedence.  Results do not depend on the tiles
+ * beyond float-summation order (the forward's not at all).  No counterpart in
+ * the reference. */
+int dgc_bp_add_tile_rule(int d_max, int a_max, int kz_forward, int kz_backward, int cta_x,
+                         int cta_y);
+int dgc_bp_clear_tile_rules(void);
+/* The tiles a call with depth D and A views uses. */
+int dgc_bp_tiles(int D, int A, int* kz_forward, int* kz_backward, int* cta_x, int* cta_y);
+
 /* volume[i] = max(volume[i], 0) in place (NaN stays NaN): the clamp that ends
  * an FDK reconstruction (filtering.py:197), after the partial volumes of a
  * view-sharded reconstruction have been summed. */

@@ -121,3 +121,71 @@ def test_autotuner_picks_fastest_and_caches(tmp_path):
     again = Autotuner(cache_path=path, measure=lambda *a: pytest.fail("cache miss"))
     assert again.choose(probs) == [(4, 8)] * 3
     assert probs[2].tiles == (4, 8)
+
+
+@pytest.fixture
+def clean_bp_rules(monkeypatch):
+    from cbct_backprojector import _native
+
+    monkeypatch.delenv("DGC_BP_KZ", raising=False)
+    monkeypatch.delenv("DGC_BP_CTA", raising=False)
+    lib = _native.lib()
+    lib.dgc_bp_clear_tile_rules()
+    yield lib
+    lib.dgc_bp_clear_tile_rules()
+
+
+def test_backprojector_tile_rules(clean_bp_rules, monkeypatch):
+    """Built-in Z blocking, rules (first match, zero fields keep the built-in
+    choice), argument checks and the environment's precedence -- host only."""
+    from cbct_backprojector import _native
+    from cbct_backprojector.autotune import backprojector_tiles
+
+    lib = clean_bp_rules
+    assert backprojector_tiles(256, 360) == (2, 4, (8, 1))
+    assert backprojector_tiles(50, 90) == (2, 2, (8, 1))
+    assert backprojector_tiles(20, 10) == (1, 1, (8, 1))
+    assert lib.dgc_bp_add_tile_rule(64, 128, 1, 0, 0, 0) == 0
+    assert lib.dgc_bp_add_tile_rule(256, 512, 8, 8, 4, 2) == 0
+    assert backprojector_tiles(50, 90) == (1, 2, (8, 1))       # first rule; kz_backward built in
+    assert backprojector_tiles(256, 360) == (8, 8, (4, 2))     # second rule
+    assert backprojector_tiles(256, 600) == (2, 4, (8, 1))     # no rule covers A = 600
+    monkeypatch.setenv("DGC_BP_KZ", "4")
+    monkeypatch.setenv("DGC_BP_CTA", "2,4")
+    assert backprojector_tiles(256, 360) == (4, 4, (2, 4))     # environment first
+    for bad in ((0, 10, 2, 2, 0, 0), (64, 10, 3, 2, 0, 0), (64, 10, 2, 2, 5, 4),
+                (64, 10, 2, 2, 4, 0)):
+        with pytest.raises(RuntimeError):
+            _native.check(lib.dgc_bp_add_tile_rule(*bad))
+    for _ in range(14):
+        assert lib.dgc_bp_add_tile_rule(1024, 1024, 2, 4, 0, 0) == 0
+    with pytest.raises(RuntimeError, match="full"):
+        _native.check(lib.dgc_bp_add_tile_rule(1024, 1024, 2, 4, 0, 0))
+
+
+def test_autotuner_tunes_backprojector(clean_bp_rules, tmp_path):
+    """Fastest forward (KZ, patch) and backward KZ per (depth, views) bucket,
+    cached as JSON and registered as a library rule."""
+    from cbct_backprojector.autotune import Autotuner, backprojector_tiles, bp_bucket
+
+    assert bp_bucket((256, 256, 256), 360) == (256, 512)
+    assert bp_bucket((100, 8, 8), 1) == (128, 1)
+    calls = []
+
+    def fake(proj, geom, px, shape, vs, off, direction, kz, cta):
+        calls.append((direction, kz, tuple(cta)))
+        if direction == "forward":
+            return 1.0 + abs(kz - 4) + (0.5 if tuple(cta) == (8, 1) else 0.0)
+        return 1.0 + abs(kz - 8)
+
+    geom = [SimpleNamespace(numel=lambda: 360)]
+    path = tmp_path / "tiles.json"
+    tuner = Autotuner(cache_path=path, measure_bp=fake)
+    e = tuner.tune_backprojector(None, geom, 1.0, (256, 256, 256), 1.0)
+    assert (e["kz_forward"], e["kz_backward"], e["cta"]) == (4, 8, [4, 2])
+    assert len(calls) == 4 * 2 + 3
+    assert backprojector_tiles(256, 360) == (4, 8, (4, 2))
+    clean_bp_rules.dgc_bp_clear_tile_rules()
+    again = Autotuner(cache_path=path, measure_bp=lambda *a: pytest.fail("cache miss"))
+    assert again.tune_backprojector(None, geom, 1.0, (200, 9, 9), 1.0)["kz_forward"] == 4
+    assert backprojector_tiles(256, 360) == (4, 8, (4, 2))

@@ -212,3 +212,30 @@ def test_column_patch_shapes_are_bitwise(cta, monkeypatch):
     torch.cuda.synchronize()
     assert torch.equal(a, b)
 
+
+
+def test_autotuner_on_backprojector(tmp_path, monkeypatch):
+    """tune_backprojector on the GPU: every candidate timed, the choice
+    registered as a library rule, the volume unchanged bit for bit."""
+    from cbct_backprojector import _native, backproject
+    from cbct_backprojector.autotune import Autotuner, backprojector_tiles
+
+    monkeypatch.delenv("DGC_BP_KZ", raising=False)
+    monkeypatch.delenv("DGC_BP_CTA", raising=False)
+    lib = _native.lib()
+    lib.dgc_bp_clear_tile_rules()
+    try:
+        case = random_case(8, px=1.0, vs=1.0, shape=(70, 21, 19))
+        proj = cuda32(case["proj"])
+        geom = [cuda32(g) for g in case["geom"]]
+        base = backproject(proj, *geom, 1.0, case["shape"], 1.0, volume_offset=case["off"])
+        tuner = Autotuner(cache_path=tmp_path / "tiles.json")
+        e = tuner.tune_backprojector(proj, geom, 1.0, case["shape"], 1.0, case["off"])
+        assert len(e["forward_ms"]) == 8 and len(e["backward_ms"]) == 3
+        assert backprojector_tiles(70, proj.shape[0]) == (e["kz_forward"], e["kz_backward"],
+                                                          tuple(e["cta"]))
+        tuned = backproject(proj, *geom, 1.0, case["shape"], 1.0, volume_offset=case["off"])
+        torch.cuda.synchronize()
+        assert torch.equal(base, tuned)
+    finally:
+        lib.dgc_bp_clear_tile_rules()
