@@ -1544,10 +1544,18 @@ int fp_launch_backward(const FpArgs& p, const FpTile& tile, bool gradvol, cudaSt
     }
 }
 
-int fp_launch_mse_grad(const FpArgs& p, const float* measured, const float* mask, float scale,
+int fp_mse_tile() {
+    if (const char* e = std::getenv("DGC_MSE_TU")) {
+        const int t = std::atoi(e);
+        if (t == 8 || t == 4 || t == 2) return t;
+    }
+    return 8;
+}
+
+namespace {
+template <int TU>
+int launch_mse_grad_tu(const FpArgs& p, const float* measured, const float* mask, float scale,
                        double* loss_partials, cudaStream_t s) {
-    DGC_TRACE("fp_mse_grad_kernel", s);
-    constexpr int TU = 8;
     const long long blocks = fp_tiles_per_view(p.U, p.V, TU) * (long long)p.A;
     const bool div = !is_pow2_float(p.voxel_size);
     const bool off = p.off_x != 0.0f || p.off_y != 0.0f || p.off_z != 0.0f;
@@ -1560,6 +1568,17 @@ int fp_launch_mse_grad(const FpArgs& p, const float* measured, const float* mask
     }
     DGC_LAUNCH_CHECK("fp_mse_grad_kernel");
     return DGC_OK;
+}
+}  // namespace
+
+int fp_launch_mse_grad(const FpArgs& p, const float* measured, const float* mask, float scale,
+                       double* loss_partials, cudaStream_t s) {
+    DGC_TRACE("fp_mse_grad_kernel", s);
+    switch (fp_mse_tile()) {
+        case 4: return launch_mse_grad_tu<4>(p, measured, mask, scale, loss_partials, s);
+        case 2: return launch_mse_grad_tu<2>(p, measured, mask, scale, loss_partials, s);
+        default: return launch_mse_grad_tu<8>(p, measured, mask, scale, loss_partials, s);
+    }
 }
 
 int fp_sum_partials(const double* x, long long n, double scale, double* out, cudaStream_t s) {
