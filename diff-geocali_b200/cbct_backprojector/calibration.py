@@ -3,7 +3,7 @@
 The reference project names a geometry-calibration pipeline but does not ship
 it (its README and docs/SOURCE.md); what it ships is the differentiable
 projector whose nine gradients make calibration possible.  This module builds
-the plain calibration loop on top of this build's operators:
+the plain calibration loop on top of this library's operators:
 
 * ``perturb_geometry``: per-view perturbations of a nominal circular scan
   (angle, source offsets, detector centre, sid/sod scale) drawn from a seed;

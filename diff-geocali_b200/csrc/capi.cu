@@ -81,7 +81,7 @@ int check_fp_common(int D, int H, int W, int A, int U, int V, float pixel_size, 
     DGC_REQUIRE(A > 0, "angles must contain at least one view");
     DGC_REQUIRE(geometry_ok(g), "geometry pointers must be non-null");
     if ((long long)(D + 2) * (H + 1) * (W + 1) >= (1LL << 31)) {
-        set_error("volume exceeds this build's 2^31 padded-voxel index limit");
+        set_error("volume exceeds the library's 2^31 padded-voxel index limit");
         return DGC_ERR_UNSUPPORTED;
     }
     if (fp_tiles_per_view(U, V, 4) * (long long)A >= (1LL << 31)) {

@@ -39,7 +39,7 @@ enum dgc_status {
     DGC_ERR_INVALID_ARGUMENT = 1, /* the reference raises RuntimeError (TORCH_CHECK) */
     DGC_ERR_CUDA = 2,             /* a CUDA runtime call or launch failed */
     DGC_ERR_WORKSPACE = 3,        /* workspace missing, misaligned or too small */
-    DGC_ERR_UNSUPPORTED = 4       /* sizes beyond this build's index limits */
+    DGC_ERR_UNSUPPORTED = 4       /* sizes beyond the library's index limits */
 };
 
 /* ABI version of the loaded library (DGC_ABI_VERSION). */

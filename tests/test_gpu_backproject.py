@@ -3,7 +3,7 @@ fixtures), the reference's own CUDA kernels and the FP64 oracle; gradients;
 edge cases.
 
 Tolerances: the reference's check_operator.py uses forward rtol/atol 2e-5 and
-gradients rtol 3e-4 / atol 3e-5 against FP64; the parity bar of this build
+gradients rtol 3e-4 / atol 3e-5 against FP64; the parity bar of this library
 is rel-L2 1e-5 (values) and 1e-4 (gradients) against the reference's CUDA.
 """
 

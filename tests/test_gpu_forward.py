@@ -3,7 +3,7 @@ own CUDA kernels and its CPU oracle (golden fixtures), gradients, edge cases.
 
 Tolerances: the reference's check_forward_operator.py uses forward
 rtol/atol 5e-5 and gradients rtol 1e-3 / atol 1e-4 against FP64; the
-parity bar for this build is rel-L2 1e-5 for projections and 1e-4 for
+parity bar for this library is rel-L2 1e-5 for projections and 1e-4 for
 gradients against the reference's CUDA path.
 """
 
