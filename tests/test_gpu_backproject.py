@@ -239,3 +239,21 @@ def test_autotuner_on_backprojector(tmp_path, monkeypatch):
         assert torch.equal(base, tuned)
     finally:
         lib.dgc_bp_clear_tile_rules()
+
+
+@pytest.mark.parametrize("shape", [(1, 1, 1), (1, 7, 5), (5, 1, 3), (33, 2, 2), (65, 3, 9)])
+def test_thin_volumes(shape, oracle):
+    """Volumes one or a few voxels thick along an axis (partial column
+    patches, partial Z blocks): values and all nine gradients against the
+    FP64 oracle."""
+    case = random_case(9, px=1.0, vs=1.0, shape=shape)
+    vol, proj, geom = run_bp(case, requires_grad=True)
+    truth = oracle.backproject(case["proj"], case["geom"], 1.0, shape, 1.0, case["off"])
+    assert rel_l2(vol.detach().cpu(), truth) < FWD_RTOL
+    up = torch.linspace(0.3, 1.2, vol.numel(), device="cuda").view_as(vol)
+    ours = torch.autograd.grad(vol, [proj, *geom], grad_outputs=up)
+    gp, gg = oracle.backproject_backward(up.cpu().numpy(), case["proj"], case["geom"], 1.0, 1.0,
+                                         case["off"])
+    assert rel_l2(ours[0].cpu(), gp) < GRAD_RTOL
+    for k, name in enumerate(GEOM_NAMES):
+        assert rel_l2(ours[1 + k].cpu(), gg[k]) < GRAD_RTOL, name
