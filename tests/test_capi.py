@@ -106,3 +106,17 @@ def test_preprocess_argument_checks(lib):
     assert b"min_ratio" in lib.dgc_last_error()
     assert lib.dgc_preprocess(p, None, None, 1, 4, 4, 1, 1e-6, p, None) == 1
     assert b"alias" in lib.dgc_last_error()
+
+
+def test_sharding_entries_check_arguments(lib):
+    """dgc_reconstruct_fdk_partial and dgc_clamp_volume reject bad arguments
+    before any CUDA call; an empty clamp is a no-op."""
+    g = _geom_ptrs()
+    for scale in (0.0, -1.0, float("inf")):
+        rc = lib.dgc_reconstruct_fdk_partial(None, 4, 8, 8, *g, 1.0, 4, 4, 4, 1.0, 0.0, 0.0, 0.0,
+                                             0.8, None, scale, None, None, 0, None)
+        assert rc == 1 and b"angle_scale" in lib.dgc_last_error()
+    assert lib.dgc_clamp_volume(None, -1, None) == 1
+    assert b"non-negative" in lib.dgc_last_error()
+    assert lib.dgc_clamp_volume(None, 5, None) == 1
+    assert lib.dgc_clamp_volume(None, 0, None) == 0
