@@ -20,8 +20,9 @@ holds only its views' projections and geometry:
 
 The exchange is one volume per call (67 MB at 256^3) after all of a rank's
 compute, so it is a single collective rather than a compute kernel fused with
-peer-memory transfers.  Without an initialised process group (or with one
-rank) the functions reduce to the single-device operators.  The reference runs
+peer-memory transfers.  Without an initialised process group the functions
+are the single-device operators (with one, the all-reduces run whatever its
+size).  The reference runs
 on one device (filtering.py:107-198, operator.py:73-127,
 source_only_forward_projector.py:119-145); no counterpart there.
 """
@@ -39,12 +40,6 @@ from .operator import backproject
 from .source_only_forward_projector import project
 
 
-def _world(group=None):
-    if not (dist.is_available() and dist.is_initialized()):
-        return 1, 0
-    return dist.get_world_size(group), dist.get_rank(group)
-
-
 def view_shard(views, world_size, rank):
     """The contiguous view range ``range(start, stop)`` of ``rank``: balanced,
     the first ``views % world_size`` ranks take one view more."""
@@ -57,7 +52,7 @@ def view_shard(views, world_size, rank):
 
 
 def _all_reduce_sum(tensor, group=None):
-    if _world(group)[0] > 1:
+    if dist.is_available() and dist.is_initialized():
         dist.all_reduce(tensor, op=dist.ReduceOp.SUM, group=group)
     return tensor
 

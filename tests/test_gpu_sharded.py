@@ -76,3 +76,46 @@ def test_one_rank_is_the_single_device_operator():
         outs.append((vb.detach(), q.grad))
     assert torch.equal(outs[0][0], outs[1][0])
     assert rel_l2(outs[0][1].cpu(), outs[1][1].cpu()) < 1e-6
+
+
+def _nccl_rank(port, out):
+    import os
+    from datetime import timedelta
+
+    import torch.distributed as dist
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    torch.cuda.set_device(0)
+    dist.init_process_group("nccl", rank=0, world_size=1, timeout=timedelta(seconds=60))
+    try:
+        from cbct_backprojector import reconstruct_fdk
+        from cbct_backprojector.sharded import reconstruct_fdk_sharded, total_views
+
+        A, U, V, shape = 30, 40, 36, (16, 20, 18)
+        proj, geom = _scan(A, U, V, 12)
+        n = total_views(A, proj.device)
+        a = reconstruct_fdk_sharded(proj, *geom, 1.0, shape, 1.0)
+        b = reconstruct_fdk(proj, *geom, 1.0, shape, 1.0)
+        torch.cuda.synchronize()
+        out.put((n, bool(torch.equal(a, b))))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_one_rank_nccl_group():
+    """The sharded reconstruction through a real NCCL process group (one
+    rank: the all-reduces run, the result is the single-device one)."""
+    import socket
+
+    import torch.multiprocessing as mp
+
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    p = ctx.Process(target=_nccl_rank, args=(port, q))
+    p.start()
+    p.join(120)
+    assert p.exitcode == 0, p.exitcode
+    assert q.get(timeout=5) == (30, True)
