@@ -137,6 +137,20 @@ def angle_error_deg(geometry_a, geometry_b):
     return float(torch.rad2deg(d).square().mean().sqrt())
 
 
+def _metric_terms(geometry_a, geometry_b, points, pixel_size):
+    """FP64 [4]: sum and count of the squared detector distances and of the
+    squared angle differences (the RMS metrics before the mean), so that
+    ranks holding different views can add them up."""
+    da = detector_coordinates(points, geometry_a, pixel_size)
+    db = detector_coordinates(points, geometry_b, pixel_size)
+    sq = (da - db).square().sum(-1)
+    dang = torch.rad2deg(geometry_a[0].double() - geometry_b[0].double())
+    return torch.stack([sq.sum(), torch.tensor(float(sq.numel()), dtype=torch.float64,
+                                                 device=sq.device),
+                        dang.square().sum(), torch.tensor(float(dang.numel()),
+                                                          dtype=torch.float64, device=sq.device)])
+
+
 @dataclass
 class CalibrationResult:
     delta: list
@@ -146,6 +160,17 @@ class CalibrationResult:
     iterations_to_target: int | None = None
     warm_start_accepted: bool | None = None
     final_loss: float = float("nan")
+
+
+def _loss_terms(volume, geometry, measured, scan, mask=None):
+    """(sum of the squared mismatch over the usable rays, their count)."""
+    p = project(volume, *geometry, scan.pixel_size, scan.U, scan.V, step_size=scan.step_size,
+                voxel_size=scan.voxel_size, off_x=scan.volume_offset[0],
+                off_y=scan.volume_offset[1], off_z=scan.volume_offset[2])
+    r = (p - measured).square()
+    if mask is None:
+        return r.sum(), torch.tensor(float(r.numel()), device=r.device)
+    return (r * mask).sum(), mask.sum()
 
 
 def _loss(volume, geometry, measured, scan, mask=None):
@@ -186,7 +211,7 @@ def calibrate(volume, measured, nominal, scan: ScanSetup, iterations=200, lr=Non
               warm_start=None, true_geometry=None, points=None, target_px=0.1,
               target_angle_deg=None, stop_at_target=False, log_every=0, mask=None,
               final_lr_fraction=1.0, lr_gamma=1.0, decay_start=0, fused=True,
-              warmup_iterations=0, betas=(0.9, 0.99)):
+              warmup_iterations=0, betas=(0.9, 0.99), reduce=None):
     """Adam on per-view geometry offsets; returns a ``CalibrationResult``.
 
     The loss is the mean squared mismatch between ``project(volume, nominal +
@@ -205,6 +230,13 @@ def calibrate(volume, measured, nominal, scan: ScanSetup, iterations=200, lr=Non
     iteration and the wall time to ``target_px`` (and ``target_angle_deg``) is
     recorded, counted from the call (network inference happens before it and is
     the caller's to add).
+
+    ``reduce`` (view sharding, ``sharded.calibrate_sharded``): each caller
+    holds only its own views, and ``reduce`` sums an FP64 tensor over all of
+    them; the loss normalisation, the warm-start judge, the recorded loss and
+    the metrics are then those of the whole scan.  The views' offsets are
+    independent, so every rank's steps equal those of one calibration over all
+    views.
     """
     t0 = time.perf_counter()
     lr = dict(DEFAULT_LR, **(lr or {}))
@@ -213,11 +245,19 @@ def calibrate(volume, measured, nominal, scan: ScanSetup, iterations=200, lr=Non
     nominal = [g.detach() for g in nominal]
     delta = [torch.zeros_like(g) for g in nominal]
     accepted = None
+
+    def loss_of(geometry):
+        if reduce is None:
+            return float(_loss(volume, geometry, measured, scan, mask))
+        s_, c_ = _loss_terms(volume, geometry, measured, scan, mask)
+        t_ = reduce(torch.stack([s_.double(), c_.double()]))
+        return float(t_[0] / t_[1].clamp_min(1.0))
+
     if warm_start is not None:
         with torch.no_grad():
-            l_nom = float(_loss(volume, nominal, measured, scan, mask))
+            l_nom = loss_of(nominal)
             start = [g + d.to(g) for g, d in zip(nominal, warm_start)]
-            l_warm = float(_loss(volume, start, measured, scan, mask))
+            l_warm = loss_of(start)
         accepted = l_warm <= l_nom
         if accepted:
             delta = [d.detach().to(g).clone() for g, d in zip(nominal, warm_start)]
@@ -239,8 +279,14 @@ def calibrate(volume, measured, nominal, scan: ScanSetup, iterations=200, lr=Non
         entry = {"iteration": it, "loss": loss_value, "time_s": time.perf_counter() - t0}
         if true_geometry is not None:
             geom = [g + d.detach() for g, d in zip(nominal, delta)]
-            entry["reproj_px"] = reprojection_error(geom, true_geometry, points, scan.pixel_size)
-            entry["angle_err_deg"] = angle_error_deg(geom, true_geometry)
+            if reduce is None:
+                entry["reproj_px"] = reprojection_error(geom, true_geometry, points,
+                                                        scan.pixel_size)
+                entry["angle_err_deg"] = angle_error_deg(geom, true_geometry)
+            else:
+                m = reduce(_metric_terms(geom, true_geometry, points, scan.pixel_size))
+                entry["reproj_px"] = float((m[0] / m[1]).sqrt())
+                entry["angle_err_deg"] = float((m[2] / m[3]).sqrt())
             ok = entry["reproj_px"] <= target_px and (
                 target_angle_deg is None or entry["angle_err_deg"] <= target_angle_deg)
             if ok and result.time_to_target_s is None:
@@ -250,21 +296,30 @@ def calibrate(volume, measured, nominal, scan: ScanSetup, iterations=200, lr=Non
         if log_every and it % log_every == 0:
             print({k: (round(v, 5) if isinstance(v, float) else v) for k, v in entry.items()})
 
-    denom = float(measured.numel() if mask is None else mask.sum().clamp_min(1.0))
+    if reduce is None:
+        denom = float(measured.numel() if mask is None else mask.sum().clamp_min(1.0))
+    else:
+        count = float(measured.numel()) if mask is None else mask.double().sum()
+        count = torch.as_tensor(count, dtype=torch.float64, device=measured.device).reshape(1)
+        denom = float(reduce(count).clamp_min(1.0))
     record(0, float("nan"))
     for it in range(1, iterations + 1):
         opt.zero_grad(set_to_none=True)
         geom = [g + d for g, d in zip(nominal, delta)]
         if fused:
             loss = _fused_loss(volume, geom, measured, scan, mask, denom)
-        else:
+        elif reduce is None:
             loss = _loss(volume, geom, measured, scan, mask)
+        else:
+            loss = _loss_terms(volume, geom, measured, scan, mask)[0] / denom
         loss.backward()
         opt.step()
         sched.step()
-        record(it, float(loss.detach()))
+        lv = loss.detach()
+        record(it, float(lv) if reduce is None else float(reduce(lv.double().reshape(1))))
         if stop_at_target and result.time_to_target_s is not None:
             break
     result.geometry = [g + d.detach() for g, d in zip(nominal, delta)]
-    result.final_loss = float(_loss(volume, result.geometry, measured, scan, mask).detach())
+    with torch.no_grad():
+        result.final_loss = loss_of(result.geometry)
     return result

@@ -17,6 +17,9 @@ holds only its views' projections and geometry:
   views: nothing is exchanged in the forward; the backward all-reduces the
   volume gradient (the adjoint summed over all views), while the geometry
   gradients stay with the views they belong to.
+* ``calibrate_sharded`` -- per-view geometry calibration of the rank's views
+  (the offsets of different views never interact); only the loss
+  normalisation and the stopping metrics are summed over the ranks.
 
 The exchange is one volume per call (67 MB at 256^3) after all of a rank's
 compute, so it is a single collective rather than a compute kernel fused with
@@ -150,5 +153,20 @@ def project_sharded(volume, angles, sid, sod, det_u0_arr, det_v0_arr, src_x_arr,
                    off_y, off_z)
 
 
+def calibrate_sharded(volume, measured, nominal, scan, group=None, **kwargs):
+    """``calibration.calibrate`` of one scan whose views are spread over the
+    ranks of ``group``: every rank passes the replicated volume and its own
+    views' ``measured`` / ``mask`` / ``nominal`` / ``warm_start`` /
+    ``true_geometry`` and gets its views' offsets.  The per-view offsets are
+    independent, so nothing is exchanged per step but the loss normalisation
+    (once), the recorded loss and the stopping metrics (a few FP64 numbers per
+    iteration); each rank's result equals one calibration over all views,
+    restricted to its views."""
+    from .calibration import calibrate
+
+    return calibrate(volume, measured, nominal, scan,
+                     reduce=lambda t: _all_reduce_sum(t.contiguous().clone(), group), **kwargs)
+
+
 __all__ = ["view_shard", "total_views", "reconstruct_fdk_sharded", "backproject_sharded",
-           "project_sharded"]
+           "project_sharded", "calibrate_sharded"]

@@ -123,3 +123,111 @@ def test_two_gloo_ranks_sharded_views():
         assert res["fdk_err"] < 1e-6 and res["fdk_negative_clamped"], res
         assert res["project_grad_err"] < 1e-12, res
         assert res["bp_value_err"] < 1e-12 and res["bp_grad_err"] < 1e-12, res
+
+
+def _calib_standins(monkeypatch_target):
+    """CPU stand-ins for the projection losses: a view's 'measurement' row
+    holds its true eight parameters and the loss is the masked squared
+    parameter mismatch, so every view's offsets only see their own view."""
+    import torch
+
+    def terms(volume, geometry, measured, scan, mask=None):
+        r = (torch.stack(list(geometry), 1) - measured).square() * mask
+        return r.sum(), mask.sum()
+
+    def fused(volume, geometry, measured, scan, mask=None, denom=None):
+        return terms(volume, geometry, measured, scan, mask)[0] / denom
+
+    monkeypatch_target._loss_terms = terms
+    monkeypatch_target._fused_loss = fused
+    monkeypatch_target._loss = lambda *a, **k: (lambda s, c: s / c)(*terms(*a, **k))
+
+
+def _calib_problem():
+    import numpy as np
+    import torch
+
+    rng = np.random.default_rng(8)
+    A = 13
+    nominal = [torch.tensor(x, dtype=torch.float32) for x in (
+        np.arange(A) * (2 * np.pi / A), np.full(A, 300.0), np.full(A, 180.0), np.full(A, 20.0),
+        np.full(A, 16.0), np.zeros(A), np.zeros(A), np.zeros(A))]
+    scale = np.array([3e-3, 2.0, 2.0, 1.0, 1.0, 0.5, 0.5, 0.5])
+    true = [g + torch.tensor(rng.normal(0, s, A), dtype=torch.float32)
+            for g, s in zip(nominal, scale)]
+    measured = torch.stack(true, 1)
+    mask = torch.tensor(rng.random((A, 8)) > 0.1, dtype=torch.float32)
+    return nominal, true, measured, mask
+
+
+def _calib_rank(rank, world, port, out):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank),
+                      WORLD_SIZE=str(world), LOCAL_RANK=str(rank))
+    import torch
+    import torch.distributed as dist
+
+    from cbct_backprojector import calibration, sharded
+    from cbct_backprojector.calibration import ScanSetup
+
+    _calib_standins(calibration)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
+    try:
+        nominal, true, measured, mask = _calib_problem()
+        v = sharded.view_shard(nominal[0].numel(), world, rank)
+        sl = slice(v.start, v.stop)
+        pts = calibration.lattice_points((8, 8, 8), device="cpu", n=3)
+        res = sharded.calibrate_sharded(
+            torch.zeros(1), measured[sl], [g[sl] for g in nominal], ScanSetup(U=8, V=8),
+            iterations=60, true_geometry=[g[sl] for g in true], points=pts, mask=mask[sl],
+            target_px=0.75)
+        out.put((rank, [d.detach().numpy().copy() for d in res.delta],  # by value
+                 [(e["reproj_px"], e["angle_err_deg"], e["loss"]) for e in res.history],
+                 res.iterations_to_target, res.final_loss))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.timeout(180)
+def test_two_gloo_ranks_sharded_calibration(monkeypatch):
+    """Each rank's offsets equal one calibration over all views, restricted to
+    its views, bit for bit; the metrics, loss and iteration to target agree."""
+    import math
+
+    import torch
+
+    from cbct_backprojector import calibration
+    from cbct_backprojector.calibration import ScanSetup
+
+    for name in ("_loss_terms", "_fused_loss", "_loss"):
+        monkeypatch.setattr(calibration, name, getattr(calibration, name))
+    _calib_standins(calibration)
+    nominal, true, measured, mask = _calib_problem()
+    pts = calibration.lattice_points((8, 8, 8), device="cpu", n=3)
+    whole = calibration.calibrate(torch.zeros(1), measured, nominal, ScanSetup(U=8, V=8),
+                                  iterations=60, true_geometry=true, points=pts, mask=mask,
+                                  target_px=0.75)
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_calib_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(150)
+    assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
+    got = {r: rest for r, *rest in (q.get(timeout=5) for _ in range(2))}
+    from cbct_backprojector.sharded import view_shard
+
+    for r in range(2):
+        delta, hist, it_target, final = got[r]
+        v = view_shard(13, 2, r)
+        for d, w in zip(delta, whole.delta):
+            assert torch.equal(torch.from_numpy(d), w.detach()[v.start:v.stop])
+        assert it_target == whole.iterations_to_target is not None
+        assert math.isclose(final, whole.final_loss, rel_tol=1e-6)
+        for (rp, ang, loss), e in zip(hist, whole.history):
+            assert math.isclose(rp, e["reproj_px"], rel_tol=1e-9)
+            assert math.isclose(ang, e["angle_err_deg"], rel_tol=1e-9)
+            assert (math.isnan(loss) and math.isnan(e["loss"])) or \
+                math.isclose(loss, e["loss"], rel_tol=1e-5)
