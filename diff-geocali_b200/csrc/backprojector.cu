@@ -470,9 +470,9 @@ void bp_grid(int D, int H, int W, int kz, unsigned& gx, unsigned& gy) {
     gy = (unsigned)ceil_div(D, 32 * kz);
 }
 
-long long bp_backward_blocks(int D, int H, int W, int A) {
+long long bp_backward_blocks(int D, int H, int W, int kz) {
     unsigned gx, gy;
-    bp_grid(D, H, W, bp_kz_backward(D, A), gx, gy);
+    bp_grid(D, H, W, kz, gx, gy);
     return (long long)gx * gy;
 }
 
@@ -518,7 +518,9 @@ int bp_launch_forward(const BpArgs& args, bool fdk, cudaStream_t s) {
 
 int bp_launch_backward(const BpArgs& p, cudaStream_t s) {
     DGC_TRACE("bp_backward_kernel", s);
-    const int kz = bp_kz_backward(p.D, p.A);
+    // the Z blocking the caller sized the partials for (a rule added by another
+    // thread in between must not change the grid)
+    const int kz = p.kz_backward ? p.kz_backward : bp_kz_backward(p.D, p.A);
     unsigned gx, gy;
     bp_grid(p.D, p.H, p.W, kz, gx, gy);
     const dim3 grid(gx, gy);

@@ -27,6 +27,7 @@ struct BpArgs {
     // forward
     float* volume;     // [D][H][W]
     int cta_x, cta_y;  // forward: columns per CTA along x and y (cta_x*cta_y <= kBpMaxWarps)
+    int kz_backward;   // backward: Z blocking chosen with the partials' size (0: choose)
     float out_scale;   // FDK epilogue scale (pi/A)
     int clamp;         // FDK epilogue: clamp at 0 (0 for a view-sharded partial volume)
     // backward
@@ -40,7 +41,7 @@ int build_proj_quads(const float* P, int A, int U, int V, float4* PQ, cudaStream
 int bp_launch_forward(const BpArgs& p, bool fdk, cudaStream_t s);
 int bp_launch_backward(const BpArgs& p, cudaStream_t s);
 int bp_clamp_volume(float* volume, long long n, cudaStream_t s);
-long long bp_backward_blocks(int D, int H, int W, int A);
+long long bp_backward_blocks(int D, int H, int W, int kz);
 // Tiles of a call with volume depth D and A views (rules, overrides, built-in
 // choice) and the rule table behind dgc_bp_add_tile_rule (0 ok, -1 invalid,
 // -2 table full).

@@ -297,6 +297,7 @@ int dgc_project_backward(const float* grad_projection, const float* volume, int 
     rc = build_volume_quads(volume, D, H, W, quads, s);
     if (rc != DGC_OK) return rc;
     if (records) fp_fill_cell_layout(p);
+    p.scatter = scatter;
     if (gpad) DGC_CUDA(cudaMemsetAsync(gpad, 0, sizeof(float) * gfloats, s));
     rc = fp_launch_backward(p, kBackwardTile, compute_grad_volume != 0, s);
     if (rc != DGC_OK) return rc;
@@ -414,7 +415,7 @@ int dgc_backproject(const float* projections, int A, int U, int V, const float* 
 size_t dgc_backproject_backward_workspace_bytes(int A, int U, int V, int D, int H, int W) {
     if (A <= 0 || U < 2 || V < 2 || D <= 0 || H <= 0 || W <= 0) return 0;
     return bp_table_bytes(A) + bp_quads_bytes(A, U, V) +
-           Workspace::align(sizeof(double) * 8 * (size_t)A * (size_t)bp_backward_blocks(D, H, W, A));
+           Workspace::align(sizeof(double) * 8 * (size_t)A * (size_t)bp_backward_blocks(D, H, W, bp_kz_backward(D, A)));
 }
 
 int dgc_backproject_backward(const float* grad_volume, const float* projections, int A, int U,
@@ -436,7 +437,8 @@ int dgc_backproject_backward(const float* grad_volume, const float* projections,
     GeometryGrad out{{grad_angles, grad_sid, grad_sod, grad_det_u0, grad_det_v0, grad_src_x,
                       grad_src_y, grad_src_z}};
     for (int k = 0; k < 8; ++k) DGC_REQUIRE(out.g[k], "geometry gradient pointers must be non-null");
-    const long long nblocks = bp_backward_blocks(D, H, W, A);
+    const int kz = bp_kz_backward(D, A);
+    const long long nblocks = bp_backward_blocks(D, H, W, kz);
     Workspace ws(workspace, workspace_bytes);
     ViewRow* vt = ws.take<ViewRow>((size_t)A);
     float4* pq = ws.take<float4>((size_t)A * (U - 1) * (V - 1));
@@ -456,6 +458,7 @@ int dgc_backproject_backward(const float* grad_volume, const float* projections,
     }
     p.grad_volume = grad_volume;
     p.partials = partials;
+    p.kz_backward = kz;
     if ((rc = bp_launch_backward(p, s)) != DGC_OK) return rc;
     return bp_reduce_partials(partials, A, nblocks, out, s);
 }

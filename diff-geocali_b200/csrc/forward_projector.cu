@@ -1429,7 +1429,10 @@ int launch_backward_tu(const FpArgs& p, bool gradvol, cudaStream_t s) {
     // (204 vs 117 ms at 256^3 / 360 x 384^2): the slab barriers hold the
     // bundle's fastest rays back, and the shared-memory additions cost about
     // what the L2 reductions they replace cost.
-    const bool brick = gradvol && fp_volume_scatter() == kScatterBrick;
+    // the scatter the caller laid the gradient buffer out for, decided once
+    const VolumeScatter scatter =
+        p.scatter ? static_cast<VolumeScatter>(p.scatter) : fp_volume_scatter();
+    const bool brick = gradvol && scatter == kScatterBrick;
     if (brick) {
         constexpr int smem = kBrickCap * (int)sizeof(float);
         static std::atomic<unsigned long long> configured{0};
@@ -1443,7 +1446,7 @@ int launch_backward_tu(const FpArgs& p, bool gradvol, cudaStream_t s) {
     } else if (!gradvol) {
         fp_backward_kernel<TU, 0><<<(unsigned)blocks, 256, 0, s>>>(p);
     } else {
-        switch (fp_volume_scatter()) {
+        switch (scatter) {
             case kScatterCells: fp_backward_kernel<TU, 3><<<(unsigned)blocks, 256, 0, s>>>(p); break;
             case kScatterLevels: fp_backward_kernel<TU, 4><<<(unsigned)blocks, 256, 0, s>>>(p); break;
             case kScatterRuns: fp_backward_kernel<TU, 5><<<(unsigned)blocks, 256, 0, s>>>(p); break;

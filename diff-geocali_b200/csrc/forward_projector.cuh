@@ -20,6 +20,7 @@ struct FpArgs {
     float* grad_pad;                // G[(yp*(W+2) + xp)*(D+2) + zp] or null
     uint32_t gz_x, gz_y, gz_bias;
     double* partials;  // [A][tiles][8]
+    int scatter;       // VolumeScatter the gradient buffer was laid out for (0: choose)
 };
 
 // Ray tile of a CTA: TU detector columns x (256/TU) rows; the 32 lanes of a
