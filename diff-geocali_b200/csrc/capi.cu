@@ -353,7 +353,8 @@ int dgc_project_mse_grad(const float* volume, int D, int H, int W, const float* 
     p.off_y = off_y;
     p.off_z = off_z;
     fp_fill_layout(p);
-    const long long tiles = fp_tiles_per_view(U, V, fp_mse_tile());
+    const int tile = fp_mse_tile();
+    const long long tiles = fp_tiles_per_view(U, V, tile);
     Workspace ws(workspace, workspace_bytes);
     float4* quads = ws.take<float4>((size_t)(D + 2) * (H + 1) * (W + 1));
     double* partials = ws.take<double>((size_t)8 * A * tiles);
@@ -369,7 +370,7 @@ int dgc_project_mse_grad(const float* volume, int D, int H, int W, const float* 
     p.projections = projections;
     rc = build_volume_quads(volume, D, H, W, quads, s);
     if (rc != DGC_OK) return rc;
-    rc = fp_launch_mse_grad(p, measured, mask, scale, lpart, s);
+    rc = fp_launch_mse_grad(p, tile, measured, mask, scale, lpart, s);
     if (rc != DGC_OK) return rc;
     rc = fp_reduce_partials(partials, A, tiles, out, s);
     if (rc != DGC_OK) return rc;

@@ -1574,10 +1574,10 @@ int launch_mse_grad_tu(const FpArgs& p, const float* measured, const float* mask
 }
 }  // namespace
 
-int fp_launch_mse_grad(const FpArgs& p, const float* measured, const float* mask, float scale,
-                       double* loss_partials, cudaStream_t s) {
+int fp_launch_mse_grad(const FpArgs& p, int tile, const float* measured, const float* mask,
+                       float scale, double* loss_partials, cudaStream_t s) {
     DGC_TRACE("fp_mse_grad_kernel", s);
-    switch (fp_mse_tile()) {
+    switch (tile) {
         case 4: return launch_mse_grad_tu<4>(p, measured, mask, scale, loss_partials, s);
         case 2: return launch_mse_grad_tu<2>(p, measured, mask, scale, loss_partials, s);
         default: return launch_mse_grad_tu<8>(p, measured, mask, scale, loss_partials, s);

@@ -103,8 +103,9 @@ int fp_launch_counts(const FpArgs& p, int64_t* counts, cudaStream_t s);
 // tiles); p.partials [A][tiles][8], loss_partials [A][tiles].
 // Columns per CTA tile of the fused calibration step (8; DGC_MSE_TU=4|2 overrides).
 int fp_mse_tile();
-int fp_launch_mse_grad(const FpArgs& p, const float* measured, const float* mask, float scale,
-                       double* loss_partials, cudaStream_t s);
+// tile: columns per CTA (fp_mse_tile(), decided with the partials' size)
+int fp_launch_mse_grad(const FpArgs& p, int tile, const float* measured, const float* mask,
+                       float scale, double* loss_partials, cudaStream_t s);
 int fp_sum_partials(const double* x, long long n, double scale, double* out, cudaStream_t s);
 int fp_reduce_partials(const double* partials, int A, long long tiles, const GeometryGrad& out,
                        cudaStream_t s);
