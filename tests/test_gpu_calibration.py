@@ -138,7 +138,7 @@ def test_fused_step_matches_project_and_autograd():
         want = torch.autograd.grad(ref, g)
         torch.cuda.synchronize()
         assert torch.equal(proj, p.detach())
-        assert math.isclose(float(loss.detach()), float(ref), rel_tol=1e-5)
+        assert math.isclose(float(loss.detach()), float(ref.detach()), rel_tol=1e-5)
         for k in range(8):
             a, b = grads[k].double(), want[k].double()
             assert float((a - b).norm() / b.norm()) < 1e-5, k
