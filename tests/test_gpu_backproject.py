@@ -176,19 +176,21 @@ def test_geometry_only_backward_skips_the_projection_gradient():
         assert torch.equal(a, b)
 
 
+@pytest.mark.parametrize("px", [1.0, 0.9])
 @pytest.mark.parametrize("kz", ["1", "2", "4", "8"])
-def test_every_z_blocking_matches_the_oracle(kz, oracle, monkeypatch):
+def test_every_z_blocking_matches_the_oracle(kz, px, oracle, monkeypatch):
     """DGC_BP_KZ: 32*KZ voxels of a column per warp (the defaults pick 2 for
     the forward, 4 for the backward); every choice, with D not a multiple of
-    the warp's span, against the FP64 oracle."""
+    the warp's span and with the dividing (non power-of-two) pixel size,
+    against the FP64 oracle."""
     monkeypatch.setenv("DGC_BP_KZ", kz)
-    case = random_case(4, px=1.0, vs=1.0, shape=(70, 21, 19))
+    case = random_case(4, px=px, vs=1.0, shape=(70, 21, 19))
     vol, proj, geom = run_bp(case, requires_grad=True)
-    truth = oracle.backproject(case["proj"], case["geom"], 1.0, case["shape"], 1.0, case["off"])
+    truth = oracle.backproject(case["proj"], case["geom"], px, case["shape"], 1.0, case["off"])
     assert rel_l2(vol.detach().cpu(), truth) < FWD_RTOL
     up = torch.linspace(-0.7, 1.3, vol.numel(), device="cuda").view_as(vol)
     ours = torch.autograd.grad(vol, [proj, *geom], grad_outputs=up)
-    gp, gg = oracle.backproject_backward(up.cpu().numpy(), case["proj"], case["geom"], 1.0, 1.0,
+    gp, gg = oracle.backproject_backward(up.cpu().numpy(), case["proj"], case["geom"], px, 1.0,
                                          case["off"])
     assert rel_l2(ours[0].cpu(), gp) < GRAD_RTOL
     for k, name in enumerate(GEOM_NAMES):
