@@ -120,3 +120,38 @@ def test_sharding_entries_check_arguments(lib):
     assert b"non-negative" in lib.dgc_last_error()
     assert lib.dgc_clamp_volume(None, 5, None) == 1
     assert lib.dgc_clamp_volume(None, 0, None) == 0
+
+
+def test_header_is_c99_and_links_from_c(tmp_path):
+    """include/dgc.h compiles as strict C99 and a C program links against
+    libdgc.so and calls it (host-only entry points, no GPU)."""
+    import shutil
+    import subprocess
+    from pathlib import Path
+
+    from cbct_backprojector import _native
+
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        pytest.skip("no C compiler")
+    root = Path(__file__).resolve().parents[1]
+    libdir = Path(_native.LIB_PATH).parent
+    src = tmp_path / "use_dgc.c"
+    src.write_text(
+        '#include "dgc.h"\n'
+        "#include <stdio.h>\n"
+        "int main(void) {\n"
+        "    double taps[16];\n"
+        "    if (dgc_abi_version() != DGC_ABI_VERSION) return 1;\n"
+        "    if (dgc_fdk_filter_taps(16, 1.0, 0.8, taps) != DGC_OK) return 2;\n"
+        "    if (dgc_fdk_filter_taps(16, 1.0, 2.0, taps) != DGC_ERR_INVALID_ARGUMENT) return 3;\n"
+        '    printf("%s\\n", dgc_last_error());\n'
+        "    return taps[0] > 0.0 ? 0 : 4;\n"
+        "}\n")
+    exe = tmp_path / "use_dgc"
+    subprocess.run([gcc, "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror",
+                    f"-I{root / 'include'}", str(src), f"-L{libdir}", "-ldgc",
+                    f"-Wl,-rpath,{libdir}", "-o", str(exe)], check=True)
+    run = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert run.returncode == 0, (run.returncode, run.stdout, run.stderr)
+    assert "alpha" in run.stdout
