@@ -74,6 +74,9 @@ SIGNATURES = {
     "dgc_parker_weights": (_I, [_P, _P, _I, _I, _F, _P, _P]),
     "dgc_reconstruct_fdk_weighted": (_I, [_P, _I, _I, _I, *_GEOM, _F, _I, _I, _I, _F, _F, _F, _F, _F,
                                           _P, _F, _P, _P, _S, _P]),
+    "dgc_fdk_filter_backward_workspace_bytes": (_S, [_I] * 3),
+    "dgc_fdk_filter_backward": (_I, [_P, _P, _P, _I, _I, _I, _F, _P, _P, _F, _P, _P, _P, _P, _S,
+                                     _P]),
     "dgc_reconstruct_fdk_partial": (_I, [_P, _I, _I, _I, *_GEOM, _F, _I, _I, _I, _F, _F, _F, _F, _F,
                                          _P, _F, _P, _P, _S, _P]),
     "dgc_clamp_volume": (_I, [_P, ctypes.c_longlong, _P]),

@@ -271,6 +271,28 @@ def fdk_filter(projections, pixel_size, sod, sid, alpha):
     return out
 
 
+def fdk_filter_backward(grad_filtered, projections, filtered, pixel_size, sod, sid, alpha,
+                        need_projections=True, need_distances=True):
+    """Gradients of ``fdk_filter`` (dgc_fdk_filter_backward): ``(grad_projections,
+    grad_sod, grad_sid)``, each None when not asked for."""
+    g = grad_filtered.contiguous()
+    A, U, V = g.shape
+    dev = g.device
+    gp = torch.empty_like(g) if need_projections else None
+    gsod = torch.empty((A,), dtype=torch.float32, device=dev) if need_distances else None
+    gsid = torch.empty((A,), dtype=torch.float32, device=dev) if need_distances else None
+    p = projections.contiguous() if need_distances else None
+    y = filtered.contiguous() if need_distances else None
+    lib = _native.lib()
+    with torch.cuda.device(dev):
+        ws = _workspace(lib.dgc_fdk_filter_backward_workspace_bytes(A, U, V), dev)
+        _native.check(lib.dgc_fdk_filter_backward(
+            g.data_ptr(), _p(p), _p(y), A, U, V, float(pixel_size), sod.data_ptr(),
+            sid.data_ptr(), float(alpha), _p(gp), _p(gsod), _p(gsid), _p(ws),
+            0 if ws is None else ws.numel(), _stream(dev)))
+    return gp, gsod, gsid
+
+
 def reconstruct_fdk(projections, geometry, pixel_size, volume_shape, voxel_size, volume_offset,
                     alpha):
     """Filter + backproject all views, * pi/A, clamp at 0, in two kernels."""

@@ -8,7 +8,9 @@ reference's zero padding to 2^bitlen(2U-1), ``pixel_size * sid / sod`` scale,
 backprojection, ``pi / A`` normalisation and a clamp at zero.
 
 Differences by design: the filter runs on the GPU as a Toeplitz product (the
-exact equivalent of the reference's padded FFT convolution) and
+exact equivalent of the reference's padded FFT convolution), with a
+hand-written backward for the projections and the per-view distances (the
+reference gets them from autograd through its torch code), and
 ``reconstruct_fdk`` filters and backprojects all views in one pass, so
 ``angle_chunk_size`` is validated but does not split the work.  Inputs must be
 CUDA tensors: there is no CPU path.
@@ -18,6 +20,7 @@ import math
 import operator
 
 import torch
+from torch.autograd.function import once_differentiable
 
 from . import _ops
 
@@ -59,6 +62,31 @@ def _per_view_distance(name, value, projections):
     return distance.contiguous()
 
 
+class _FdkFilter(torch.autograd.Function):
+    """``fdk_filter`` under autograd: gradients for the projections and the
+    per-view distances (the reference's torch filter has them from autograd,
+    filtering.py:54-104); the backward is ``dgc_fdk_filter_backward``."""
+
+    @staticmethod
+    def forward(ctx, projections, sod, sid, pixel_size, alpha):
+        out = _ops.fdk_filter(projections, pixel_size, sod, sid, alpha)
+        ctx.save_for_backward(projections, sod, sid, out)
+        ctx.settings = (pixel_size, alpha)
+        return out
+
+    @staticmethod
+    @once_differentiable
+    def backward(ctx, grad):
+        projections, sod, sid, out = ctx.saved_tensors
+        pixel_size, alpha = ctx.settings
+        need_p, need_sod, need_sid = ctx.needs_input_grad[:3]
+        gp, gsod, gsid = _ops.fdk_filter_backward(grad, projections, out, pixel_size, sod, sid,
+                                                  alpha, need_projections=need_p,
+                                                  need_distances=need_sod or need_sid)
+        return (gp if need_p else None, gsod if need_sod else None,
+                gsid if need_sid else None, None, None)
+
+
 def fdk_filter(projections, pixel_size, sod, sid, alpha=0.8):
     """Centred cosine weighting and Hann-windowed discrete ramp filter along U.
 
@@ -79,6 +107,9 @@ def fdk_filter(projections, pixel_size, sod, sid, alpha=0.8):
     sid = _per_view_distance("sid", sid, projections)
     if not projections.is_cuda:
         raise ValueError("fdk_filter requires CUDA projections (there is no CPU path)")
+    if torch.is_grad_enabled() and (projections.requires_grad or sod.requires_grad or
+                                    sid.requires_grad):
+        return _FdkFilter.apply(projections, sod, sid, pixel_size, alpha)
     return _ops.fdk_filter(projections, pixel_size, sod, sid, alpha)
 
 

@@ -513,6 +513,47 @@ int dgc_fdk_filter(const float* projections, int A, int U, int V, float pixel_si
     return fdk_launch_filter(f, s);
 }
 
+size_t dgc_fdk_filter_backward_workspace_bytes(int A, int U, int V) {
+    if (A <= 0 || U <= 0 || V <= 0) return 0;
+    return Workspace::align(sizeof(float) * (size_t)U) +
+           Workspace::align(sizeof(double) * 2 * (size_t)A * (size_t)fdk_filter_tiles(U, V));
+}
+
+int dgc_fdk_filter_backward(const float* grad_filtered, const float* projections,
+                            const float* filtered, int A, int U, int V, float pixel_size,
+                            const float* sod, const float* sid, float alpha,
+                            float* grad_projections, float* grad_sod, float* grad_sid,
+                            void* workspace, size_t workspace_bytes, void* stream) {
+    clear_error();
+    cudaStream_t s = (cudaStream_t)stream;
+    int rc = check_fdk(A, U, V, pixel_size, alpha);
+    if (rc != DGC_OK) return rc;
+    DGC_REQUIRE(grad_filtered && sod && sid, "grad_filtered, sod and sid must be non-null");
+    const bool dist = grad_sod || grad_sid;
+    DGC_REQUIRE(!dist || (projections && filtered),
+                "the distance gradients need projections and filtered");
+    if (!grad_projections && !dist) return DGC_OK;
+    const long long tiles = fdk_filter_tiles(U, V);
+    Workspace ws(workspace, workspace_bytes);
+    float* taps = ws.take<float>((size_t)U);
+    double* partials = ws.take<double>((size_t)2 * A * tiles);
+    if (!taps || !partials) {
+        set_error("workspace too small: dgc_fdk_filter_backward needs " +
+                  std::to_string(dgc_fdk_filter_backward_workspace_bytes(A, U, V)) + " bytes");
+        return DGC_ERR_WORKSPACE;
+    }
+    if ((rc = fdk_upload_taps(U, pixel_size, alpha, taps, s)) != DGC_OK) return rc;
+    FdkArgs f{projections, sod, sid, taps, nullptr, A, U, V, pixel_size};
+    f.grad_filtered = grad_filtered;
+    f.forward_out = filtered;
+    f.grad_projections = grad_projections;
+    f.partials = dist ? partials : nullptr;
+    if ((rc = fdk_launch_filter_adjoint(f, s)) != DGC_OK) return rc;
+    if (!dist) return DGC_OK;
+    return fdk_reduce_distance_grads(partials, A, tiles, sod, sid, pixel_size, grad_sod, grad_sid,
+                                     s);
+}
+
 size_t dgc_reconstruct_fdk_workspace_bytes(int A, int U, int V, int D, int H, int W) {
     if (A <= 0 || U < 2 || V < 2) return 0;
     return dgc_fdk_filter_workspace_bytes(A, U, V) +

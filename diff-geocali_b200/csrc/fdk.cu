@@ -88,9 +88,15 @@ constexpr int FBM = 128;  // output rows (U) per CTA
 constexpr int FBN = 128;  // output columns (V) per CTA
 constexpr int FBK = 16;   // reduction slice
 
+// ADJ = false: y = c H(w P) (the filter).  ADJ = true: its adjoint, z = H(g)
+// for the upstream gradient g (H is symmetric), grad P = c w z, and per CTA
+// the FP64 sums of g*y and z*P*dw/dsid for the distance gradients; c =
+// pixel*sid/sod, w = sid/dist the cosine weight, dw/dsid = (u^2+v^2)/dist^3.
+template <bool ADJ>
 __global__ void __launch_bounds__(256) fdk_filter_kernel(FdkArgs p) {
     __shared__ __align__(16) float ws[FBK][FBN];
     __shared__ float gw[FBM + FBK];
+    __shared__ double s_part[8][2];
     const int a = blockIdx.z;
     const int m0 = blockIdx.y * FBM;
     const int n0 = blockIdx.x * FBN;
@@ -99,6 +105,7 @@ __global__ void __launch_bounds__(256) fdk_filter_kernel(FdkArgs p) {
     const float sid = p.sid[a], sod = p.sod[a];
     const float sid2 = sid * sid;
     const float* __restrict__ Pa = p.projections + (long long)a * p.U * p.V;
+    const float* __restrict__ Ga = ADJ ? p.grad_filtered + (long long)a * p.U * p.V : nullptr;
     const float cu = 0.5f * (p.U - 1), cv = 0.5f * (p.V - 1);
 
     float acc[8][8];
@@ -120,9 +127,13 @@ __global__ void __launch_bounds__(256) fdk_filter_kernel(FdkArgs p) {
                 const int v = n0 + c0 + j;
                 float val = 0.0f;
                 if (k < p.U && v < p.V) {
-                    const float vv = ((float)v - cv) * p.pixel_size;
-                    const float dist = sqrtf(sid2 + uu * uu + vv * vv);
-                    val = Pa[(long long)k * p.V + v] * (sid / dist) * wk;
+                    if (ADJ) {
+                        val = Ga[(long long)k * p.V + v];
+                    } else {
+                        const float vv = ((float)v - cv) * p.pixel_size;
+                        const float dist = sqrtf(sid2 + uu * uu + vv * vv);
+                        val = Pa[(long long)k * p.V + v] * (sid / dist) * wk;
+                    }
                 }
                 vals[j] = val;
             }
@@ -152,16 +163,84 @@ __global__ void __launch_bounds__(256) fdk_filter_kernel(FdkArgs p) {
     }
     // filtering.py:104: filtered * pixel_size * (sid / sod)
     const float ratio = sid / sod;
-    float* __restrict__ Oa = p.filtered + (long long)a * p.U * p.V;
+    if (!ADJ) {
+        float* __restrict__ Oa = p.filtered + (long long)a * p.U * p.V;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int u = m0 + ty * 8 + i;
+            if (u >= p.U) continue;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int v = n0 + tx * 8 + j;
+                if (v < p.V) Oa[(long long)u * p.V + v] = (acc[i][j] * p.pixel_size) * ratio;
+            }
+        }
+        return;
+    }
+    // adjoint epilogue: acc = z = H(g) at (u, v)
+    const long long base = (long long)a * p.U * p.V;
+    double s_gy = 0.0, s_zpw = 0.0;
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
         const int u = m0 + ty * 8 + i;
         if (u >= p.U) continue;
+        const float uu = ((float)u - cu) * p.pixel_size;
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
             const int v = n0 + tx * 8 + j;
-            if (v < p.V) Oa[(long long)u * p.V + v] = (acc[i][j] * p.pixel_size) * ratio;
+            if (v >= p.V) continue;
+            const long long idx = (long long)u * p.V + v;
+            const float vv = ((float)v - cv) * p.pixel_size;
+            const float r2 = uu * uu + vv * vv;
+            const float dist = sqrtf(sid2 + r2);
+            const float z = acc[i][j];
+            if (p.grad_projections)
+                p.grad_projections[base + idx] = (z * p.pixel_size) * ratio * (sid / dist);
+            if (p.partials) {
+                s_gy += (double)Ga[idx] * (double)p.forward_out[base + idx];
+                s_zpw += (double)z * (double)Pa[idx] * ((double)r2 / ((double)dist * dist * dist));
+            }
         }
+    }
+    if (!p.partials) return;
+    // CTA sums in a fixed order: warp shuffles, then the eight warps in turn
+    s_gy = warp_sum(s_gy);
+    s_zpw = warp_sum(s_zpw);
+    const int lane = tid & 31, warp = tid >> 5;
+    if (lane == 0) {
+        s_part[warp][0] = s_gy;
+        s_part[warp][1] = s_zpw;
+    }
+    __syncthreads();
+    if (tid < 2) {
+        double t = 0.0;
+        for (int w8 = 0; w8 < 8; ++w8) t += s_part[w8][tid];
+        const long long tiles = (long long)gridDim.x * gridDim.y;
+        const long long tile = (long long)blockIdx.y * gridDim.x + blockIdx.x;
+        p.partials[((long long)a * tiles + tile) * 2 + tid] = t;
+    }
+}
+
+// dL/dsid = sum(g y)/sid + pixel*(sid/sod) * sum(H(g) P dw/dsid),
+// dL/dsod = -sum(g y)/sod, per view from the CTA partials in a fixed order.
+__global__ void fdk_distance_grads_kernel(const double* __restrict__ partials, long long tiles,
+                                          const float* __restrict__ sod,
+                                          const float* __restrict__ sid, float px,
+                                          float* __restrict__ grad_sod,
+                                          float* __restrict__ grad_sid) {
+    const int a = blockIdx.x;
+    const int lane = threadIdx.x;  // one warp
+    double gy = 0.0, zpw = 0.0;
+    for (long long t = lane; t < tiles; t += 32) {
+        gy += partials[((long long)a * tiles + t) * 2];
+        zpw += partials[((long long)a * tiles + t) * 2 + 1];
+    }
+    gy = warp_sum(gy);
+    zpw = warp_sum(zpw);
+    if (lane == 0) {
+        const double d_sid = sid[a], d_sod = sod[a];
+        if (grad_sid) grad_sid[a] = (float)(gy / d_sid + (double)px * (d_sid / d_sod) * zpw);
+        if (grad_sod) grad_sod[a] = (float)(-gy / d_sod);
     }
 }
 
@@ -219,8 +298,32 @@ int fdk_launch_filter(const FdkArgs& p, cudaStream_t s) {
         return DGC_ERR_UNSUPPORTED;
     }
     const dim3 grid(ceil_div(p.V, FBN), ceil_div(p.U, FBM), p.A);
-    fdk_filter_kernel<<<grid, 256, 0, s>>>(p);
+    fdk_filter_kernel<false><<<grid, 256, 0, s>>>(p);
     DGC_LAUNCH_CHECK("fdk_filter_kernel");
+    return DGC_OK;
+}
+
+long long fdk_filter_tiles(int U, int V) { return (long long)ceil_div(V, FBN) * ceil_div(U, FBM); }
+
+int fdk_launch_filter_adjoint(const FdkArgs& p, cudaStream_t s) {
+    DGC_TRACE("fdk_filter_adjoint_kernel", s);
+    if (p.A > 65535) {
+        set_error("fdk filter: more than 65535 views per launch");
+        return DGC_ERR_UNSUPPORTED;
+    }
+    const dim3 grid(ceil_div(p.V, FBN), ceil_div(p.U, FBM), p.A);
+    fdk_filter_kernel<true><<<grid, 256, 0, s>>>(p);
+    DGC_LAUNCH_CHECK("fdk_filter_adjoint_kernel");
+    return DGC_OK;
+}
+
+int fdk_reduce_distance_grads(const double* partials, int A, long long tiles, const float* sod,
+                              const float* sid, float pixel_size, float* grad_sod,
+                              float* grad_sid, cudaStream_t s) {
+    DGC_TRACE("fdk_distance_grads", s);
+    fdk_distance_grads_kernel<<<A, 32, 0, s>>>(partials, tiles, sod, sid, pixel_size, grad_sod,
+                                               grad_sid);
+    DGC_LAUNCH_CHECK("fdk_distance_grads");
     return DGC_OK;
 }
 

@@ -179,6 +179,25 @@ int dgc_fdk_filter_noalloc(const float* projections, int A, int U, int V, float 
                            const float* sod, const float* sid, float alpha,
                            float* filtered, void* stream);
 
+/* Scratch of dgc_fdk_filter_backward. */
+size_t dgc_fdk_filter_backward_workspace_bytes(int A, int U, int V);
+
+/* Gradients of dgc_fdk_filter, which the reference's torch implementation of
+ * fdk_filter (filtering.py:54-104) gets from autograd: for the upstream
+ * gradient grad_filtered of filtered = c H(w P) (H the symmetric Toeplitz
+ * filter along U, w = sid/dist the centred cosine weight, c = pixel*sid/sod),
+ *   grad_projections = c w H(grad_filtered)                       [A,U,V]
+ *   grad_sid[a] = sum(g y)/sid + c sum(H(g) P dw/dsid),  grad_sod[a] = -sum(g y)/sod
+ * with y = filtered (the forward's output) and dw/dsid = (u^2+v^2)/dist^3; the
+ * per-view sums in FP64, fixed order.  Any of grad_projections, grad_sod,
+ * grad_sid may be NULL (not computed); projections and filtered are read only
+ * for the distance gradients. */
+int dgc_fdk_filter_backward(const float* grad_filtered, const float* projections,
+                            const float* filtered, int A, int U, int V, float pixel_size,
+                            const float* sod, const float* sid, float alpha,
+                            float* grad_projections, float* grad_sod, float* grad_sid,
+                            void* workspace, size_t workspace_bytes, void* stream);
+
 /* Scratch of dgc_reconstruct_fdk. */
 size_t dgc_reconstruct_fdk_workspace_bytes(int A, int U, int V, int D, int H, int W);
 

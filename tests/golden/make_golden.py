@@ -11,7 +11,8 @@ It imports, unmodified and read-only, the reference's FP64 CPU oracles
   ``scalar_loss``) for the backprojector,
 * ``examples/check_forward_operator.py`` (``make_case``, ``reference_project``)
   for the forward projector,
-* ``cbct_backprojector/filtering.py``    (``fdk_filter`` on CPU float32),
+* ``cbct_backprojector/filtering.py``    (``fdk_filter`` on CPU float32, and
+  its autograd gradients),
 
 evaluates them on the reference's own test cases and on the config-1 operator
 case (16x20x24 volume, 24 views, 48x40 detector), and stores inputs, outputs
@@ -150,9 +151,43 @@ def fdk_cases(filtering):
     np.savez_compressed(HERE / "fdk_filter.npz", **d)
 
 
+def fdk_grad_cases(filtering):
+    """Autograd gradients of the reference's torch fdk_filter for the
+    projections and per-view sod / sid tensors, under a random upstream
+    gradient."""
+    gen = torch.Generator().manual_seed(11)
+    cases = [
+        dict(shape=(3, 9, 7), pixel=0.9, sod=[12.0, 12.4, 11.8], sid=[18.0, 18.7, 17.8], alpha=0.8),
+        dict(shape=(2, 40, 33), pixel=1.0, sod=[120.0, 121.0], sid=[180.0, 178.5], alpha=0.8),
+        dict(shape=(2, 17, 5), pixel=0.75, sod=[600.0, 610.0], sid=[1000.0, 990.0], alpha=1.0),
+    ]
+    d = {}
+    for i, c in enumerate(cases):
+        p = (torch.rand(c["shape"], generator=gen, dtype=torch.float32) * 3.0).requires_grad_()
+        sod = torch.tensor(c["sod"], dtype=torch.float32, requires_grad=True)
+        sid = torch.tensor(c["sid"], dtype=torch.float32, requires_grad=True)
+        g = torch.rand(c["shape"], generator=gen, dtype=torch.float32) - 0.5
+        out = filtering.fdk_filter(p, c["pixel"], sod, sid, c["alpha"])
+        gp, gsod, gsid = torch.autograd.grad(out, [p, sod, sid], grad_outputs=g)
+        d[f"c{i}_in"] = _np(p)
+        d[f"c{i}_up"] = _np(g)
+        d[f"c{i}_out"] = _np(out)
+        d[f"c{i}_pixel"] = c["pixel"]
+        d[f"c{i}_alpha"] = c["alpha"]
+        d[f"c{i}_sod"] = _np(sod)
+        d[f"c{i}_sid"] = _np(sid)
+        d[f"c{i}_grad_in"] = _np(gp)
+        d[f"c{i}_grad_sod"] = _np(gsod)
+        d[f"c{i}_grad_sid"] = _np(gsid)
+    d["n_cases"] = len(cases)
+    np.savez_compressed(HERE / "fdk_filter_grad.npz", **d)
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--only", nargs="*", default=None,
+                    help="fixture groups to write (bp_check fp_check fdk fdk_grad config1)")
     args = ap.parse_args(argv)
     sys.path.insert(0, args.reference)
     torch.set_num_threads(max(1, torch.get_num_threads()))
@@ -160,11 +195,18 @@ def main(argv=None):
     from examples import check_operator as cop
     from cbct_backprojector import filtering
 
-    bp_check_case(cop)
-    fp_check_case(fop)
-    fdk_cases(filtering)
-    proj = fp_config1(fop)
-    bp_config1(cop, proj)
+    want = set(args.only or ("bp_check", "fp_check", "fdk", "fdk_grad", "config1"))
+    if "bp_check" in want:
+        bp_check_case(cop)
+    if "fp_check" in want:
+        fp_check_case(fop)
+    if "fdk" in want:
+        fdk_cases(filtering)
+    if "fdk_grad" in want:
+        fdk_grad_cases(filtering)
+    if "config1" in want:
+        proj = fp_config1(fop)
+        bp_config1(cop, proj)
     print("golden fixtures written to", HERE)
 
 

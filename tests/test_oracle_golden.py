@@ -129,3 +129,35 @@ def test_oracle_subset_matches_full(golden, oracle, mode):
     rays = np.arange(0, full.size, 97)
     sub = oracle.project_rays(d["in_data"], geom, 1.0, 48, 40, 0.5, 1.0, rays, mode=mode)
     np.testing.assert_array_equal(sub, full.reshape(-1)[rays])
+
+
+def test_fdk_filter_gradients_of_the_reference(golden, oracle):
+    """The reference's autograd gradients of fdk_filter (golden) against the
+    FP64 oracle: the projection gradient as the transpose of the linear
+    filter (applied to every basis vector), the distance gradients by central
+    differences -- the formulas the GPU backward implements."""
+    d = golden("fdk_filter_grad.npz")
+    for i in range(int(d["n_cases"])):
+        p, up = d[f"c{i}_in"].astype(np.float64), d[f"c{i}_up"].astype(np.float64)
+        px, alpha = float(d[f"c{i}_pixel"]), float(d[f"c{i}_alpha"])
+        sod, sid = d[f"c{i}_sod"].astype(np.float64), d[f"c{i}_sid"].astype(np.float64)
+        A, U, V = p.shape
+        if A * U * V <= 600:  # transpose by basis vectors on the small cases
+            gp = np.zeros_like(p)
+            for idx in np.ndindex(*p.shape):
+                e = np.zeros_like(p)
+                e[idx] = 1.0
+                gp[idx] = float((oracle.fdk_filter(e, px, sod, sid, alpha) * up).sum())
+            assert rel_l2(d[f"c{i}_grad_in"], gp) < 1e-5, i
+        for name, vec in (("sid", sid), ("sod", sod)):
+            fd = np.zeros(A)
+            for a in range(A):
+                h = 1e-4 * vec[a]
+                hi, lo = vec.copy(), vec.copy()
+                hi[a] += h
+                lo[a] -= h
+                args = lambda v: (v, sid) if name == "sod" else (sod, v)  # noqa: E731
+                yh = oracle.fdk_filter(p, px, *args(hi), alpha)
+                yl = oracle.fdk_filter(p, px, *args(lo), alpha)
+                fd[a] = float(((yh - yl) * up).sum()) / (2 * h)
+            assert rel_l2(d[f"c{i}_grad_{name}"], fd) < 1e-4, (i, name)
