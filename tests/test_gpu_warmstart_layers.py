@@ -10,7 +10,8 @@ pytestmark = pytest.mark.gpu
 
 
 def rel(a, b):
-    return float((a.float() - b.float()).norm() / b.float().norm().clamp_min(1e-12))
+    a, b = a.detach().float(), b.detach().float()
+    return float((a - b).norm() / b.norm().clamp_min(1e-12))
 
 
 @pytest.mark.parametrize("B,H,Cin,Cout,stride", [(3, 20, 2, 32, 2), (2, 12, 32, 64, 1),
