@@ -10,7 +10,8 @@ reconstruction, which raises the entropy of its intensity distribution, so
 geometry is adjusted to make the reconstruction sharp.
 
 Each iteration: FDK-filtered projections (filtered once, with the nominal
-sid/sod) are backprojected through ``nominal + delta`` (``backproject``, whose
+sid/sod, or every iteration with the current ones: ``refilter``) are
+backprojected through ``nominal + delta`` (``backproject``, whose
 hand-written backward gives the eight per-view geometry gradients), scaled by
 pi/A, and the Shannon entropy of the normalised absolute intensities is
 minimised with Adam.  Stage 1 fits one offset per geometry family shared by
@@ -58,14 +59,18 @@ DEFAULT_STEP = {"angles": 1e-3, "sid": 1.0, "sod": 1.0, "det_u0": 0.1, "det_v0":
 def entropy_calibrate(projections, nominal, pixel_size, volume_shape, voxel_size,
                       volume_offset=(0.0, 0.0, 0.0),
                       stages=(("det_u0", "det_v0"), ("det_u0", "det_v0")), iterations=(40, 40),
-                      lr=None, alpha=0.8, true_geometry=None, points=None, log_every=0):
+                      lr=None, alpha=0.8, true_geometry=None, points=None, log_every=0,
+                      refilter=False):
     """Two-stage entropy self-calibration; returns a ``SelfCalibrationResult``.
 
     ``stages[0]`` lists the families fitted with one offset shared by all
     views, ``stages[1]`` those fitted per view (starting from stage 1's
     result); ``iterations`` gives each stage's Adam iterations.  With
     ``true_geometry`` (and optionally ``points``) the RMS reprojection error
-    [pixels] and angle error are recorded every iteration.
+    [pixels] and angle error are recorded every iteration.  ``refilter``
+    filters the projections every iteration with the current sid / sod, so
+    that the entropy's gradient reaches those distances through the filter
+    too (the whole FDK differentiated; ``fdk_filter``'s own backward).
     """
     t0 = time.perf_counter()
     step = dict(DEFAULT_STEP, **(lr or {}))
@@ -109,7 +114,9 @@ def entropy_calibrate(projections, nominal, pixel_size, volume_shape, voxel_size
                     geom.append(g + d + params[name] if shared else g + params[name])
                 else:
                     geom.append(g + d)
-            vol = backproject(filtered, *geom, pixel_size, volume_shape, voxel_size,
+            filt = (fdk_filter(projections.detach(), pixel_size, geom[2], geom[1], alpha)
+                    if refilter else filtered)
+            vol = backproject(filt, *geom, pixel_size, volume_shape, voxel_size,
                               volume_offset) * scale
             loss = image_entropy(vol)
             loss.backward()
