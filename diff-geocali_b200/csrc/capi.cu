@@ -312,7 +312,7 @@ int dgc_project_backward(const float* grad_projection, const float* volume, int 
 
 size_t dgc_project_mse_grad_workspace_bytes(int D, int H, int W, int A, int U, int V) {
     if (D <= 0 || H <= 0 || W <= 0 || A <= 0 || U <= 0 || V <= 0) return 0;
-    const size_t tiles = (size_t)fp_tiles_per_view(U, V, fp_mse_tile()) * (size_t)A;
+    const size_t tiles = (size_t)fp_tiles_per_view(U, V, fp_mse_tile(D, H, W)) * (size_t)A;
     return quad_volume_bytes(D, H, W) + Workspace::align(sizeof(double) * 8 * tiles) +
            Workspace::align(sizeof(double) * tiles);
 }
@@ -353,7 +353,7 @@ int dgc_project_mse_grad(const float* volume, int D, int H, int W, const float* 
     p.off_y = off_y;
     p.off_z = off_z;
     fp_fill_layout(p);
-    const int tile = fp_mse_tile();
+    const int tile = fp_mse_tile(D, H, W);
     const long long tiles = fp_tiles_per_view(U, V, tile);
     Workspace ws(workspace, workspace_bytes);
     float4* quads = ws.take<float4>((size_t)(D + 2) * (H + 1) * (W + 1));

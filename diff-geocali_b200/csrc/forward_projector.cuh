@@ -101,8 +101,9 @@ int fp_launch_backward(const FpArgs& p, const FpTile& tile, bool gradvol, cudaSt
 int fp_launch_counts(const FpArgs& p, int64_t* counts, cudaStream_t s);
 // Fused projection -> masked squared error -> geometry-gradient terms (8-column
 // tiles); p.partials [A][tiles][8], loss_partials [A][tiles].
-// Columns per CTA tile of the fused calibration step (8; DGC_MSE_TU=4|2 overrides).
-int fp_mse_tile();
+// Columns per CTA tile of the fused calibration step (by volume size;
+// DGC_MSE_TU=8|4|2 overrides).
+int fp_mse_tile(int D, int H, int W);
 // tile: columns per CTA (fp_mse_tile(), decided with the partials' size)
 int fp_launch_mse_grad(const FpArgs& p, int tile, const float* measured, const float* mask,
                        float scale, double* loss_partials, cudaStream_t s);
