@@ -695,7 +695,7 @@ def run_tour(args):
     """Every kernel of the library on the fdk256 instance (honouring --views /
     --volume / --detector), ``--steps`` times: project, its backward with the
     volume gradient, the fused calibration step, backproject and its backward,
-    reconstruct_fdk, a two-instance batched step and one warm-start network
+    reconstruct_fdk, the filter's backward, a two-instance batched step and one warm-start network
     forward/backward (tensor-core GEMMs).  Prints the per-kernel device times
     of the last pass; meant for profiler captures of small cases."""
     import torch
@@ -732,6 +732,10 @@ def run_tour(args):
         b = cb.backproject(pr, *g2, w["pixel"], shape, w["voxel"])
         torch.autograd.grad(b, [pr, *g2], grad_outputs=torch.ones_like(b))
         cb.reconstruct_fdk(p.detach(), *geom, w["pixel"], shape, w["voxel"], alpha=w["alpha"])
+        pf = p.detach().requires_grad_()
+        sid = geom[1].detach().requires_grad_()
+        f = cb.fdk_filter(pf, w["pixel"], geom[2], sid, w["alpha"])
+        torch.autograd.grad(f, [pf, sid], grad_outputs=torch.ones_like(f))
         batch.step()
         out = net(x)
         out.square().sum().backward()
