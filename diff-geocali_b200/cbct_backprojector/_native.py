@@ -79,6 +79,12 @@ SIGNATURES = {
                                      _P]),
     "dgc_reconstruct_fdk_partial": (_I, [_P, _I, _I, _I, *_GEOM, _F, _I, _I, _I, _F, _F, _F, _F, _F,
                                          _P, _F, _P, _P, _S, _P]),
+    "dgc_fdk_filter_ex": (_I, [_P, _I, _I, _I, _F, _P, _P, _P, _P, _P, _F, _P, _P, _S, _P]),
+    "dgc_fdk_filter_backward_ex": (_I, [_P, _P, _P, _I, _I, _I, _F, *([_P] * 5), _F,
+                                        *([_P] * 6), _P, _S, _P]),
+    "dgc_parker_weights_ex": (_I, [_P, _P, _P, _P, _I, _I, _F, _P, _P]),
+    "dgc_reconstruct_fdk_ex": (_I, [_P, _I, _I, _I, *_GEOM, _F, _I, _I, _I, _F, _F, _F, _F, _F,
+                                    _P, _P, _P, _P, _F, _I, _P, _P, _S, _P]),
     "dgc_clamp_volume": (_I, [_P, ctypes.c_longlong, _P]),
     "dgc_bp_add_tile_rule": (_I, [_I] * 6),
     "dgc_bp_clear_tile_rules": (_I, []),

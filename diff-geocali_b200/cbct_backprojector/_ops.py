@@ -293,6 +293,88 @@ def fdk_filter_backward(grad_filtered, projections, filtered, pixel_size, sod, s
     return gp, gsod, gsid
 
 
+def _frame(frame):
+    """A preweight frame (dist, u, v) as contiguous tensors (None entries kept)."""
+    frame = (None, None, None) if frame is None else tuple(frame)
+    _require(len(frame) == 3, "a preweight frame is (dist, u, v)")
+    return [None if t is None else t.contiguous() for t in frame]
+
+
+def fdk_filter_framed(projections, pixel_size, sod, sid, alpha, frame):
+    """``fdk_filter`` with the cosine preweight in a per-view frame
+    (dgc_fdk_filter_ex): ``frame = (dist, u, v)``, each a CUDA float32 [A]
+    tensor or None (sid, (U-1)/2, (V-1)/2)."""
+    A, U, V = projections.shape
+    p = projections.contiguous()
+    dev = p.device
+    frame = _frame(frame)
+    ptrs = [_p(t) for t in frame]
+    out = torch.empty_like(p)
+    lib = _native.lib()
+    with torch.cuda.device(dev):
+        ws = _workspace(lib.dgc_fdk_filter_workspace_bytes(A, U, V), dev)
+        _native.check(lib.dgc_fdk_filter_ex(
+            p.data_ptr(), A, U, V, float(pixel_size), sod.data_ptr(), sid.data_ptr(), *ptrs,
+            float(alpha), out.data_ptr(), _p(ws), 0 if ws is None else ws.numel(),
+            _stream(dev)))
+    return out
+
+
+def fdk_filter_backward_framed(grad_filtered, projections, filtered, pixel_size, sod, sid, alpha,
+                               frame, need_projections, need_sod, need_sid, need_frame):
+    """Gradients of ``fdk_filter_framed`` (dgc_fdk_filter_backward_ex):
+    ``(grad_projections, grad_sod, grad_sid, grad_dist, grad_u, grad_v)``,
+    each None when not asked for (``need_frame`` three flags)."""
+    g = grad_filtered.contiguous()
+    A, U, V = g.shape
+    dev = g.device
+    frame = _frame(frame)
+    ptrs = [_p(t) for t in frame]
+
+    def vec(need):
+        return torch.empty((A,), dtype=torch.float32, device=dev) if need else None
+
+    gp = torch.empty_like(g) if need_projections else None
+    gsod, gsid = vec(need_sod), vec(need_sid)
+    gframe = [vec(n and t is not None) for n, t in zip(need_frame, frame)]
+    dist = need_sod or need_sid or any(t is not None for t in gframe)
+    p = projections.contiguous() if dist else None
+    y = filtered.contiguous() if dist else None
+    lib = _native.lib()
+    with torch.cuda.device(dev):
+        ws = _workspace(lib.dgc_fdk_filter_backward_workspace_bytes(A, U, V), dev)
+        _native.check(lib.dgc_fdk_filter_backward_ex(
+            g.data_ptr(), _p(p), _p(y), A, U, V, float(pixel_size), sod.data_ptr(),
+            sid.data_ptr(), *ptrs, float(alpha), _p(gp), _p(gsod), _p(gsid),
+            *[_p(t) for t in gframe], _p(ws), 0 if ws is None else ws.numel(), _stream(dev)))
+    return (gp, gsod, gsid, *gframe)
+
+
+def reconstruct_fdk_ex(projections, geometry, pixel_size, volume_shape, voxel_size, volume_offset,
+                       alpha, frame, uweights, angle_scale, clamp=True):
+    """The general reconstruction (dgc_reconstruct_fdk_ex): preweight frame
+    ``frame`` (or None), per-(view, column) weights ``uweights`` (or None),
+    angular factor ``angle_scale``, optional clamp."""
+    p = projections.contiguous()
+    geom = [t.contiguous() for t in geometry]
+    w = None if uweights is None else uweights.contiguous()
+    frame = _frame(frame)
+    ptrs = [_p(t) for t in frame]
+    A, U, V = p.shape
+    D, H, W = volume_shape
+    dev = p.device
+    vol = torch.empty((D, H, W), dtype=torch.float32, device=dev)
+    lib = _native.lib()
+    with torch.cuda.device(dev):
+        ws = _workspace(lib.dgc_reconstruct_fdk_workspace_bytes(A, U, V, D, H, W), dev)
+        _native.check(lib.dgc_reconstruct_fdk_ex(
+            p.data_ptr(), A, U, V, *[g.data_ptr() for g in geom], float(pixel_size), D, H, W,
+            float(voxel_size), *map(float, volume_offset), float(alpha), *ptrs, _p(w),
+            float(angle_scale), 1 if clamp else 0, vol.data_ptr(), _p(ws),
+            0 if ws is None else ws.numel(), _stream(dev)))
+    return vol
+
+
 def reconstruct_fdk(projections, geometry, pixel_size, volume_shape, voxel_size, volume_offset,
                     alpha):
     """Filter + backproject all views, * pi/A, clamp at 0, in two kernels."""
@@ -312,16 +394,26 @@ def reconstruct_fdk(projections, geometry, pixel_size, volume_shape, voxel_size,
     return vol
 
 
-def parker_weights(angles, sid, U, pixel_size):
-    """float32 [A,U] Parker short-scan weights of the scan ``angles`` (dgc_parker_weights)."""
+def parker_weights(angles, sid, U, pixel_size, frame_dist=None, frame_u=None):
+    """float32 [A,U] Parker short-scan weights of the scan ``angles``
+    (dgc_parker_weights; dgc_parker_weights_ex with fan angles taken in a
+    preweight frame when ``frame_dist`` / ``frame_u`` are given)."""
     a = angles.contiguous()
     d = sid.contiguous()
     A = a.numel()
     out = torch.empty((A, int(U)), dtype=torch.float32, device=a.device)
+    lib = _native.lib()
     with torch.cuda.device(a.device):
-        _native.check(_native.lib().dgc_parker_weights(a.data_ptr(), d.data_ptr(), A, int(U),
-                                                       float(pixel_size), out.data_ptr(),
-                                                       _stream(a.device)))
+        if frame_dist is None and frame_u is None:
+            _native.check(lib.dgc_parker_weights(a.data_ptr(), d.data_ptr(), A, int(U),
+                                                 float(pixel_size), out.data_ptr(),
+                                                 _stream(a.device)))
+        else:
+            fd = None if frame_dist is None else frame_dist.contiguous()
+            fu = None if frame_u is None else frame_u.contiguous()
+            _native.check(lib.dgc_parker_weights_ex(a.data_ptr(), d.data_ptr(), _p(fd), _p(fu),
+                                                    A, int(U), float(pixel_size),
+                                                    out.data_ptr(), _stream(a.device)))
     return out
 
 

@@ -7,6 +7,11 @@ reference), Hann-windowed discrete Ram-Lak filter along U with the
 reference's zero padding to 2^bitlen(2U-1), ``pixel_size * sid / sod`` scale,
 backprojection, ``pi / A`` normalisation and a clamp at zero.
 
+Additions beyond the reference's signatures, off by default: Parker-weighted
+short scans (``reconstruct_fdk(short_scan=True)``) and an offset-aware cosine
+preweight (``fdk_filter(frame=...)``, ``reconstruct_fdk(offset_preweight=True)``,
+``preweight_frame``).
+
 Differences by design: the filter runs on the GPU as a Toeplitz product (the
 exact equivalent of the reference's padded FFT convolution), with a
 hand-written backward for the projections and the per-view distances (the
@@ -62,33 +67,88 @@ def _per_view_distance(name, value, projections):
     return distance.contiguous()
 
 
+def _per_view_value(name, value, projections):
+    """A finite scalar or one value per view, as a float32 [A] tensor on the projections' device."""
+    values = torch.as_tensor(value, dtype=projections.dtype, device=projections.device)
+    values = values.reshape(-1)
+    views = projections.shape[0]
+    if values.numel() == 1:
+        values = values.expand(views)
+    elif values.numel() != views:
+        raise ValueError(f"{name} must be a scalar or have one value per view")
+    if not bool(torch.isfinite(values).all()):
+        raise ValueError(f"{name} must contain finite values")
+    return values.contiguous()
+
+
+def _check_frame(frame, projections):
+    """``frame = (dist, u, v)`` with None entries as float32 [A] tensors (or None)."""
+    if frame is None:
+        return (None, None, None)
+    if not isinstance(frame, (tuple, list)) or len(frame) != 3:
+        raise TypeError("frame must be a (dist, u, v) triple")
+    dist, u, v = frame
+    return (None if dist is None else _per_view_distance("frame dist", dist, projections),
+            None if u is None else _per_view_value("frame u", u, projections),
+            None if v is None else _per_view_value("frame v", v, projections))
+
+
+def preweight_frame(angles, sid, sod, det_u0, det_v0, src_x, src_y, src_z, pixel_size):
+    """The cosine preweight's frame of each view from the scan geometry (the
+    eight per-view arrays in the operators' order; ``sod`` does not enter),
+    as differentiable torch ops: ``(dist, u, v)`` with ``dist = sid + ds_n``
+    the source's distance to the detector plane and ``(u, v) = (det_u0 +
+    ds_u / pixel_size, det_v0 + src_z / pixel_size)`` the pixel indices where
+    the perpendicular from the source meets the detector, ``ds_u`` and
+    ``ds_n`` the source offset along the detector's U axis and its normal in
+    the rotated system (the backprojector's, bp.cu:53-56).  With zero source
+    offsets and centred detectors it is the reference's centred weight
+    (filtering.py:82-85)."""
+    pixel_size = _positive_scalar("pixel_size", pixel_size)
+    c, s = torch.cos(angles), torch.sin(angles)
+    ds_u = src_x * c + src_y * s
+    ds_n = -src_x * s + src_y * c
+    return sid + ds_n, det_u0 + ds_u / pixel_size, det_v0 + src_z / pixel_size
+
+
 class _FdkFilter(torch.autograd.Function):
-    """``fdk_filter`` under autograd: gradients for the projections and the
-    per-view distances (the reference's torch filter has them from autograd,
-    filtering.py:54-104); the backward is ``dgc_fdk_filter_backward``."""
+    """``fdk_filter`` under autograd: gradients for the projections, the
+    per-view distances and the preweight frame (the reference's torch filter
+    has the first two from autograd, filtering.py:54-104); the backward is
+    ``dgc_fdk_filter_backward`` (``dgc_fdk_filter_backward_ex`` with a frame)."""
 
     @staticmethod
-    def forward(ctx, projections, sod, sid, pixel_size, alpha):
-        out = _ops.fdk_filter(projections, pixel_size, sod, sid, alpha)
-        ctx.save_for_backward(projections, sod, sid, out)
+    def forward(ctx, projections, sod, sid, dist, fu, fv, pixel_size, alpha):
+        frame = (dist, fu, fv)
+        ctx.framed = any(t is not None for t in frame)
+        if ctx.framed:
+            out = _ops.fdk_filter_framed(projections, pixel_size, sod, sid, alpha, frame)
+        else:
+            out = _ops.fdk_filter(projections, pixel_size, sod, sid, alpha)
+        ctx.save_for_backward(projections, sod, sid, out, dist, fu, fv)
         ctx.settings = (pixel_size, alpha)
         return out
 
     @staticmethod
     @once_differentiable
     def backward(ctx, grad):
-        projections, sod, sid, out = ctx.saved_tensors
+        projections, sod, sid, out, dist, fu, fv = ctx.saved_tensors
         pixel_size, alpha = ctx.settings
-        need_p, need_sod, need_sid = ctx.needs_input_grad[:3]
-        gp, gsod, gsid = _ops.fdk_filter_backward(grad, projections, out, pixel_size, sod, sid,
-                                                  alpha, need_projections=need_p,
-                                                  need_distances=need_sod or need_sid)
-        return (gp if need_p else None, gsod if need_sod else None,
-                gsid if need_sid else None, None, None)
+        need = ctx.needs_input_grad
+        if ctx.framed:
+            grads = _ops.fdk_filter_backward_framed(grad, projections, out, pixel_size, sod, sid,
+                                                    alpha, (dist, fu, fv), need[0], need[1],
+                                                    need[2], need[3:6])
+        else:
+            grads = _ops.fdk_filter_backward(grad, projections, out, pixel_size, sod, sid, alpha,
+                                             need_projections=need[0],
+                                             need_distances=need[1] or need[2])
+            grads = (*grads, None, None, None)
+        return (*(g if n else None for g, n in zip(grads, need[:6])), None, None)
 
 
-def fdk_filter(projections, pixel_size, sod, sid, alpha=0.8):
-    """Centred cosine weighting and Hann-windowed discrete ramp filter along U.
+def fdk_filter(projections, pixel_size, sod, sid, alpha=0.8, *, frame=None):
+    """Cosine weighting and Hann-windowed discrete ramp filter along U.
 
     Args:
         projections: CUDA float32 line integrals ``[A, U, V]``.
@@ -96,6 +156,14 @@ def fdk_filter(projections, pixel_size, sod, sid, alpha=0.8):
         sod: source-origin distance, scalar or one value per view.
         sid: source-detector distance, scalar or one value per view.
         alpha: Hann cutoff as a fraction of Nyquist, ``0 < alpha <= 1``.
+        frame: (an addition to the reference's signature) ``(dist, u, v)``,
+            each None, a scalar or one value per view: the cosine preweight is
+            ``dist / sqrt(dist^2 + ((i - u) px)^2 + ((j - v) px)^2)`` at pixel
+            ``(i, j)``, i.e. taken from a source at distance ``dist`` from the
+            detector plane whose perpendicular meets it at pixel ``(u, v)``
+            (``preweight_frame`` builds it from the geometry).  None entries
+            keep the reference's centred weight (sid, (U-1)/2, (V-1)/2).
+            Differentiable in each entry.
 
     Returns a contiguous float32 tensor of the same shape, scaled by
     ``pixel_size * sid / sod``.
@@ -105,11 +173,15 @@ def fdk_filter(projections, pixel_size, sod, sid, alpha=0.8):
     alpha = _check_alpha(alpha)
     sod = _per_view_distance("sod", sod, projections)
     sid = _per_view_distance("sid", sid, projections)
+    frame = _check_frame(frame, projections)
     if not projections.is_cuda:
         raise ValueError("fdk_filter requires CUDA projections (there is no CPU path)")
-    if torch.is_grad_enabled() and (projections.requires_grad or sod.requires_grad or
-                                    sid.requires_grad):
-        return _FdkFilter.apply(projections, sod, sid, pixel_size, alpha)
+    framed = any(t is not None for t in frame)
+    if torch.is_grad_enabled() and any(t is not None and t.requires_grad
+                                       for t in (projections, sod, sid, *frame)):
+        return _FdkFilter.apply(projections, sod, sid, *frame, pixel_size, alpha)
+    if framed:
+        return _ops.fdk_filter_framed(projections, pixel_size, sod, sid, alpha, frame)
     return _ops.fdk_filter(projections, pixel_size, sod, sid, alpha)
 
 
@@ -177,6 +249,7 @@ def reconstruct_fdk(
     alpha=0.8,
     angle_chunk_size=32,
     short_scan=False,
+    offset_preweight=False,
 ):
     """FDK reconstruction: filter, backproject, multiply by ``pi / A``, clamp at 0.
 
@@ -190,6 +263,12 @@ def reconstruct_fdk(
     views as a uniformly spaced short scan over ``angles[0] .. angles[-1]``
     (monotone, covering pi plus twice the largest fan angle): Parker weights
     multiply the cosine preweight and the view spacing replaces ``pi / A``.
+
+    ``offset_preweight=True`` (also an addition) takes the cosine preweight,
+    and the Parker fan angles, in each view's ``preweight_frame``: the cosine
+    of each ray's angle to the detector normal from the actual source
+    position, where the reference centres it on the detector array whatever
+    the detector and source offsets (filtering.py:1-8, 70-71).
     """
     _check_projections(projections)
     if not projections.is_cuda:
@@ -199,10 +278,19 @@ def reconstruct_fdk(
         projections, geometry, pixel_size, volume_shape, voxel_size, volume_offset, alpha,
         angle_chunk_size)
     views = projections.shape[0]
+    frame = preweight_frame(*geometry, pixel_size) if offset_preweight else None
+    U = projections.shape[1]
     if short_scan:
         a0, a1 = float(angles[0]), float(angles[-1])
         span = abs(a1 - a0)
-        fan = math.atan(((projections.shape[1] - 1) / 2 * pixel_size) / float(sid.min()))
+        if frame is None:
+            fan = math.atan(((U - 1) / 2 * pixel_size) / float(sid.min()))
+        else:
+            dist, fu = frame[0], frame[1]
+            if bool((dist <= 0).any()):
+                raise ValueError("the source must lie in front of the detector plane")
+            reach = torch.maximum(fu, (U - 1) - fu) * pixel_size
+            fan = float(torch.atan(reach / dist).max())
         if views < 2 or span < math.pi + 2 * fan - 1e-6:
             raise ValueError("a short scan must cover pi plus twice the largest fan angle "
                              f"({math.degrees(math.pi + 2 * fan):.2f} deg); got "
@@ -210,9 +298,19 @@ def reconstruct_fdk(
         steps = torch.diff(angles.double()) * (1.0 if a1 >= a0 else -1.0)
         if bool((steps <= 0).any()):
             raise ValueError("short-scan angles must be strictly monotone")
-        weights = _ops.parker_weights(angles, sid, projections.shape[1], pixel_size)
-        return _ops.reconstruct_fdk_weighted(projections, geometry, pixel_size, volume_shape,
-                                             voxel_size, offset, alpha, weights,
-                                             span / (views - 1))
+        if frame is None:
+            weights = _ops.parker_weights(angles, sid, U, pixel_size)
+            return _ops.reconstruct_fdk_weighted(projections, geometry, pixel_size, volume_shape,
+                                                 voxel_size, offset, alpha, weights,
+                                                 span / (views - 1))
+        weights = _ops.parker_weights(angles, sid, U, pixel_size, frame[0], frame[1])
+        return _ops.reconstruct_fdk_ex(projections, geometry, pixel_size, volume_shape,
+                                       voxel_size, offset, alpha, frame, weights,
+                                       span / (views - 1))
+    if frame is not None:
+        if bool((frame[0] <= 0).any()):
+            raise ValueError("the source must lie in front of the detector plane")
+        return _ops.reconstruct_fdk_ex(projections, geometry, pixel_size, volume_shape,
+                                       voxel_size, offset, alpha, frame, None, math.pi / views)
     return _ops.reconstruct_fdk(projections, geometry, pixel_size, volume_shape, voxel_size,
                                 offset, alpha)

@@ -493,9 +493,10 @@ static int check_fdk(int A, int U, int V, float pixel_size, float alpha) {
     return DGC_OK;
 }
 
-int dgc_fdk_filter(const float* projections, int A, int U, int V, float pixel_size,
-                   const float* sod, const float* sid, float alpha, float* filtered,
-                   void* workspace, size_t workspace_bytes, void* stream) {
+int dgc_fdk_filter_ex(const float* projections, int A, int U, int V, float pixel_size,
+                      const float* sod, const float* sid, const float* frame_dist,
+                      const float* frame_u, const float* frame_v, float alpha, float* filtered,
+                      void* workspace, size_t workspace_bytes, void* stream) {
     clear_error();
     cudaStream_t s = (cudaStream_t)stream;
     int rc = check_fdk(A, U, V, pixel_size, alpha);
@@ -510,33 +511,49 @@ int dgc_fdk_filter(const float* projections, int A, int U, int V, float pixel_si
     }
     if ((rc = fdk_upload_taps(U, pixel_size, alpha, taps, s)) != DGC_OK) return rc;
     FdkArgs f{projections, sod, sid, taps, filtered, A, U, V, pixel_size};
+    f.frame_dist = frame_dist;
+    f.frame_u = frame_u;
+    f.frame_v = frame_v;
     return fdk_launch_filter(f, s);
+}
+
+int dgc_fdk_filter(const float* projections, int A, int U, int V, float pixel_size,
+                   const float* sod, const float* sid, float alpha, float* filtered,
+                   void* workspace, size_t workspace_bytes, void* stream) {
+    return dgc_fdk_filter_ex(projections, A, U, V, pixel_size, sod, sid, nullptr, nullptr, nullptr,
+                             alpha, filtered, workspace, workspace_bytes, stream);
 }
 
 size_t dgc_fdk_filter_backward_workspace_bytes(int A, int U, int V) {
     if (A <= 0 || U <= 0 || V <= 0) return 0;
     return Workspace::align(sizeof(float) * (size_t)U) +
-           Workspace::align(sizeof(double) * 2 * (size_t)A * (size_t)fdk_filter_tiles(U, V));
+           Workspace::align(sizeof(double) * kFdkPartials * (size_t)A *
+                            (size_t)fdk_filter_tiles(U, V));
 }
 
-int dgc_fdk_filter_backward(const float* grad_filtered, const float* projections,
-                            const float* filtered, int A, int U, int V, float pixel_size,
-                            const float* sod, const float* sid, float alpha,
-                            float* grad_projections, float* grad_sod, float* grad_sid,
-                            void* workspace, size_t workspace_bytes, void* stream) {
+int dgc_fdk_filter_backward_ex(const float* grad_filtered, const float* projections,
+                               const float* filtered, int A, int U, int V, float pixel_size,
+                               const float* sod, const float* sid, const float* frame_dist,
+                               const float* frame_u, const float* frame_v, float alpha,
+                               float* grad_projections, float* grad_sod, float* grad_sid,
+                               float* grad_frame_dist, float* grad_frame_u, float* grad_frame_v,
+                               void* workspace, size_t workspace_bytes, void* stream) {
     clear_error();
     cudaStream_t s = (cudaStream_t)stream;
     int rc = check_fdk(A, U, V, pixel_size, alpha);
     if (rc != DGC_OK) return rc;
     DGC_REQUIRE(grad_filtered && sod && sid, "grad_filtered, sod and sid must be non-null");
-    const bool dist = grad_sod || grad_sid;
+    DGC_REQUIRE((!grad_frame_dist || frame_dist) && (!grad_frame_u || frame_u) &&
+                    (!grad_frame_v || frame_v),
+                "a frame gradient needs the frame array it belongs to");
+    const bool dist = grad_sod || grad_sid || grad_frame_dist || grad_frame_u || grad_frame_v;
     DGC_REQUIRE(!dist || (projections && filtered),
-                "the distance gradients need projections and filtered");
+                "the distance and frame gradients need projections and filtered");
     if (!grad_projections && !dist) return DGC_OK;
     const long long tiles = fdk_filter_tiles(U, V);
     Workspace ws(workspace, workspace_bytes);
     float* taps = ws.take<float>((size_t)U);
-    double* partials = ws.take<double>((size_t)2 * A * tiles);
+    double* partials = ws.take<double>((size_t)kFdkPartials * A * tiles);
     if (!taps || !partials) {
         set_error("workspace too small: dgc_fdk_filter_backward needs " +
                   std::to_string(dgc_fdk_filter_backward_workspace_bytes(A, U, V)) + " bytes");
@@ -548,10 +565,25 @@ int dgc_fdk_filter_backward(const float* grad_filtered, const float* projections
     f.forward_out = filtered;
     f.grad_projections = grad_projections;
     f.partials = dist ? partials : nullptr;
+    f.frame_dist = frame_dist;
+    f.frame_u = frame_u;
+    f.frame_v = frame_v;
+    f.frame_grads = (grad_frame_u || grad_frame_v) ? 1 : 0;
     if ((rc = fdk_launch_filter_adjoint(f, s)) != DGC_OK) return rc;
     if (!dist) return DGC_OK;
-    return fdk_reduce_distance_grads(partials, A, tiles, sod, sid, pixel_size, grad_sod, grad_sid,
-                                     s);
+    const FdkGrads g{grad_sod, grad_sid, grad_frame_dist, grad_frame_u, grad_frame_v};
+    return fdk_reduce_distance_grads(partials, A, tiles, f, g, s);
+}
+
+int dgc_fdk_filter_backward(const float* grad_filtered, const float* projections,
+                            const float* filtered, int A, int U, int V, float pixel_size,
+                            const float* sod, const float* sid, float alpha,
+                            float* grad_projections, float* grad_sod, float* grad_sid,
+                            void* workspace, size_t workspace_bytes, void* stream) {
+    return dgc_fdk_filter_backward_ex(grad_filtered, projections, filtered, A, U, V, pixel_size,
+                                      sod, sid, nullptr, nullptr, nullptr, alpha,
+                                      grad_projections, grad_sod, grad_sid, nullptr, nullptr,
+                                      nullptr, workspace, workspace_bytes, stream);
 }
 
 size_t dgc_reconstruct_fdk_workspace_bytes(int A, int U, int V, int D, int H, int W) {
@@ -566,9 +598,11 @@ static int reconstruct_fdk_impl(const float* projections, int A, int U, int V,
                                 const float* det_u0, const float* det_v0, const float* src_x,
                                 const float* src_y, const float* src_z, float pixel_size, int D,
                                 int H, int W, float voxel_size, float off_x, float off_y,
-                                float off_z, float alpha, const float* uweights,
-                                float angle_scale, bool clamp, float* volume, void* workspace,
-                                size_t workspace_bytes, void* stream) {
+                                float off_z, float alpha, const float* frame_dist,
+                                const float* frame_u, const float* frame_v,
+                                const float* uweights, float angle_scale, bool clamp,
+                                float* volume, void* workspace, size_t workspace_bytes,
+                                void* stream) {
     clear_error();
     cudaStream_t s = (cudaStream_t)stream;
     const Geometry g = make_geometry(angles, sid, sod, det_u0, det_v0, src_x, src_y, src_z);
@@ -589,6 +623,9 @@ static int reconstruct_fdk_impl(const float* projections, int A, int U, int V,
     }
     if ((rc = fdk_upload_taps(U, pixel_size, alpha, taps, s)) != DGC_OK) return rc;
     FdkArgs f{projections, sod, sid, taps, filtered, A, U, V, pixel_size, uweights};
+    f.frame_dist = frame_dist;
+    f.frame_u = frame_u;
+    f.frame_v = frame_v;
     if ((rc = fdk_launch_filter(f, s)) != DGC_OK) return rc;
     if ((rc = bp_view_table(g, A, vt, s)) != DGC_OK) return rc;
     if ((rc = build_proj_quads(filtered, A, U, V, pq, s)) != DGC_OK) return rc;
@@ -607,8 +644,9 @@ int dgc_reconstruct_fdk(const float* projections, int A, int U, int V, const flo
                         float* volume, void* workspace, size_t workspace_bytes, void* stream) {
     return reconstruct_fdk_impl(projections, A, U, V, angles, sid, sod, det_u0, det_v0, src_x,
                                 src_y, src_z, pixel_size, D, H, W, voxel_size, off_x, off_y, off_z,
-                                alpha, nullptr, (float)(M_PI / (double)A), true, volume,
-                                workspace, workspace_bytes, stream);
+                                alpha, nullptr, nullptr, nullptr, nullptr,
+                                (float)(M_PI / (double)A), true, volume, workspace,
+                                workspace_bytes, stream);
 }
 
 int dgc_reconstruct_fdk_weighted(const float* projections, int A, int U, int V,
@@ -624,8 +662,8 @@ int dgc_reconstruct_fdk_weighted(const float* projections, int A, int U, int V,
                 "angle_scale must be positive and finite");
     return reconstruct_fdk_impl(projections, A, U, V, angles, sid, sod, det_u0, det_v0, src_x,
                                 src_y, src_z, pixel_size, D, H, W, voxel_size, off_x, off_y, off_z,
-                                alpha, uweights, angle_scale, true, volume, workspace,
-                                workspace_bytes, stream);
+                                alpha, nullptr, nullptr, nullptr, uweights, angle_scale, true,
+                                volume, workspace, workspace_bytes, stream);
 }
 
 int dgc_reconstruct_fdk_partial(const float* projections, int A, int U, int V,
@@ -641,8 +679,25 @@ int dgc_reconstruct_fdk_partial(const float* projections, int A, int U, int V,
                 "angle_scale must be positive and finite");
     return reconstruct_fdk_impl(projections, A, U, V, angles, sid, sod, det_u0, det_v0, src_x,
                                 src_y, src_z, pixel_size, D, H, W, voxel_size, off_x, off_y, off_z,
-                                alpha, uweights, angle_scale, false, volume, workspace,
-                                workspace_bytes, stream);
+                                alpha, nullptr, nullptr, nullptr, uweights, angle_scale, false,
+                                volume, workspace, workspace_bytes, stream);
+}
+
+int dgc_reconstruct_fdk_ex(const float* projections, int A, int U, int V, const float* angles,
+                           const float* sid, const float* sod, const float* det_u0,
+                           const float* det_v0, const float* src_x, const float* src_y,
+                           const float* src_z, float pixel_size, int D, int H, int W,
+                           float voxel_size, float off_x, float off_y, float off_z, float alpha,
+                           const float* frame_dist, const float* frame_u, const float* frame_v,
+                           const float* uweights, float angle_scale, int clamp, float* volume,
+                           void* workspace, size_t workspace_bytes, void* stream) {
+    clear_error();
+    DGC_REQUIRE(std::isfinite(angle_scale) && angle_scale > 0.0f,
+                "angle_scale must be positive and finite");
+    return reconstruct_fdk_impl(projections, A, U, V, angles, sid, sod, det_u0, det_v0, src_x,
+                                src_y, src_z, pixel_size, D, H, W, voxel_size, off_x, off_y, off_z,
+                                alpha, frame_dist, frame_u, frame_v, uweights, angle_scale,
+                                clamp != 0, volume, workspace, workspace_bytes, stream);
 }
 
 int dgc_bp_add_tile_rule(int d_max, int a_max, int kz_forward, int kz_backward, int cta_x,
@@ -682,14 +737,21 @@ int dgc_clamp_volume(float* volume, long long n, void* stream) {
     return bp_clamp_volume(volume, n, (cudaStream_t)stream);
 }
 
-int dgc_parker_weights(const float* angles, const float* sid, int A, int U, float pixel_size,
-                       float* weights, void* stream) {
+int dgc_parker_weights_ex(const float* angles, const float* sid, const float* frame_dist,
+                          const float* frame_u, int A, int U, float pixel_size, float* weights,
+                          void* stream) {
     clear_error();
     DGC_REQUIRE(angles && sid && weights, "angles, sid and weights must be non-null");
     DGC_REQUIRE(A >= 2 && U >= 1, "a short scan needs A >= 2 views and U >= 1");
     DGC_REQUIRE((long long)A * U <= INT_MAX, "A*U exceeds the 32-bit launch limit");
     DGC_REQUIRE(std::isfinite(pixel_size) && pixel_size > 0.0f, "pixel_size must be positive");
-    return fdk_parker_weights(angles, sid, A, U, pixel_size, weights, (cudaStream_t)stream);
+    return fdk_parker_weights(angles, sid, frame_dist, frame_u, A, U, pixel_size, weights,
+                              (cudaStream_t)stream);
+}
+
+int dgc_parker_weights(const float* angles, const float* sid, int A, int U, float pixel_size,
+                       float* weights, void* stream) {
+    return dgc_parker_weights_ex(angles, sid, nullptr, nullptr, A, U, pixel_size, weights, stream);
 }
 
 // ---------------------------------------------------------- tensor-core GEMM

@@ -90,23 +90,29 @@ constexpr int FBK = 16;   // reduction slice
 
 // ADJ = false: y = c H(w P) (the filter).  ADJ = true: its adjoint, z = H(g)
 // for the upstream gradient g (H is symmetric), grad P = c w z, and per CTA
-// the FP64 sums of g*y and z*P*dw/dsid for the distance gradients; c =
-// pixel*sid/sod, w = sid/dist the cosine weight, dw/dsid = (u^2+v^2)/dist^3.
+// the FP64 sums of g*y, z*P*dw/dD and (frame_grads) z*P*u_c/dist^3,
+// z*P*v_c/dist^3 for the distance and centre gradients; c = pixel*sid/sod,
+// w = D/dist the cosine weight with D the source's distance to the detector
+// plane (sid unless a frame is given), u_c, v_c the pixel's offsets from the
+// frame centre in length units, dist^2 = D^2 + u_c^2 + v_c^2, and
+// dw/dD = (u_c^2 + v_c^2)/dist^3.
 template <bool ADJ>
 __global__ void __launch_bounds__(256) fdk_filter_kernel(FdkArgs p) {
     __shared__ __align__(16) float ws[FBK][FBN];
     __shared__ float gw[FBM + FBK];
-    __shared__ double s_part[8][2];
+    __shared__ double s_part[8][kFdkPartials];
     const int a = blockIdx.z;
     const int m0 = blockIdx.y * FBM;
     const int n0 = blockIdx.x * FBN;
     const int tid = threadIdx.x;
     const int tx = tid & 15, ty = tid >> 4;
     const float sid = p.sid[a], sod = p.sod[a];
-    const float sid2 = sid * sid;
+    const float dn = p.frame_dist ? p.frame_dist[a] : sid;  // preweight distance D
+    const float dn2 = dn * dn;
     const float* __restrict__ Pa = p.projections + (long long)a * p.U * p.V;
     const float* __restrict__ Ga = ADJ ? p.grad_filtered + (long long)a * p.U * p.V : nullptr;
-    const float cu = 0.5f * (p.U - 1), cv = 0.5f * (p.V - 1);
+    const float cu = p.frame_u ? p.frame_u[a] : 0.5f * (p.U - 1);
+    const float cv = p.frame_v ? p.frame_v[a] : 0.5f * (p.V - 1);
 
     float acc[8][8];
 #pragma unroll
@@ -131,8 +137,8 @@ __global__ void __launch_bounds__(256) fdk_filter_kernel(FdkArgs p) {
                         val = Ga[(long long)k * p.V + v];
                     } else {
                         const float vv = ((float)v - cv) * p.pixel_size;
-                        const float dist = sqrtf(sid2 + uu * uu + vv * vv);
-                        val = Pa[(long long)k * p.V + v] * (sid / dist) * wk;
+                        const float dist = sqrtf(dn2 + uu * uu + vv * vv);
+                        val = Pa[(long long)k * p.V + v] * (dn / dist) * wk;
                     }
                 }
                 vals[j] = val;
@@ -179,7 +185,7 @@ __global__ void __launch_bounds__(256) fdk_filter_kernel(FdkArgs p) {
     }
     // adjoint epilogue: acc = z = H(g) at (u, v)
     const long long base = (long long)a * p.U * p.V;
-    double s_gy = 0.0, s_zpw = 0.0;
+    double s_gy = 0.0, s_zpw = 0.0, s_zpu = 0.0, s_zpv = 0.0;
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
         const int u = m0 + ty * 8 + i;
@@ -192,13 +198,19 @@ __global__ void __launch_bounds__(256) fdk_filter_kernel(FdkArgs p) {
             const long long idx = (long long)u * p.V + v;
             const float vv = ((float)v - cv) * p.pixel_size;
             const float r2 = uu * uu + vv * vv;
-            const float dist = sqrtf(sid2 + r2);
+            const float dist = sqrtf(dn2 + r2);
             const float z = acc[i][j];
             if (p.grad_projections)
-                p.grad_projections[base + idx] = (z * p.pixel_size) * ratio * (sid / dist);
+                p.grad_projections[base + idx] = (z * p.pixel_size) * ratio * (dn / dist);
             if (p.partials) {
+                const double zp = (double)z * (double)Pa[idx];
+                const double d3 = (double)dist * dist * dist;
                 s_gy += (double)Ga[idx] * (double)p.forward_out[base + idx];
-                s_zpw += (double)z * (double)Pa[idx] * ((double)r2 / ((double)dist * dist * dist));
+                s_zpw += zp * ((double)r2 / d3);
+                if (p.frame_grads) {
+                    s_zpu += zp * ((double)uu / d3);
+                    s_zpv += zp * ((double)vv / d3);
+                }
             }
         }
     }
@@ -206,47 +218,60 @@ __global__ void __launch_bounds__(256) fdk_filter_kernel(FdkArgs p) {
     // CTA sums in a fixed order: warp shuffles, then the eight warps in turn
     s_gy = warp_sum(s_gy);
     s_zpw = warp_sum(s_zpw);
+    s_zpu = warp_sum(s_zpu);
+    s_zpv = warp_sum(s_zpv);
     const int lane = tid & 31, warp = tid >> 5;
     if (lane == 0) {
         s_part[warp][0] = s_gy;
         s_part[warp][1] = s_zpw;
+        s_part[warp][2] = s_zpu;
+        s_part[warp][3] = s_zpv;
     }
     __syncthreads();
-    if (tid < 2) {
+    if (tid < kFdkPartials) {
         double t = 0.0;
         for (int w8 = 0; w8 < 8; ++w8) t += s_part[w8][tid];
         const long long tiles = (long long)gridDim.x * gridDim.y;
         const long long tile = (long long)blockIdx.y * gridDim.x + blockIdx.x;
-        p.partials[((long long)a * tiles + tile) * 2 + tid] = t;
+        p.partials[((long long)a * tiles + tile) * kFdkPartials + tid] = t;
     }
 }
 
-// dL/dsid = sum(g y)/sid + pixel*(sid/sod) * sum(H(g) P dw/dsid),
-// dL/dsod = -sum(g y)/sod, per view from the CTA partials in a fixed order.
+// Per view, from the CTA partials in a fixed order, with c = pixel*sid/sod:
+//   dL/dsod = -sum(g y)/sod
+//   dL/dsid = sum(g y)/sid + c sum(H(g) P dw/dD)   (D = sid: no frame distance)
+//   dL/dD   = c sum(H(g) P dw/dD)                  (a frame distance D given)
+//   dL/du   = c D pixel sum(H(g) P u_c/dist^3),  dL/dv likewise,
+// u, v the frame centre (w = D/dist falls off away from it).
 __global__ void fdk_distance_grads_kernel(const double* __restrict__ partials, long long tiles,
-                                          const float* __restrict__ sod,
-                                          const float* __restrict__ sid, float px,
-                                          float* __restrict__ grad_sod,
-                                          float* __restrict__ grad_sid) {
+                                          FdkArgs p, FdkGrads g) {
     const int a = blockIdx.x;
     const int lane = threadIdx.x;  // one warp
-    double gy = 0.0, zpw = 0.0;
+    double s[kFdkPartials] = {0.0, 0.0, 0.0, 0.0};
     for (long long t = lane; t < tiles; t += 32) {
-        gy += partials[((long long)a * tiles + t) * 2];
-        zpw += partials[((long long)a * tiles + t) * 2 + 1];
+        const double* row = partials + ((long long)a * tiles + t) * kFdkPartials;
+#pragma unroll
+        for (int k = 0; k < kFdkPartials; ++k) s[k] += row[k];
     }
-    gy = warp_sum(gy);
-    zpw = warp_sum(zpw);
+#pragma unroll
+    for (int k = 0; k < kFdkPartials; ++k) s[k] = warp_sum(s[k]);
     if (lane == 0) {
-        const double d_sid = sid[a], d_sod = sod[a];
-        if (grad_sid) grad_sid[a] = (float)(gy / d_sid + (double)px * (d_sid / d_sod) * zpw);
-        if (grad_sod) grad_sod[a] = (float)(-gy / d_sod);
+        const double d_sid = p.sid[a], d_sod = p.sod[a];
+        const double c = (double)p.pixel_size * (d_sid / d_sod);
+        const double dn = p.frame_dist ? (double)p.frame_dist[a] : d_sid;
+        const double gy = s[0], zpw = s[1];
+        if (g.sid) g.sid[a] = (float)(p.frame_dist ? gy / d_sid : gy / d_sid + c * zpw);
+        if (g.sod) g.sod[a] = (float)(-gy / d_sod);
+        if (g.frame_dist) g.frame_dist[a] = (float)(c * zpw);
+        if (g.frame_u) g.frame_u[a] = (float)(c * dn * (double)p.pixel_size * s[2]);
+        if (g.frame_v) g.frame_v[a] = (float)(c * dn * (double)p.pixel_size * s[3]);
     }
 }
 
 // Parker's short-scan weights (D. L. Parker, Med. Phys. 9(2), 1982): for a
-// scan over beta in [0, pi + 2*Gamma] and the fan angle gamma = atan(u_c/sid)
-// of detector column u (u_c centred as in the cosine preweight),
+// scan over beta in [0, pi + 2*Gamma] and the fan angle gamma = atan(u_c/D)
+// of detector column u (u_c = (u - (U-1)/2) * pixel and D = sid, or the
+// preweight frame's centre and distance where one is given),
 //   w = sin^2(pi/4 * beta / (Gamma - gamma))                 beta <  2(Gamma - gamma)
 //   w = 1                                                   beta <= pi - 2 gamma
 //   w = sin^2(pi/4 * (pi + 2 Gamma - beta) / (Gamma + gamma)) beta <= pi + 2 Gamma
@@ -257,7 +282,9 @@ __global__ void fdk_distance_grads_kernel(const double* __restrict__ partials, l
 // angles[0] in the direction of the scan; for a decreasing scan gamma flips
 // sign with it.  FP64 (a table of A*U values).
 __global__ void parker_weights_kernel(const float* __restrict__ angles,
-                                      const float* __restrict__ sid, int A, int U, float px,
+                                      const float* __restrict__ sid,
+                                      const float* __restrict__ frame_dist,
+                                      const float* __restrict__ frame_u, int A, int U, float px,
                                       float* __restrict__ out) {
     const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (i >= (long long)A * U) return;
@@ -266,8 +293,10 @@ __global__ void parker_weights_kernel(const float* __restrict__ angles,
     const double dir = bl >= b0 ? 1.0 : -1.0;
     const double beta = dir * ((double)angles[a] - b0);
     const double Gam = 0.5 * (dir * (bl - b0) - M_PI);
-    const double uc = ((double)u - 0.5 * (U - 1)) * (double)px;
-    const double gam = dir * atan(uc / (double)sid[a]);
+    const double centre = frame_u ? (double)frame_u[a] : 0.5 * (U - 1);
+    const double dn = frame_dist ? (double)frame_dist[a] : (double)sid[a];
+    const double uc = ((double)u - centre) * (double)px;
+    const double gam = dir * atan(uc / dn);
     double w = 0.0;
     if (beta >= 0.0 && beta < 2.0 * (Gam - gam)) {
         const double sw = sin(0.25 * M_PI * beta / (Gam - gam));
@@ -281,12 +310,13 @@ __global__ void parker_weights_kernel(const float* __restrict__ angles,
     out[i] = (float)w;
 }
 
-int fdk_parker_weights(const float* angles, const float* sid, int A, int U, float pixel_size,
-                       float* weights, cudaStream_t s) {
+int fdk_parker_weights(const float* angles, const float* sid, const float* frame_dist,
+                       const float* frame_u, int A, int U, float pixel_size, float* weights,
+                       cudaStream_t s) {
     DGC_TRACE("parker_weights", s);
     const long long n = (long long)A * U;
-    parker_weights_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(angles, sid, A, U, pixel_size,
-                                                                       weights);
+    parker_weights_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(
+        angles, sid, frame_dist, frame_u, A, U, pixel_size, weights);
     DGC_LAUNCH_CHECK("parker_weights");
     return DGC_OK;
 }
@@ -317,12 +347,10 @@ int fdk_launch_filter_adjoint(const FdkArgs& p, cudaStream_t s) {
     return DGC_OK;
 }
 
-int fdk_reduce_distance_grads(const double* partials, int A, long long tiles, const float* sod,
-                              const float* sid, float pixel_size, float* grad_sod,
-                              float* grad_sid, cudaStream_t s) {
+int fdk_reduce_distance_grads(const double* partials, int A, long long tiles, const FdkArgs& p,
+                              const FdkGrads& g, cudaStream_t s) {
     DGC_TRACE("fdk_distance_grads", s);
-    fdk_distance_grads_kernel<<<A, 32, 0, s>>>(partials, tiles, sod, sid, pixel_size, grad_sod,
-                                               grad_sid);
+    fdk_distance_grads_kernel<<<A, 32, 0, s>>>(partials, tiles, p, g);
     DGC_LAUNCH_CHECK("fdk_distance_grads");
     return DGC_OK;
 }

@@ -22,8 +22,21 @@ struct FdkArgs {
     const float* grad_filtered;  // [A][U][V]
     const float* forward_out;    // [A][U][V]
     float* grad_projections;     // [A][U][V]
-    double* partials;            // [A][tiles][2]
+    double* partials;            // [A][tiles][kFdkPartials]
+    // Preweight frame per view, each null for the reference's centred weight:
+    // the source's distance to the detector plane (null: sid) and the pixel
+    // indices (u, v) of the foot of the perpendicular from the source (null:
+    // (U-1)/2, (V-1)/2).  The preweight is dist_n / |source - pixel|, the
+    // cosine of the ray's angle to the detector normal.
+    const float* frame_dist;     // [A]
+    const float* frame_u;        // [A]
+    const float* frame_v;        // [A]
+    int frame_grads;             // adjoint: also the sums for the frame-centre gradients
 };
+
+// FP64 sums per (view, tile) of the adjoint: g*y, H(g) P dw/ddist,
+// H(g) P u_c/|r|^3, H(g) P v_c/|r|^3 (u_c, v_c in length units).
+constexpr int kFdkPartials = 4;
 
 int fdk_taps_host(int U, double px, double alpha, std::vector<double>& out);
 int fdk_upload_taps(int U, float px, float alpha, float* dst, cudaStream_t s);
@@ -32,11 +45,22 @@ int fdk_launch_filter(const FdkArgs& p, cudaStream_t s);
 // g*y and H(g)*P*dw/dsid (partials), then dgc's distance gradients from them.
 long long fdk_filter_tiles(int U, int V);
 int fdk_launch_filter_adjoint(const FdkArgs& p, cudaStream_t s);
-int fdk_reduce_distance_grads(const double* partials, int A, long long tiles, const float* sod,
-                              const float* sid, float pixel_size, float* grad_sod,
-                              float* grad_sid, cudaStream_t s);
-// Parker short-scan weights w[a][u] of a scan over angles[0] .. angles[A-1].
-int fdk_parker_weights(const float* angles, const float* sid, int A, int U, float pixel_size,
-                       float* weights, cudaStream_t s);
+// Per-view gradients from the partials: sod, sid, and, where the frame was
+// given, its distance and centres (any output may be null).
+struct FdkGrads {
+    float* sod;
+    float* sid;
+    float* frame_dist;
+    float* frame_u;
+    float* frame_v;
+};
+int fdk_reduce_distance_grads(const double* partials, int A, long long tiles, const FdkArgs& p,
+                              const FdkGrads& g, cudaStream_t s);
+// Parker short-scan weights w[a][u] of a scan over angles[0] .. angles[A-1];
+// the fan angle of column u is atan((u - centre) * pixel / dist) with the
+// frame's centre and distance (null: (U-1)/2 and sid).
+int fdk_parker_weights(const float* angles, const float* sid, const float* frame_dist,
+                       const float* frame_u, int A, int U, float pixel_size, float* weights,
+                       cudaStream_t s);
 
 }  // namespace dgc

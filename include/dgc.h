@@ -157,6 +157,22 @@ int dgc_fdk_filter(const float* projections, int A, int U, int V, float pixel_si
                    float* filtered,
                    void* workspace, size_t workspace_bytes, void* stream);
 
+/* dgc_fdk_filter with the cosine preweight taken in a per-view frame: w =
+ * dist_n / sqrt(dist_n^2 + ((u - fu) px)^2 + ((v - fv) px)^2), the cosine of
+ * the ray's angle to the detector normal for a source at distance dist_n =
+ * frame_dist[a] from the detector plane whose perpendicular meets it at pixel
+ * (fu, fv) = (frame_u[a], frame_v[a]).  Each of frame_dist, frame_u, frame_v
+ * is a device array [A] or NULL for the reference's centred weight (sid,
+ * (U-1)/2, (V-1)/2); with all three NULL this is dgc_fdk_filter, bit for bit.
+ * frame_dist must be positive (not checked on the device).  The reference's
+ * preweight is centred whatever the detector and source offsets
+ * (filtering.py:1-8, 70-71, 82-85; README.md:115); no counterpart there.  Same
+ * workspace as dgc_fdk_filter. */
+int dgc_fdk_filter_ex(const float* projections, int A, int U, int V, float pixel_size,
+                      const float* sod, const float* sid, const float* frame_dist,
+                      const float* frame_u, const float* frame_v, float alpha, float* filtered,
+                      void* workspace, size_t workspace_bytes, void* stream);
+
 /* Maximum detector width U accepted by dgc_fdk_filter_noalloc. */
 #define DGC_FDK_NOALLOC_MAX_U 8192
 
@@ -198,6 +214,22 @@ int dgc_fdk_filter_backward(const float* grad_filtered, const float* projections
                             float* grad_projections, float* grad_sod, float* grad_sid,
                             void* workspace, size_t workspace_bytes, void* stream);
 
+/* Gradients of dgc_fdk_filter_ex: those of dgc_fdk_filter_backward (with the
+ * frame's dist_n in place of sid inside the preweight; grad_sid then holds
+ * only sum(g y)/sid, the scale's share) and, for each frame array given, its
+ * per-view gradient: grad_frame_dist = c sum(H(g) P dw/ddist_n),
+ * grad_frame_u = c dist_n px sum(H(g) P (u - fu) px / r^3) and grad_frame_v
+ * likewise, r the source-pixel distance.  A frame gradient needs its frame
+ * array; any gradient may be NULL.  Same workspace as
+ * dgc_fdk_filter_backward.  No counterpart in the reference. */
+int dgc_fdk_filter_backward_ex(const float* grad_filtered, const float* projections,
+                               const float* filtered, int A, int U, int V, float pixel_size,
+                               const float* sod, const float* sid, const float* frame_dist,
+                               const float* frame_u, const float* frame_v, float alpha,
+                               float* grad_projections, float* grad_sod, float* grad_sid,
+                               float* grad_frame_dist, float* grad_frame_u, float* grad_frame_v,
+                               void* workspace, size_t workspace_bytes, void* stream);
+
 /* Scratch of dgc_reconstruct_fdk. */
 size_t dgc_reconstruct_fdk_workspace_bytes(int A, int U, int V, int D, int H, int W);
 
@@ -220,6 +252,14 @@ int dgc_reconstruct_fdk(const float* projections, int A, int U, int V,
  * circle (README.md:115, filtering.py:1-8); no counterpart there. */
 int dgc_parker_weights(const float* angles, const float* sid, int A, int U, float pixel_size,
                        float* weights, void* stream);
+
+/* dgc_parker_weights with the fan angle of column u taken in the preweight
+ * frame of dgc_fdk_filter_ex: gamma = atan((u - frame_u[a]) px /
+ * frame_dist[a]) (either array NULL: (U-1)/2, sid).  No counterpart in the
+ * reference. */
+int dgc_parker_weights_ex(const float* angles, const float* sid, const float* frame_dist,
+                          const float* frame_u, int A, int U, float pixel_size, float* weights,
+                          void* stream);
 
 /* dgc_reconstruct_fdk with a per-(view, column) weight multiplied into the
  * cosine preweight (uweights [A][U], e.g. dgc_parker_weights; NULL for none)
@@ -250,6 +290,22 @@ int dgc_reconstruct_fdk_partial(const float* projections, int A, int U, int V,
                                 float off_x, float off_y, float off_z, float alpha,
                                 const float* uweights, float angle_scale, float* volume,
                                 void* workspace, size_t workspace_bytes, void* stream);
+
+/* The general FDK reconstruction the three above specialise: the filter in
+ * the preweight frame of dgc_fdk_filter_ex (frame_dist, frame_u, frame_v,
+ * each NULL for the centred default), the per-(view, column) weights
+ * uweights (NULL for none), the angular factor angle_scale, then the clamp at
+ * zero if clamp != 0.  Same workspace as dgc_reconstruct_fdk.  Extends
+ * filtering.py:107-198; no counterpart in the reference. */
+int dgc_reconstruct_fdk_ex(const float* projections, int A, int U, int V,
+                           const float* angles, const float* sid, const float* sod,
+                           const float* det_u0, const float* det_v0,
+                           const float* src_x, const float* src_y, const float* src_z,
+                           float pixel_size, int D, int H, int W, float voxel_size,
+                           float off_x, float off_y, float off_z, float alpha,
+                           const float* frame_dist, const float* frame_u, const float* frame_v,
+                           const float* uweights, float angle_scale, int clamp, float* volume,
+                           void* workspace, size_t workspace_bytes, void* stream);
 
 /* Backprojector tile rules (what the autotuner chose per shape bucket): a
  * call with volume depth D <= d_max and A <= a_max views uses Z blocking

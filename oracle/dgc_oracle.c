@@ -787,6 +787,9 @@ typedef struct {
     double* out;
     int A, U, V;
     double px;
+    const double* frame_dist; /* [A] or NULL: sid */
+    const double* frame_u;    /* [A] or NULL: (U-1)/2 */
+    const double* frame_v;    /* [A] or NULL: (V-1)/2 */
 } FdkJob;
 
 static void fdk_column(long av, void* vctx) {
@@ -794,12 +797,15 @@ static void fdk_column(long av, void* vctx) {
     int a = (int)(av / j->V), v = (int)(av % j->V), U = j->U;
     long V = j->V;
     double* wcol = (double*)malloc(sizeof(double) * U);
-    double vv = (v - (V - 1) / 2.0) * j->px;
     double sid = j->sid[a], sod = j->sod[a];
+    double dn = j->frame_dist ? j->frame_dist[a] : sid;
+    double cu = j->frame_u ? j->frame_u[a] : (U - 1) / 2.0;
+    double cv = j->frame_v ? j->frame_v[a] : (V - 1) / 2.0;
+    double vv = (v - cv) * j->px;
     for (int k = 0; k < U; ++k) {
-        double uu = (k - (U - 1) / 2.0) * j->px;
-        double dist = sqrt(sid * sid + uu * uu + vv * vv);
-        wcol[k] = j->proj[((long)a * U + k) * V + v] * (sid / dist);
+        double uu = (k - cu) * j->px;
+        double dist = sqrt(dn * dn + uu * uu + vv * vv);
+        wcol[k] = j->proj[((long)a * U + k) * V + v] * (dn / dist);
     }
     for (int u = 0; u < U; ++u) {
         double acc = 0.0;
@@ -811,13 +817,24 @@ static void fdk_column(long av, void* vctx) {
 
 /*
  * fdk_filter (filtering.py:54-104): out = [sum_k h[|u-k|] * p[k,v] * sid/dist(k,v)]
- * * px * sid/sod, per view; sid/sod are per-view arrays [A].
+ * * px * sid/sod, per view; sid/sod are per-view arrays [A].  The preweight
+ * frame (frame_dist, frame_u, frame_v; each NULL for the centred default of
+ * filtering.py:82-85) replaces sid and the array centre inside the cosine
+ * weight: dn / sqrt(dn^2 + ((k-fu) px)^2 + ((v-fv) px)^2), no counterpart in
+ * the reference.
  */
-void oracle_fdk_filter(const double* proj, int A, int U, int V, double px, const double* sod,
-                       const double* sid, double alpha, double* out) {
+void oracle_fdk_filter_frame(const double* proj, int A, int U, int V, double px,
+                             const double* sod, const double* sid, const double* frame_dist,
+                             const double* frame_u, const double* frame_v, double alpha,
+                             double* out) {
     double* h = (double*)malloc(sizeof(double) * U);
     oracle_fdk_taps(U, px, alpha, h);
-    FdkJob j = {proj, sod, sid, h, out, A, U, V, px};
+    FdkJob j = {proj, sod, sid, h, out, A, U, V, px, frame_dist, frame_u, frame_v};
     parallel_for((long)A * V, 4, fdk_column, &j);
     free(h);
+}
+
+void oracle_fdk_filter(const double* proj, int A, int U, int V, double px, const double* sod,
+                       const double* sid, double alpha, double* out) {
+    oracle_fdk_filter_frame(proj, A, U, V, px, sod, sid, NULL, NULL, NULL, alpha, out);
 }

@@ -59,6 +59,8 @@ def _load():
         lib.oracle_backproject_backward.argtypes = [_dp, _dp] + bp_args + [_dp, _dp]
         lib.oracle_fdk_taps.argtypes = [_c_int, _c_d, _c_d, _dp]
         lib.oracle_fdk_filter.argtypes = [_dp, _c_int, _c_int, _c_int, _c_d, _dp, _dp, _c_d, _dp]
+        lib.oracle_fdk_filter_frame.argtypes = [_dp, _c_int, _c_int, _c_int, _c_d, _dp, _dp, _dp,
+                                                _dp, _dp, _c_d, _dp]
         lib.oracle_num_threads.restype = _c_int
         lib.oracle_set_num_threads.argtypes = [_c_int]
         env = os.environ.get("DGC_ORACLE_THREADS")
@@ -193,30 +195,60 @@ def fdk_taps(U, pixel_size, alpha=0.8):
     return h
 
 
-def fdk_filter(projections, pixel_size, sod, sid, alpha=0.8):
+def fdk_filter(projections, pixel_size, sod, sid, alpha=0.8, frame=None):
+    """filtering.py:54-104 in FP64; ``frame = (dist, u, v)`` (each None, a
+    scalar or [A]) takes the cosine preweight in that frame instead of the
+    centred one (no counterpart in the reference)."""
     p = _f64(projections)
     A, U, V = p.shape
-    sod = _f64(np.broadcast_to(np.asarray(sod, np.float64).reshape(-1), (A,)))
-    sid = _f64(np.broadcast_to(np.asarray(sid, np.float64).reshape(-1), (A,)))
+
+    def per_view(x):
+        return _f64(np.broadcast_to(np.asarray(x, np.float64).reshape(-1), (A,)))
+
+    sod, sid = per_view(sod), per_view(sid)
     out = np.empty_like(p)
-    _load().oracle_fdk_filter(_ptr(p), A, U, V, float(pixel_size), _ptr(sod), _ptr(sid),
-                              float(alpha), _ptr(out))
+    if frame is None:
+        _load().oracle_fdk_filter(_ptr(p), A, U, V, float(pixel_size), _ptr(sod), _ptr(sid),
+                                  float(alpha), _ptr(out))
+        return out
+    fr = [None if x is None else per_view(x) for x in frame]
+    ptrs = [_dp() if x is None else _ptr(x) for x in fr]
+    _load().oracle_fdk_filter_frame(_ptr(p), A, U, V, float(pixel_size), _ptr(sod), _ptr(sid),
+                                    *ptrs, float(alpha), _ptr(out))
     return out
 
 
-def parker_weights(angles, sid, U, pixel_size):
+def preweight_frame(geometry, pixel_size):
+    """FP64 (dist, u, v) per view: the source's distance to the detector plane
+    and the pixel indices of the foot of its perpendicular, from the
+    projector's source and detector points (fp.cu:115-170 as restated in
+    ``dgc_oracle.c``): source O = (-sod sin b + sx, sod cos b + sy, sz),
+    detector point T(u, v) = ((u-u0) px cos b - (sod-sid) sin b,
+    (u-u0) px sin b + (sod-sid) cos b, (v-v0) px)."""
+    g = _geom(geometry)
+    b, sid, sod, u0, v0, sx, sy, sz = g
+    ds_u = sx * np.cos(b) + sy * np.sin(b)
+    ds_n = -sx * np.sin(b) + sy * np.cos(b)
+    return sid + ds_n, u0 + ds_u / pixel_size, v0 + sz / pixel_size
+
+
+def parker_weights(angles, sid, U, pixel_size, frame_dist=None, frame_u=None):
     """FP64 [A,U] short-scan weights (Parker, Med. Phys. 9(2), 1982), as
     dgc_parker_weights defines them: beta from angles[0] in the scan's
     direction, Gamma = (range - pi) / 2, gamma = atan(u_c / sid) with the
     centred u_c of filtering.py's cosine preweight, gamma's sign following the
-    scan direction."""
+    scan direction.  ``frame_dist`` / ``frame_u`` replace sid and the centre
+    (U-1)/2 in gamma (the offset-aware preweight frame)."""
     a = np.asarray(angles, np.float64)
-    d = np.broadcast_to(np.asarray(sid, np.float64), a.shape)
+    d = np.broadcast_to(np.asarray(sid if frame_dist is None else frame_dist, np.float64),
+                        a.shape)
+    centre = np.broadcast_to(np.asarray(0.5 * (U - 1) if frame_u is None else frame_u,
+                                        np.float64), a.shape)
     direction = 1.0 if a[-1] >= a[0] else -1.0
     beta = (direction * (a - a[0]))[:, None]
     gam_max = 0.5 * (direction * (a[-1] - a[0]) - np.pi)
-    uc = (np.arange(U) - 0.5 * (U - 1)) * pixel_size
-    gam = direction * np.arctan(uc[None, :] / d[:, None])
+    uc = (np.arange(U)[None, :] - centre[:, None]) * pixel_size
+    gam = direction * np.arctan(uc / d[:, None])
     w = np.zeros((a.size, U))
     with np.errstate(divide="ignore", invalid="ignore"):
         rise = np.sin(0.25 * np.pi * beta / (gam_max - gam)) ** 2
@@ -231,10 +263,12 @@ def parker_weights(angles, sid, U, pixel_size):
 
 
 def reconstruct_fdk(projections, geometry, pixel_size, volume_shape, voxel_size,
-                    offset=(0.0, 0.0, 0.0), alpha=0.8):
-    """filtering.py:107-198 in FP64: filter, backproject, * pi/A, clamp >= 0."""
+                    offset=(0.0, 0.0, 0.0), alpha=0.8, offset_preweight=False):
+    """filtering.py:107-198 in FP64: filter, backproject, * pi/A, clamp >= 0
+    (``offset_preweight``: the cosine preweight in ``preweight_frame``)."""
     g = _geom(geometry)
-    filtered = fdk_filter(projections, pixel_size, g[2], g[1], alpha)
+    frame = preweight_frame(g, pixel_size) if offset_preweight else None
+    filtered = fdk_filter(projections, pixel_size, g[2], g[1], alpha, frame)
     vol = backproject(filtered, g, pixel_size, volume_shape, voxel_size, offset)
     return np.maximum(vol * (np.pi / g.shape[1]), 0.0)
 
@@ -242,7 +276,7 @@ def reconstruct_fdk(projections, geometry, pixel_size, volume_shape, voxel_size,
 __all__ = [
     "build", "num_threads", "set_num_threads", "project", "project_rays", "sample_counts",
     "ray_traces", "project_backward", "backproject", "backproject_backward", "fdk_taps", "fdk_filter",
-    "reconstruct_fdk", "parker_weights", "usable_cpus",
+    "reconstruct_fdk", "parker_weights", "preweight_frame", "usable_cpus",
 ]
 
 

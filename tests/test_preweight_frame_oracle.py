@@ -1,0 +1,134 @@
+"""The offset-aware cosine preweight on the CPU: the FP64 oracle's frame
+restatement against the pinned centred filter (a centred frame reproduces it
+bit for bit), the frame against the projector's own source and detector points
+(the weight is the cosine of each ray's angle to the detector normal), the
+torch ``preweight_frame`` against the oracle's, Parker weights in a frame, and
+``fdk_filter``'s frame argument checks."""
+
+import math
+
+import numpy as np
+import pytest
+import torch
+
+
+def _geometry(A, U, V, seed, px):
+    rng = np.random.default_rng(seed)
+    return np.stack([
+        rng.uniform(0, 2 * np.pi, A), 300 + rng.normal(0, 3, A), 180 + rng.normal(0, 2, A),
+        (U - 1) / 2 + rng.normal(0, 2, A), (V - 1) / 2 + rng.normal(0, 2, A),
+        rng.normal(0, 1.5, A), rng.normal(0, 1.5, A), rng.normal(0, 1.5, A)])
+
+
+def test_centred_frame_is_the_pinned_filter(oracle):
+    A, U, V = 3, 21, 14
+    rng = np.random.default_rng(1)
+    p = rng.random((A, U, V))
+    sod, sid = 180 + rng.normal(0, 2, A), 300 + rng.normal(0, 3, A)
+    plain = oracle.fdk_filter(p, 0.9, sod, sid, 0.8)
+    framed = oracle.fdk_filter(p, 0.9, sod, sid, 0.8, frame=(sid, (U - 1) / 2, (V - 1) / 2))
+    assert np.array_equal(plain, framed)
+    # each entry alone falls back to its centred default
+    assert np.array_equal(plain, oracle.fdk_filter(p, 0.9, sod, sid, 0.8, (None, None, None)))
+
+
+def test_frame_weight_is_the_ray_cosine(oracle):
+    """An impulse at pixel (k, j) of view a filters to h[0] * w * px * sid/sod
+    at that pixel, so the oracle's weight w in the frame of
+    ``oracle.preweight_frame`` must be the cosine between the ray from the
+    source to the detector point of (k, j) and the detector normal, with the
+    source and detector points of the projector (fp.cu:115-170)."""
+    A, U, V, px = 6, 33, 27, 0.7
+    g = _geometry(A, U, V, 2, px)
+    rng = np.random.default_rng(3)
+    ks, js = rng.integers(0, U, A), rng.integers(0, V, A)
+    p = np.zeros((A, U, V))
+    p[np.arange(A), ks, js] = 1.0
+    out = oracle.fdk_filter(p, px, g[2], g[1], 0.8, frame=oracle.preweight_frame(g, px))
+    h0 = oracle.fdk_taps(U, px, 0.8)[0]
+    for a in range(A):
+        b, sid, sod, u0, v0, sx, sy, sz = g[:, a]
+        c, s = math.cos(b), math.sin(b)
+        src = np.array([-sod * s + sx, sod * c + sy, sz])
+        up, vp = (ks[a] - u0) * px, (js[a] - v0) * px
+        det = np.array([up * c - (sod - sid) * s, up * s + (sod - sid) * c, vp])
+        ray = det - src
+        normal = np.array([-s, c, 0.0])
+        cosine = abs(ray @ normal) / np.linalg.norm(ray)
+        w = out[a, ks[a], js[a]] / (h0 * px * sid / sod)
+        assert math.isclose(w, cosine, rel_tol=1e-12), (a, w, cosine)
+
+
+def test_frame_foot_is_perpendicular(oracle):
+    """The frame's centre is the foot of the perpendicular from the source and
+    its distance the source's distance to the detector plane; the torch
+    ``preweight_frame`` agrees with the oracle's."""
+    from cbct_backprojector.filtering import preweight_frame
+
+    A, U, V, px = 9, 40, 30, 1.3
+    g = _geometry(A, U, V, 4, px)
+    dist, fu, fv = oracle.preweight_frame(g, px)
+    for a in range(A):
+        b, sid, sod, u0, v0, sx, sy, sz = g[:, a]
+        c, s = math.cos(b), math.sin(b)
+        src = np.array([-sod * s + sx, sod * c + sy, sz])
+        up, vp = (fu[a] - u0) * px, (fv[a] - v0) * px
+        foot = np.array([up * c - (sod - sid) * s, up * s + (sod - sid) * c, vp])
+        ray = foot - src
+        normal = np.array([-s, c, 0.0])
+        assert np.linalg.norm(np.cross(ray, normal)) < 1e-9 * np.linalg.norm(ray)
+        assert math.isclose(np.linalg.norm(ray), dist[a], rel_tol=1e-12)
+    t = preweight_frame(*[torch.tensor(x) for x in g], px)
+    for mine, ref in zip(t, (dist, fu, fv)):
+        assert np.allclose(mine.numpy(), ref, rtol=0, atol=1e-10)
+    # no offsets, centred detector: the reference's centred weight
+    z = g.copy()
+    z[3], z[4], z[5:] = (U - 1) / 2, (V - 1) / 2, 0.0
+    dist0, fu0, fv0 = oracle.preweight_frame(z, px)
+    assert np.array_equal(dist0, z[1]) and np.all(fu0 == (U - 1) / 2) and np.all(fv0 == (V - 1) / 2)
+
+
+def test_parker_weights_in_a_frame(oracle):
+    A, U, px, sid = 40, 31, 1.0, 300.0
+    fan = math.atan(((U - 1) / 2 + 4) * px / (sid - 5))
+    angles = np.linspace(0.0, math.pi + 2 * fan + 0.01, A)
+    base = oracle.parker_weights(angles, np.full(A, sid), U, px)
+    same = oracle.parker_weights(angles, np.full(A, sid), U, px, np.full(A, sid),
+                                 np.full(A, (U - 1) / 2))
+    assert np.array_equal(base, same)
+    # a frame shifted by s columns is the centred table of a detector shifted the same way
+    shifted = oracle.parker_weights(angles, np.full(A, sid), U, px, np.full(A, sid - 5.0),
+                                    np.full(A, (U - 1) / 2 + 4))
+    gam = np.arctan((np.arange(U) - ((U - 1) / 2 + 4)) * px / (sid - 5.0))
+    beta = angles[:, None]
+    gmax = 0.5 * (angles[-1] - angles[0] - math.pi)
+    inner = (beta >= 2 * (gmax - gam)) & (beta <= math.pi - 2 * gam)
+    assert np.all(shifted[inner] == 1.0)
+    # every ray and its conjugate weigh 1 together (sampled where the conjugate lands inside)
+    for a in range(0, A, 5):
+        for u in range(U):
+            bc = angles[a] + math.pi + 2 * gam[u]
+            if bc > angles[-1] or not gmax > abs(gam[u]):
+                continue
+            gc = -gam[u]
+            rise = (bc < 2 * (gmax - gc))
+            w_c = (math.sin(0.25 * math.pi * bc / (gmax - gc)) ** 2 if rise else
+                   1.0 if bc <= math.pi - 2 * gc else
+                   math.sin(0.25 * math.pi * (math.pi + 2 * gmax - bc) / (gmax + gc)) ** 2)
+            assert math.isclose(shifted[a, u] + w_c, 1.0, abs_tol=1e-9)
+
+
+def test_fdk_filter_frame_argument_checks():
+    from cbct_backprojector import fdk_filter
+
+    p = torch.zeros(3, 8, 6)
+    with pytest.raises(TypeError, match="frame must be"):
+        fdk_filter(p, 1.0, 180.0, 300.0, frame=(1.0, 2.0))
+    with pytest.raises(ValueError, match="frame dist"):
+        fdk_filter(p, 1.0, 180.0, 300.0, frame=(-1.0, None, None))
+    with pytest.raises(ValueError, match="frame u"):
+        fdk_filter(p, 1.0, 180.0, 300.0, frame=(None, float("nan"), None))
+    with pytest.raises(ValueError, match="one value per view"):
+        fdk_filter(p, 1.0, 180.0, 300.0, frame=(None, None, torch.zeros(2)))
+    with pytest.raises(ValueError, match="CUDA"):
+        fdk_filter(p, 1.0, 180.0, 300.0, frame=(300.0, 3.5, 2.5))
