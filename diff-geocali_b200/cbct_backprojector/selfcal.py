@@ -33,7 +33,7 @@ from dataclasses import dataclass, field
 import torch
 
 from .calibration import GEOMETRY_NAMES, angle_error_deg, reprojection_error
-from .filtering import fdk_filter
+from .filtering import fdk_filter, preweight_frame
 from .operator import backproject
 
 
@@ -60,7 +60,7 @@ def entropy_calibrate(projections, nominal, pixel_size, volume_shape, voxel_size
                       volume_offset=(0.0, 0.0, 0.0),
                       stages=(("det_u0", "det_v0"), ("det_u0", "det_v0")), iterations=(40, 40),
                       lr=None, alpha=0.8, true_geometry=None, points=None, log_every=0,
-                      refilter=False):
+                      refilter=False, offset_preweight=False):
     """Two-stage entropy self-calibration; returns a ``SelfCalibrationResult``.
 
     ``stages[0]`` lists the families fitted with one offset shared by all
@@ -71,13 +71,21 @@ def entropy_calibrate(projections, nominal, pixel_size, volume_shape, voxel_size
     filters the projections every iteration with the current sid / sod, so
     that the entropy's gradient reaches those distances through the filter
     too (the whole FDK differentiated; ``fdk_filter``'s own backward).
+    ``offset_preweight`` takes the filter's cosine preweight in each view's
+    ``preweight_frame`` (the current geometry's with ``refilter``, so that the
+    gradient also reaches the detector centres and source offsets through the
+    weights; the nominal one otherwise).
     """
     t0 = time.perf_counter()
     step = dict(DEFAULT_STEP, **(lr or {}))
     nominal = [g.detach() for g in nominal]
     A = nominal[0].numel()
+    def frame_of(geometry):
+        return preweight_frame(*geometry, pixel_size) if offset_preweight else None
+
     with torch.no_grad():
-        filtered = fdk_filter(projections.detach(), pixel_size, nominal[2], nominal[1], alpha)
+        filtered = fdk_filter(projections.detach(), pixel_size, nominal[2], nominal[1], alpha,
+                              frame=frame_of(nominal))
     scale = math.pi / A
     delta = [torch.zeros_like(g) for g in nominal]
     result = SelfCalibrationResult(delta=delta, geometry=nominal)
@@ -114,8 +122,8 @@ def entropy_calibrate(projections, nominal, pixel_size, volume_shape, voxel_size
                     geom.append(g + d + params[name] if shared else g + params[name])
                 else:
                     geom.append(g + d)
-            filt = (fdk_filter(projections.detach(), pixel_size, geom[2], geom[1], alpha)
-                    if refilter else filtered)
+            filt = (fdk_filter(projections.detach(), pixel_size, geom[2], geom[1], alpha,
+                               frame=frame_of(geom)) if refilter else filtered)
             vol = backproject(filt, *geom, pixel_size, volume_shape, voxel_size,
                               volume_offset) * scale
             loss = image_entropy(vol)

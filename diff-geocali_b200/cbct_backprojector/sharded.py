@@ -38,7 +38,7 @@ import torch
 import torch.distributed as dist
 
 from . import _ops
-from .filtering import _fdk_arguments
+from .filtering import _fdk_arguments, preweight_frame
 from .operator import backproject
 from .source_only_forward_projector import project
 
@@ -94,11 +94,14 @@ class _SumGradAcrossRanks(torch.autograd.Function):
 
 
 def _partial_volume(projections, geometry, pixel_size, volume_shape, voxel_size, offset, alpha,
-                    angle_scale):
+                    angle_scale, frame=None):
     if not projections.is_cuda:
         raise ValueError("reconstruct_fdk_sharded requires CUDA projections")
-    return _ops.reconstruct_fdk_partial(projections, geometry, pixel_size, volume_shape,
-                                        voxel_size, offset, alpha, None, angle_scale)
+    if frame is None:
+        return _ops.reconstruct_fdk_partial(projections, geometry, pixel_size, volume_shape,
+                                            voxel_size, offset, alpha, None, angle_scale)
+    return _ops.reconstruct_fdk_ex(projections, geometry, pixel_size, volume_shape, voxel_size,
+                                   offset, alpha, frame, None, angle_scale, clamp=False)
 
 
 def _clamp(volume):
@@ -108,14 +111,16 @@ def _clamp(volume):
 @torch.no_grad()
 def reconstruct_fdk_sharded(projections, angles, sid, sod, det_u0, det_v0, src_x, src_y, src_z,
                             pixel_size, volume_shape, voxel_size, volume_offset=(0.0, 0.0, 0.0),
-                            alpha=0.8, angle_chunk_size=32, views_total=None, group=None):
+                            alpha=0.8, angle_chunk_size=32, views_total=None, group=None,
+                            offset_preweight=False):
     """``reconstruct_fdk`` of a full circular scan whose views are spread over
     the ranks of ``group``; every rank passes its own views (``[A_r, U, V]``
     projections and ``[A_r]`` geometry) and receives the whole volume.
 
     ``views_total`` (the scan's view count) is summed over the ranks when
-    omitted.  Argument checks and errors are those of ``reconstruct_fdk`` on
-    the rank's views.
+    omitted.  ``offset_preweight`` is ``reconstruct_fdk``'s (the frames are
+    per view, so each rank computes its own).  Argument checks and errors are
+    those of ``reconstruct_fdk`` on the rank's views.
     """
     geometry = (angles, sid, sod, det_u0, det_v0, src_x, src_y, src_z)
     pixel_size, volume_shape, voxel_size, offset, alpha = _fdk_arguments(
@@ -125,8 +130,13 @@ def reconstruct_fdk_sharded(projections, angles, sid, sod, det_u0, det_v0, src_x
         views_total = total_views(projections.shape[0], projections.device, group)
     if int(views_total) < projections.shape[0]:
         raise ValueError("views_total must count the views of every rank")
+    frame = None
+    if offset_preweight:
+        frame = preweight_frame(*geometry, pixel_size)
+        if bool((frame[0] <= 0).any()):
+            raise ValueError("the source must lie in front of the detector plane")
     volume = _partial_volume(projections, geometry, pixel_size, volume_shape, voxel_size, offset,
-                             alpha, math.pi / int(views_total))
+                             alpha, math.pi / int(views_total), frame)
     _all_reduce_sum(volume, group)
     return _clamp(volume)
 

@@ -49,6 +49,30 @@ def test_two_view_shards_sum_to_the_reconstruction(oracle):
     assert rel_l2(acc.cpu(), truth) < 1e-5
 
 
+def test_two_view_shards_offset_preweight():
+    """The unclamped partial reconstruction with the offset-aware preweight
+    (dgc_reconstruct_fdk_ex, clamp off) of two view shards, summed and
+    clamped, against reconstruct_fdk(offset_preweight=True)."""
+    from cbct_backprojector import _ops, reconstruct_fdk
+    from cbct_backprojector.filtering import preweight_frame
+    from cbct_backprojector.sharded import view_shard
+
+    A, U, V, shape, off = 33, 44, 38, (18, 22, 20), (0.2, 0.3, -0.1)
+    proj, geom = _scan(A, U, V, 21)
+    full = reconstruct_fdk(proj, *geom, 1.0, shape, 1.0, volume_offset=off,
+                           offset_preweight=True)
+    acc = torch.zeros(shape, dtype=torch.float32, device="cuda")
+    for r in range(2):
+        s = view_shard(A, 2, r)
+        mine = [g[s.start:s.stop] for g in geom]
+        acc += _ops.reconstruct_fdk_ex(proj[s.start:s.stop], mine, 1.0, shape, 1.0, off, 0.8,
+                                       preweight_frame(*mine, 1.0), None, math.pi / A,
+                                       clamp=False)
+    _ops.clamp_volume(acc)
+    torch.cuda.synchronize()
+    assert rel_l2(acc.cpu(), full.cpu()) < 1e-5
+
+
 def test_one_rank_is_the_single_device_operator():
     from cbct_backprojector import backproject, project, reconstruct_fdk
     from cbct_backprojector.sharded import (backproject_sharded, project_sharded,

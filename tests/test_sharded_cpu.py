@@ -58,9 +58,10 @@ def _rank(rank, world, port, out):
         res["total"] = sharded.total_views(len(mine), "cpu")
 
         # FDK: oracle filter + backprojection as the rank's partial volume
-        def partial(p, geometry, pixel, vshape, voxel, offset, a, scale):
+        def partial(p, geometry, pixel, vshape, voxel, offset, a, scale, frame=None):
             g = np.stack([t.numpy() for t in geometry])
-            f = O.fdk_filter(p.numpy(), pixel, g[2], g[1], a)
+            fr = None if frame is None else [t.numpy() for t in frame]
+            f = O.fdk_filter(p.numpy(), pixel, g[2], g[1], a, fr)
             return torch.from_numpy(O.backproject(f, g, pixel, vshape, voxel, offset) * scale)
 
         sharded._partial_volume = partial
@@ -72,6 +73,12 @@ def _rank(rank, world, port, out):
         truth = O.reconstruct_fdk(proj, geom, px, shape, vox, off, alpha)
         res["fdk_err"] = float(np.linalg.norm(vol.numpy() - truth) / np.linalg.norm(truth))
         res["fdk_negative_clamped"] = bool((vol >= 0).all())
+        # the offset-aware preweight: each rank's frames from its own views
+        vol = sharded.reconstruct_fdk_sharded(
+            torch.from_numpy(proj[mine.start:mine.stop].copy()), *local, px, shape, vox,
+            volume_offset=off, alpha=alpha, offset_preweight=True)
+        truth = O.reconstruct_fdk(proj, geom, px, shape, vox, off, alpha, offset_preweight=True)
+        res["fdk_frame_err"] = float(np.linalg.norm(vol.numpy() - truth) / np.linalg.norm(truth))
 
         # project: linear stand-in p_a = M_a vol; loss = 0.5 sum over this rank's p^2
         n = shape[0] * shape[1] * shape[2]
@@ -121,6 +128,7 @@ def test_two_gloo_ranks_sharded_views():
         res = got[r]
         assert res["total"] == 11
         assert res["fdk_err"] < 1e-6 and res["fdk_negative_clamped"], res
+        assert res["fdk_frame_err"] < 1e-6, res
         assert res["project_grad_err"] < 1e-12, res
         assert res["bp_value_err"] < 1e-12 and res["bp_grad_err"] < 1e-12, res
 
