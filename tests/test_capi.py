@@ -122,6 +122,34 @@ def test_sharding_entries_check_arguments(lib):
     assert lib.dgc_clamp_volume(None, 0, None) == 0
 
 
+def test_frame_entries_check_arguments(lib):
+    """The preweight-frame entries reject bad arguments before any CUDA call:
+    a frame gradient without its frame array, a bad alpha, a bad angular
+    factor, a short scan of one view; the backward's scratch holds four FP64
+    sums per (view, filter tile)."""
+    g = _geom_ptrs()
+    p = ctypes.c_void_p(256)
+    for k in range(3):  # grad_frame_dist / _u / _v without frame_dist / _u / _v
+        grads = [None, None, None]
+        grads[k] = p
+        frames = [p, p, p]
+        frames[k] = None
+        rc = lib.dgc_fdk_filter_backward_ex(p, p, p, 2, 8, 8, 1.0, p, p, *frames, 0.8, None, None,
+                                            None, *grads, None, 0, None)
+        assert rc == 1 and b"frame gradient" in lib.dgc_last_error(), k
+    rc = lib.dgc_fdk_filter_ex(p, 2, 8, 8, 1.0, p, p, None, None, None, 1.5, p, None, 0, None)
+    assert rc == 1 and b"alpha" in lib.dgc_last_error()
+    for scale in (0.0, float("nan")):
+        rc = lib.dgc_reconstruct_fdk_ex(None, 4, 8, 8, *g, 1.0, 4, 4, 4, 1.0, 0.0, 0.0, 0.0, 0.8,
+                                        None, None, None, None, scale, 1, None, None, 0, None)
+        assert rc == 1 and b"angle_scale" in lib.dgc_last_error()
+    assert lib.dgc_parker_weights_ex(p, p, None, None, 1, 8, 1.0, p, None) == 1
+    assert b"A >= 2" in lib.dgc_last_error()
+    A, U, V = 360, 384, 384
+    tiles = -(-V // 128) * -(-U // 128)
+    assert lib.dgc_fdk_filter_backward_workspace_bytes(A, U, V) >= 4 * 8 * A * tiles + 4 * U
+
+
 def test_header_is_c99_and_links_from_c(tmp_path):
     """include/dgc.h compiles as strict C99 and a C program links against
     libdgc.so and calls it (host-only entry points, no GPU)."""
