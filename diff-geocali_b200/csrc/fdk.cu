@@ -90,13 +90,14 @@ constexpr int FBK = 16;   // reduction slice
 
 // ADJ = false: y = c H(w P) (the filter).  ADJ = true: its adjoint, z = H(g)
 // for the upstream gradient g (H is symmetric), grad P = c w z, and per CTA
-// the FP64 sums of g*y, z*P*dw/dD and (frame_grads) z*P*u_c/dist^3,
-// z*P*v_c/dist^3 for the distance and centre gradients; c = pixel*sid/sod,
+// the FP64 sums of g*y, z*P*dw/dD and (CG, the frame centre's gradients
+// asked for) z*P*u_c/dist^3, z*P*v_c/dist^3 -- zeros without CG -- for the
+// distance and centre gradients; c = pixel*sid/sod,
 // w = D/dist the cosine weight with D the source's distance to the detector
 // plane (sid unless a frame is given), u_c, v_c the pixel's offsets from the
 // frame centre in length units, dist^2 = D^2 + u_c^2 + v_c^2, and
 // dw/dD = (u_c^2 + v_c^2)/dist^3.
-template <bool ADJ>
+template <bool ADJ, bool CG = false>
 __global__ void __launch_bounds__(256) fdk_filter_kernel(FdkArgs p) {
     __shared__ __align__(16) float ws[FBK][FBN];
     __shared__ float gw[FBM + FBK];
@@ -207,7 +208,7 @@ __global__ void __launch_bounds__(256) fdk_filter_kernel(FdkArgs p) {
                 const double d3 = (double)dist * dist * dist;
                 s_gy += (double)Ga[idx] * (double)p.forward_out[base + idx];
                 s_zpw += zp * ((double)r2 / d3);
-                if (p.frame_grads) {
+                if (CG) {
                     s_zpu += zp * ((double)uu / d3);
                     s_zpv += zp * ((double)vv / d3);
                 }
@@ -216,21 +217,27 @@ __global__ void __launch_bounds__(256) fdk_filter_kernel(FdkArgs p) {
     }
     if (!p.partials) return;
     // CTA sums in a fixed order: warp shuffles, then the eight warps in turn
+    constexpr int kSums = CG ? 4 : 2;  // sums this variant accumulates
     s_gy = warp_sum(s_gy);
     s_zpw = warp_sum(s_zpw);
-    s_zpu = warp_sum(s_zpu);
-    s_zpv = warp_sum(s_zpv);
+    if (CG) {
+        s_zpu = warp_sum(s_zpu);
+        s_zpv = warp_sum(s_zpv);
+    }
     const int lane = tid & 31, warp = tid >> 5;
     if (lane == 0) {
         s_part[warp][0] = s_gy;
         s_part[warp][1] = s_zpw;
-        s_part[warp][2] = s_zpu;
-        s_part[warp][3] = s_zpv;
+        if (CG) {
+            s_part[warp][2] = s_zpu;
+            s_part[warp][3] = s_zpv;
+        }
     }
     __syncthreads();
     if (tid < kFdkPartials) {
         double t = 0.0;
-        for (int w8 = 0; w8 < 8; ++w8) t += s_part[w8][tid];
+        if (tid < kSums)
+            for (int w8 = 0; w8 < 8; ++w8) t += s_part[w8][tid];
         const long long tiles = (long long)gridDim.x * gridDim.y;
         const long long tile = (long long)blockIdx.y * gridDim.x + blockIdx.x;
         p.partials[((long long)a * tiles + tile) * kFdkPartials + tid] = t;
@@ -342,7 +349,10 @@ int fdk_launch_filter_adjoint(const FdkArgs& p, cudaStream_t s) {
         return DGC_ERR_UNSUPPORTED;
     }
     const dim3 grid(ceil_div(p.V, FBN), ceil_div(p.U, FBM), p.A);
-    fdk_filter_kernel<true><<<grid, 256, 0, s>>>(p);
+    if (p.frame_grads)
+        fdk_filter_kernel<true, true><<<grid, 256, 0, s>>>(p);
+    else
+        fdk_filter_kernel<true, false><<<grid, 256, 0, s>>>(p);
     DGC_LAUNCH_CHECK("fdk_filter_adjoint_kernel");
     return DGC_OK;
 }

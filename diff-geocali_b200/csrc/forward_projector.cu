@@ -316,6 +316,27 @@ __device__ __forceinline__ uint32_t quad_index(const Cell& c, const FpArgs& p) {
     return c.bz + c.bx * p.zq_x + c.by * p.zq_y + p.zq_bias;
 }
 
+// The two quads (z and z+1) of cell qi.  Consecutive samples of a ray often
+// stay in one cell (about half of them at step 0.5 voxel along an axis), and
+// then read the same 32 bytes: those keep the previous sample's registers and
+// issue no load.  Bitwise the same values as loading every sample.  Used by
+// the value march only: at 256^3 / 360 x 384^2 it takes the forward from
+// 40.1 to 38.7 ms and the batched forward from 50.9 to 48.1 ms, while the
+// gradient marches, which hold more live values, slowed by 2-17 % with it.
+struct CellQuads {
+    uint32_t qi = 0xffffffffu;  // no quad index reaches 2^32 - 1
+    ulonglong2 q0 = {0ull, 0ull}, q1 = {0ull, 0ull};
+};
+
+__device__ __forceinline__ void load_cell(const ulonglong2* __restrict__ Q, uint32_t qi,
+                                          CellQuads& cq) {
+    if (qi != cq.qi) {
+        cq.q0 = __ldg(Q + qi);
+        cq.q1 = __ldg(Q + qi + 1);
+        cq.qi = qi;
+    }
+}
+
 // Sum of the trilinear samples along the ray (fp.cu:321-335).  The quads
 // hold the y-pairs of x0 and x1 as 64-bit halves, so the interpolation runs
 // as packed pairs: along x for (y0, y1) at z0 and z1, along z, then along y.
@@ -327,12 +348,12 @@ __device__ __forceinline__ float march_sum(const RaySetup& r, const ViewGeo& vg,
     float acc = 0.0f;
     float t = r.tmin;
     int n = 0;
+    CellQuads cq;
 #pragma unroll 1
     for (; t <= r.tmax && (!GUARD || n < nmax); t += p.step_size, n += GUARD ? 1 : 0) {
         const Cell c = sample_cell<CLAMP, DIV, OFF, true>(t, r, vg, p, k);
-        const uint32_t qi = quad_index(c, p);
-        const ulonglong2 q0 = __ldg(Q + qi);
-        const ulonglong2 q1 = __ldg(Q + qi + 1);
+        load_cell(Q, quad_index(c, p), cq);
+        const ulonglong2 q0 = cq.q0, q1 = cq.q1;
         const f32x2 wx = pack2(c.fx, c.fx);
         const f32x2 e0 = lerp2(q0.x, q0.y, wx);  // (y0, y1) at z0
         const f32x2 e1 = lerp2(q1.x, q1.y, wx);  // (y0, y1) at z1
