@@ -320,9 +320,10 @@ __device__ __forceinline__ uint32_t quad_index(const Cell& c, const FpArgs& p) {
 // stay in one cell (about half of them at step 0.5 voxel along an axis), and
 // then read the same 32 bytes: those keep the previous sample's registers and
 // issue no load.  Bitwise the same values as loading every sample.  Used by
-// the value march only: at 256^3 / 360 x 384^2 it takes the forward from
-// 40.1 to 38.7 ms and the batched forward from 50.9 to 48.1 ms, while the
-// gradient marches, which hold more live values, slowed by 2-17 % with it.
+// the value march only: it takes the forward at 256^3 / 360 x 384^2 from
+// 40.1 to 38.7 ms and the batched forward of that instance plus its half
+// from 50.9 to 48.1 ms, while the gradient marches, which hold more live
+// values, slowed by 2-17 % with it.
 struct CellQuads {
     uint32_t qi = 0xffffffffu;  // no quad index reaches 2^32 - 1
     ulonglong2 q0 = {0ull, 0ull}, q1 = {0ull, 0ull};
