@@ -257,7 +257,8 @@ def reconstruct_fdk(
     float32 ``[A]`` tensors on the same device (radians, pixel-index detector
     centres).  ``volume_shape`` is ``(D, H, W)``; ``volume_offset`` follows
     ``backproject``.  Uniform angular weights assume a complete, uniformly
-    sampled circular scan; the cosine preweight is centred.
+    sampled circular scan; the cosine preweight is centred unless
+    ``offset_preweight`` is set.
 
     ``short_scan=True`` (an addition to the reference's signature) treats the
     views as a uniformly spaced short scan over ``angles[0] .. angles[-1]``
@@ -278,7 +279,11 @@ def reconstruct_fdk(
         projections, geometry, pixel_size, volume_shape, voxel_size, volume_offset, alpha,
         angle_chunk_size)
     views = projections.shape[0]
-    frame = preweight_frame(*geometry, pixel_size) if offset_preweight else None
+    frame = None
+    if offset_preweight:
+        frame = preweight_frame(*geometry, pixel_size)
+        if bool((frame[0] <= 0).any()):
+            raise ValueError("the source must lie in front of the detector plane")
     U = projections.shape[1]
     if short_scan:
         a0, a1 = float(angles[0]), float(angles[-1])
@@ -286,11 +291,8 @@ def reconstruct_fdk(
         if frame is None:
             fan = math.atan(((U - 1) / 2 * pixel_size) / float(sid.min()))
         else:
-            dist, fu = frame[0], frame[1]
-            if bool((dist <= 0).any()):
-                raise ValueError("the source must lie in front of the detector plane")
-            reach = torch.maximum(fu, (U - 1) - fu) * pixel_size
-            fan = float(torch.atan(reach / dist).max())
+            reach = torch.maximum(frame[1], (U - 1) - frame[1]) * pixel_size
+            fan = float(torch.atan(reach / frame[0]).max())
         if views < 2 or span < math.pi + 2 * fan - 1e-6:
             raise ValueError("a short scan must cover pi plus twice the largest fan angle "
                              f"({math.degrees(math.pi + 2 * fan):.2f} deg); got "
@@ -308,8 +310,6 @@ def reconstruct_fdk(
                                        voxel_size, offset, alpha, frame, weights,
                                        span / (views - 1))
     if frame is not None:
-        if bool((frame[0] <= 0).any()):
-            raise ValueError("the source must lie in front of the detector plane")
         return _ops.reconstruct_fdk_ex(projections, geometry, pixel_size, volume_shape,
                                        voxel_size, offset, alpha, frame, None, math.pi / views)
     return _ops.reconstruct_fdk(projections, geometry, pixel_size, volume_shape, voxel_size,

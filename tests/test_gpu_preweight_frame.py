@@ -133,6 +133,12 @@ def test_offset_preweight_reconstruction(oracle):
     a = reconstruct_fdk(cuda32(proj), *map(cuda32, c), px, shape, 1.0, offset_preweight=True)
     b = reconstruct_fdk(cuda32(proj), *map(cuda32, c), px, shape, 1.0)
     assert torch.equal(a, b)
+    # a source offset that puts it behind the detector plane is refused
+    behind = [x.copy() for x in c]
+    behind[6][0] = -400.0  # src_y at angle 0: ds_n = -400 < -sid
+    with pytest.raises(ValueError, match="in front of the detector plane"):
+        reconstruct_fdk(cuda32(proj), *map(cuda32, behind), px, shape, 1.0,
+                        offset_preweight=True)
 
 
 def test_offset_preweight_short_scan(oracle):
