@@ -20,7 +20,6 @@ from __future__ import annotations
 
 import argparse
 import json
-import math
 import os
 import statistics
 import subprocess
@@ -276,8 +275,6 @@ def run_reference(args):
         return 0
     import numpy as np
     import torch
-
-    from cbct_backprojector.phantoms import ellipsoid_parameters  # noqa: F401
 
     w = WORKLOAD
     # the same phantom as the GPU arm, generated on the CPU

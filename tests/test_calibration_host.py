@@ -4,7 +4,6 @@ the autotuner-free parts of the warm-start module."""
 
 import math
 
-import pytest
 import torch
 
 

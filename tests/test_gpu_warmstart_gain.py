@@ -10,7 +10,6 @@ same calibration started from nominal.  Uses the committed weights
 """
 
 import pytest
-import torch
 
 pytestmark = pytest.mark.gpu
 
