@@ -15,23 +15,23 @@ struct FdkArgs {
     float* filtered;           // [A][U][V]
     int A, U, V;
     float pixel_size;
-    const float* uweight;      // [A][U] extra per-column weight (short-scan), or null
+    const float* uweight = nullptr;  // [A][U] extra per-column weight (short-scan), or null
     // adjoint (fdk_launch_filter_adjoint): upstream gradient of `filtered`, the
     // forward output, the projection gradient (or null) and FP64 per-(view,
     // tile) partial sums (or null: no distance gradients)
-    const float* grad_filtered;  // [A][U][V]
-    const float* forward_out;    // [A][U][V]
-    float* grad_projections;     // [A][U][V]
-    double* partials;            // [A][tiles][kFdkPartials]
+    const float* grad_filtered = nullptr;  // [A][U][V]
+    const float* forward_out = nullptr;    // [A][U][V]
+    float* grad_projections = nullptr;     // [A][U][V]
+    double* partials = nullptr;            // [A][tiles][kFdkPartials]
     // Preweight frame per view, each null for the reference's centred weight:
     // the source's distance to the detector plane (null: sid) and the pixel
     // indices (u, v) of the foot of the perpendicular from the source (null:
     // (U-1)/2, (V-1)/2).  The preweight is dist_n / |source - pixel|, the
     // cosine of the ray's angle to the detector normal.
-    const float* frame_dist;     // [A]
-    const float* frame_u;        // [A]
-    const float* frame_v;        // [A]
-    int frame_grads;             // adjoint: also the sums for the frame-centre gradients
+    const float* frame_dist = nullptr;  // [A]
+    const float* frame_u = nullptr;     // [A]
+    const float* frame_v = nullptr;     // [A]
+    int frame_grads = 0;  // adjoint: also the sums for the frame-centre gradients
 };
 
 // FP64 sums per (view, tile) of the adjoint: g*y, H(g) P dw/ddist,
