@@ -20,6 +20,12 @@ holds only its views' projections and geometry:
 * ``calibrate_sharded`` -- per-view geometry calibration of the rank's views
   (the offsets of different views never interact); only the loss
   normalisation and the stopping metrics are summed over the ranks.
+* ``reconstruct_fdk_slab`` -- the other split: every rank holds all views and
+  reconstructs only its slab of depth rows (``slab_shard``), a sub-volume
+  whose ``volume_offset`` puts its voxels where the whole volume's are.
+  Nothing is exchanged (``gather_slabs`` assembles the volume when a caller
+  wants it whole), each rank holds 1/N of the volume, and short scans work
+  (each rank sees the whole scan).
 
 The exchange is one volume per call (67 MB at 256^3) after all of a rank's
 compute, so it is a single collective rather than a compute kernel fused with
@@ -178,5 +184,71 @@ def calibrate_sharded(volume, measured, nominal, scan, group=None, **kwargs):
                      reduce=lambda t: _all_reduce_sum(t.contiguous().clone(), group), **kwargs)
 
 
+def slab_shard(depth, world_size, rank):
+    """The contiguous range of depth rows (z indices) of ``rank``: balanced as
+    ``view_shard``."""
+    return view_shard(depth, world_size, rank)
+
+
+def slab_offset(volume_shape, voxel_size, volume_offset, rows):
+    """``volume_offset`` of the sub-volume made of depth rows ``rows`` (a
+    range) of a ``volume_shape`` volume, so that its voxel centres are the
+    whole volume's: the centre of depth row z is ``(z - D/2) * voxel +
+    off_z`` (bp.cu:37-39), so the slab's is ``off_z + (start + d/2 - D/2) *
+    voxel`` for ``d`` rows from ``start``."""
+    D = int(volume_shape[0])
+    d = len(rows)
+    ox, oy, oz = (float(v) for v in volume_offset)
+    return (ox, oy, oz + (rows.start + d / 2 - D / 2) * float(voxel_size))
+
+
+def _world(group):
+    if dist.is_available() and dist.is_initialized():
+        return dist.get_world_size(group), dist.get_rank(group)
+    return 1, 0
+
+
+def reconstruct_fdk_slab(projections, angles, sid, sod, det_u0, det_v0, src_x, src_y, src_z,
+                         pixel_size, volume_shape, voxel_size, volume_offset=(0.0, 0.0, 0.0),
+                         alpha=0.8, angle_chunk_size=32, short_scan=False,
+                         offset_preweight=False, group=None):
+    """This rank's slab of ``reconstruct_fdk`` of the whole scan: every rank
+    passes all views and gets ``(slab, rows)``, ``slab`` the ``[len(rows), H,
+    W]`` depth rows ``rows = slab_shard(D, world, rank)`` of the volume (up to
+    the float rounding of the voxel centres).  No collective.  Without a
+    process group it is the whole volume.  Arguments as ``reconstruct_fdk``."""
+    from .filtering import reconstruct_fdk
+
+    world, rank = _world(group)
+    shape = tuple(int(n) for n in volume_shape)
+    if len(shape) != 3:
+        raise ValueError("volume_shape must contain three positive dimensions (D, H, W)")
+    rows = slab_shard(shape[0], world, rank)
+    if len(rows) == 0:
+        return projections.new_empty((0, shape[1], shape[2])), rows
+    slab = reconstruct_fdk(projections, angles, sid, sod, det_u0, det_v0, src_x, src_y, src_z,
+                           pixel_size, (len(rows), shape[1], shape[2]), voxel_size,
+                           volume_offset=slab_offset(shape, voxel_size, volume_offset, rows),
+                           alpha=alpha, angle_chunk_size=angle_chunk_size, short_scan=short_scan,
+                           offset_preweight=offset_preweight)
+    return slab, rows
+
+
+def gather_slabs(slab, depth, group=None):
+    """The whole ``[depth, H, W]`` volume on every rank from each rank's
+    ``slab_shard`` slab (one all-gather of equal-size padded slabs)."""
+    world, _ = _world(group)
+    if world == 1:
+        return slab
+    rows = [slab_shard(depth, world, r) for r in range(world)]
+    most = max(len(r) for r in rows)
+    pad = slab.new_zeros((most,) + tuple(slab.shape[1:]))
+    pad[:slab.shape[0]] = slab
+    parts = [torch.empty_like(pad) for _ in range(world)]
+    dist.all_gather(parts, pad, group=group)
+    return torch.cat([part[:len(r)] for part, r in zip(parts, rows)])
+
+
 __all__ = ["view_shard", "total_views", "reconstruct_fdk_sharded", "backproject_sharded",
-           "project_sharded", "calibrate_sharded"]
+           "project_sharded", "calibrate_sharded", "slab_shard", "slab_offset",
+           "reconstruct_fdk_slab", "gather_slabs"]

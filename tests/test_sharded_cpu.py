@@ -239,3 +239,79 @@ def test_two_gloo_ranks_sharded_calibration(monkeypatch):
             assert math.isclose(ang, e["angle_err_deg"], rel_tol=1e-9)
             assert (math.isnan(loss) and math.isnan(e["loss"])) or \
                 math.isclose(loss, e["loss"], rel_tol=1e-5)
+
+
+def _slab_rank(rank, world, port, out):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank),
+                      WORLD_SIZE=str(world), LOCAL_RANK=str(rank))
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from cbct_backprojector import filtering, sharded
+    from oracle import oracle as O
+
+    def oracle_fdk(projections, *args, volume_offset=(0.0, 0.0, 0.0), alpha=0.8,
+                   offset_preweight=False, **_):
+        geometry, (pixel, vshape, voxel) = args[:8], args[8:11]
+        g = np.stack([t.numpy() for t in geometry])
+        vol = O.reconstruct_fdk(projections.numpy(), g, pixel, vshape, voxel, volume_offset,
+                                alpha, offset_preweight)
+        return torch.from_numpy(vol).to(projections.dtype)  # float32, as the library's
+
+    filtering.reconstruct_fdk = oracle_fdk  # this rank's process only
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
+    try:
+        A, U, V, px, vox, off, alpha = 9, 12, 10, 1.0, 1.0, (0.3, -0.2, 0.45), 0.8
+        rng = np.random.default_rng(5)  # the same scan on every rank
+        proj = (rng.random((A, U, V)) * 4).astype(np.float32)
+        cols = [np.arange(A) * (2 * np.pi / A), np.full(A, 300.0), np.full(A, 180.0),
+                np.full(A, (U - 1) / 2 + 0.4), np.full(A, (V - 1) / 2 - 0.3),
+                rng.normal(0, 1, A), rng.normal(0, 1, A), rng.normal(0, 1, A)]
+        geom = [torch.from_numpy(c.astype(np.float32)) for c in cols]
+        res = {}
+        for shape in ((7, 6, 8), (1, 5, 5)):
+            slab, rows = sharded.reconstruct_fdk_slab(torch.from_numpy(proj), *geom, px, shape,
+                                                      vox, volume_offset=off, alpha=alpha,
+                                                      offset_preweight=True)
+            whole = sharded.gather_slabs(slab, shape[0])
+            g32 = np.stack([c.astype(np.float32) for c in cols])  # the ranks' geometry
+            truth = O.reconstruct_fdk(proj, g32, px, shape, vox, off, alpha, True)
+            res[shape] = ((rows.start, rows.stop), tuple(slab.shape),
+                          float(np.abs(slab.numpy() - truth[rows.start:rows.stop]).max(
+                              initial=0.0)),
+                          float(np.abs(whole.numpy() - truth).max()), float(np.abs(truth).max()))
+        out.put((rank, res))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.timeout(180)
+def test_two_gloo_ranks_slab_sharded_reconstruction():
+    """Depth-slab sharding: each rank's slab (the FP64 oracle as its
+    reconstruction, on the slab's shifted volume offset, rounded to float32
+    as the library's output is) equals the same rows of the whole volume, and
+    gathering the slabs gives the whole volume, also when a rank has no
+    rows."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_slab_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(150)
+    assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
+    got = dict(q.get(timeout=5) for _ in range(2))
+    assert got[0][(7, 6, 8)][:2] == ((0, 4), (4, 6, 8))
+    assert got[1][(7, 6, 8)][:2] == ((4, 7), (3, 6, 8))
+    assert got[1][(1, 5, 5)][:2] == ((1, 1), (0, 5, 5))
+    for r in (0, 1):
+        for shape, (_, _, slab_err, whole_err, scale) in got[r].items():
+            assert slab_err <= 1e-6 * scale and whole_err <= 1e-6 * scale, (r, shape)
+    from cbct_backprojector.sharded import slab_offset
+
+    # row z of the slab sits where row start + z of the whole volume does
+    assert slab_offset((10, 4, 4), 1.0, (0.0, 0.0, 0.5), range(3, 6)) == (0.0, 0.0, 0.0)
+    assert slab_offset((8, 4, 4), 0.5, (1.0, 2.0, 3.0), range(0, 8)) == (1.0, 2.0, 3.0)
