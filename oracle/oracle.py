@@ -218,6 +218,58 @@ def fdk_filter(projections, pixel_size, sod, sid, alpha=0.8, frame=None):
     return out
 
 
+def fdk_filter_backward(grad_filtered, projections, pixel_size, sod, sid, alpha=0.8,
+                        frame=None):
+    """FP64 gradients of ``fdk_filter`` for the upstream gradient g, restated
+    analytically: with y = c H(w P), c = px sid/sod, w = D/r, r^2 = D^2 +
+    u_c^2 + v_c^2 (D = frame dist or sid, u_c, v_c the pixel's offsets from
+    the frame centre in length units) and z = H g (H symmetric Toeplitz):
+    grad P = c w z; grad sod = -sum(g y)/sod; grad sid = sum(g y)/sid, plus
+    c sum(z P (u_c^2+v_c^2)/r^3) when D is sid; grad D = c sum(z P
+    (u_c^2+v_c^2)/r^3); grad u = c D px sum(z P u_c/r^3), grad v likewise.
+    Returns a dict of float64 arrays (``P``, ``sod``, ``sid`` and, for the
+    frame entries given, ``dist``, ``u``, ``v``)."""
+    g = _f64(grad_filtered)
+    p = _f64(projections)
+    A, U, V = p.shape
+
+    def per_view(x):
+        return np.broadcast_to(np.asarray(x, np.float64).reshape(-1), (A,)).copy()
+
+    sod, sid = per_view(sod), per_view(sid)
+    fr = (None, None, None) if frame is None else tuple(frame)
+    dist = sid if fr[0] is None else per_view(fr[0])
+    cu = np.full(A, (U - 1) / 2.0) if fr[1] is None else per_view(fr[1])
+    cv = np.full(A, (V - 1) / 2.0) if fr[2] is None else per_view(fr[2])
+    h = fdk_taps(U, pixel_size, alpha)
+    idx = np.arange(U)
+    H = h[np.abs(idx[:, None] - idx[None, :])]
+    y = fdk_filter(p, pixel_size, sod, sid, alpha, frame)
+    out = {k: np.empty(A) for k in ("sod", "sid", "dist", "u", "v")}
+    out["P"] = np.empty_like(p)
+    for a in range(A):
+        uc = (idx - cu[a]) * pixel_size
+        vc = (np.arange(V) - cv[a]) * pixel_size
+        r2 = uc[:, None] ** 2 + vc[None, :] ** 2
+        r = np.sqrt(dist[a] ** 2 + r2)
+        w = dist[a] / r
+        c = pixel_size * sid[a] / sod[a]
+        z = H @ g[a]
+        out["P"][a] = c * w * z
+        gy = float((g[a] * y[a]).sum())
+        zp = z * p[a]
+        zpw = float((zp * r2 / r ** 3).sum())
+        out["sod"][a] = -gy / sod[a]
+        out["sid"][a] = gy / sid[a] + (0.0 if fr[0] is not None else c * zpw)
+        out["dist"][a] = c * zpw
+        out["u"][a] = c * dist[a] * pixel_size * float((zp * uc[:, None] / r ** 3).sum())
+        out["v"][a] = c * dist[a] * pixel_size * float((zp * vc[None, :] / r ** 3).sum())
+    for k, x in zip(("dist", "u", "v"), fr):
+        if x is None:
+            del out[k]
+    return out
+
+
 def preweight_frame(geometry, pixel_size):
     """FP64 (dist, u, v) per view: the source's distance to the detector plane
     and the pixel indices of the foot of its perpendicular, from the
@@ -276,7 +328,7 @@ def reconstruct_fdk(projections, geometry, pixel_size, volume_shape, voxel_size,
 __all__ = [
     "build", "num_threads", "set_num_threads", "project", "project_rays", "sample_counts",
     "ray_traces", "project_backward", "backproject", "backproject_backward", "fdk_taps", "fdk_filter",
-    "reconstruct_fdk", "parker_weights", "preweight_frame", "usable_cpus",
+    "reconstruct_fdk", "parker_weights", "preweight_frame", "fdk_filter_backward", "usable_cpus",
 ]
 
 

@@ -2,8 +2,9 @@
 restatement against the pinned centred filter (a centred frame reproduces it
 bit for bit), the frame against the projector's own source and detector points
 (the weight is the cosine of each ray's angle to the detector normal), the
-torch ``preweight_frame`` against the oracle's, Parker weights in a frame, and
-``fdk_filter``'s frame argument checks."""
+torch ``preweight_frame`` against the oracle's, Parker weights in a frame,
+``fdk_filter``'s frame argument checks, and the oracle's analytic filter
+gradients (the adjoint's formulas) against its own finite differences."""
 
 import math
 
@@ -132,3 +133,40 @@ def test_fdk_filter_frame_argument_checks():
         fdk_filter(p, 1.0, 180.0, 300.0, frame=(None, None, torch.zeros(2)))
     with pytest.raises(ValueError, match="CUDA"):
         fdk_filter(p, 1.0, 180.0, 300.0, frame=(300.0, 3.5, 2.5))
+
+
+@pytest.mark.parametrize("framed", [False, True])
+def test_filter_gradient_restatement(oracle, framed):
+    """The oracle's analytic filter gradients (the formulas the CUDA adjoint
+    evaluates) against central differences of the oracle filter, per view,
+    with and without a preweight frame; the projection gradient by the
+    dot-product identity <grad_P, Q> = <g, F(Q)>."""
+    A, U, V, px, alpha = 3, 17, 11, 0.9, 0.85
+    rng = np.random.default_rng(21)
+    p = rng.random((A, U, V))
+    g = rng.standard_normal((A, U, V))
+    sod, sid = 180 + rng.normal(0, 2, A), 300 + rng.normal(0, 3, A)
+    frame = ([sid + rng.normal(0, 4, A), (U - 1) / 2 + rng.normal(0, 2, A),
+              (V - 1) / 2 + rng.normal(0, 2, A)] if framed else None)
+    grads = oracle.fdk_filter_backward(g, p, px, sod, sid, alpha, frame)
+    names = ["sod", "sid"] + (["dist", "u", "v"] if framed else [])
+    assert sorted(grads) == sorted(names + ["P"])
+    base = [sod, sid] + (list(frame) if framed else [])
+
+    def loss(vals):
+        fr = vals[2:] if framed else None
+        return float((g * oracle.fdk_filter(p, px, vals[0], vals[1], alpha, fr)).sum())
+
+    for k, name in enumerate(names):
+        h = 1e-4 * (100.0 if k < 3 else 1.0)
+        for a in range(A):
+            plus = [b.copy() for b in base]
+            minus = [b.copy() for b in base]
+            plus[k][a] += h
+            minus[k][a] -= h
+            fd = (loss(plus) - loss(minus)) / (2 * h)
+            assert math.isclose(grads[name][a], fd, rel_tol=1e-6, abs_tol=1e-9), (name, a)
+    q = rng.standard_normal((A, U, V))
+    lhs = float((grads["P"] * q).sum())
+    rhs = float((g * oracle.fdk_filter(q, px, sod, sid, alpha, frame)).sum())
+    assert math.isclose(lhs, rhs, rel_tol=1e-12)
