@@ -73,6 +73,26 @@ def test_two_view_shards_offset_preweight():
     assert rel_l2(acc.cpu(), full.cpu()) < 1e-5
 
 
+def test_depth_slabs_are_the_reconstruction():
+    """Depth-slab sharding on one device: without a process group the slab is
+    the whole volume (bit for bit), and each of three slabs, reconstructed as
+    a sub-volume at its slab_offset, is the same rows of the whole volume (up
+    to the float rounding of the voxel centres)."""
+    from cbct_backprojector import reconstruct_fdk
+    from cbct_backprojector.sharded import reconstruct_fdk_slab, slab_offset, slab_shard
+
+    A, U, V, shape, off = 30, 40, 36, (19, 20, 18), (0.3, -0.2, 0.45)
+    proj, geom = _scan(A, U, V, 17)
+    full = reconstruct_fdk(proj, *geom, 1.0, shape, 1.0, volume_offset=off)
+    whole, rows = reconstruct_fdk_slab(proj, *geom, 1.0, shape, 1.0, volume_offset=off)
+    assert rows == range(0, shape[0]) and torch.equal(whole, full)
+    for r in range(3):
+        s = slab_shard(shape[0], 3, r)
+        part = reconstruct_fdk(proj, *geom, 1.0, (len(s),) + shape[1:], 1.0,
+                               volume_offset=slab_offset(shape, 1.0, off, s))
+        assert rel_l2(part.cpu(), full[s.start:s.stop].cpu()) < 1e-5, r
+
+
 def test_one_rank_is_the_single_device_operator():
     from cbct_backprojector import backproject, project, reconstruct_fdk
     from cbct_backprojector.sharded import (backproject_sharded, project_sharded,
