@@ -170,3 +170,27 @@ def test_filter_gradient_restatement(oracle, framed):
     lhs = float((grads["P"] * q).sum())
     rhs = float((g * oracle.fdk_filter(q, px, sod, sid, alpha, frame)).sum())
     assert math.isclose(lhs, rhs, rel_tol=1e-12)
+
+
+def test_preweight_frame_gradients_reach_the_geometry():
+    """preweight_frame is torch arithmetic, so autograd carries frame
+    gradients into the geometry: d(dist)/d(sid) = 1, d(u)/d(det_u0) = 1,
+    d(u)/d(src_x) = cos(b)/px, d(dist)/d(src_x) = -sin(b), d(v)/d(src_z) = 1/px,
+    and d(u)/d(angle) = (-sx sin b + sy cos b)/px; sod does not enter."""
+    from cbct_backprojector.filtering import preweight_frame
+
+    A, px = 5, 0.8
+    g = [torch.tensor(x, requires_grad=True) for x in _geometry(A, 16, 12, 9, px)]
+    dist, u, v = preweight_frame(*g, px)
+    b, sx, sy = (t.detach() for t in (g[0], g[5], g[6]))
+    gd = torch.autograd.grad(dist.sum(), g, allow_unused=True, retain_graph=True)
+    gu = torch.autograd.grad(u.sum(), g, allow_unused=True, retain_graph=True)
+    gv = torch.autograd.grad(v.sum(), g, allow_unused=True)
+    assert torch.allclose(gd[1], torch.ones(A, dtype=torch.float64))
+    assert torch.allclose(gd[5], -torch.sin(b)) and torch.allclose(gd[6], torch.cos(b))
+    assert torch.allclose(gu[3], torch.ones(A, dtype=torch.float64))
+    assert torch.allclose(gu[5], torch.cos(b) / px) and torch.allclose(gu[6], torch.sin(b) / px)
+    assert torch.allclose(gu[0], (-sx * torch.sin(b) + sy * torch.cos(b)) / px)
+    assert torch.allclose(gv[4], torch.ones(A, dtype=torch.float64))
+    assert torch.allclose(gv[7], torch.full((A,), 1 / px, dtype=torch.float64))
+    assert gd[2] is None and gu[2] is None and gv[2] is None  # sod
