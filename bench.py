@@ -191,7 +191,7 @@ class ClockSampler:
 def make_instance(device, seed):
     import torch
 
-    from cbct_backprojector.phantoms import circular_geometry, ellipsoid_phantom
+    from dgc_b200.phantoms import circular_geometry, ellipsoid_phantom
 
     w = WORKLOAD
     vol = ellipsoid_phantom((w["D"], w["H"], w["W"]), n=w["ellipsoids"], seed=seed,
@@ -278,7 +278,7 @@ def run_reference(args):
 
     w = WORKLOAD
     # the same phantom as the GPU arm, generated on the CPU
-    from cbct_backprojector.phantoms import circular_geometry, ellipsoid_phantom
+    from dgc_b200.phantoms import circular_geometry, ellipsoid_phantom
 
     vol = ellipsoid_phantom((w["D"], w["H"], w["W"]), n=w["ellipsoids"], seed=instance_seed(0),
                             voxel_size=w["voxel"], device="cpu").numpy()
@@ -315,7 +315,7 @@ def run_ours(args):
     import numpy as np
     import torch
 
-    from cbct_backprojector import _native, _ops
+    from dgc_b200 import _native, _ops
 
     world, rank, local = dist_env()
     if not torch.cuda.is_available():
@@ -504,9 +504,9 @@ def make_batch64(device, n, seed, c=None):
     detector cover the magnified volume."""
     import numpy as np
 
-    from cbct_backprojector.batch import Problem
-    from cbct_backprojector.calibration import perturb_geometry
-    from cbct_backprojector.phantoms import circular_geometry, ellipsoid_phantom
+    from dgc_b200.batch import Problem
+    from dgc_b200.calibration import perturb_geometry
+    from dgc_b200.phantoms import circular_geometry, ellipsoid_phantom
 
     c = BATCH64 if c is None else c
     rng = np.random.default_rng(seed)
@@ -542,9 +542,9 @@ def plain_step(problems):
 def run_batch64(args):
     import torch
 
-    from cbct_backprojector import _native, _ops
-    from cbct_backprojector.autotune import Autotuner
-    from cbct_backprojector.batch import ProjectionBatch
+    from dgc_b200 import _native, _ops
+    from dgc_b200.autotune import Autotuner
+    from dgc_b200.batch import ProjectionBatch
 
     world, rank, local = dist_env()
     torch.cuda.set_device(local)
@@ -657,7 +657,7 @@ def run_calib(args):
     the nominal reprojection and the network inference."""
     import torch
 
-    from cbct_backprojector import warmstart as WS
+    from dgc_b200 import warmstart as WS
 
     torch.cuda.set_device(0)
     acq = WS.HALF if args.acq == "half" else WS.EVAL
@@ -698,9 +698,9 @@ def run_tour(args):
     import torch
 
     import cbct_backprojector as cb
-    from cbct_backprojector import _native, _ops
-    from cbct_backprojector import warmstart as WS
-    from cbct_backprojector.batch import Problem, ProjectionBatch
+    from dgc_b200 import _native, _ops
+    from dgc_b200 import warmstart as WS
+    from dgc_b200.batch import Problem, ProjectionBatch
 
     torch.cuda.set_device(0)
     device = torch.device("cuda", 0)
@@ -762,8 +762,8 @@ def run_gemm(args):
     M = 256, N = 2304, K = 360*6*6)."""
     import torch
 
-    from cbct_backprojector import _native
-    from cbct_backprojector.warmstart import gemm
+    from dgc_b200 import _native
+    from dgc_b200.warmstart import gemm
 
     torch.cuda.set_device(0)
     try:

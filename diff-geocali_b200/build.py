@@ -2,7 +2,7 @@
 
 Usage: ``python diff-geocali_b200/build.py [--force] [--jobs N]``.
 
-The library lands in ``diff-geocali_b200/cbct_backprojector/_lib/libdgc.so``,
+The library lands in ``diff-geocali_b200/dgc_b200/_lib/libdgc.so``,
 next to the Python package that loads it.  Object files go to ``_build/``.
 Every translation unit is compiled for ``sm_100a`` only.
 """
@@ -22,7 +22,7 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 INCLUDE = ROOT / "include"
 BUILD = PKG / "_build"
-LIB = PKG / "cbct_backprojector" / "_lib" / "libdgc.so"
+LIB = PKG / "dgc_b200" / "_lib" / "libdgc.so"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",

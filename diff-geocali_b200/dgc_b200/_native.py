@@ -1,7 +1,7 @@
 """ctypes binding of ``libdgc.so`` (the C ABI declared in ``include/dgc.h``).
 
 The library is built in-tree by ``diff-geocali_b200/build.py`` into
-``cbct_backprojector/_lib/libdgc.so``.  There is no fallback: if the library
+``dgc_b200/_lib/libdgc.so``.  There is no fallback: if the library
 is missing or fails to load, every operator raises ``RuntimeError``.
 """
 

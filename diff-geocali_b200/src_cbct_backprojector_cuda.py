@@ -7,7 +7,7 @@ The reference's Python wrappers import ``src_cbct_backprojector_cuda`` by name
 ``sys.path`` those calls run on libdgc's sm_100a kernels.
 """
 
-from cbct_backprojector._ops import bp_backward as backward
-from cbct_backprojector._ops import bp_forward as forward
+from dgc_b200._ops import bp_backward as backward
+from dgc_b200._ops import bp_forward as forward
 
 __all__ = ["forward", "backward"]

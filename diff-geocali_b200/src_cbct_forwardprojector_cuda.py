@@ -7,7 +7,7 @@ and call ``forward`` / ``backward`` with the signatures of
 ``sys.path`` those calls run on libdgc's sm_100a kernels.
 """
 
-from cbct_backprojector._ops import fp_backward as backward
-from cbct_backprojector._ops import fp_forward as forward
+from dgc_b200._ops import fp_backward as backward
+from dgc_b200._ops import fp_forward as forward
 
 __all__ = ["forward", "backward"]

@@ -9,8 +9,11 @@ drop-in modules can be imported in one process and compared on the same
 inputs.  Output goes only to ``oracle/_ref/`` (git-ignored; it travels to GPU
 machines with the working tree).  Nothing in the product imports this.
 
-Usage: ``python oracle/build_ref.py [--reference DIR]`` (default
-``/root/reference``).  Exits 0 with a message when the reference is absent.
+Usage: ``python oracle/build_ref.py [--reference DIR]``.  The reference's
+checkout is ``--reference``, else the environment variable
+``DGC_REFERENCE_DIR``, else this recipe's default location
+``/root/reference`` (where the development container mounts it read-only).
+Exits 0 with a message when the sources are absent.
 """
 
 import argparse
@@ -20,6 +23,7 @@ import sys
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
+DEFAULT_REFERENCE = "/root/reference"
 OUT = HERE / "_ref"
 
 MODULES = {
@@ -30,7 +34,7 @@ MODULES = {
 
 def main(argv=None):
     parser = argparse.ArgumentParser(description=__doc__.splitlines()[0])
-    parser.add_argument("--reference", default="/root/reference")
+    parser.add_argument("--reference", default=os.environ.get("DGC_REFERENCE_DIR", DEFAULT_REFERENCE))
     args = parser.parse_args(argv)
     ref = Path(args.reference)
     if not all((ref / src).is_file() for src in MODULES.values()):

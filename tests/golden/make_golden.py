@@ -1,9 +1,12 @@
 """Generate the golden fixtures in ``tests/golden/`` from the reference's own CPU code.
 
 Run in a container where the reference project (TomSHINING/diff-geoCali) is
-checked out (default ``/root/reference``)::
+checked out::
 
     python tests/golden/make_golden.py [--reference DIR]
+
+The checkout is ``--reference``, else ``DGC_REFERENCE_DIR``, else this
+script's default location ``/root/reference``.
 
 It imports, unmodified and read-only, the reference's FP64 CPU oracles
 
@@ -22,6 +25,7 @@ time and nothing imports it.
 """
 
 import argparse
+import os
 import math
 import sys
 import time
@@ -185,7 +189,7 @@ def fdk_grad_cases(filtering):
 
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("DGC_REFERENCE_DIR", "/root/reference"))
     ap.add_argument("--only", nargs="*", default=None,
                     help="fixture groups to write (bp_check fp_check fdk fdk_grad config1)")
     args = ap.parse_args(argv)

@@ -11,7 +11,7 @@ import pytest
 
 
 def _instances(specs, grad_volume=True):
-    from cbct_backprojector import _native
+    from dgc_b200 import _native
 
     arr = (_native.FpInstance * len(specs))()
     for inst, (D, H, W, A, U, V, tb) in zip(arr, specs):
@@ -33,7 +33,7 @@ def _align(n):
 def test_workspace_bytes_follow_the_layout(scatter, monkeypatch):
     """Volume-gradient buffers: 16-byte level records over (D+2)(H+1)(W+1)
     cells by default, the padded volume with DGC_SCATTER=pairs."""
-    from cbct_backprojector import _native
+    from dgc_b200 import _native
 
     if scatter:
         monkeypatch.setenv("DGC_SCATTER", scatter)
@@ -62,7 +62,7 @@ def test_workspace_bytes_follow_the_layout(scatter, monkeypatch):
 
 
 def test_prepare_rejects_bad_instances():
-    from cbct_backprojector import _native
+    from dgc_b200 import _native
 
     lib = _native.lib()
     plan = _native.BatchPlan()
@@ -93,7 +93,7 @@ def _problem(shape, A, U, V, voxel=1.0):
 
 
 def test_buckets():
-    from cbct_backprojector.autotune import bucket
+    from dgc_b200.autotune import bucket
 
     a = bucket(_problem((256, 256, 256), 360, 384, 384))
     assert a == "vol2^24-U384-V384-mul"
@@ -103,7 +103,7 @@ def test_buckets():
 
 
 def test_autotuner_picks_fastest_and_caches(tmp_path):
-    from cbct_backprojector.autotune import Autotuner
+    from dgc_b200.autotune import Autotuner
 
     calls = []
 
@@ -125,7 +125,7 @@ def test_autotuner_picks_fastest_and_caches(tmp_path):
 
 @pytest.fixture
 def clean_bp_rules(monkeypatch):
-    from cbct_backprojector import _native
+    from dgc_b200 import _native
 
     monkeypatch.delenv("DGC_BP_KZ", raising=False)
     monkeypatch.delenv("DGC_BP_CTA", raising=False)
@@ -138,8 +138,8 @@ def clean_bp_rules(monkeypatch):
 def test_backprojector_tile_rules(clean_bp_rules, monkeypatch):
     """Built-in Z blocking, rules (first match, zero fields keep the built-in
     choice), argument checks and the environment's precedence -- host only."""
-    from cbct_backprojector import _native
-    from cbct_backprojector.autotune import backprojector_tiles
+    from dgc_b200 import _native
+    from dgc_b200.autotune import backprojector_tiles
 
     lib = clean_bp_rules
     assert backprojector_tiles(256, 360) == (2, 4, (8, 1))
@@ -166,7 +166,7 @@ def test_backprojector_tile_rules(clean_bp_rules, monkeypatch):
 def test_autotuner_tunes_backprojector(clean_bp_rules, tmp_path):
     """Fastest forward (KZ, patch) and backward KZ per (depth, views) bucket,
     cached as JSON and registered as a library rule."""
-    from cbct_backprojector.autotune import Autotuner, backprojector_tiles, bp_bucket
+    from dgc_b200.autotune import Autotuner, backprojector_tiles, bp_bucket
 
     assert bp_bucket((256, 256, 256), 360) == (256, 512)
     assert bp_bucket((100, 8, 8), 1) == (128, 1)

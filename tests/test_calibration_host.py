@@ -8,13 +8,13 @@ import torch
 
 
 def nominal(A=12, U=64, V=48, px=1.0):
-    from cbct_backprojector.phantoms import circular_geometry
+    from dgc_b200.phantoms import circular_geometry
 
     return circular_geometry(A, U, V, 1000.0, 600.0, px, device="cpu")
 
 
 def test_reprojection_error_zero_and_detector_shift():
-    from cbct_backprojector.calibration import lattice_points, reprojection_error
+    from dgc_b200.calibration import lattice_points, reprojection_error
 
     g = nominal()
     pts = lattice_points((32, 32, 32), device="cpu")
@@ -30,7 +30,7 @@ def test_reprojection_error_zero_and_detector_shift():
 def test_detector_coordinates_match_the_backprojector_mapping():
     """A voxel at the isocentre lands on (u0, v0); one at height z lands
     z * sid / sod / pixel above it (bp.cu:48-72)."""
-    from cbct_backprojector.calibration import detector_coordinates
+    from dgc_b200.calibration import detector_coordinates
 
     g = nominal(A=4, px=0.5)
     pts = torch.tensor([[0.0, 0.0, 0.0], [0.0, 0.0, 10.0]], dtype=torch.float64)
@@ -42,7 +42,7 @@ def test_detector_coordinates_match_the_backprojector_mapping():
 
 
 def test_perturbation_model_is_seeded_and_sized():
-    from cbct_backprojector.calibration import angle_error_deg, perturb_geometry
+    from dgc_b200.calibration import angle_error_deg, perturb_geometry
 
     g = nominal(A=2000)
     a = perturb_geometry(g, 3)
@@ -57,7 +57,7 @@ def test_perturbation_model_is_seeded_and_sized():
 
 
 def test_warm_start_scales_and_settings():
-    from cbct_backprojector import warmstart as WS
+    from dgc_b200 import warmstart as WS
 
     s = WS.output_scales(WS.EVAL, device="cpu")
     assert s.shape == (8,)
@@ -71,7 +71,7 @@ def test_warm_start_scales_and_settings():
 
 
 def test_committed_weights_load_on_cpu():
-    from cbct_backprojector import warmstart as WS
+    from dgc_b200 import warmstart as WS
 
     ck = torch.load(WS.default_checkpoint(), map_location="cpu", weights_only=False)
     net = WS.WarmStartNet()

@@ -20,13 +20,13 @@ def declared_functions():
 
 @pytest.fixture(scope="module")
 def lib():
-    from cbct_backprojector import _native
+    from dgc_b200 import _native
 
     return _native.lib()
 
 
 def test_exports_every_declared_symbol(lib):
-    from cbct_backprojector import _native
+    from dgc_b200 import _native
 
     names = declared_functions()
     assert len(names) >= 15
@@ -157,7 +157,7 @@ def test_header_is_c99_and_links_from_c(tmp_path):
     import subprocess
     from pathlib import Path
 
-    from cbct_backprojector import _native
+    from dgc_b200 import _native
 
     gcc = shutil.which("gcc")
     if gcc is None:

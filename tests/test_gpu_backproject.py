@@ -155,7 +155,7 @@ def test_geometry_only_backward_skips_the_projection_gradient():
     """With projections that need no gradient the scatter is skipped
     (grad_projections NULL in the C ABI); the geometry gradients are bitwise
     those of the full backward."""
-    from cbct_backprojector import _ops
+    from dgc_b200 import _ops
 
     case = random_case(5)
     vol, proj, geom = run_bp(case, requires_grad=True)
@@ -219,8 +219,8 @@ def test_column_patch_shapes_are_bitwise(cta, monkeypatch):
 def test_autotuner_on_backprojector(tmp_path, monkeypatch):
     """tune_backprojector on the GPU: every candidate timed, the choice
     registered as a library rule, the volume unchanged bit for bit."""
-    from cbct_backprojector import _native, backproject
-    from cbct_backprojector.autotune import Autotuner, backprojector_tiles
+    from dgc_b200 import _native, backproject
+    from dgc_b200.autotune import Autotuner, backprojector_tiles
 
     monkeypatch.delenv("DGC_BP_KZ", raising=False)
     monkeypatch.delenv("DGC_BP_CTA", raising=False)

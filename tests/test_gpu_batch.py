@@ -21,7 +21,7 @@ pytestmark = pytest.mark.gpu
 
 
 def make_problems(seed=0):
-    from cbct_backprojector.batch import Problem
+    from dgc_b200.batch import Problem
 
     rng = np.random.default_rng(seed)
     specs = [  # (D, H, W), A, U, V, px, vox, step, offset, tiles
@@ -59,7 +59,7 @@ def plain(pr):
 @pytest.mark.parametrize("scatter", ["cells", "levels", "runs", "pairs", "plain"])
 def test_batch_matches_plain_calls(scatter, monkeypatch):
     """Every volume-gradient scatter: batched launches against per-problem calls."""
-    from cbct_backprojector.batch import ProjectionBatch
+    from dgc_b200.batch import ProjectionBatch
 
     monkeypatch.setenv("DGC_SCATTER", scatter)
     problems = make_problems()
@@ -83,7 +83,7 @@ def test_batch_against_reference_and_oracle(oracle, ref_native):
     (the geometry gradients of a random geometry meet sample-cell boundaries,
     where FP32 and FP64 take different one-sided derivatives; the reference's
     FP32 kernels take the same side)."""
-    from cbct_backprojector.batch import ProjectionBatch
+    from dgc_b200.batch import ProjectionBatch
 
     ref_fp, _ = ref_native
     pr = make_problems(1)[1]  # non power-of-two voxel size, ROI offset, 4-column tiles
@@ -110,7 +110,7 @@ def test_batch_against_reference_and_oracle(oracle, ref_native):
 
 
 def test_graph_replay_and_rebuild():
-    from cbct_backprojector.batch import ProjectionBatch
+    from dgc_b200.batch import ProjectionBatch
 
     problems = make_problems(2)
     batch = ProjectionBatch(problems, grad_volume=False)
@@ -138,7 +138,7 @@ def test_graph_replay_and_rebuild():
 
 
 def test_autotuner_on_gpu(tmp_path):
-    from cbct_backprojector.autotune import Autotuner
+    from dgc_b200.autotune import Autotuner
 
     problems = make_problems(3)[:2]
     tuner = Autotuner(cache_path=tmp_path / "tiles.json")

@@ -11,8 +11,8 @@ pytestmark = pytest.mark.gpu
 
 
 def setup_case(size=64, A=90, det=128, seed=5, I0=None):
-    from cbct_backprojector import calibration as C
-    from cbct_backprojector.phantoms import circular_geometry, ellipsoid_phantom
+    from dgc_b200 import calibration as C
+    from dgc_b200.phantoms import circular_geometry, ellipsoid_phantom
 
     vol = ellipsoid_phantom((size,) * 3, seed=seed, device="cuda",
                             axis_range=(10 * size / 256, 80 * size / 256))
@@ -35,7 +35,7 @@ def test_loss_gradient_finite_differences_on_32_views(oracle):
     relative to the summed magnitude of the ray contributions (the FP64
     oracle with FP64 ray set-up agrees with the analytic formula to 1e-8).
     """
-    from cbct_backprojector import _ops, project
+    from dgc_b200 import _ops, project
 
     C, vol, nominal, true, scan, meas, _ = setup_case(size=48, A=64, det=96)
 
@@ -123,7 +123,7 @@ def test_fused_step_matches_project_and_autograd():
     explicit fmaf / __fmul_rn, so both kernels march the same rays), the loss
     to 1e-5, the eight geometry gradients to 1e-5 (the upstream gradient
     2*scale*mask*(p - m) is rounded in a different order)."""
-    from cbct_backprojector import _ops, project
+    from dgc_b200 import _ops, project
 
     C, vol, nominal, true, scan, meas, mask = setup_case(size=40, A=48, det=72, I0=1e5)
     geom = [n + 0.5 * (t - n) for t, n in zip(true, nominal)]
@@ -160,8 +160,8 @@ def test_sharded_calibration_two_view_halves():
     halves standing in for the all-reduce: each half's offsets equal the
     whole calibration's bit for bit (the views' offsets are independent and
     the loss normalisation is the whole scan's)."""
-    from cbct_backprojector import calibration as C2
-    from cbct_backprojector.sharded import view_shard
+    from dgc_b200 import calibration as C2
+    from dgc_b200.sharded import view_shard
 
     C, vol, nominal, true, scan, meas, mask = setup_case(I0=1e5)
     whole = C.calibrate(vol, meas, nominal, scan, iterations=12, true_geometry=true, mask=mask)

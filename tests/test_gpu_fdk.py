@@ -93,7 +93,7 @@ def test_short_scan_matches_oracle(direction, oracle):
     against the FP64 oracle's, and the weighted reconstruction against the
     oracle pipeline (weights x projections -> filter -> backprojection x view
     spacing -> clamp) at the parity bar."""
-    from cbct_backprojector import _ops, reconstruct_fdk
+    from dgc_b200 import _ops, reconstruct_fdk
 
     A, U, V, px, sid, sod = 58, 48, 40, 1.0, 300.0, 180.0
     fan = math.atan(((U - 1) / 2 * px) / sid)

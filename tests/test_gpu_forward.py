@@ -244,7 +244,7 @@ def test_config1_finite_differences(golden, oracle):
     and are quantised to ~1e-5, which at eps=1e-3 is a few percent of the
     displacement a source shift produces (the FP64 oracle shows the same).
     """
-    from cbct_backprojector import _ops
+    from dgc_b200 import _ops
 
     d = golden("fp_config1.npz")
     case = config1_case(d)

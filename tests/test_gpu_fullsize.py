@@ -50,7 +50,7 @@ def test_projector_adjoint_dot_product(scatter, monkeypatch):
 def test_constant_volume_projects_to_the_sample_count():
     """A volume of ones: each ray's integral is exactly step x its FP32
     sample count (the trilinear interpolant of a constant is that constant)."""
-    from cbct_backprojector import _ops, project
+    from dgc_b200 import _ops, project
 
     geom = geometry()
     p = project(torch.ones((D, D, D), device="cuda"), *geom, PX, U, V, step_size=STEP,
@@ -80,7 +80,7 @@ def test_fdk_reconstructs_the_phantom():
     size: the reconstruction follows the phantom (FDK's cone-beam and
     sampling errors are far below the phantom's contrast)."""
     from cbct_backprojector import project, reconstruct_fdk
-    from cbct_backprojector.phantoms import ellipsoid_phantom
+    from dgc_b200.phantoms import ellipsoid_phantom
 
     vol = ellipsoid_phantom((D, D, D), n=12, seed=3, device="cuda")
     geom = geometry()

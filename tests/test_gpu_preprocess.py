@@ -22,7 +22,7 @@ def reference(raw, dark, flat, layout, min_ratio):
 @pytest.mark.parametrize("layout", ["AVU", "AUV"])
 @pytest.mark.parametrize("A,U,V", [(3, 70, 45), (1, 32, 32), (5, 1, 67)])
 def test_preprocess_matches_formula(layout, A, U, V):
-    from cbct_backprojector.preprocessing import preprocess
+    from dgc_b200.preprocessing import preprocess
 
     rng = np.random.default_rng(A * 100 + U + V)
     shape = (A, V, U) if layout == "AVU" else (A, U, V)
@@ -47,8 +47,8 @@ def test_preprocess_feeds_the_operators():
     import math
 
     import cbct_backprojector as cb
-    from cbct_backprojector.phantoms import circular_geometry, ellipsoid_phantom
-    from cbct_backprojector.preprocessing import preprocess
+    from dgc_b200.phantoms import circular_geometry, ellipsoid_phantom
+    from dgc_b200.preprocessing import preprocess
 
     vol = ellipsoid_phantom((32, 32, 32), seed=3, device="cuda", axis_range=(2.0, 8.0))
     geom = circular_geometry(6, 40, 36, 200.0, 120.0, 1.0, device="cuda")

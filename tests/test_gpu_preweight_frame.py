@@ -142,8 +142,8 @@ def test_offset_preweight_reconstruction(oracle):
 
 
 def test_offset_preweight_short_scan(oracle):
-    from cbct_backprojector import _ops, reconstruct_fdk
-    from cbct_backprojector.filtering import preweight_frame
+    from dgc_b200 import _ops, reconstruct_fdk
+    from dgc_b200.filtering import preweight_frame
 
     A, U, V, px, shape, off = 60, 48, 40, 1.0, (20, 24, 24), (0.3, -0.2, 0.1)
     probe = _offset_geometry(A, U, V, 8)  # the offsets; the angles below do not draw

@@ -13,9 +13,9 @@ pytestmark = pytest.mark.gpu
 
 def test_entropy_recovers_detector_shift():
     from cbct_backprojector import project
-    from cbct_backprojector.calibration import lattice_points, reprojection_error
-    from cbct_backprojector.phantoms import circular_geometry, ellipsoid_phantom
-    from cbct_backprojector.selfcal import entropy_calibrate, image_entropy
+    from dgc_b200.calibration import lattice_points, reprojection_error
+    from dgc_b200.phantoms import circular_geometry, ellipsoid_phantom
+    from dgc_b200.selfcal import entropy_calibrate, image_entropy
 
     N, A, U, V, px = 64, 90, 128, 128, 1.0
     vol = ellipsoid_phantom((N, N, N), n=8, seed=11, device="cuda", axis_range=(4.0, 16.0))
@@ -44,8 +44,8 @@ def test_refiltering_each_iteration():
     the fixed-filter run exactly; fitting sid, the entropy's gradient reaches
     sid through the filter as well (a different, finite trajectory)."""
     from cbct_backprojector import project
-    from cbct_backprojector.phantoms import circular_geometry, ellipsoid_phantom
-    from cbct_backprojector.selfcal import entropy_calibrate
+    from dgc_b200.phantoms import circular_geometry, ellipsoid_phantom
+    from dgc_b200.selfcal import entropy_calibrate
 
     N, A, U, V, px = 48, 60, 96, 96, 1.0
     vol = ellipsoid_phantom((N, N, N), n=6, seed=4, device="cuda", axis_range=(3.0, 12.0))
@@ -71,9 +71,9 @@ def test_offset_preweight_in_self_calibration():
     filter's frame as well (a different trajectory from the centred
     preweight's), and the shift is still recovered."""
     from cbct_backprojector import project
-    from cbct_backprojector.calibration import lattice_points, reprojection_error
-    from cbct_backprojector.phantoms import circular_geometry, ellipsoid_phantom
-    from cbct_backprojector.selfcal import entropy_calibrate
+    from dgc_b200.calibration import lattice_points, reprojection_error
+    from dgc_b200.phantoms import circular_geometry, ellipsoid_phantom
+    from dgc_b200.selfcal import entropy_calibrate
 
     N, A, U, V, px = 48, 60, 96, 96, 1.0
     vol = ellipsoid_phantom((N, N, N), n=6, seed=4, device="cuda", axis_range=(3.0, 12.0))

@@ -26,8 +26,8 @@ def _scan(A, U, V, seed):
 
 
 def test_two_view_shards_sum_to_the_reconstruction(oracle):
-    from cbct_backprojector import _ops, reconstruct_fdk
-    from cbct_backprojector.sharded import view_shard
+    from dgc_b200 import _ops, reconstruct_fdk
+    from dgc_b200.sharded import view_shard
 
     A, U, V, shape, off = 37, 48, 40, (20, 24, 22), (0.4, -0.3, 0.2)
     proj, geom = _scan(A, U, V, 9)
@@ -53,9 +53,9 @@ def test_two_view_shards_offset_preweight():
     """The unclamped partial reconstruction with the offset-aware preweight
     (dgc_reconstruct_fdk_ex, clamp off) of two view shards, summed and
     clamped, against reconstruct_fdk(offset_preweight=True)."""
-    from cbct_backprojector import _ops, reconstruct_fdk
-    from cbct_backprojector.filtering import preweight_frame
-    from cbct_backprojector.sharded import view_shard
+    from dgc_b200 import _ops, reconstruct_fdk
+    from dgc_b200.filtering import preweight_frame
+    from dgc_b200.sharded import view_shard
 
     A, U, V, shape, off = 33, 44, 38, (18, 22, 20), (0.2, 0.3, -0.1)
     proj, geom = _scan(A, U, V, 21)
@@ -79,7 +79,7 @@ def test_depth_slabs_are_the_reconstruction():
     a sub-volume at its slab_offset, is the same rows of the whole volume (up
     to the float rounding of the voxel centres)."""
     from cbct_backprojector import reconstruct_fdk
-    from cbct_backprojector.sharded import reconstruct_fdk_slab, slab_offset, slab_shard
+    from dgc_b200.sharded import reconstruct_fdk_slab, slab_offset, slab_shard
 
     A, U, V, shape, off = 30, 40, 36, (19, 20, 18), (0.3, -0.2, 0.45)
     proj, geom = _scan(A, U, V, 17)
@@ -95,7 +95,7 @@ def test_depth_slabs_are_the_reconstruction():
 
 def test_one_rank_is_the_single_device_operator():
     from cbct_backprojector import backproject, project, reconstruct_fdk
-    from cbct_backprojector.sharded import (backproject_sharded, project_sharded,
+    from dgc_b200.sharded import (backproject_sharded, project_sharded,
                                             reconstruct_fdk_sharded)
 
     A, U, V, shape = 24, 32, 28, (16, 18, 20)
@@ -133,7 +133,7 @@ def _nccl_rank(port, out):
     dist.init_process_group("nccl", rank=0, world_size=1, timeout=timedelta(seconds=60))
     try:
         from cbct_backprojector import reconstruct_fdk
-        from cbct_backprojector.sharded import reconstruct_fdk_sharded, total_views
+        from dgc_b200.sharded import reconstruct_fdk_sharded, total_views
 
         A, U, V, shape = 30, 40, 36, (16, 20, 18)
         proj, geom = _scan(A, U, V, 12)

@@ -10,7 +10,7 @@ pytestmark = pytest.mark.gpu
 
 
 def run(A, B, C, bias=None, relu=False, accumulate=False, alpha=1.0):
-    from cbct_backprojector import _native
+    from dgc_b200 import _native
 
     lib = _native.lib()
     err = torch.zeros(1, dtype=torch.int32, device="cuda")
@@ -43,7 +43,7 @@ def test_gemm_matches_fp32(M, N, K, pipeline, monkeypatch):
     B = torch.randn(N, K, device="cuda", generator=g).to(torch.bfloat16)
     want = A.float() @ B.float().t()
     C = torch.full((M, N), float("nan"), device="cuda")
-    from cbct_backprojector import _native
+    from dgc_b200 import _native
 
     with _native.trace() as tr:
         got = run(A, B, C)

@@ -18,7 +18,7 @@ HELD_OUT = (7, 11, 23, 42, 77, 101)
 
 @pytest.fixture(scope="module")
 def net():
-    from cbct_backprojector import warmstart as WS
+    from dgc_b200 import warmstart as WS
 
     path = WS.default_checkpoint()
     assert path.exists(), f"trained weights missing: {path}"
@@ -28,8 +28,8 @@ def net():
 
 
 def test_prediction_beats_nominal(net):
-    from cbct_backprojector import warmstart as WS
-    from cbct_backprojector.calibration import lattice_points
+    from dgc_b200 import warmstart as WS
+    from dgc_b200.calibration import lattice_points
 
     acq = WS.TRAIN
     pts = lattice_points((acq.volume,) * 3, acq.voxel, device="cuda")
@@ -50,8 +50,8 @@ def test_warm_started_calibration_reaches_target_faster(net):
     """From the network's multi-stage start with its calibration settings, the
     0.1 px target comes in fewer than half the iterations of calibration from
     nominal (46-52 vs 7-12 on held-out stacks when the settings were chosen)."""
-    from cbct_backprojector import warmstart as WS
-    from cbct_backprojector.calibration import calibrate, lattice_points
+    from dgc_b200 import warmstart as WS
+    from dgc_b200.calibration import calibrate, lattice_points
 
     acq = WS.TRAIN
     st = WS.make_stack(acq, 42)

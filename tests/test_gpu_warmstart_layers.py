@@ -17,7 +17,7 @@ def rel(a, b):
 @pytest.mark.parametrize("B,H,Cin,Cout,stride", [(3, 20, 2, 32, 2), (2, 12, 32, 64, 1),
                                                  (4, 9, 16, 8, 2)])
 def test_conv2d_layer(B, H, Cin, Cout, stride):
-    from cbct_backprojector.warmstart import _Conv2d, _round8
+    from dgc_b200.warmstart import _Conv2d, _round8
 
     g = torch.Generator(device="cuda").manual_seed(B * 100 + Cin)
     x = torch.randn(B, H, H, Cin, device="cuda", generator=g).to(torch.bfloat16)
@@ -44,7 +44,7 @@ def test_conv2d_layer(B, H, Cin, Cout, stride):
 
 
 def test_view_conv_and_network():
-    from cbct_backprojector.warmstart import WarmStartNet, _ViewConv
+    from dgc_b200.warmstart import WarmStartNet, _ViewConv
 
     g = torch.Generator(device="cuda").manual_seed(1)
     A, Cin, Cout, k = 37, 64, 24, 5

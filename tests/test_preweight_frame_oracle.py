@@ -64,7 +64,7 @@ def test_frame_foot_is_perpendicular(oracle):
     """The frame's centre is the foot of the perpendicular from the source and
     its distance the source's distance to the detector plane; the torch
     ``preweight_frame`` agrees with the oracle's."""
-    from cbct_backprojector.filtering import preweight_frame
+    from dgc_b200.filtering import preweight_frame
 
     A, U, V, px = 9, 40, 30, 1.3
     g = _geometry(A, U, V, 4, px)
@@ -177,7 +177,7 @@ def test_preweight_frame_gradients_reach_the_geometry():
     gradients into the geometry: d(dist)/d(sid) = 1, d(u)/d(det_u0) = 1,
     d(u)/d(src_x) = cos(b)/px, d(dist)/d(src_x) = -sin(b), d(v)/d(src_z) = 1/px,
     and d(u)/d(angle) = (-sx sin b + sy cos b)/px; sod does not enter."""
-    from cbct_backprojector.filtering import preweight_frame
+    from dgc_b200.filtering import preweight_frame
 
     A, px = 5, 0.8
     g = [torch.tensor(x, requires_grad=True) for x in _geometry(A, 16, 12, 9, px)]

@@ -21,7 +21,7 @@ def _free_port():
 
 
 def test_view_shard_ranges():
-    from cbct_backprojector.sharded import view_shard
+    from dgc_b200.sharded import view_shard
 
     for views in (0, 1, 7, 360):
         for world in (1, 2, 3, 8):
@@ -39,7 +39,7 @@ def _rank(rank, world, port, out):
     import torch
     import torch.distributed as dist
 
-    from cbct_backprojector import sharded
+    from dgc_b200 import sharded
     from oracle import oracle as O
 
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
@@ -174,8 +174,8 @@ def _calib_rank(rank, world, port, out):
     import torch
     import torch.distributed as dist
 
-    from cbct_backprojector import calibration, sharded
-    from cbct_backprojector.calibration import ScanSetup
+    from dgc_b200 import calibration, sharded
+    from dgc_b200.calibration import ScanSetup
 
     _calib_standins(calibration)
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
@@ -204,8 +204,8 @@ def test_two_gloo_ranks_sharded_calibration(monkeypatch):
 
     import torch
 
-    from cbct_backprojector import calibration
-    from cbct_backprojector.calibration import ScanSetup
+    from dgc_b200 import calibration
+    from dgc_b200.calibration import ScanSetup
 
     for name in ("_loss_terms", "_fused_loss", "_loss"):
         monkeypatch.setattr(calibration, name, getattr(calibration, name))
@@ -225,7 +225,7 @@ def test_two_gloo_ranks_sharded_calibration(monkeypatch):
         p.join(150)
     assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
     got = {r: rest for r, *rest in (q.get(timeout=5) for _ in range(2))}
-    from cbct_backprojector.sharded import view_shard
+    from dgc_b200.sharded import view_shard
 
     for r in range(2):
         delta, hist, it_target, final = got[r]
@@ -248,7 +248,7 @@ def _slab_rank(rank, world, port, out):
     import torch
     import torch.distributed as dist
 
-    from cbct_backprojector import filtering, sharded
+    from dgc_b200 import filtering, sharded
     from oracle import oracle as O
 
     def oracle_fdk(projections, *args, volume_offset=(0.0, 0.0, 0.0), alpha=0.8,
@@ -310,7 +310,7 @@ def test_two_gloo_ranks_slab_sharded_reconstruction():
     for r in (0, 1):
         for shape, (_, _, slab_err, whole_err, scale) in got[r].items():
             assert slab_err <= 1e-6 * scale and whole_err <= 1e-6 * scale, (r, shape)
-    from cbct_backprojector.sharded import slab_offset
+    from dgc_b200.sharded import slab_offset
 
     # row z of the slab sits where row start + z of the whole volume does
     assert slab_offset((10, 4, 4), 1.0, (0.0, 0.0, 0.5), range(3, 6)) == (0.0, 0.0, 0.0)

@@ -37,7 +37,7 @@ def test_conjugate_rays_sum_to_one(oracle, direction):
 
 @pytest.mark.parametrize("direction", [1.0, -1.0])
 def test_short_scan_reconstruction_matches_full_scan(oracle, direction):
-    from cbct_backprojector.phantoms import ellipsoid_phantom
+    from dgc_b200.phantoms import ellipsoid_phantom
 
     N, U, V, px, sid, sod = 32, 64, 64, 1.0, 200.0, 120.0
     vol = ellipsoid_phantom((N, N, N), n=6, seed=2, device="cpu",
