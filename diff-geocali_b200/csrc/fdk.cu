@@ -19,6 +19,7 @@
 #include "fdk.cuh"
 
 #include <cmath>
+#include <cstddef>
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -398,32 +399,85 @@ int fdk_upload_taps(int U, float px, float alpha, float* dst, cudaStream_t s) {
 // Allocation-free variant (dgc_fdk_filter_noalloc, see include/dgc.h)
 // ---------------------------------------------------------------------------
 
-// The filter taps of the allocation-free entry point.  Host code must not pass
-// this name to a kernel (on the host it is only a stand-in symbol); its device
-// address is looked up once per device with cudaGetSymbolAddress.
-static __device__ __align__(256) float g_noalloc_taps[DGC_FDK_NOALLOC_MAX_U];
+// Scratch of the allocation-free entry point: the filter's spectrum H[k],
+// k in [0, P/2] (P/2 <= DGC_FDK_NOALLOC_MAX_U for U <= DGC_FDK_NOALLOC_MAX_U),
+// and its taps h[m], m in [0, U).  98 KiB held by every GPU that loads the
+// library.  Host code must not pass this name to a kernel (on the host it is
+// only a stand-in symbol); its device address comes from cudaGetSymbolAddress.
+struct NoallocScratch {
+    double spectrum[DGC_FDK_NOALLOC_MAX_U + 1];
+    float taps[DGC_FDK_NOALLOC_MAX_U];
+};
+static __device__ __align__(256) NoallocScratch g_noalloc_scratch;
 
 namespace dgc {
 namespace {
 
-std::mutex g_noalloc_mu;
-std::map<int, float*> g_noalloc_taps_by_device;
+// fdk_taps_host's first sum on the device, one warp per bin k (lanes split
+// the odd n, then a shuffle tree): H[k] = R[k] * hann[k].  cospi's argument
+// 2j/P is exact because P is a power of two.
+__global__ void noalloc_spectrum_kernel(double* H, int P, double px, double alpha) {
+    const int half = P / 2;
+    const int k = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (k > half) return;
+    const unsigned mask = (unsigned)P - 1u;
+    double R = 0.0;
+    for (int n = 1 + 2 * lane; n <= half; n += 64) {
+        const double pn = M_PI * (double)n * px;
+        const double weight = (n == half) ? 1.0 : 2.0;
+        const unsigned j = ((unsigned)k * (unsigned)n) & mask;
+        R += weight * (-1.0 / (pn * pn)) * cospi(2.0 * (double)j / (double)P);
+    }
+    for (int o = 16; o > 0; o >>= 1) R += __shfl_xor_sync(0xffffffffu, R, o);
+    if (lane == 0) {
+        R += 1.0 / (4.0 * px * px);
+        const double f = (k == half) ? -0.5 : (double)k / (double)P;
+        const double hann = fabs(f) <= alpha * 0.5 ? 0.5 + 0.5 * cospi(2.0 * f / alpha) : 0.0;
+        H[k] = R * hann;
+    }
+}
 
-// Device address of g_noalloc_taps on the current device (first call per
-// device performs the lookup).
-int noalloc_taps_address(float** out) {
+// fdk_taps_host's second sum, one warp per tap m:
+// h[m] = (H[0] + 2 sum_{0<k<P/2} H[k] cos(2 pi k m / P) + H[P/2] cos(pi m)) / P.
+__global__ void noalloc_taps_kernel(const double* H, int P, int U, float* taps) {
+    const int half = P / 2;
+    const int m = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (m >= U) return;
+    const unsigned mask = (unsigned)P - 1u;
+    double acc = 0.0;
+    for (int k = 1 + lane; k < half; k += 32) {
+        const unsigned j = ((unsigned)k * (unsigned)m) & mask;
+        acc += 2.0 * H[k] * cospi(2.0 * (double)j / (double)P);
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) {
+        acc += H[0] + H[half] * ((m & 1) ? -1.0 : 1.0);
+        taps[m] = (float)(acc / (double)P);
+    }
+}
+
+std::mutex g_noalloc_mu;
+std::map<int, char*> g_noalloc_scratch_by_device;
+
+// Device address of g_noalloc_scratch on the current device.  The first call
+// on a device looks it up (loading the library's module there if needed) and
+// caches it for the process; a cudaDeviceReset of that device invalidates the
+// cached address.
+int noalloc_scratch_address(char** out) {
     int dev = 0;
     DGC_CUDA(cudaGetDevice(&dev));
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    auto it = g_noalloc_taps_by_device.find(dev);
-    if (it != g_noalloc_taps_by_device.end()) {
+    auto it = g_noalloc_scratch_by_device.find(dev);
+    if (it != g_noalloc_scratch_by_device.end()) {
         *out = it->second;
         return DGC_OK;
     }
     void* p = nullptr;
-    DGC_CUDA(cudaGetSymbolAddress(&p, g_noalloc_taps));
-    g_noalloc_taps_by_device[dev] = static_cast<float*>(p);
-    *out = static_cast<float*>(p);
+    DGC_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    g_noalloc_scratch_by_device[dev] = static_cast<char*>(p);
+    *out = static_cast<char*>(p);
     return DGC_OK;
 }
 
@@ -448,14 +502,28 @@ extern "C" int dgc_fdk_filter_noalloc(const float* projections, int A, int U, in
                   "-tap static scratch; use dgc_fdk_filter with a workspace");
         return DGC_ERR_UNSUPPORTED;
     }
-    float* taps = nullptr;
-    int rc = noalloc_taps_address(&taps);
+    char* scratch = nullptr;
+    int rc = noalloc_scratch_address(&scratch);
     if (rc != DGC_OK) return rc;
-    std::vector<double> h;
-    if ((rc = fdk_taps_host(U, (double)pixel_size, (double)alpha, h)) != DGC_OK) return rc;
-    std::vector<float> hf(h.begin(), h.end());
-    // Pageable source: the call returns once the taps are staged, so hf may go.
-    DGC_CUDA(cudaMemcpyAsync(taps, hf.data(), sizeof(float) * (size_t)U, cudaMemcpyHostToDevice, s));
+    double* spectrum = reinterpret_cast<double*>(scratch + offsetof(NoallocScratch, spectrum));
+    float* taps = reinterpret_cast<float*>(scratch + offsetof(NoallocScratch, taps));
+    int bl = 0;
+    for (int n = 2 * U - 1; n; n >>= 1) ++bl;
+    const int P = 1 << bl;
+    // The taps are written on the device, in stream order before the filter
+    // reads them: the call reads no host memory after it returns and does not
+    // wait for the stream.
+    {
+        DGC_TRACE("noalloc_spectrum_kernel", s);
+        noalloc_spectrum_kernel<<<ceil_div((long long)(P / 2 + 1) * 32, 256), 256, 0, s>>>(
+            spectrum, P, (double)pixel_size, (double)alpha);
+        DGC_LAUNCH_CHECK("noalloc_spectrum_kernel");
+    }
+    {
+        DGC_TRACE("noalloc_taps_kernel", s);
+        noalloc_taps_kernel<<<ceil_div((long long)U * 32, 256), 256, 0, s>>>(spectrum, P, U, taps);
+        DGC_LAUNCH_CHECK("noalloc_taps_kernel");
+    }
     FdkArgs f{projections, sod, sid, taps, filtered, A, U, V, pixel_size};
     return fdk_launch_filter(f, s);
 }

@@ -181,16 +181,22 @@ int dgc_fdk_filter_ex(const float* projections, int A, int U, int V, float pixel
  * hands each library a fixed budget, a plugin that must not grow the process's
  * device footprint, or a latency-bound pipeline that keeps cudaMalloc and
  * cudaFree (which can synchronise the device) out of its steady state.  It
- * takes no workspace: the only scratch, the filter taps, lives in a static
- * device array of DGC_FDK_NOALLOC_MAX_U floats (32 KiB) that every GPU loading
- * the library holds until the process exits; U above that maximum returns
- * DGC_ERR_UNSUPPORTED.  The first call on a device looks up the array's device
- * address (cudaGetSymbolAddress) and caches it; make that first call before
- * any stream capture.  Every call overwrites taps[0..U-1] before its filter
- * reads them, so nothing needs to start at zero, but all calls share the one
- * array: calls that overlap on the GPU (different streams, no ordering
- * between them) race on it.  Same inputs, outputs and results as
- * dgc_fdk_filter. */
+ * takes no workspace and allocates nothing: its scratch, the filter's spectrum
+ * and taps, lives in one static device array of 98 KiB
+ * (DGC_FDK_NOALLOC_MAX_U + 1 doubles and DGC_FDK_NOALLOC_MAX_U floats) that
+ * every GPU loading the library holds until the process exits; U above
+ * DGC_FDK_NOALLOC_MAX_U returns DGC_ERR_UNSUPPORTED.  Two small kernels write
+ * the taps on the device, in stream order before the filter, so a call reads
+ * no host memory after it returns and never waits on the host for earlier
+ * work in its stream.  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress) and keeps it for the process; make that
+ * first call before any stream capture.  A cudaDeviceReset of that device
+ * invalidates the kept address, so do not call this entry point on a device
+ * after resetting it.  Every call rewrites the spectrum and taps[0..U-1]
+ * before its filter reads them, so nothing needs to start at zero, but all
+ * calls share the one array: calls that overlap on the GPU (different
+ * streams, no ordering between them) race on it.  Same inputs and outputs as
+ * dgc_fdk_filter; results equal its within the taps' FP64 rounding. */
 int dgc_fdk_filter_noalloc(const float* projections, int A, int U, int V, float pixel_size,
                            const float* sod, const float* sid, float alpha,
                            float* filtered, void* stream);
