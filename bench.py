@@ -1,19 +1,24 @@
-"""Benchmark of the cone-beam operators on the FDK workload (256^3, 360 x 384^2).
+"""Benchmark of the cone-beam operators at the target size (512^3, 720 x 768^2).
 
-One step = forward projection of a 256^3 twelve-ellipsoid phantom onto 360
-views of a 384x384 detector (sid 1000, sod 600, pixel 1, step 0.5, voxel 1)
-followed by ``reconstruct_fdk`` of those projections into 256^3 -- the
-"plain FDK at medium size" workload.  ``value`` is rays per second through the
-whole step (Grays/s) with inputs resident in HBM; the forward projector alone
-(Grays/s) and the backprojection alone (Gvoxel-views/s) are reported beside it.
+One step = forward projection of a 512^3 twelve-ellipsoid phantom onto 720
+views of a 768x768 detector (sid 1000, sod 600, pixel 1, step 0.5, voxel 1)
+followed by ``reconstruct_fdk`` of those projections into 512^3.  ``value``
+is rays per second through the whole step (Grays/s) with inputs resident in
+HBM; the forward projector alone (Grays/s) and the backprojection alone
+(Gvoxel-views/s) are reported beside it, each kernel's algorithmic gather
+bytes against the L1 / L2 ceilings measured in the same run.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload target512|fdk256|fdk-sharded|batch64|calib|tour|gemm]
 
-N > 1 runs under torch.distributed (one process per GPU, NCCL): every rank
-reconstructs its own phantom (independent objects, weak scaling, no data-path
-collective); time = max over ranks.  ``--impl reference`` times the
-reference's CPU path (the FP64 oracle port of its CPU checks) on the host
-cores over a bounded sample of the same workload and prints the same line.
+N > 1 runs under torch.distributed (one process per GPU, NCCL).  The default
+workloads give every rank its own phantom (independent objects, weak scaling,
+no data-path collective); ``fdk-sharded`` splits one object's views over the
+ranks (``project_sharded`` + ``reconstruct_fdk_sharded``: one all-reduce of
+the volume per step, strong scaling).  Time = max over ranks.
+``--impl reference`` times the reference's CPU path (the FP64 oracle port of
+its CPU checks) on the host cores over a bounded, stated fraction of the same
+step and prints the same line.
 """
 
 from __future__ import annotations
@@ -33,15 +38,25 @@ for _p in (str(ROOT / "diff-geocali_b200"), str(ROOT)):
     if _p not in sys.path:
         sys.path.insert(0, _p)
 
-WORKLOAD = dict(name="fdk256: project 256^3 -> 360x384^2, then reconstruct_fdk 256^3",
-                D=256, H=256, W=256, A=360, U=384, V=384, sid=1000.0, sod=600.0, pixel=1.0,
-                step=0.5, voxel=1.0, ellipsoids=12, alpha=0.8)
+WORKLOADS = {
+    "target512": dict(name="target512: project 512^3 -> 720x768^2, then reconstruct_fdk 512^3",
+                      D=512, H=512, W=512, A=720, U=768, V=768, sid=1000.0, sod=600.0, pixel=1.0,
+                      step=0.5, voxel=1.0, ellipsoids=12, alpha=0.8),
+    "fdk256": dict(name="fdk256: project 256^3 -> 360x384^2, then reconstruct_fdk 256^3",
+                   D=256, H=256, W=256, A=360, U=384, V=384, sid=1000.0, sod=600.0, pixel=1.0,
+                   step=0.5, voxel=1.0, ellipsoids=12, alpha=0.8),
+}
+WORKLOADS["fdk-sharded"] = dict(
+    WORKLOADS["target512"],
+    name="fdk-sharded: one 512^3 object, its 720 views of 768^2 split over the ranks: "
+         "project_sharded, then reconstruct_fdk_sharded (one volume all-reduce)")
+WORKLOAD = dict(WORKLOADS["target512"])
 METRIC = "fwd Grays/s, backproj Gvoxel-views/s; calib time to 0.1 px reproj, NN vs plain"
 UNIT = "Grays/s"
-# DRAM bytes (read + write) of one 360-view fp_forward_kernel launch: an ncu
-# capture of the 24-view case (bench.py --workload tour --views 24) measured
-# 351.7 + 17.9 MB, scaled by the view count (x15).
-FWD_DRAM_BYTES_PER_LAUNCH = (351.7e6 + 17.9e6) * 15
+# DRAM bytes (read + write) of one fp_forward_kernel launch of a workload: an
+# ncu capture of a few of its views, scaled by the view count (the profile
+# summaries under profiles/ give the commands and the captured figures).
+FWD_DRAM_BYTES = {"fdk256": (351.7e6 + 17.9e6) * 15, "target512": None}
 FALLBACK_HBM_GBS = 6650.0
 FALLBACK_BF16_TFLOPS = 1590.0
 
@@ -57,9 +72,12 @@ def parse_args(argv=None):
                     help="override the view count (smaller cases for profiler captures)")
     ap.add_argument("--volume", type=int, default=None, help="override the cubic volume size")
     ap.add_argument("--detector", type=int, default=None, help="override the square detector size")
-    ap.add_argument("--workload", choices=["fdk256", "batch64", "calib", "tour", "gemm"],
-                    default="fdk256",
-                    help="fdk256: the FDK step (default); batch64: 64 uneven project+backward "
+    ap.add_argument("--workload", default="target512",
+                    choices=["target512", "fdk256", "fdk-sharded", "batch64", "calib", "tour",
+                             "gemm"],
+                    help="target512: the FDK step at 512^3 / 720 x 768^2 (default); fdk256: the "
+                         "same step at 256^3 / 360 x 384^2; fdk-sharded: one target512 object "
+                         "split by views over the ranks; batch64: 64 uneven project+backward "
                          "instances, batched vs sequential; calib: calibration wall time to "
                          "0.1 px, learned warm start vs plain; tour: every kernel once on the "
                          "fdk256 instance (profiler captures); gemm: the tcgen05 GEMM at "
@@ -72,7 +90,13 @@ def parse_args(argv=None):
                     help="batch64 shape sets: config4 (128^3..384x384x256, 90-720 views, "
                          "256-512 detectors) or small (48^3..64x96x96, 30-90 views, 96-160)")
     ap.add_argument("--tune-cache", default=None, help="batch64: autotuner JSON cache path")
+    ap.add_argument("--seeds", type=int, default=1, help="calib: held-out seeds per arm")
     args = ap.parse_args(argv)
+    base = "fdk256" if args.workload == "tour" else args.workload
+    if base in WORKLOADS:
+        WORKLOAD.clear()
+        WORKLOAD.update(WORKLOADS[base])
+        WORKLOAD["key"] = base
     if args.views:
         WORKLOAD["A"] = args.views
     if args.volume:
@@ -188,6 +212,13 @@ class ClockSampler:
 # ------------------------------------------------------------------- workload
 
 
+def axis_range(w):
+    """Ellipsoid semi-axes of the config-2 family (10-80 voxels at 256^3),
+    scaled with the volume so that a larger volume holds the same phantom."""
+    f = w["D"] / 256.0
+    return (10.0 * f, 80.0 * f)
+
+
 def make_instance(device, seed):
     import torch
 
@@ -195,7 +226,7 @@ def make_instance(device, seed):
 
     w = WORKLOAD
     vol = ellipsoid_phantom((w["D"], w["H"], w["W"]), n=w["ellipsoids"], seed=seed,
-                            voxel_size=w["voxel"], device=device)
+                            voxel_size=w["voxel"], device=device, axis_range=axis_range(w))
     geom = circular_geometry(w["A"], w["U"], w["V"], w["sid"], w["sod"], w["pixel"], device=device)
     torch.cuda.synchronize(device)
     return vol, geom
@@ -212,6 +243,20 @@ def step(vol, geom):
     return proj, recon
 
 
+def sharded_step(vol, geom):
+    """fdk-sharded: this rank's views of one object (``geom`` holds only
+    them): ``project_sharded``, then ``reconstruct_fdk_sharded`` (the volume
+    all-reduce over the ranks)."""
+    from dgc_b200.sharded import project_sharded, reconstruct_fdk_sharded
+
+    w = WORKLOAD
+    proj = project_sharded(vol, *geom, w["pixel"], w["U"], w["V"], step_size=w["step"],
+                           voxel_size=w["voxel"])
+    recon = reconstruct_fdk_sharded(proj, *geom, w["pixel"], (w["D"], w["H"], w["W"]), w["voxel"],
+                                    alpha=w["alpha"], views_total=w["A"])
+    return proj, recon
+
+
 def measured_peak_hbm():
     path = ROOT / "MEASURED_PEAKS.json"
     try:
@@ -221,18 +266,95 @@ def measured_peak_hbm():
         return FALLBACK_HBM_GBS, "fallback"
 
 
+def backprojection_valid_count(geom, shape, pixel, voxel, U, V):
+    """Voxel-views that pass the backprojector's mask (bp.cu:43-75: q > 1e-6,
+    sid + ds_n > 1e-6, 0 <= u_idx < U-1, 0 <= v_idx < V-1): per view and
+    (y, x) column the mask's u part is fixed and v_idx is linear in z, so the
+    valid z form an interval, counted in closed form (FP32 on the device;
+    voxels exactly on an edge of the detector may be counted either way)."""
+    import torch
+
+    D, H, W = shape
+    dev = geom[0].device
+    xs = (torch.arange(W, device=dev, dtype=torch.float64) - W * 0.5) * voxel
+    ys = (torch.arange(H, device=dev, dtype=torch.float64) - H * 0.5) * voxel
+    total = 0
+    for a0 in range(0, geom[0].numel(), 32):
+        g = [x[a0:a0 + 32].double().view(-1, 1, 1) for x in geom]
+        beta, sid, sod, u0, v0, sx, sy, sz = g
+        c, s = torch.cos(beta), torch.sin(beta)
+        px = xs.view(1, 1, -1) * c + ys.view(1, -1, 1) * s
+        py = -xs.view(1, 1, -1) * s + ys.view(1, -1, 1) * c
+        ds_u, ds_n = sx * c + sy * s, -sx * s + sy * c
+        q = sod + ds_n - py
+        ll = sid + ds_n
+        t = ll / q
+        ui = (ds_u + t * (px - ds_u)) / pixel + u0
+        ok = (q > 1e-6) & (ll > 1e-6) & (ui >= 0) & (ui < U - 1)
+        # 0 <= (sz + t (vz - sz)) / pixel + v0 < V - 1, vz = (z - D/2) voxel
+        lo = sz + (-v0 * pixel - sz) / t
+        hi = sz + ((V - 1 - v0) * pixel - sz) / t
+        zlo = torch.ceil(lo / voxel + D * 0.5).clamp(0, D)
+        zhi = torch.ceil(hi / voxel + D * 0.5).clamp(0, D)
+        total += int(((zhi - zlo).clamp_min(0) * ok).sum().item())
+    return total
+
+
+def measure_ceilings(device, repeats=5):
+    """Ceilings of this GPU for the gather-bound kernels (csrc/ceilings.cu),
+    best of ``repeats`` launches each, CUDA events on the launching stream:
+    16-byte warp loads served by L1 and by L2 (GB/s), and FFMA warp
+    instructions per second."""
+    import ctypes
+
+    import torch
+
+    from dgc_b200 import _native
+
+    lib = _native.lib()
+    buf = torch.zeros(64 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
+    sink = torch.zeros(4, dtype=torch.float32, device=device)
+    stream = torch.cuda.current_stream(device)
+    out = {}
+
+    def best(launch):
+        rate = 0.0
+        for _ in range(repeats + 1):
+            amount = ctypes.c_double()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            _native.check(launch(ctypes.byref(amount)))
+            b.record(stream)
+            b.synchronize()
+            rate = max(rate, amount.value / (a.elapsed_time(b) * 1e-3))
+        return rate
+
+    for level, key, iters in ((1, "l1_gather_gbs", 16384), (2, "l2_gather_gbs", 4096)):
+        out[key] = best(lambda ref, lv=level, it=iters: lib.dgc_ceiling_gather(
+            buf.data_ptr(), buf.numel() * 4, lv, it, 4, sink.data_ptr(), ref,
+            stream.cuda_stream)) / 1e9
+    out["issue_warp_inst_per_s"] = best(lambda ref: lib.dgc_ceiling_issue(
+        2048, 4, sink.data_ptr(), ref, stream.cuda_stream))
+    out["source"] = ("csrc/ceilings.cu, measured in this run: 16-byte warp loads of 512 "
+                     "contiguous bytes from a 32 KiB (L1) or 64 MiB (L2) buffer in random "
+                     "order; independent FFMA chains")
+    del buf
+    return out
+
+
 # ------------------------------------------------------------- CPU baseline
 
 
-def cpu_baseline_sample(vol_np, geom_np, threads=None, fwd_rays=None, filt_views=1, slab=4,
-                        bp_views=None):
+def cpu_baseline_sample(vol_np, geom_np, threads=None, fwd_views=(0,), ray_stride=1, filt_views=1,
+                        slab=4, bp_views=None):
     """Time the FP64 oracle (a port of the reference's CPU checks) on a bounded sample.
 
-    Sample: the forward projection of the first ``fwd_rays`` rays of view 0
-    (default one full view), the FDK filter of ``filt_views`` views, and the
+    Sample: the forward projection of every ``ray_stride``-th ray of views
+    ``fwd_views``, the FDK filter of ``filt_views`` views, and the
     backprojection of a ``slab``-slice z-slab over the first ``bp_views``
-    views (default all).  Each part is scaled to the full step by its share of
-    the work.  Returns (seconds per full step, threads used, description).
+    views (default all).  Each part is scaled to the full step by its share
+    of the work.  Returns (seconds per full step, threads used, description,
+    fraction of the step's work computed).
     """
     import numpy as np
 
@@ -242,12 +364,13 @@ def cpu_baseline_sample(vol_np, geom_np, threads=None, fwd_rays=None, filt_views
         oracle.set_num_threads(threads)
     w = WORKLOAD
     A, U, V = w["A"], w["U"], w["V"]
-    fwd_rays = U * V if fwd_rays is None else int(fwd_rays)
     bp_views = A if bp_views is None else int(bp_views)
+    rays = np.concatenate([np.arange(a * U * V, (a + 1) * U * V, ray_stride, dtype=np.int64)
+                           for a in fwd_views])
     t0 = time.perf_counter()
-    rays = np.arange(0, fwd_rays, dtype=np.int64)
     oracle.project_rays(vol_np, geom_np, w["pixel"], U, V, w["step"], w["voxel"], rays, mode=1)
-    t_fwd = (time.perf_counter() - t0) * (A * U * V / fwd_rays)
+    fwd_share = rays.size / (A * U * V)
+    t_fwd = (time.perf_counter() - t0) / fwd_share
     proj_part = np.ones((filt_views, U, V), np.float32)
     t0 = time.perf_counter()
     filt = oracle.fdk_filter(proj_part, w["pixel"], geom_np[2][:filt_views],
@@ -258,11 +381,23 @@ def cpu_baseline_sample(vol_np, geom_np, threads=None, fwd_rays=None, filt_views
     # the central slab: slab voxel z' sits where full-volume voxel D/2 - slab/2 + z' does
     oracle.backproject(proj_all, [g[:bp_views] for g in geom_np], w["pixel"],
                        (slab, w["H"], w["W"]), w["voxel"], offset=(0.0, 0.0, 0.0))
-    t_bp = (time.perf_counter() - t0) * (w["D"] / slab) * (A / bp_views)
-    desc = (f"FP64 oracle on {oracle.num_threads()} threads: forward of {fwd_rays} rays of one "
-            f"view, filter of {filt_views} view(s), backprojection of a {slab}-slice slab over "
-            f"{bp_views} views; each scaled to the full step")
-    return t_fwd + t_filt + t_bp, oracle.num_threads(), desc
+    bp_share = (slab / w["D"]) * (bp_views / A)
+    t_bp = (time.perf_counter() - t0) / bp_share
+    t_step = t_fwd + t_filt + t_bp
+    # fraction of the step computed, weighting each part by its share of the
+    # full step's CPU time
+    fraction = (t_fwd * fwd_share + t_filt * filt_views / A + t_bp * bp_share) / t_step
+    desc = (f"FP64 oracle on {oracle.num_threads()} threads: forward of every {ray_stride}-th ray "
+            f"of {len(fwd_views)} view(s) ({rays.size} rays), filter of {filt_views} view(s), "
+            f"backprojection of a {slab}-slice slab over {bp_views} views; each part timed and "
+            f"scaled by its share of the full step")
+    return t_step, oracle.num_threads(), desc, fraction
+
+
+def host_threads():
+    import torch
+
+    return {"os_cpu_count": os.cpu_count(), "torch_num_threads": torch.get_num_threads()}
 
 
 # ------------------------------------------------------------------------ arms
@@ -274,26 +409,29 @@ def run_reference(args):
     if rank != 0:
         return 0
     import numpy as np
-    import torch
 
     w = WORKLOAD
     # the same phantom as the GPU arm, generated on the CPU
     from dgc_b200.phantoms import circular_geometry, ellipsoid_phantom
 
     vol = ellipsoid_phantom((w["D"], w["H"], w["W"]), n=w["ellipsoids"], seed=instance_seed(0),
-                            voxel_size=w["voxel"], device="cpu").numpy()
+                            voxel_size=w["voxel"], device="cpu", axis_range=axis_range(w)).numpy()
     geom = [g.numpy().astype(np.float64) for g in
             circular_geometry(w["A"], w["U"], w["V"], w["sid"], w["sod"], w["pixel"], device="cpu")]
-    # a small sample per step (a few seconds of host work), so that the
-    # driver's --steps/--warmup run ends within minutes
-    sample = dict(fwd_rays=w["U"] * w["V"] // 2, filt_views=1, slab=2, bp_views=w["A"] // 2)
-    for _ in range(args.warmup):
-        cpu_baseline_sample(vol, geom, **sample)
-    times = []
+    # a bounded sample per step (about two seconds of host work), so that the
+    # driver's --steps/--warmup run ends within minutes; each step samples a
+    # different view
+    big = w["D"] >= 512
+    sample = dict(ray_stride=4 if big else 2, filt_views=1, slab=2, bp_views=w["A"] // 2)
+    for i in range(args.warmup):
+        cpu_baseline_sample(vol, geom, fwd_views=(i % w["A"],), **sample)
+    times, fractions = [], []
     threads, desc = 1, ""
-    for _ in range(args.steps):
-        t, threads, desc = cpu_baseline_sample(vol, geom, **sample)
+    for i in range(args.steps):
+        view = (37 * (i + 1)) % w["A"]
+        t, threads, desc, frac = cpu_baseline_sample(vol, geom, fwd_views=(view,), **sample)
         times.append(t)
+        fractions.append(frac)
     t_step = sum(times) / len(times)
     rays = w["A"] * w["U"] * w["V"]
     value = rays / t_step / 1e9
@@ -301,13 +439,16 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_step * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": {"workload": w["name"]},
+        "data": "synthetic", "config": {"workload": w["name"], "volume": [w["D"], w["H"], w["W"]],
+                                        "views": w["A"], "detector": [w["U"], w["V"]]},
+        "sample_fraction": statistics.mean(fractions),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": desc},
+                         "sample": desc + "; one such sample per step, its time scaled to the "
+                                          "full step (sample_fraction = share computed)",
+                         **host_threads()},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
-    del torch
     return 0
 
 
@@ -316,6 +457,7 @@ def run_ours(args):
     import torch
 
     from dgc_b200 import _native, _ops
+    from dgc_b200.sharded import view_shard
 
     world, rank, local = dist_env()
     if not torch.cuda.is_available():
@@ -324,17 +466,30 @@ def run_ours(args):
     device = torch.device("cuda", local)
     dist = init_dist(world, "nccl")
     w = WORKLOAD
-    vol, geom = make_instance(device, instance_seed(rank))
-    R = w["A"] * w["U"] * w["V"]
-    N = w["D"] * w["H"] * w["W"] * w["A"]
+    sharded = args.workload == "fdk-sharded"
+    # fdk-sharded: one object (same seed on every rank), this rank's views;
+    # otherwise an object per rank with all views
+    vol, geom = make_instance(device, instance_seed(0 if sharded else rank))
+    run_step = step
+    if sharded:
+        views = view_shard(w["A"], world, rank)
+        geom = [g[views.start:views.stop].contiguous() for g in geom]
+        run_step = sharded_step
+    A_local = geom[0].numel()
+    R_local = A_local * w["U"] * w["V"]
+    R_job = w["A"] * w["U"] * w["V"] * (1 if sharded else world)
+    N_local = w["D"] * w["H"] * w["W"] * A_local
     counts = _ops.project_sample_counts((w["D"], w["H"], w["W"]), geom, w["pixel"], w["U"], w["V"],
                                         w["step"], w["voxel"])
     S = int(counts.sum().item())
     del counts
+    n_valid = backprojection_valid_count(geom, (w["D"], w["H"], w["W"]), w["pixel"], w["voxel"],
+                                         w["U"], w["V"])
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
+    ceilings = measure_ceilings(device)
 
     for _ in range(max(args.warmup, 1)):
-        step(vol, geom)
+        run_step(vol, geom)
     torch.cuda.synchronize(device)
 
     # ---- device-resident timed region
@@ -347,7 +502,7 @@ def run_ours(args):
         for i in range(args.steps):
             flush.zero_()  # L2 flush between timed steps (outside the events)
             starts[i].record()
-            step(vol, geom)
+            run_step(vol, geom)
             stops[i].record()
         torch.cuda.synchronize(device)
     if dist is not None:
@@ -355,15 +510,15 @@ def run_ours(args):
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, stops)]
     total_ms = max_over_ranks(sum(step_ms), dist, device)
     ms_per_step = total_ms / args.steps
-    value = world * R * args.steps / (total_ms * 1e-3) / 1e9
+    value = R_job * args.steps / (total_ms * 1e-3) / 1e9
     kern = {}
     for name, ms in tr.records:
         kern.setdefault(name, []).append(ms)
     launches = len(tr.records)
-    fwd_ms = statistics.mean(kern["fp_forward_kernel"])
-    bp_ms = statistics.mean(kern["bp_forward_kernel<fdk>"])
-    fwd_ms = max_over_ranks(fwd_ms, dist, device)
-    bp_ms = max_over_ranks(bp_ms, dist, device)
+    fwd_ms = max_over_ranks(statistics.mean(kern["fp_forward_kernel"]), dist, device)
+    bp_key = "bp_forward_kernel<fdk>" if "bp_forward_kernel<fdk>" in kern else \
+        "bp_forward_kernel<fdk-partial>"
+    bp_ms = max_over_ranks(statistics.mean(kern[bp_key]), dist, device) if bp_key in kern else None
 
     # ---- end to end through the public API with host buffers
     vol_host = vol.cpu().pin_memory()
@@ -373,7 +528,7 @@ def run_ours(args):
     vol_dev = torch.empty_like(vol)
     for _ in range(max(1, min(args.warmup, 2))):
         vol_dev.copy_(vol_host, non_blocking=True)
-        _, r = step(vol_dev, geom)
+        _, r = run_step(vol_dev, geom)
         out_host.copy_(r, non_blocking=True)
     torch.cuda.synchronize(device)
     if dist is not None:
@@ -382,13 +537,13 @@ def run_ours(args):
         flush.zero_()
         e_start[i].record()
         vol_dev.copy_(vol_host, non_blocking=True)
-        _, r = step(vol_dev, geom)
+        _, r = run_step(vol_dev, geom)
         out_host.copy_(r, non_blocking=True)
         e_stop[i].record()
     torch.cuda.synchronize(device)
     serial_ms = max_over_ranks(sum(s.elapsed_time(e) for s, e in zip(e_start, e_stop)), dist,
                                device)
-    serial_value = world * R * args.steps / (serial_ms * 1e-3) / 1e9
+    serial_value = R_job * args.steps / (serial_ms * 1e-3) / 1e9
 
     # ---- the same K steps as a stream of jobs: step i+1's volume upload and
     # step i-1's reconstruction download run on a copy stream while step i
@@ -419,7 +574,7 @@ def run_ours(args):
                     uploaded[nb].record(copy)
             flush.zero_()
             cur.wait_event(uploaded[b])
-            _, r = step(bufs[b], geom)
+            _, r = run_step(bufs[b], geom)
             consumed[b].record(cur)
             with torch.cuda.stream(copy):
                 copy.wait_event(consumed[b])
@@ -437,32 +592,53 @@ def run_ours(args):
     pipelined(args.steps, p_start, p_stop)
     torch.cuda.synchronize(device)
     e2e_ms = max_over_ranks(p_start.elapsed_time(p_stop), dist, device)
-    e2e_value = world * R * args.steps / (e2e_ms * 1e-3) / 1e9
+    e2e_value = R_job * args.steps / (e2e_ms * 1e-3) / 1e9
     nbytes = vol.numel() * 4
 
-    # ---- roofline of the dominant kernel (forward projector)
-    peak, peak_kind = measured_peak_hbm()
-    alg_bytes = 32 * S + 4 * R  # trilinear gathers + projection writes per launch
-    achieved = alg_bytes / (fwd_ms * 1e-3) / 1e9
-    roofline = {"bound": "hbm", "kernel": "fp_forward_kernel", "achieved": achieved, "peak": peak,
-                "unit": "GB/s", "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",
-                "traffic": FWD_DRAM_BYTES_PER_LAUNCH, "algorithmic_bytes": alg_bytes,
-                "samples": S, "ms": fwd_ms}
+    # ---- rooflines: algorithmic bytes per launch over the kernel's average
+    # duration, against the L1 ceiling of 16-byte gathers measured above
+    hbm_peak, hbm_kind = measured_peak_hbm()
+    l1 = ceilings["l1_gather_gbs"]
+    fwd_bytes = 32 * S + 4 * R_local  # two 16-byte quads per sample + projection writes
+    fwd_gbs = fwd_bytes / (fwd_ms * 1e-3) / 1e9
+    traffic = FWD_DRAM_BYTES.get(w.get("key", ""))
+    if traffic is not None and sharded:
+        traffic = traffic * A_local / w["A"]
+    roofline = {"bound": "l1", "kernel": "fp_forward_kernel", "achieved": fwd_gbs, "peak": l1,
+                "unit": "GB/s", "frac": fwd_gbs / l1,
+                "peak_source": "l1_gather_gbs of this run's ceilings (csrc/ceilings.cu)",
+                "traffic": traffic, "algorithmic_bytes": fwd_bytes, "samples": S, "ms": fwd_ms,
+                "l2_frac": fwd_gbs / ceilings["l2_gather_gbs"],
+                "dram_gbs": None if traffic is None else traffic / (fwd_ms * 1e-3) / 1e9,
+                "hbm_peak_gbs": hbm_peak, "hbm_peak_source": f"{hbm_kind} hbm_gbs"}
+    rooflines = {"fp_forward_kernel": {k: roofline[k] for k in ("achieved", "frac", "ms")}}
+    bp_bytes = 16 * n_valid + 4 * w["D"] * w["H"] * w["W"] + 4 * R_local
+    if bp_ms is not None:
+        bp_gbs = bp_bytes / (bp_ms * 1e-3) / 1e9
+        rooflines[bp_key] = {"bound": "l1", "achieved": bp_gbs, "frac": bp_gbs / l1, "ms": bp_ms,
+                             "algorithmic_bytes": bp_bytes, "valid_voxel_views": n_valid}
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "scaling": "strong" if sharded else "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
         "config": {"workload": w["name"], "volume": [w["D"], w["H"], w["W"]],
                    "views": w["A"], "detector": [w["U"], w["V"]], "sid": w["sid"], "sod": w["sod"],
-                   "step": w["step"], "ellipsoids": w["ellipsoids"],
-                   "l2": "flushed between timed steps (256 MiB write)",
-                   "parallelism": f"independent objects x{world}"},
-        "fwd_grays_per_s": world * R / (fwd_ms * 1e-3) / 1e9,
-        "backproj_gvoxel_views_per_s": world * N / (bp_ms * 1e-3) / 1e9,
+                   "step": w["step"], "pixel": w["pixel"], "voxel": w["voxel"],
+                   "ellipsoids": w["ellipsoids"], "semi_axes_voxels": list(axis_range(w)),
+                   "l2": "flushed between timed steps (256 MiB write); inputs exceed L2",
+                   "parallelism": (f"views split over {world} ranks, one all-reduce of the "
+                                   f"volume per step" if sharded else
+                                   f"independent objects x{world}")},
+        "fwd_grays_per_s": world * R_local / (fwd_ms * 1e-3) / 1e9,
+        "backproj_gvoxel_views_per_s": None if bp_ms is None else
+        world * N_local / (bp_ms * 1e-3) / 1e9,
         "kernel_ms": {k: statistics.mean(v) for k, v in kern.items()},
         "gpu_launches": launches,
         "roofline": roofline,
+        "rooflines": rooflines,
+        "ceilings": ceilings,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": nbytes,
                 "d2h_bytes_per_step": nbytes, "ms_per_step": e2e_ms / args.steps,
                 "transfers": "volume upload and reconstruction download of every step, on a "
@@ -473,9 +649,11 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         vol_np = vol.cpu().numpy()
         geom_np = [g.cpu().numpy().astype(np.float64) for g in geom]
-        t_cpu, threads, desc = cpu_baseline_sample(vol_np, geom_np)
-        line["cpu_baseline"] = {"value": R / t_cpu / 1e9, "unit": UNIT, "cores": threads,
-                                "kind": "port", "sample": desc}
+        t_cpu, threads, desc, frac = cpu_baseline_sample(
+            vol_np, geom_np, fwd_views=(0, w["A"] // 3), ray_stride=1, filt_views=2, slab=4)
+        line["cpu_baseline"] = {"value": w["A"] * w["U"] * w["V"] / t_cpu / 1e9, "unit": UNIT,
+                                "cores": threads, "kind": "port", "sample": desc,
+                                "sample_fraction": frac, **host_threads()}
     if rank == 0:
         print(json.dumps(line))
     if dist is not None:

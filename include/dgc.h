@@ -476,6 +476,28 @@ int dgc_trace_get(int index, char* name, int name_len, float* ms);
 /* Drop all records. */
 void dgc_trace_clear(void);
 
+/* ---------------------------------------------------------------------- */
+/* Ceilings (no counterpart in the reference; measurement support)          */
+/* ---------------------------------------------------------------------- */
+
+/* Launches one pass of 16-byte loads on every SM (ctas_per_sm CTAs of 256
+ * threads per SM, `iterations` loads per thread, a multiple of 8): each warp
+ * load covers 512 contiguous bytes, groups in a random order.  level 1: the
+ * groups of a 32 KiB window of `buffer` (resident in every SM's L1); level 2:
+ * of the largest power-of-two prefix of `buffer` (at least 16 MiB; made far
+ * larger than an SM's L1 and smaller than L2, its loads are served by L2).
+ * *bytes receives the bytes the launch loads (16 per lane and load), for a
+ * rate over the caller's event timing.  `buffer` should be zeroed; `sink` is
+ * a float that the kernel never writes for zeroed input. */
+int dgc_ceiling_gather(const void* buffer, size_t buffer_bytes, int level, int iterations,
+                       int ctas_per_sm, float* sink, double* bytes, void* stream);
+
+/* Launches independent FFMA chains on every SM (ctas_per_sm CTAs of 256
+ * threads per SM, 128 FFMA per iteration and thread); *warp_instructions
+ * receives the FFMA warp instructions of the launch. */
+int dgc_ceiling_issue(int iterations, int ctas_per_sm, float* sink, double* warp_instructions,
+                      void* stream);
+
 #ifdef __cplusplus
 }
 #endif

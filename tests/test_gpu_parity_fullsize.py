@@ -1,0 +1,396 @@
+"""Value parity at the benchmark sizes: the reference's own CUDA and the FP64 oracle.
+
+Two sizes:
+
+* config 2 -- a 256^3 phantom of 12 random ellipsoids (1 mm voxels), 360
+  views over 2 pi, a 384^2 detector of 1 mm pixels, sid 1000, sod 600, step
+  0.5.  The projector and its backward run at a config-3 geometry (nominal +
+  per-view perturbations: angle 0.3 deg, sources 1 mm, detector centre 2 px,
+  sid/sod 0.5 %), with the upstream gradient of config 3's loss
+  ``mean((p - m)^2)`` against a projection ``m`` at another perturbation;
+* the target size -- 512^3, 720 views, 768^2 (same distances and pixels).
+
+Against the reference's CUDA kernels (built unmodified from its sources into
+``oracle/_ref``; ``src_cbct_forwardprojector_cuda.cu:258-528``,
+``src_cbct_backprojector_cuda.cu:15-295``) the bars are rel-L2 1e-5 for
+projections, backprojections and reconstructions and 1e-4 for gradients.
+``reconstruct_fdk`` is compared with the reference's pipeline
+(``filtering.py:107-198``): its FFT ramp filter restated below with
+``torch.fft`` on the GPU, the reference's CUDA backprojector over chunks of
+32 views, then ``* pi/A`` and the clamp.
+
+Against the FP64 oracle (same bars) on subsets it finishes in seconds: whole
+views of rays (sample positions of the FP32 kernels, oracle ``mode=1``) with
+their volume and geometry gradients, a slab of depth rows of the
+backprojection and of its gradients, a few views of the filter.
+
+Each test also appends its measured errors as one JSON line to the file named
+by ``DGC_PARITY_LOG``, when that variable is set.
+"""
+
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import GEOM_NAMES, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+SID, SOD, PX, STEP, VOX = 1000.0, 600.0, 1.0, 0.5, 1.0
+FWD_RTOL = 1e-5
+GRAD_RTOL = 1e-4
+ORIGIN = (0.0, 0.0, 0.0)
+
+
+def log(record):
+    path = os.environ.get("DGC_PARITY_LOG")
+    if path:
+        with open(path, "a") as f:
+            f.write(json.dumps(record) + "\n")
+    print(json.dumps(record))
+
+
+def view(geom, ks):
+    """The eight geometry arrays of views ``ks`` as FP64 numpy (oracle input)."""
+    return [g.detach()[ks].double().cpu().numpy() for g in geom]
+
+
+def rel(a, b):
+    return rel_l2(torch.as_tensor(a).double().cpu().numpy() if torch.is_tensor(a) else a,
+                  torch.as_tensor(b).double().cpu().numpy() if torch.is_tensor(b) else b)
+
+
+def make_case(D, A, U, seed):
+    from dgc_b200.calibration import perturb_geometry
+    from dgc_b200.phantoms import circular_geometry, ellipsoid_phantom
+
+    vol = ellipsoid_phantom((D, D, D), n=12, seed=seed, device="cuda",
+                            axis_range=(10.0 * D / 256, 80.0 * D / 256))
+    nominal = circular_geometry(A, U, U, SID, SOD, PX, device="cuda")
+    return dict(vol=vol, nominal=nominal, geom=perturb_geometry(nominal, seed + 100),
+                other=perturb_geometry(nominal, seed + 200), D=D, A=A, U=U)
+
+
+def reference_filter(p, px, sod, sid, alpha=0.8):
+    """filtering.py:82-104 (the reference's fdk_filter), restated with torch.fft
+    on the GPU in FP32: centred cosine preweight, zero padding along U to
+    2^bitlen(2U-1), the DFT of the discrete Ram-Lak kernel (real part) times
+    the Hann window, inverse transform, crop, * pixel * sid/sod."""
+    A, U, V = p.shape
+    dev = p.device
+    u = (torch.arange(U, device=dev, dtype=torch.float32) - (U - 1) / 2) * px
+    v = (torch.arange(V, device=dev, dtype=torch.float32) - (V - 1) / 2) * px
+    sid3, sod3 = sid.view(-1, 1, 1), sod.view(-1, 1, 1)
+    dist = torch.sqrt(sid3.square() + u.view(1, -1, 1).square() + v.view(1, 1, -1).square())
+    P = 1 << (2 * U - 1).bit_length()
+    n = torch.arange(P, device=dev)
+    n = torch.where(n > P // 2, n - P, n)
+    ramp = torch.zeros(P, device=dev, dtype=torch.float32)
+    ramp[0] = 1.0 / (4.0 * px * px)
+    odd = n % 2 != 0
+    ramp[odd] = -1.0 / (math.pi * n[odd].float() * px).square()
+    response = torch.fft.rfft(ramp).real
+    f = torch.arange(P // 2 + 1, device=dev, dtype=torch.float32) / P
+    hann = torch.where(f <= alpha * 0.5, 0.5 + 0.5 * torch.cos(2.0 * math.pi * f / alpha),
+                       torch.zeros_like(f))
+    spec = torch.fft.rfft(p * (sid3 / dist), n=P, dim=1) * (response * hann).view(1, -1, 1)
+    return torch.fft.irfft(spec, n=P, dim=1)[:, :U, :] * px * (sid3 / sod3)
+
+
+def reference_reconstruct(ref_bp, p, geom, shape, chunk=32):
+    """filtering.py:107-198's loop: filter and backproject chunks of views
+    (reference CUDA backprojector), sum, * pi/A, clamp at zero."""
+    A = p.shape[0]
+    vol = torch.zeros(shape, device=p.device)
+    for s in range(0, A, chunk):
+        e = min(s + chunk, A)
+        g = [x[s:e].contiguous() for x in geom]
+        filt = reference_filter(p[s:e], PX, g[2], g[1]).contiguous()
+        vol += ref_bp.forward(filt, *g, PX, *shape, VOX, *ORIGIN)
+    return (vol * (math.pi / A)).clamp_min(0.0)
+
+
+def geometry_errors(ours, theirs):
+    return {name: rel(a, b) for name, a, b in zip(GEOM_NAMES, ours, theirs)}
+
+
+# --------------------------------------------------------------------- config 2
+
+
+@pytest.fixture(scope="module")
+def cfg2():
+    return make_case(256, 360, 384, seed=2)
+
+
+def test_config2_projection_and_gradients(cfg2, ref_native, oracle):
+    from cbct_backprojector import project
+
+    ref_fp, _ = ref_native
+    c = cfg2
+    U = V = c["U"]
+    vol = c["vol"].clone().requires_grad_()
+    geom = [g.clone().requires_grad_() for g in c["geom"]]
+    p = project(vol, *geom, PX, U, V, step_size=STEP, voxel_size=VOX)
+    with torch.no_grad():
+        m = project(c["vol"], *c["other"], PX, U, V, step_size=STEP, voxel_size=VOX)
+    up = (2.0 * (p.detach() - m) / p.numel()).contiguous()
+    ours = torch.autograd.grad(p, [vol, *geom], grad_outputs=up)
+    theirs_p = ref_fp.forward(c["vol"], *c["geom"], PX, U, V, STEP, VOX, *ORIGIN)
+    theirs = ref_fp.backward(up, c["vol"], *c["geom"], PX, STEP, VOX, True, *ORIGIN)
+    torch.cuda.synchronize()
+    rec = {"case": "config2 project", "vs_reference": {"projection": rel(p.detach(), theirs_p),
+                                                       "grad_volume": rel(ours[0], theirs[0]),
+                                                       **geometry_errors(ours[1:], theirs[1:])}}
+    # FP64 oracle on whole views: projection values and the per-view geometry gradients
+    ks = [37, 151, 299]
+    vol_np = c["vol"].double().cpu().numpy()
+    truth_p = oracle.project(vol_np, view(c["geom"], ks), PX, U, V, STEP, VOX, mode=1)
+    _, truth_g = oracle.project_backward(up[ks].cpu().numpy(), vol_np, view(c["geom"], ks), PX,
+                                         STEP, VOX, mode=1, compute_grad_volume=False)
+    ours_g = [g[ks] for g in ours[1:]]
+    rec["vs_oracle"] = {"projection": rel(p.detach()[ks], truth_p),
+                        **geometry_errors(ours_g, list(truth_g))}
+    # volume gradient of one view against the oracle's (the same view alone on the GPU)
+    k = ks[0]
+    vol1 = c["vol"].clone().requires_grad_()
+    p1 = project(vol1, *[g.detach()[k:k + 1] for g in c["geom"]], PX, U, V, step_size=STEP,
+                 voxel_size=VOX)
+    (gv1,) = torch.autograd.grad(p1, [vol1], grad_outputs=up[k:k + 1])
+    truth_gv, _ = oracle.project_backward(up[k:k + 1].cpu().numpy(), vol_np, view(c["geom"], [k]),
+                                          PX, STEP, VOX, mode=1)
+    rec["vs_oracle"]["grad_volume_one_view"] = rel(gv1, truth_gv)
+    log(rec)
+    r, o = rec["vs_reference"], rec["vs_oracle"]
+    assert r["projection"] < FWD_RTOL and o["projection"] < FWD_RTOL
+    assert o["grad_volume_one_view"] < GRAD_RTOL and r["grad_volume"] < GRAD_RTOL
+    for name in GEOM_NAMES:
+        assert o[name] < GRAD_RTOL, (name, o[name])
+        assert r[name] < GRAD_RTOL, (name, r[name])
+
+
+def test_config2_backprojection_and_gradients(cfg2, ref_native, oracle):
+    from cbct_backprojector import backproject, project
+    from dgc_b200.sharded import slab_offset
+
+    _, ref_bp = ref_native
+    c = cfg2
+    D, U = c["D"], c["U"]
+    shape = (D, D, D)
+    with torch.no_grad():
+        q0 = project(c["vol"], *c["geom"], PX, U, U, step_size=STEP, voxel_size=VOX)
+    q = q0.clone().requires_grad_()
+    geom = [g.clone().requires_grad_() for g in c["geom"]]
+    vol = backproject(q, *geom, PX, shape, VOX)
+    w = (c["vol"] - 0.1).contiguous()
+    ours = torch.autograd.grad(vol, [q, *geom], grad_outputs=w)
+    theirs_v = ref_bp.forward(q0, *c["geom"], PX, *shape, VOX, *ORIGIN)
+    theirs = ref_bp.backward(w, q0, *c["geom"], PX, VOX, *ORIGIN)
+    torch.cuda.synchronize()
+    rec = {"case": "config2 backproject", "vs_reference": {
+        "volume": rel(vol.detach(), theirs_v), "grad_projections": rel(ours[0], theirs[0]),
+        **geometry_errors(ours[1:], theirs[1:])}}
+    # FP64 oracle on a slab of 4 depth rows: values, and the gradients of an
+    # upstream gradient that is zero outside the slab
+    rows = range(120, 124)
+    off = slab_offset(shape, VOX, ORIGIN, rows)
+    q_np = q0.double().cpu().numpy()
+    g_np = view(c["geom"], slice(None))
+    truth_v = oracle.backproject(q_np, g_np, PX, (len(rows), D, D), VOX, off)
+    w_slab = torch.zeros_like(w)
+    w_slab[rows.start:rows.stop] = w[rows.start:rows.stop]
+    ours_slab = torch.autograd.grad(backproject(q, *geom, PX, shape, VOX), [q, *geom],
+                                    grad_outputs=w_slab)
+    truth_gp, truth_gg = oracle.backproject_backward(w[rows.start:rows.stop].cpu().numpy(), q_np,
+                                                     g_np, PX, VOX, off)
+    rec["vs_oracle"] = {"volume_slab": rel(vol.detach()[rows.start:rows.stop], truth_v),
+                        "grad_projections_slab": rel(ours_slab[0], truth_gp),
+                        **geometry_errors(ours_slab[1:], list(truth_gg))}
+    log(rec)
+    r, o = rec["vs_reference"], rec["vs_oracle"]
+    assert r["volume"] < FWD_RTOL and o["volume_slab"] < FWD_RTOL
+    assert r["grad_projections"] < GRAD_RTOL and o["grad_projections_slab"] < GRAD_RTOL
+    for name in GEOM_NAMES:
+        assert o[name] < GRAD_RTOL, (name, o[name])
+        assert r[name] < GRAD_RTOL, (name, r[name])
+
+
+def fdk_parity(c, ref_bp, oracle, views, rows, label):
+    from cbct_backprojector import fdk_filter, project, reconstruct_fdk
+    from dgc_b200.sharded import slab_offset
+
+    D, U = c["D"], c["U"]
+    shape = (D, D, D)
+    g = c["nominal"]
+    with torch.no_grad():
+        p = project(c["vol"], *g, PX, U, U, step_size=STEP, voxel_size=VOX)
+        ours = reconstruct_fdk(p, *g, PX, shape, VOX)
+        theirs = reference_reconstruct(ref_bp, p, g, shape)
+        filt = fdk_filter(p, PX, g[2], g[1])
+        ref_filt = reference_filter(p[views], PX, g[2][views], g[1][views])
+    torch.cuda.synchronize()
+    rec = {"case": f"{label} reconstruct_fdk",
+           "vs_reference": {"volume": rel(ours, theirs), "filter_views": rel(filt[views], ref_filt)}}
+    p_np = p[views].double().cpu().numpy()
+    truth_f = oracle.fdk_filter(p_np, PX, SOD, SID)
+    # the slab from the library's filtered projections (checked just above)
+    off = slab_offset(shape, VOX, ORIGIN, rows)
+    truth_v = oracle.backproject(filt.double().cpu().numpy(), view(g, slice(None)), PX,
+                                 (len(rows), D, D), VOX, off)
+    truth_v = np.maximum(truth_v * (math.pi / c["A"]), 0.0)
+    rec["vs_oracle"] = {"filter_views": rel(filt[views], truth_f),
+                        "volume_slab": rel(ours[rows.start:rows.stop], truth_v)}
+    log(rec)
+    for side in ("vs_reference", "vs_oracle"):
+        for key, err in rec[side].items():
+            assert err < FWD_RTOL, (side, key, err)
+
+
+def test_config2_reconstruct_fdk(cfg2, ref_native, oracle):
+    fdk_parity(cfg2, ref_native[1], oracle, views=[0, 97, 211], rows=range(126, 130),
+               label="config2")
+
+
+def test_config3_loss_gradient_finite_differences_on_32_views(cfg2, oracle):
+    """Config 3's loss at config 2's size: the fused calibration step's
+    geometry gradients (``dgc_project_mse_grad``) against central differences
+    on 32 random views, one parameter each.
+
+    A view's parameters move only that view's rays, so each difference is
+    taken on its view alone (a one-view projection, bitwise the rays of the
+    whole scan) with the whole scan's normalisation.  Rays whose trace (entry
+    face, sample count, cells; FP64 oracle and the kernel's own counts) a
+    +-eps step changes are masked out of the loss, for the analytic gradient
+    too.  The bound is relative to the summed magnitude of the per-ray
+    contributions, since a view's gradient is a sum of ray terms that largely
+    cancel (ray set-up in FP32, as the reference's)."""
+    from dgc_b200 import _ops, project
+
+    c = cfg2
+    A, U = c["A"], c["U"]
+    vol = c["vol"]
+    with torch.no_grad():
+        meas = project(vol, *c["other"], PX, U, U, step_size=STEP, voxel_size=VOX)
+    nominal, true = c["nominal"], c["other"]
+    geom = [n + 0.7 * (t - n) for t, n in zip(true, nominal)]
+    rng = np.random.default_rng(0)
+    views = rng.choice(A, 32, replace=False)
+    eps_by_family = [2e-4, 5e-2, 5e-2, 1e-2, 1e-2, 1e-2, 1e-2, 1e-2]
+    keep = torch.ones((A, U, U), device="cuda")
+    steps = {}
+
+    def one_view(g, a):
+        return [x[a:a + 1].contiguous() for x in g]
+
+    def counts(g):
+        return _ops.project_sample_counts(vol.shape, g, PX, U, U, STEP, VOX).cpu().numpy()
+
+    for i, a in enumerate(views):
+        k = i % 8
+        g1 = one_view(geom, a)
+        base = oracle.ray_traces(vol.shape, [x.cpu().numpy() for x in g1], PX, U, U, STEP, VOX,
+                                 mode=1)
+        base_counts = counts(g1)
+        for eps in (eps_by_family[k] / 2**j for j in range(4)):
+            plus = [x.clone() for x in g1]
+            minus = [x.clone() for x in g1]
+            plus[k] += eps
+            minus[k] -= eps
+            tp = oracle.ray_traces(vol.shape, [x.cpu().numpy() for x in plus], PX, U, U, STEP, VOX,
+                                   mode=1)
+            tm = oracle.ray_traces(vol.shape, [x.cpu().numpy() for x in minus], PX, U, U, STEP,
+                                   VOX, mode=1)
+            ok = ((base != 0) & (base == tp) & (base == tm) &
+                  (counts(plus) == base_counts) & (counts(minus) == base_counts))
+            if ok.mean() >= 0.5:
+                break
+        keep[a] = torch.tensor(ok[0].astype(np.float32), device="cuda")
+        steps[int(a)] = (k, plus, minus)
+    denom = float(keep.sum())
+    _, grads, _ = _ops.fp_mse_grad(vol, geom, PX, U, U, STEP, VOX, meas, keep, 1.0 / denom)
+    worst = 0.0
+    checked = 0
+    for a, (k, plus, minus) in steps.items():
+        if float(keep[a].mean()) < 0.5:
+            continue
+        with torch.no_grad():
+            m1, w1 = meas[a:a + 1].double(), keep[a:a + 1].double()
+            p0 = project(vol, *one_view(geom, a), PX, U, U, step_size=STEP).double()
+            pp = project(vol, *plus, PX, U, U, step_size=STEP).double()
+            pm = project(vol, *minus, PX, U, U, step_size=STEP).double()
+            h = float(plus[k] - minus[k])
+            fd = float((((pp - m1).square() - (pm - m1).square()) * w1).sum()) / denom / h
+            scale = float(((2 * (p0 - m1) * (pp - pm) / h).abs() * w1).sum()) / denom
+        analytic = float(grads[k][a])
+        err = abs(analytic - fd) / (scale + 1e-30)
+        worst = max(worst, err)
+        assert abs(analytic - fd) <= 2e-2 * scale + 1e-12, (GEOM_NAMES[k], a, analytic, fd, scale)
+        checked += 1
+    log({"case": "config3 finite differences, 32 views at 256^3 / 360 x 384^2",
+         "checked": checked, "worst_error_over_scale": worst})
+    assert checked >= 28
+
+
+# ------------------------------------------------------------------ target size
+
+
+@pytest.fixture(scope="module")
+def target():
+    return make_case(512, 720, 768, seed=5)
+
+
+def test_target_projection(target, ref_native, oracle):
+    from cbct_backprojector import project
+
+    ref_fp, _ = ref_native
+    c = target
+    U = c["U"]
+    with torch.no_grad():
+        p = project(c["vol"], *c["geom"], PX, U, U, step_size=STEP, voxel_size=VOX)
+    theirs = ref_fp.forward(c["vol"], *c["geom"], PX, U, U, STEP, VOX, *ORIGIN)
+    torch.cuda.synchronize()
+    err_ref = rel(p, theirs)
+    del theirs
+    # FP64 oracle on every 7th ray of two whole views
+    k0, k1 = 101, 530
+    rays = np.concatenate([np.arange(k * U * U, (k + 1) * U * U, 7) for k in (k0, k1)])
+    truth = oracle.project_rays(c["vol"].double().cpu().numpy(), view(c["geom"], slice(None)),
+                                PX, U, U, STEP, VOX, rays, mode=1)
+    err_or = rel(p.reshape(-1)[torch.as_tensor(rays, device="cuda")], truth)
+    log({"case": "target 512^3 / 720 x 768^2 project",
+         "vs_reference": {"projection": err_ref},
+         "vs_oracle": {"projection_rays": err_or, "rays": int(rays.size)}})
+    assert err_ref < FWD_RTOL and err_or < FWD_RTOL
+
+
+def test_target_backprojection(target, ref_native, oracle):
+    from cbct_backprojector import backproject, project
+    from dgc_b200.sharded import slab_offset
+
+    _, ref_bp = ref_native
+    c = target
+    D, U = c["D"], c["U"]
+    shape = (D, D, D)
+    with torch.no_grad():
+        q = project(c["vol"], *c["geom"], PX, U, U, step_size=STEP, voxel_size=VOX)
+        vol = backproject(q, *c["geom"], PX, shape, VOX)
+    theirs = ref_bp.forward(q, *c["geom"], PX, *shape, VOX, *ORIGIN)
+    torch.cuda.synchronize()
+    err_ref = rel(vol, theirs)
+    del theirs
+    rows = range(300, 302)
+    off = slab_offset(shape, VOX, ORIGIN, rows)
+    truth = oracle.backproject(q.double().cpu().numpy(), view(c["geom"], slice(None)), PX,
+                               (len(rows), D, D), VOX, off)
+    err_or = rel(vol[rows.start:rows.stop], truth)
+    log({"case": "target 512^3 / 720 x 768^2 backproject",
+         "vs_reference": {"volume": err_ref}, "vs_oracle": {"volume_slab": err_or}})
+    assert err_ref < FWD_RTOL and err_or < FWD_RTOL
+
+
+def test_target_reconstruct_fdk(target, ref_native, oracle):
+    fdk_parity(target, ref_native[1], oracle, views=[3], rows=range(255, 257),
+               label="target 512^3 / 720 x 768^2")
