@@ -82,8 +82,9 @@ def parse_args(argv=None):
                          "0.1 px, learned warm start vs plain; tour: every kernel once on the "
                          "fdk256 instance (profiler captures); gemm: the tcgen05 GEMM at "
                          "8192^3 and at the network's largest layer shapes")
-    ap.add_argument("--acq", choices=["half", "eval"], default="half",
-                    help="calib: 256^3/360/384^2 (half) or 512^3/720/768^2 (eval)")
+    ap.add_argument("--acq", choices=["half", "eval", "config3"], default="half",
+                    help="calib: 256^3 x 2 mm / 360 / 384^2 x 2 mm (half), 512^3 / 720 / 768^2 "
+                         "(eval) or 256^3 x 1 mm / 360 / 384^2 x 1 mm (config3)")
     ap.add_argument("--max-iterations", type=int, default=300, help="calib: iteration cap")
     ap.add_argument("--instances", type=int, default=64, help="batch64: number of instances")
     ap.add_argument("--batch-set", choices=["config4", "small"], default="config4",
@@ -832,32 +833,63 @@ def run_calib(args):
     0.05 deg RMS angle error: calibration from the network's warm start vs
     from nominal, same GPU, same projector, each arm with its own settings;
     every iteration timed on the host, the warm-start arm's time includes
-    the nominal reprojection and the network inference."""
+    the nominal reprojection and the network inference.  ``--seeds`` held-out
+    stacks (seeds 7, 8, ...; the network was trained on seeds >= 10^6), each
+    with its own clock record; the line gives the median and the range."""
     import torch
 
     from dgc_b200 import warmstart as WS
 
     torch.cuda.set_device(0)
-    acq = WS.HALF if args.acq == "half" else WS.EVAL
+    acq = {"half": WS.HALF, "eval": WS.EVAL, "config3": WS.CONFIG3}[args.acq]
     net, meta = WS.load(WS.default_checkpoint())
-    res = WS.evaluate(net, acq, seed=7, iterations=args.max_iterations, target_mm=0.1 * acq.pixel,
-                      target_angle_deg=0.05, stop_at_target=True)
-    p, n = res["plain"], res["warm_start"]
+    runs = []
+    for k in range(max(1, args.seeds)):
+        seed = 7 + k
+        with ClockSampler(0) as clocks:
+            res = WS.evaluate(net, acq, seed=seed, iterations=args.max_iterations,
+                              target_mm=0.1 * acq.pixel, target_angle_deg=0.05,
+                              stop_at_target=True)
+        res["seed"] = seed
+        res["clocks"] = clocks.summary()
+        runs.append(res)
+
+    def spread(values):
+        vals = [v for v in values if v is not None]
+        if not vals:
+            return None
+        return {"median": statistics.median(vals), "min": min(vals), "max": max(vals),
+                "n": len(vals), "of": len(values)}
+
+    def arm(name, key):
+        return spread([r[name][key] for r in runs])
+
+    summary = {
+        "plain_time_to_0.1px_s": arm("plain", "time_to_px_target_s"),
+        "warm_time_to_0.1px_s": arm("warm_start", "time_to_px_target_s"),
+        "plain_time_to_0.1px_and_0.05deg_s": arm("plain", "time_to_target_s"),
+        "warm_time_to_0.1px_and_0.05deg_s": arm("warm_start", "time_to_target_s"),
+        "speedup_to_0.1px": spread([r["speedup_px_target"] for r in runs]),
+        "speedup_to_0.1px_and_0.05deg": spread([r["speedup"] for r in runs]),
+    }
+    warm = summary["warm_time_to_0.1px_s"]
     line = {
         "metric": "calibration wall time to 0.1 px RMS reprojection error", "unit": "s",
-        "value": n["time_to_px_target_s"], "higher_is_better": False, "n_gpus": 1,
-        "steps": 1, "warmup": 0, "dtype": "f32 (network bf16/fp32)", "data": "synthetic",
-        "vs_baseline": None,
+        "value": None if warm is None else warm["median"], "higher_is_better": False,
+        "n_gpus": 1, "steps": len(runs), "warmup": 0, "dtype": "f32 (network bf16/fp32)",
+        "data": "synthetic", "vs_baseline": None,
         "config": {"workload": f"calibration {acq.volume}^3 x {acq.voxel} mm, {acq.views} views, "
                                f"{acq.detector}^2 x {acq.pixel} mm detector, config-3 "
                                "perturbations, Poisson I0=1e5",
+                   "acquisition": args.acq, "seeds": [r["seed"] for r in runs],
                    "max_iterations": args.max_iterations, "target_px": 0.1,
                    "target_angle_deg": 0.05, "network_training_steps": meta.get("steps")},
-        "plain": p, "warm_start": n,
-        "speedup_to_0.1px": res["speedup_px_target"],
-        "speedup_to_0.1px_and_0.05deg": res["speedup"],
-        "stages": res["stages"], "warm_calibration": res["warm_calibration"],
-        "warm_start_accepted": res["warm_start_accepted"], "inference_s": res["inference_s"],
+        "summary": summary,
+        "runs": [{k: r[k] for k in ("seed", "plain", "warm_start", "speedup_px_target", "speedup",
+                                    "warm_start_accepted", "inference_s", "clocks")}
+                 for r in runs],
+        "stages": runs[0]["stages"], "warm_calibration": runs[0]["warm_calibration"],
+        "clocks": runs[-1]["clocks"],
     }
     print(json.dumps(line))
     return 0
@@ -919,14 +951,16 @@ def run_tour(args):
         one_pass()
     torch.cuda.synchronize()
     kern = {}
-    for _ in range(max(1, args.steps)):
-        with _native.trace() as tr:
-            one_pass()
-            torch.cuda.synchronize()
-        kern = {}
-        for name, ms in tr.records:
-            kern[name] = round(kern.get(name, 0.0) + ms, 4)
-    print(json.dumps({"workload": "tour: " + w["name"], "kernel_ms": kern}))
+    with ClockSampler(0) as clocks:
+        for _ in range(max(1, args.steps)):
+            with _native.trace() as tr:
+                one_pass()
+                torch.cuda.synchronize()
+            kern = {}
+            for name, ms in tr.records:
+                kern[name] = round(kern.get(name, 0.0) + ms, 4)
+    print(json.dumps({"workload": "tour: " + w["name"], "kernel_ms": kern,
+                      "clocks": clocks.summary()}))
     return 0
 
 
@@ -952,6 +986,7 @@ def run_gemm(args):
     shapes = [(8192, 8192, 8192), (360 * 36, 256, 2304), (256, 2304, 360 * 36)]
     out = {}
     g = torch.Generator(device="cuda").manual_seed(0)
+    clocks = ClockSampler(0).__enter__()
     for M, N, K in shapes:
         A = torch.randn(M, K, device="cuda", generator=g).to(torch.bfloat16)
         B = torch.randn(N, K, device="cuda", generator=g).to(torch.bfloat16)
@@ -976,8 +1011,9 @@ def run_gemm(args):
         out[f"{M}x{N}x{K}"] = {"ms": ms, "tflops": tf, "kernels": sorted({n for n, _ in tr.records}),
                                "frac_of_measured_peak":
                                None if peak is None else tf / peak, "max_abs_err": err}
+    clocks.__exit__(None, None, None)
     print(json.dumps({"workload": "tcgen05 bf16 GEMM", "peak_bf16_tflops": peak,
-                      "peak_source": peak_source, "shapes": out}))
+                      "peak_source": peak_source, "shapes": out, "clocks": clocks.summary()}))
     return 0
 
 

@@ -89,6 +89,9 @@ TRAIN = Acquisition(volume=128, voxel=4.0, views=180, detector=256, pixel=3.0)
 EVAL = Acquisition(volume=512, voxel=1.0, views=720, detector=768, pixel=1.0)
 # the same physical scan at half resolution (benchmark-sized)
 HALF = Acquisition(volume=256, voxel=2.0, views=360, detector=384, pixel=2.0)
+# config 3 as written: 256^3 of 1 mm voxels, 360 views of 384^2 1 mm pixels (a
+# scan of half the physical extent the network was trained on)
+CONFIG3 = Acquisition(volume=256, voxel=1.0, views=360, detector=384, pixel=1.0)
 
 # physical perturbation model (1 sigma)
 PERTURB = dict(angle_deg=0.3, src_mm=1.0, det_mm=2.0, dist_rel=0.005)
@@ -513,6 +516,6 @@ def default_checkpoint():
     return Path(__file__).resolve().parent / "warmstart_weights.pt"
 
 
-__all__ = ["Acquisition", "TRAIN", "EVAL", "HALF", "WarmStartNet", "gemm", "make_stack",
+__all__ = ["Acquisition", "TRAIN", "EVAL", "HALF", "CONFIG3", "WarmStartNet", "gemm", "make_stack",
            "network_input", "predict", "train", "save", "load", "reprojection_loss", "evaluate",
            "GEOMETRY_NAMES", "replace"]
