@@ -21,7 +21,6 @@
 //   * The backward sums the per-voxel terms over Z in four accumulators and
 //     applies the (column, view) chain-rule coefficients once per warp; the
 //     eight per-view gradients are reduced in FP64 in a fixed order.
-#include <cstdio>
 #include <mutex>
 
 #include "common.cuh"
@@ -377,31 +376,9 @@ __global__ void __launch_bounds__(256) bp_reduce_partials_kernel(const double* _
 // without the projection gradient: 45.9 / 28.7 / 21.3 / 28.2 ms,
 // 2.38 / 1.43 / 1.04 / 1.34 ms, 96.0 / 56.2 / 37.1 / 45.6 ms (with it
 // 36.1-36.9 ms at KZ 2-4 for 256^3, 62.0 ms at KZ 4 for 512^3).
-// DGC_BP_KZ=1|2|4|8 overrides both (tuning experiments).
-static int bp_kz_override() {
-    if (const char* e = std::getenv("DGC_BP_KZ")) {
-        const int k = std::atoi(e);
-        if (k == 1 || k == 2 || k == 4 || k == 8) return k;
-    }
-    return 0;
-}
-
-static bool bp_cta_override(int& cx, int& cy) {
-    if (const char* e = std::getenv("DGC_BP_CTA")) {
-        int a = 0, b = 0;
-        if (std::sscanf(e, "%d,%d", &a, &b) == 2 && a >= 1 && b >= 1 && a * b <= kBpMaxWarps) {
-            cx = a;
-            cy = b;
-            return true;
-        }
-    }
-    return false;
-}
-
 // Tile rules registered by the autotuner (dgc_bp_add_tile_rule): the first
 // rule with D <= d_max and A <= a_max applies; a zero field keeps the
-// built-in choice.  Precedence: DGC_BP_KZ / DGC_BP_CTA, then the rules, then
-// the built-in choice.
+// built-in choice.
 namespace {
 struct BpTileRule {
     int d_max, a_max, kz_forward, kz_backward, cta_x, cta_y;
@@ -439,14 +416,12 @@ void bp_clear_tile_rules() {
 }
 
 int bp_kz_forward(int D, int A) {
-    if (const int k = bp_kz_override()) return k;
     BpTileRule r;
     if (bp_rule(D, A, r) && r.kz_forward) return r.kz_forward;
     return D <= 32 ? 1 : 2;
 }
 
 int bp_kz_backward(int D, int A) {
-    if (const int k = bp_kz_override()) return k;
     BpTileRule r;
     if (bp_rule(D, A, r) && r.kz_backward) return r.kz_backward;
     return D <= 32 ? 1 : D <= 64 ? 2 : 4;
@@ -454,7 +429,6 @@ int bp_kz_backward(int D, int A) {
 
 // Column patch of a forward CTA (cx*cy <= kBpMaxWarps); 8 x 1 built in.
 void bp_forward_cta(int D, int A, int& cx, int& cy) {
-    if (bp_cta_override(cx, cy)) return;
     BpTileRule r;
     if (bp_rule(D, A, r) && r.cta_x) {
         cx = r.cta_x;

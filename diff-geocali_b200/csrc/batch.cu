@@ -8,8 +8,8 @@
 //   view[n+1] | fold_block[n+1] | counters[2] |
 //   per instance: quads | partials            | ... |
 //   per instance with a volume gradient: gradient buffer | ...
-// (cell records or the padded volume, by fp_volume_scatter).  The gradient
-// buffers are contiguous, so one memset clears all of them.
+// (level records).  The gradient buffers are contiguous, so one memset
+// clears all of them.
 #include <string>
 #include <vector>
 
@@ -25,12 +25,9 @@ size_t quads_bytes(const dgc_fp_instance& in) {
     return align256(sizeof(float4) * (size_t)(in.D + 2) * (size_t)(in.H + 1) * (size_t)(in.W + 1));
 }
 
-// volume-gradient buffer: cell records or the padded volume (fp_volume_scatter)
+// volume-gradient buffer (level records)
 size_t gpad_bytes(const dgc_fp_instance& in) {
-    const VolumeScatter scatter = fp_volume_scatter();
-    if (fp_record_floats(scatter) > 0)
-        return align256(sizeof(float) * fp_record_buffer_floats(scatter, in.D, in.H, in.W));
-    return align256(sizeof(float) * (size_t)(in.D + 2) * (size_t)(in.H + 2) * (size_t)(in.W + 2));
+    return align256(sizeof(float) * fp_record_buffer_floats(in.D, in.H, in.W));
 }
 
 int tile_fwd(const dgc_fp_instance& in) { return in.tile_forward == 0 ? 8 : in.tile_forward; }
@@ -168,11 +165,9 @@ int dgc_batch_prepare(const dgc_fp_instance* instances, int n, void* workspace,
         inst_off += partials_bytes(in);
         p.projections = in.projections;
         p.grad_projections = in.grad_projections;
-        const VolumeScatter scatter = fp_volume_scatter();
         if (in.grad_volume) {
             p.grad_pad = reinterpret_cast<float*>(base + gpad_off + gpad_total);
             gpad_total += gpad_bytes(in);
-            if (fp_record_floats(scatter) > 0) fp_fill_cell_layout(p);
         }
         b.volume = in.volume;
         b.grad_volume = in.grad_volume;
@@ -181,11 +176,7 @@ int dgc_batch_prepare(const dgc_fp_instance* instances, int n, void* workspace,
         b.tile_fwd = tile_fwd(in);
         b.tile_bwd = tile_bwd(in);
         b.flags = (is_pow2_float(in.voxel_size) ? 0 : kBatchDiv) |
-                  ((in.off_x != 0.0f || in.off_y != 0.0f || in.off_z != 0.0f) ? kBatchOff : 0) |
-                  (scatter == kScatterPairs ? kBatchMerge : 0) |
-                  (scatter == kScatterCells ? kBatchCells : 0) |
-                  (scatter == kScatterLevels ? kBatchLevels : 0) |
-                  (scatter == kScatterRuns ? kBatchRuns : 0);
+                  ((in.off_x != 0.0f || in.off_y != 0.0f || in.off_z != 0.0f) ? kBatchOff : 0);
         b.quad_gx = ceil_div(in.W + 1, 32) * (in.H + 1);
         b.tiles_bwd = fp_tiles_per_view(in.U, in.V, b.tile_bwd);
         host[i] = b;

@@ -48,28 +48,14 @@ size_t quad_volume_bytes(int D, int H, int W) {
     return Workspace::align(sizeof(float4) * (size_t)(D + 2) * (size_t)(H + 1) * (size_t)(W + 1));
 }
 
-size_t padded_volume_bytes(int D, int H, int W) {
-    return Workspace::align(sizeof(float) * (size_t)(D + 2) * (size_t)(H + 2) * (size_t)(W + 2));
-}
-
-// volume-gradient buffer of the selected scatter (fp_volume_scatter)
+// volume-gradient buffer (level records)
 size_t gradient_buffer_bytes(int D, int H, int W) {
-    const VolumeScatter scatter = fp_volume_scatter();
-    if (fp_record_floats(scatter) > 0)
-        return Workspace::align(sizeof(float) * fp_record_buffer_floats(scatter, D, H, W));
-    return padded_volume_bytes(D, H, W);
+    return Workspace::align(sizeof(float) * fp_record_buffer_floats(D, H, W));
 }
 
-// Ray tile of the forward projector: DGC_FP_TILE="tu,wu" overrides the default.
-FpTile forward_tile() {
-    FpTile t{8, 1};
-    if (const char* e = std::getenv("DGC_FP_TILE")) {
-        int tu = 0, wu = 0;
-        if (sscanf(e, "%d,%d", &tu, &wu) == 2) t = FpTile{tu, wu};
-    }
-    return t;
-}
-
+// Ray tile of the forward projector (8 detector columns x 32 rows per CTA):
+// the batched launches take per-instance tiles from the autotuner.
+constexpr FpTile kForwardTile{8, 1};
 constexpr FpTile kBackwardTile{8, 1};
 
 int check_fp_common(int D, int H, int W, int A, int U, int V, float pixel_size, float step_size,
@@ -199,7 +185,7 @@ static int project_impl(const float* volume, int D, int H, int W, const Geometry
     p.projections = projections;
     rc = build_volume_quads(volume, D, H, W, quads, s);
     if (rc != DGC_OK) return rc;
-    return fp_launch_forward(p, forward_tile(), s);
+    return fp_launch_forward(p, kForwardTile, s);
 }
 
 int dgc_project(const float* volume, int D, int H, int W, const float* angles, const float* sid,
@@ -277,10 +263,7 @@ int dgc_project_backward(const float* grad_projection, const float* volume, int 
     const long long tiles = fp_tiles_per_view(U, V, kBackwardTile.tu);
     Workspace ws(workspace, workspace_bytes);
     float4* quads = ws.take<float4>((size_t)(D + 2) * (H + 1) * (W + 1));
-    const VolumeScatter scatter = fp_volume_scatter();
-    const bool records = compute_grad_volume && fp_record_floats(scatter) > 0;
-    const size_t gfloats = records ? fp_record_buffer_floats(scatter, D, H, W)
-                                   : (size_t)(D + 2) * (H + 2) * (W + 2);
+    const size_t gfloats = fp_record_buffer_floats(D, H, W);
     float* gpad = compute_grad_volume ? ws.take<float>(gfloats) : nullptr;
     double* partials = ws.take<double>((size_t)8 * A * tiles);
     if (!quads || !partials || (compute_grad_volume && !gpad)) {
@@ -296,15 +279,12 @@ int dgc_project_backward(const float* grad_projection, const float* volume, int 
     p.partials = partials;
     rc = build_volume_quads(volume, D, H, W, quads, s);
     if (rc != DGC_OK) return rc;
-    if (records) fp_fill_cell_layout(p);
-    p.scatter = scatter;
     if (gpad) DGC_CUDA(cudaMemsetAsync(gpad, 0, sizeof(float) * gfloats, s));
     rc = fp_launch_backward(p, kBackwardTile, compute_grad_volume != 0, s);
     if (rc != DGC_OK) return rc;
     rc = fp_reduce_partials(partials, A, tiles, out, s);
     if (rc != DGC_OK) return rc;
-    if (gpad) return records ? fp_fold_records(scatter, gpad, D, H, W, grad_volume, s)
-                             : fp_fold_gradient(gpad, D, H, W, grad_volume, s);
+    if (gpad) return fp_fold_records(gpad, D, H, W, grad_volume, s);
     return DGC_OK;
 }
 

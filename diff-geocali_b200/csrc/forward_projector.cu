@@ -464,123 +464,22 @@ struct RayGrad {
     float s1x, s1y, s1z, s2x, s2y, s2z;
 };
 
-// Scatter of one trilinear sample's eight weights into the padded gradient,
-// merged across lane pairs first.  The lanes of a warp march 32 consecutive
-// detector rows of one column, so at a given instruction two neighbouring
-// lanes usually sample the same (x, y) cell column at the same or adjacent z:
-// the odd lane then adds its partner's weights that land on its own eight
-// addresses (all eight for the same cell, four for a cell one z above or
-// below) and the even lane leaves those reductions out.  Sums are unchanged
-// (up to float reassociation, as with any atomics); the L2 sees up to half
-// the reductions.  Lanes whose partner is not converged here scatter alone.
-__device__ __forceinline__ void scatter_cell_pairwise(const FpArgs& p, uint32_t gi, float (&lo)[4],
-                                                      float (&hi)[4]) {
-    const unsigned mask = __activemask();
-    const int lane = threadIdx.x & 31;
-    const int partner = lane ^ 1;
-    const bool odd = lane & 1;
-    const uint32_t gpart = __shfl_sync(mask, gi, partner);
-    float plo[4], phi[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        plo[k] = __shfl_sync(mask, lo[k], partner);
-        phi[k] = __shfl_sync(mask, hi[k], partner);
-    }
-    // cell of the odd lane minus cell of the even lane; 0 or +-1 means the
-    // same (x, y) column (z differs by at most D+1 < the x stride D+2)
-    const int d = (int)(odd ? gi - gpart : gpart - gi);
-    const int mode = !((mask >> partner) & 1u) ? 0 : d == 0 ? 1 : d == 1 ? 2 : d == -1 ? 3 : 0;
-    bool emit_lo = true, emit_hi = true;
-    if (odd) {
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            if (mode == 1) {
-                lo[k] += plo[k];
-                hi[k] += phi[k];
-            } else if (mode == 2) {
-                lo[k] += phi[k];  // even lane's z+1 level is this lane's z level
-            } else if (mode == 3) {
-                hi[k] += plo[k];  // even lane's z level is this lane's z+1 level
-            }
-        }
-    } else {
-        emit_lo = mode == 0 || mode == 2;
-        emit_hi = mode == 0 || mode == 3;
-    }
-    float* g = p.grad_pad + gi;
-    const uint32_t off[4] = {0u, p.gz_x, p.gz_y, p.gz_y + p.gz_x};
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        if (emit_lo) red_add_global(g + off[k], lo[k]);
-        if (emit_hi) red_add_global(g + off[k] + 1, hi[k]);
-    }
-}
-
-// The eight weights of a sample into a cell-major buffer of records, RS
-// floats per cell at cell index ci (z stride D+2, so a cell-index difference
-// of +-1 always means the same (x, y) column):
-//   RS = 8 (cells): record ci holds the weights of the corners ci + (dz, dy,
-//     dx) at k = dz*4 + dy*2 + dx -- the sample's z level at o[0..3], its
-//     z+1 level at o[4..7];
-//   RS = 4 (levels): record ci holds the corners ci + (0, dy, dx) at k = dy*2
-//     + dx, so the sample's z+1 level is the next record, again at o[4..7].
-// fold_record_voxel sums the records onto the voxels.  Lane pairs merge first,
-// as in scatter_cell_pairwise: the same cell gives one 16-byte reduction per
-// lane (even lane the z level, odd lane z+1), cells adjacent in z give three
-// (the corners the two share go to the upper cell's z level, o[0..3] of its
-// record), other pairs four.
-template <int RS>
-__device__ __forceinline__ void scatter_cell_records(const FpArgs& p, uint32_t ci, f32x2 (&lo)[2],
-                                                     f32x2 (&hi)[2]) {
-    static_assert(RS == 8 || RS == 4, "records of 8 (cells) or 4 (levels) floats");
-    const unsigned mask = __activemask();
-    const int lane = threadIdx.x & 31;
-    const int partner = lane ^ 1;
-    const bool odd = lane & 1;
-    const uint32_t cpart = __shfl_sync(mask, ci, partner);
-    // cell of the odd lane minus cell of the even lane
-    const int d = (int)(odd ? ci - cpart : cpart - ci);
-    const int mode = !((mask >> partner) & 1u) ? 0 : d == 0 ? 1 : d == 1 ? 2 : d == -1 ? 3 : 0;
-    const bool m1 = mode == 1, m2 = mode == 2, m3 = mode == 3;
-    // Each lane needs at most one level of its partner, so each sends one:
-    // mode 1 (same cell): the even lane emits both z levels, the odd lane both
-    // z+1 levels; mode 2 (odd = even + 1) / 3 (even = odd + 1): the upper
-    // lane's z-level record takes the lower lane's z+1 level, which the lower
-    // lane then does not emit.  Branch-free: selects, then the two records as
-    // predicated reductions.
-    const bool lo_add = odd ? m2 : (m1 || m3);
-    const bool hi_add = odd && m1;
-    const bool emit_lo = !(odd && m1);
-    const bool emit_hi = odd ? !m3 : !(m1 || m2);
-    const f32x2 zero = pack2(0.0f, 0.0f);
-    f32x2 vlo[2], vhi[2];
-#pragma unroll
-    for (int k = 0; k < 2; ++k) {
-        const f32x2 snd = (odd && m1) ? lo[k] : hi[k];
-        const f32x2 rcv = __shfl_sync(mask, snd, partner);
-        vlo[k] = add2(lo[k], lo_add ? rcv : zero);
-        vhi[k] = add2(hi[k], hi_add ? rcv : zero);
-    }
-    float* o = p.grad_pad + (unsigned long long)RS * ci;
-    const float2 a0 = unpack2(vlo[0]), a1 = unpack2(vlo[1]);
-    const float2 b0 = unpack2(vhi[0]), b1 = unpack2(vhi[1]);
-    red_add4_global_if(emit_lo, o, a0.x, a0.y, a1.x, a1.y);
-    red_add4_global_if(emit_hi, o + 4, b0.x, b0.y, b1.x, b1.y);
-}
-
-// GV: 0 = no volume gradient, 1 = scatter every sample's eight weights,
-// 2 = merge them across lane pairs first (scatter_cell_pairwise), 3 / 4 =
-// merge lane pairs into per-cell records of 8 / 4 floats (scatter_cell_records),
-// 5 = merge a lane's consecutive samples of one cell into level records.
-template <bool CLAMP, int GV>
+// GRADVOL: also scatter the adjoint of every sample into p.grad_pad, a
+// cell-major buffer of 16-byte level records R[(cy*(W+1) + cx)*(D+2) + cz]
+// (cells at padded index floor+1): record c holds the weights of the four
+// corners (cz, cy+dy, cx+dx) of its z level at dy*2 + dx, so a sample adds
+// its z level to its cell's record and its z+1 level to the next record;
+// fold_record_gradient_kernel then sums the records onto the voxels.  A
+// lane's consecutive samples of one cell are first added in registers.
+template <bool CLAMP, bool GRADVOL>
 __device__ __forceinline__ RayGrad march_grad(const RaySetup& r, const ViewGeo& vg,
                                               const FpArgs& p, float gs) {
     const ulonglong2* __restrict__ Q = reinterpret_cast<const ulonglong2*>(p.quads);
     const XYPacks k = make_xy_packs(r, vg, p);
     RayGrad rg{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     const int nmax = step_bound(r, p.step_size);
-    // GV == 5: this lane's pending level records (cell run_ci: its z level and
-    // z+1 level), flushed when the ray leaves the cell
+    // this lane's pending level records (cell run_ci: its z level and z+1
+    // level), flushed when the ray leaves the cell
     const f32x2 zero = pack2(0.0f, 0.0f);
     uint32_t run_ci = 0u;
     bool run_have = false;
@@ -612,8 +511,8 @@ __device__ __forceinline__ RayGrad march_grad(const RaySetup& r, const ViewGeo& 
         rg.s2x = fmaf(gx, tau, rg.s2x);
         rg.s2y = fmaf(gy, tau, rg.s2y);
         rg.s2z = fmaf(gz, tau, rg.s2z);
-        if (GV != 0) {
-            // adjoint of the trilinear sample (fp.cu:231-240), padded z-fastest buffer
+        if (GRADVOL) {
+            // adjoint of the trilinear sample (fp.cu:231-240) into the level records
             const float mx = 1.0f - c.fx, my = 1.0f - c.fy, mz = 1.0f - c.fz;
             const float gy0 = gs * my, gy1 = gs * c.fy;
             // (x, y) corner columns 00, 10, 01, 11 at the cell's z (lo) and z+1
@@ -625,11 +524,7 @@ __device__ __forceinline__ RayGrad march_grad(const RaySetup& r, const ViewGeo& 
             f32x2 lo2[2] = {mul2(w0, zl), mul2(w1, zl)};
             f32x2 hi2[2] = {mul2(w0, zh), mul2(w1, zh)};
             const uint32_t gi = c.bz + c.bx * p.gz_x + c.by * p.gz_y + p.gz_bias;
-            const float2 l0 = unpack2(lo2[0]), l1 = unpack2(lo2[1]);
-            const float2 h0 = unpack2(hi2[0]), h1 = unpack2(hi2[1]);
-            float lo[4] = {l0.x, l0.y, l1.x, l1.y};
-            float hi[4] = {h0.x, h0.y, h1.x, h1.y};
-            if (GV == 5) {
+            {
                 // Consecutive samples of the ray mostly share a cell: add them
                 // in registers and emit a cell's two level records when the
                 // ray moves on.  A move to the cell above (below) in z shares a
@@ -652,24 +547,10 @@ __device__ __forceinline__ RayGrad march_grad(const RaySetup& r, const ViewGeo& 
                 }
                 run_ci = gi;
                 run_have = true;
-            } else if (GV == 3) {
-                scatter_cell_records<8>(p, gi, lo2, hi2);
-            } else if (GV == 4) {
-                scatter_cell_records<4>(p, gi, lo2, hi2);
-            } else if (GV == 2) {
-                scatter_cell_pairwise(p, gi, lo, hi);
-            } else {
-                float* g = p.grad_pad + gi;
-                const uint32_t off[4] = {0u, p.gz_x, p.gz_y, p.gz_y + p.gz_x};
-#pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    red_add_global(g + off[k], lo[k]);
-                    red_add_global(g + off[k] + 1, hi[k]);
-                }
             }
         }
     }
-    if (GV == 5 && run_have) {
+    if (GRADVOL && run_have) {
         float* o = p.grad_pad + 4ull * run_ci;
         const float2 a0 = unpack2(run_lo[0]), a1 = unpack2(run_lo[1]);
         const float2 b0 = unpack2(run_hi[0]), b1 = unpack2(run_hi[1]);
@@ -723,9 +604,9 @@ __device__ __forceinline__ void ray_geometry_terms(const FpArgs& p, const ViewGe
 }
 
 // The eight per-view geometry terms of one ray (zero for rays outside the
-// detector, missing the volume or with a zero upstream gradient); with GV
-// (march_grad) the ray's adjoint samples are scattered into p.grad_pad.
-template <int GV>
+// detector, missing the volume or with a zero upstream gradient); with
+// GRADVOL (march_grad) the ray's adjoint samples go into p.grad_pad.
+template <bool GRADVOL>
 __device__ __forceinline__ void backward_ray(const FpArgs& p, const ViewGeo& vg, int a, int u,
                                              int v, float (&terms)[8]) {
 #pragma unroll
@@ -739,8 +620,8 @@ __device__ __forceinline__ void backward_ray(const FpArgs& p, const ViewGeo& vg,
         if (r.ok && r.hit) {
             const float gs = grad_out * p.step_size;
             const RayGrad rg = ray_inside_pad<false>(r, vg, p)
-                                   ? march_grad<false, GV>(r, vg, p, gs)
-                                   : march_grad<true, GV>(r, vg, p, gs);
+                                   ? march_grad<false, GRADVOL>(r, vg, p, gs)
+                                   : march_grad<true, GRADVOL>(r, vg, p, gs);
             ray_geometry_terms(p, vg, r, u, rg, gs, terms);
         }
     }
@@ -766,7 +647,7 @@ __device__ __forceinline__ void reduce_terms_to_partials(const float (&terms)[8]
     }
 }
 
-template <int TU, int GV>
+template <int TU, bool GRADVOL>
 __global__ void __launch_bounds__(256) fp_backward_kernel(FpArgs p) {
     constexpr int TV = 256 / TU;
     __shared__ ViewGeo s_view;
@@ -782,7 +663,7 @@ __global__ void __launch_bounds__(256) fp_backward_kernel(FpArgs p) {
     int u, v;
     tile_ray<TU>(tc, u, v);
     float terms[8];
-    backward_ray<GV>(p, vg, a, u, v, terms);
+    backward_ray<GRADVOL>(p, vg, a, u, v, terms);
     reduce_terms_to_partials(terms, s_red, p.partials + ((long long)a * tiles + tile) * 8);
 }
 
@@ -916,240 +797,6 @@ __global__ void __launch_bounds__(256) sum_partials_kernel(const double* __restr
     }
 }
 
-// ---------------------------------------------------------------------------
-// Backward with the volume gradient accumulated in shared-memory bricks
-// ---------------------------------------------------------------------------
-//
-// The 256 rays of a CTA (one view, 8 detector columns x 32 rows) form a thin,
-// nearly parallel bundle.  Their march is cut into slabs of kBrickL voxel
-// cells along the main horizontal axis of the bundle (x or y, whichever the
-// rays run along more); all threads process one slab at a time, in the
-// direction of travel, each continuing its own t recurrence.  The trilinear
-// weights of a slab's samples are added into a shared-memory brick that
-// covers the slab's part of the bundle (bounded from the four corner rays of
-// the tile, which hold the extreme cross-axis positions), and after a barrier
-// the brick is flushed to the padded gradient with one reduction per
-// non-zero cell.  A sample whose cell falls outside the brick (only through
-// rounding at its edge, or when the bundle is too wide for the buffer) is
-// scattered to global memory directly.  The samples, their order within a
-// ray and the geometry sums are those of fp_backward_kernel; only the order
-// of the float additions into the volume gradient differs.
-
-constexpr int kBrickL = 8;         // cells per slab along the main axis
-constexpr int kBrickCap = 12288;   // floats of the brick buffer (48 KiB)
-
-struct BrickSlab {
-    int m_lo, c_lo, z_lo;  // padded indices of the brick's first cell
-    int bc, bz;            // extents along the cross axis and z (main: kBrickL + 1)
-    int ok;                // the brick fits the buffer
-};
-
-// Padded-voxel cross-axis and z ranges that the corner rays cover between
-// main-axis coordinates xm0 and xm1 (voxel units), with one cell of margin.
-__device__ __forceinline__ void corner_extent(const float (&dir)[4][3], const ViewGeo& vg,
-                                              const FpArgs& p, int axis, float xm0, float xm1,
-                                              BrickSlab& b) {
-    const int n_m = axis == 0 ? p.W : p.H, n_c = axis == 0 ? p.H : p.W;
-    const float off_m = axis == 0 ? p.off_x : p.off_y, off_c = axis == 0 ? p.off_y : p.off_x;
-    const float o_m = axis == 0 ? vg.ox : vg.oy, o_c = axis == 0 ? vg.oy : vg.ox;
-    float cmin = FLT_MAX, cmax = -FLT_MAX, zmin = FLT_MAX, zmax = -FLT_MAX;
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        const float dm = axis == 0 ? dir[i][0] : dir[i][1];
-        const float dc = axis == 0 ? dir[i][1] : dir[i][0];
-#pragma unroll
-        for (int e = 0; e < 2; ++e) {
-            const float xm = e ? xm1 : xm0;
-            const float pm = (xm - n_m * 0.5f) * p.voxel_size + off_m;
-            const float t = (pm - o_m) / dm;
-            const float xc = (o_c + t * dc - off_c) / p.voxel_size + n_c * 0.5f;
-            const float xz = (vg.oz + t * dir[i][2] - p.off_z) / p.voxel_size + p.D * 0.5f;
-            cmin = fminf(cmin, xc);
-            cmax = fmaxf(cmax, xc);
-            zmin = fminf(zmin, xz);
-            zmax = fmaxf(zmax, xz);
-        }
-    }
-    // cell floors, one cell of margin, clamped like the samples ([-1, n-1])
-    const int fc0 = max(-1, min(n_c - 1, (int)floorf(cmin) - 1));
-    const int fc1 = max(-1, min(n_c - 1, (int)floorf(cmax) + 1));
-    const int fz0 = max(-1, min(p.D - 1, (int)floorf(zmin) - 1));
-    const int fz1 = max(-1, min(p.D - 1, (int)floorf(zmax) + 1));
-    b.c_lo = fc0 + 1;
-    b.z_lo = fz0 + 1;
-    b.bc = fc1 - fc0 + 2;  // corners of cells fc0..fc1
-    b.bz = fz1 - fz0 + 2;
-    const long long cells = (long long)(kBrickL + 1) * b.bc * b.bz;
-    b.ok = (isfinite(cmin) && isfinite(cmax) && isfinite(zmin) && isfinite(zmax) &&
-            cells <= kBrickCap) ? 1 : 0;
-}
-
-// Samples of one ray inside main-axis floors [f_lo, f_hi] (in travel order),
-// continuing (t, n); stops at the first sample of a later slab.
-template <bool CLAMP>
-__device__ __forceinline__ void march_grad_slab(const RaySetup& r, const ViewGeo& vg,
-                                                const FpArgs& p, const XYPacks& k, float gs,
-                                                int axis, int dir, int f_lo, int f_hi,
-                                                const BrickSlab& b, float* brick, float& t,
-                                                int& n, int nmax, RayGrad& rg) {
-    const float4* __restrict__ Q = p.quads;
-#pragma unroll 1
-    for (; t <= r.tmax && n < nmax; t += p.step_size, ++n) {
-        const Cell c = sample_cell<CLAMP, false, true, false>(t, r, vg, p, k);
-        const int fx = (int)(c.bx - kFloorMagicBits), fy = (int)(c.by - kFloorMagicBits);
-        const int fz = (int)(c.bz - kFloorMagicBits);
-        const int fm = axis == 0 ? fx : fy, fcr = axis == 0 ? fy : fx;
-        if (dir > 0 ? fm > f_hi : fm < f_lo) break;  // belongs to a later slab
-        const uint32_t qi = quad_index(c, p);
-        const float4 q0 = __ldg(Q + qi);
-        const float4 q1 = __ldg(Q + qi + 1);
-        const float gx = lerpf(lerpf(q0.z - q0.x, q0.w - q0.y, c.fy),
-                               lerpf(q1.z - q1.x, q1.w - q1.y, c.fy), c.fz);
-        const float gy = lerpf(lerpf(q0.y - q0.x, q0.w - q0.z, c.fx),
-                               lerpf(q1.y - q1.x, q1.w - q1.z, c.fx), c.fz);
-        const float gz = lerpf(lerpf(q1.x - q0.x, q1.z - q0.z, c.fx),
-                               lerpf(q1.y - q0.y, q1.w - q0.w, c.fx), c.fy);
-        const float tau = t - r.tmin;
-        rg.s1x += gx;
-        rg.s1y += gy;
-        rg.s1z += gz;
-        rg.s2x = fmaf(gx, tau, rg.s2x);
-        rg.s2y = fmaf(gy, tau, rg.s2y);
-        rg.s2z = fmaf(gz, tau, rg.s2z);
-        // adjoint of the trilinear sample (fp.cu:231-240)
-        const float mx = 1.0f - c.fx, my = 1.0f - c.fy, mz = 1.0f - c.fz;
-        const float gy0 = gs * my, gy1 = gs * c.fy;
-        const float w00 = gy0 * mx, w01 = gy0 * c.fx, w10 = gy1 * mx, w11 = gy1 * c.fx;
-        const int im = fm + 1 - b.m_lo, ic = fcr + 1 - b.c_lo, iz = fz + 1 - b.z_lo;
-        if (b.ok && im >= 0 && im < kBrickL && ic >= 0 && ic <= b.bc - 2 && iz >= 0 &&
-            iz <= b.bz - 2) {
-            // brick cell (im, ic, iz) at (im * bc + ic) * bz + iz; x/y map to m/c
-            const int sm = b.bc * b.bz, sc = b.bz;
-            const int sx = axis == 0 ? sm : sc, sy = axis == 0 ? sc : sm;
-            float* g = brick + (im * b.bc + ic) * b.bz + iz;
-            atomicAdd(g, w00 * mz);
-            atomicAdd(g + 1, w00 * c.fz);
-            atomicAdd(g + sx, w01 * mz);
-            atomicAdd(g + sx + 1, w01 * c.fz);
-            atomicAdd(g + sy, w10 * mz);
-            atomicAdd(g + sy + 1, w10 * c.fz);
-            atomicAdd(g + sx + sy, w11 * mz);
-            atomicAdd(g + sx + sy + 1, w11 * c.fz);
-        } else {
-            float* g0 = p.grad_pad + (c.bz + c.bx * p.gz_x + c.by * p.gz_y + p.gz_bias);
-            float* g1 = g0 + p.gz_y;
-            red_add_global(g0, w00 * mz);
-            red_add_global(g0 + 1, w00 * c.fz);
-            red_add_global(g0 + p.gz_x, w01 * mz);
-            red_add_global(g0 + p.gz_x + 1, w01 * c.fz);
-            red_add_global(g1, w10 * mz);
-            red_add_global(g1 + 1, w10 * c.fz);
-            red_add_global(g1 + p.gz_x, w11 * mz);
-            red_add_global(g1 + p.gz_x + 1, w11 * c.fz);
-        }
-    }
-}
-
-template <int TU>
-__global__ void __launch_bounds__(256) fp_backward_brick_kernel(FpArgs p) {
-    constexpr int TV = 256 / TU;
-    extern __shared__ float brick[];  // kBrickCap floats
-    __shared__ ViewGeo s_view;
-    __shared__ double s_red[8][8];
-    __shared__ float s_dir[4][3];
-    __shared__ int s_axis, s_dirsign, s_nslab;
-    __shared__ BrickSlab s_slab;
-    const int tiles_u = (p.U + TU - 1) / TU;
-    const int tiles = tiles_u * ((p.V + TV - 1) / TV);
-    const TileCoord tc = tile_coord(p, tiles_u);
-    const int a = tc.a;
-    const int tile = tc.tv * tiles_u + tc.tu;
-    if (threadIdx.x == 0) load_view(p.g, a, s_view);
-    for (int i = threadIdx.x; i < kBrickCap; i += 256) brick[i] = 0.0f;
-    __syncthreads();
-    const ViewGeo vg = s_view;
-    if (threadIdx.x == 0) {
-        // corner rays of the tile (clamped to the detector) and the main axis
-        const int u0 = tc.tu * TU, u1 = min(p.U - 1, u0 + TU - 1);
-        const int v0 = tc.tv * TV, v1 = min(p.V - 1, v0 + TV - 1);
-        float sx = 0.0f, sy = 0.0f;
-        for (int i = 0; i < 4; ++i) {
-            const RaySetup cr = setup_ray(vg, (i & 1) ? u1 : u0, (i & 2) ? v1 : v0, p);
-            s_dir[i][0] = cr.dx;
-            s_dir[i][1] = cr.dy;
-            s_dir[i][2] = cr.dz;
-            sx += cr.dx;
-            sy += cr.dy;
-        }
-        const int axis = fabsf(sx) >= fabsf(sy) ? 0 : 1;
-        s_axis = axis;
-        s_dirsign = (axis == 0 ? sx : sy) >= 0.0f ? 1 : -1;
-        s_nslab = ((axis == 0 ? p.W : p.H) + 1 + kBrickL - 1) / kBrickL;
-    }
-    __syncthreads();
-    const int axis = s_axis, dir = s_dirsign, nslab = s_nslab;
-    int u, v;
-    tile_ray<TU>(tc, u, v);
-
-    float terms[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    const bool in_range = u < p.U && v < p.V;
-    const float grad_out =
-        in_range ? p.grad_projections[((long long)a * p.U + u) * p.V + v] : 0.0f;
-    RaySetup r = setup_ray(vg, in_range ? u : 0, in_range ? v : 0, p);
-    // fp.cu:381 -- rays with a zero upstream gradient contribute nothing.
-    const bool active = in_range && grad_out != 0.0f && r.ok && r.hit;
-    const bool inside = active && ray_inside_pad<false>(r, vg, p);
-    const XYPacks k = make_xy_packs(r, vg, p);
-    const float gs = grad_out * p.step_size;
-    const int nmax = active ? step_bound(r, p.step_size) : 0;
-    float t = r.tmin;
-    int n = 0;
-    RayGrad rg{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-
-    for (int si = 0; si < nslab; ++si) {
-        const int sl = dir > 0 ? si : nslab - 1 - si;
-        const int f_lo = -1 + sl * kBrickL, f_hi = f_lo + kBrickL - 1;
-        if (threadIdx.x == 0) {
-            BrickSlab b;
-            b.m_lo = f_lo + 1;
-            corner_extent(s_dir, vg, p, axis, (float)f_lo, (float)(f_hi + 1), b);
-            s_slab = b;
-        }
-        __syncthreads();
-        const BrickSlab b = s_slab;
-        if (active) {
-            if (inside)
-                march_grad_slab<false>(r, vg, p, k, gs, axis, dir, f_lo, f_hi, b, brick, t, n,
-                                       nmax, rg);
-            else
-                march_grad_slab<true>(r, vg, p, k, gs, axis, dir, f_lo, f_hi, b, brick, t, n,
-                                      nmax, rg);
-        }
-        __syncthreads();
-        if (b.ok) {
-            // flush: one reduction per non-zero brick cell, z fastest (coalesced)
-            const int cells = (kBrickL + 1) * b.bc * b.bz;
-            for (int i = threadIdx.x; i < cells; i += 256) {
-                const float val = brick[i];
-                if (val != 0.0f) {
-                    brick[i] = 0.0f;
-                    const int iz = i % b.bz;
-                    const int rest = i / b.bz;
-                    const int ic = rest % b.bc, im = rest / b.bc;
-                    const int pm = b.m_lo + im, pc = b.c_lo + ic, pz = b.z_lo + iz;
-                    const int xp = axis == 0 ? pm : pc, yp = axis == 0 ? pc : pm;
-                    if (xp <= p.W + 1 && yp <= p.H + 1 && pz <= p.D + 1)
-                        red_add_global(p.grad_pad + ((long long)yp * (p.W + 2) + xp) * (p.D + 2) + pz,
-                                       val);
-                }
-            }
-        }
-        __syncthreads();
-    }
-    if (active) ray_geometry_terms(p, vg, r, u, rg, gs, terms);
-    reduce_terms_to_partials(terms, s_red, p.partials + ((long long)a * tiles + tile) * 8);
-}
-
 // Per-view sum of the CTA partials, warp k owning gradient k (fixed order).
 __global__ void __launch_bounds__(256) reduce_view_partials_kernel(const double* __restrict__ partials,
                                                                    int tiles, GeometryGrad out) {
@@ -1161,52 +808,14 @@ __global__ void __launch_bounds__(256) reduce_view_partials_kernel(const double*
     if (lane == 0) out.g[k][a] = (float)acc;
 }
 
-// grad_volume[z,y,x] = sum of the padded cells that clamp onto (z,y,x); the
-// padded buffer is z-fastest: G[(yp*(W+2) + xp)*(D+2) + zp].
-__device__ __forceinline__ float fold_voxel(const float* __restrict__ gpad, int D, int H, int W,
-                                            long long i) {
-    const long long PZ = D + 2, PX = W + 2;
-    const int x = (int)(i % W);
-    const long long r = i / W;
-    const int y = (int)(r % H);
-    const int z = (int)(r / H);
-    int xs[3], ys[3], zs[3];
-    int nx = 0, ny = 0, nz = 0;
-    xs[nx++] = x + 1;
-    if (x == 0) xs[nx++] = 0;
-    if (x == W - 1) xs[nx++] = W + 1;
-    ys[ny++] = y + 1;
-    if (y == 0) ys[ny++] = 0;
-    if (y == H - 1) ys[ny++] = H + 1;
-    zs[nz++] = z + 1;
-    if (z == 0) zs[nz++] = 0;
-    if (z == D - 1) zs[nz++] = D + 1;
-    float acc = 0.0f;
-    for (int iy = 0; iy < ny; ++iy)
-        for (int ix = 0; ix < nx; ++ix)
-            for (int iz = 0; iz < nz; ++iz)
-                acc += gpad[((long long)ys[iy] * PX + xs[ix]) * PZ + zs[iz]];
-    return acc;
-}
-
-__global__ void fold_padded_gradient_kernel(const float* __restrict__ gpad, int D, int H, int W,
-                                            float* __restrict__ grad) {
-    const long long total = (long long)D * H * W;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
-         i += (long long)gridDim.x * blockDim.x)
-        grad[i] = fold_voxel(gpad, D, H, W, i);
-}
-
-// Volume gradient from a cell-major record buffer O[((cy*(W+1) + cx)*(D+2) + cz)*RS + k]
-// (scatter_cell_records; cells at padded index floor+1 in [0, n]): a padded
-// corner P gets entry k of record P - (dz, dy, dx) for every record in range
-// (cells: cz <= D, dz = k >> 2; levels: cz <= D+1, dz = 0), and padded corners
-// fold onto clamped voxels as in fold_padded_gradient_kernel.
-template <int RS>
+// Volume gradient from the level records R[((cy*(W+1) + cx)*(D+2) + cz)*4 + k]
+// (march_grad; cells at padded index floor+1 in [0, n]): a padded corner P
+// gets entry k = dy*2 + dx of record P - (0, dy, dx) for every record in range,
+// and padded corners fold onto the clamped voxels (index 0 onto 0, n+1 onto
+// n-1, as the clamped neighbours of fp.cu:200-213 sample them).
 __device__ __forceinline__ float fold_record_voxel(const float* __restrict__ O, int D, int H, int W,
                                                    long long i) {
     const long long CZ = D + 2, CX = W + 1;
-    const int zmax = RS == 8 ? D : D + 1;
     const int x = (int)(i % W);
     const long long r = i / W;
     const int y = (int)(r % H);
@@ -1227,22 +836,21 @@ __device__ __forceinline__ float fold_record_voxel(const float* __restrict__ O, 
         for (int ix = 0; ix < nx; ++ix)
             for (int iz = 0; iz < nz; ++iz)
 #pragma unroll
-                for (int k = 0; k < RS; ++k) {
-                    const int dz = k >> 2, dy = (k >> 1) & 1, dx = k & 1;
-                    const int cz = zs[iz] - dz, cy = ys[iy] - dy, cx = xs[ix] - dx;
-                    if (cz < 0 || cz > zmax || cy < 0 || cy > H || cx < 0 || cx > W) continue;
-                    acc += O[((cy * CX + cx) * CZ + cz) * RS + k];
+                for (int k = 0; k < 4; ++k) {
+                    const int dy = k >> 1, dx = k & 1;
+                    const int cz = zs[iz], cy = ys[iy] - dy, cx = xs[ix] - dx;
+                    if (cy < 0 || cy > H || cx < 0 || cx > W) continue;
+                    acc += O[((cy * CX + cx) * CZ + cz) * 4 + k];
                 }
     return acc;
 }
 
-template <int RS>
 __global__ void fold_record_gradient_kernel(const float* __restrict__ O, int D, int H, int W,
                                             float* __restrict__ grad) {
     const long long total = (long long)D * H * W;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
          i += (long long)gridDim.x * blockDim.x)
-        grad[i] = fold_record_voxel<RS>(O, D, H, W, i);
+        grad[i] = fold_record_voxel(O, D, H, W, i);
 }
 
 // ---------------------------------------------------------------------------
@@ -1355,15 +963,11 @@ __global__ void __launch_bounds__(256, 6) batch_forward_kernel(BatchTables t) {
 
 template <int TU>
 __device__ __forceinline__ void backward_item(const FpArgs& p, const ViewGeo& vg,
-                                              const TileCoord& tc, int flags, float (&terms)[8]) {
+                                              const TileCoord& tc, float (&terms)[8]) {
     int u, v;
     tile_ray<TU>(tc, u, v);
-    if (!p.grad_pad) backward_ray<0>(p, vg, tc.a, u, v, terms);
-    else if (flags & kBatchCells) backward_ray<3>(p, vg, tc.a, u, v, terms);
-    else if (flags & kBatchLevels) backward_ray<4>(p, vg, tc.a, u, v, terms);
-    else if (flags & kBatchRuns) backward_ray<5>(p, vg, tc.a, u, v, terms);
-    else if (flags & kBatchMerge) backward_ray<2>(p, vg, tc.a, u, v, terms);
-    else backward_ray<1>(p, vg, tc.a, u, v, terms);
+    if (p.grad_pad) backward_ray<true>(p, vg, tc.a, u, v, terms);
+    else backward_ray<false>(p, vg, tc.a, u, v, terms);
 }
 
 __global__ void __launch_bounds__(256, 4) batch_backward_kernel(BatchTables t) {
@@ -1379,8 +983,8 @@ __global__ void __launch_bounds__(256, 4) batch_backward_kernel(BatchTables t) {
         const ViewGeo vg = s_view;
         const TileCoord tc = s_tc;
         float terms[8];
-        if (s_tu == 8) backward_item<8>(p, vg, tc, s_flags, terms);
-        else backward_item<4>(p, vg, tc, s_flags, terms);
+        if (s_tu == 8) backward_item<8>(p, vg, tc, terms);
+        else backward_item<4>(p, vg, tc, terms);
         const long long tiles = fp_tiles_per_view_dev(p.U, p.V, s_tu);
         reduce_terms_to_partials(terms, s_red, p.partials + ((long long)tc.a * tiles + s_tile) * 8);
         __syncthreads();
@@ -1408,16 +1012,8 @@ __global__ void __launch_bounds__(256) batch_fold_kernel(BatchTables t) {
     const long long total = (long long)in.p.D * in.p.H * in.p.W;
     const long long v0 = (blockIdx.x - t.fold_block[i]) * (long long)kFoldChunk;
     const long long v1 = v0 + kFoldChunk < total ? v0 + kFoldChunk : total;
-    if (in.flags & kBatchCells) {
-        for (long long v = v0 + threadIdx.x; v < v1; v += blockDim.x)
-            in.grad_volume[v] = fold_record_voxel<8>(in.p.grad_pad, in.p.D, in.p.H, in.p.W, v);
-    } else if (in.flags & (kBatchLevels | kBatchRuns)) {
-        for (long long v = v0 + threadIdx.x; v < v1; v += blockDim.x)
-            in.grad_volume[v] = fold_record_voxel<4>(in.p.grad_pad, in.p.D, in.p.H, in.p.W, v);
-    } else {
-        for (long long v = v0 + threadIdx.x; v < v1; v += blockDim.x)
-            in.grad_volume[v] = fold_voxel(in.p.grad_pad, in.p.D, in.p.H, in.p.W, v);
-    }
+    for (long long v = v0 + threadIdx.x; v < v1; v += blockDim.x)
+        in.grad_volume[v] = fold_record_voxel(in.p.grad_pad, in.p.D, in.p.H, in.p.W, v);
 }
 
 // ---------------------------------------------------------------------------
@@ -1446,84 +1042,23 @@ template <int TU>
 int launch_backward_tu(const FpArgs& p, bool gradvol, cudaStream_t s) {
     DGC_TRACE(gradvol ? "fp_backward_kernel<gradvol>" : "fp_backward_kernel", s);
     const long long blocks = fp_tiles_per_view(p.U, p.V, TU) * (long long)p.A;
-    // DGC_SCATTER=brick selects the shared-memory brick adjoint.  It is not
-    // the default: measured 1.7-2.1x slower than the plain direct scatter
-    // (204 vs 117 ms at 256^3 / 360 x 384^2): the slab barriers hold the
-    // bundle's fastest rays back, and the shared-memory additions cost about
-    // what the L2 reductions they replace cost.
-    // the scatter the caller laid the gradient buffer out for, decided once
-    const VolumeScatter scatter =
-        p.scatter ? static_cast<VolumeScatter>(p.scatter) : fp_volume_scatter();
-    const bool brick = gradvol && scatter == kScatterBrick;
-    if (brick) {
-        constexpr int smem = kBrickCap * (int)sizeof(float);
-        static std::atomic<unsigned long long> configured{0};
-        const int rc = once_per_device(configured, []() -> int {
-            DGC_CUDA(cudaFuncSetAttribute(fp_backward_brick_kernel<TU>,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-            return DGC_OK;
-        });
-        if (rc != DGC_OK) return rc;
-        fp_backward_brick_kernel<TU><<<(unsigned)blocks, 256, smem, s>>>(p);
-    } else if (!gradvol) {
-        fp_backward_kernel<TU, 0><<<(unsigned)blocks, 256, 0, s>>>(p);
-    } else {
-        switch (scatter) {
-            case kScatterCells: fp_backward_kernel<TU, 3><<<(unsigned)blocks, 256, 0, s>>>(p); break;
-            case kScatterLevels: fp_backward_kernel<TU, 4><<<(unsigned)blocks, 256, 0, s>>>(p); break;
-            case kScatterRuns: fp_backward_kernel<TU, 5><<<(unsigned)blocks, 256, 0, s>>>(p); break;
-            case kScatterPairs: fp_backward_kernel<TU, 2><<<(unsigned)blocks, 256, 0, s>>>(p); break;
-            default: fp_backward_kernel<TU, 1><<<(unsigned)blocks, 256, 0, s>>>(p); break;
-        }
-    }
+    if (gradvol) fp_backward_kernel<TU, true><<<(unsigned)blocks, 256, 0, s>>>(p);
+    else fp_backward_kernel<TU, false><<<(unsigned)blocks, 256, 0, s>>>(p);
     DGC_LAUNCH_CHECK("fp_backward_kernel");
     return DGC_OK;
 }
 
 }  // namespace
 
-VolumeScatter fp_volume_scatter() {
-    // Level records with a lane's consecutive samples of a cell merged first
-    // by default: the backward (sid 1000, sod 600, step 0.5) at 256^3 / 360 x
-    // 384^2, 128^3 / 180 x 256^2 and 512^3 / 90 x 512^2 took 109 / 10.1 /
-    // 125 ms with them, 130 / 12.2 / 147 ms with lane pairs merged into level
-    // records, 214 / 18.5 / 273 ms with every sample alone (and 262 / 319 /
-    // 549 ms at 256^3, step 0.2).
-    if (const char* e = std::getenv("DGC_SCATTER")) {
-        if (std::strcmp(e, "pairs") == 0) return kScatterPairs;
-        if (std::strcmp(e, "plain") == 0) return kScatterPlain;
-        if (std::strcmp(e, "brick") == 0) return kScatterBrick;
-        if (std::strcmp(e, "cells") == 0) return kScatterCells;
-        if (std::strcmp(e, "levels") == 0) return kScatterLevels;
-        if (std::strcmp(e, "runs") == 0) return kScatterRuns;
-    }
-    return kScatterRuns;
+size_t fp_record_buffer_floats(int D, int H, int W) {
+    return 4 * (size_t)(D + 2) * (size_t)(H + 1) * (size_t)(W + 1);
 }
 
-int fp_record_floats(VolumeScatter scatter) {
-    return scatter == kScatterCells ? 8 : (scatter == kScatterLevels || scatter == kScatterRuns) ? 4 : 0;
-}
-
-size_t fp_record_buffer_floats(VolumeScatter scatter, int D, int H, int W) {
-    return (size_t)fp_record_floats(scatter) * (size_t)(D + 2) * (size_t)(H + 1) * (size_t)(W + 1);
-}
-
-void fp_fill_cell_layout(FpArgs& p) {
-    // cell record index of padded cell (floor+1) from the biased floors
-    p.gz_x = (uint32_t)(p.D + 2);
-    p.gz_y = (uint32_t)(p.W + 1) * (uint32_t)(p.D + 2);
-    p.gz_bias = (1u + p.gz_x + p.gz_y) - kFloorMagicBits * (1u + p.gz_x + p.gz_y);
-}
-
-int fp_fold_records(VolumeScatter scatter, const float* records, int D, int H, int W, float* grad,
-                    cudaStream_t s) {
+int fp_fold_records(const float* records, int D, int H, int W, float* grad, cudaStream_t s) {
     DGC_TRACE("fold_record_gradient", s);
     const long long total = (long long)D * H * W;
     const int blocks = (int)std::min<long long>((total + 255) / 256, 148LL * 16);
-    if (scatter == kScatterCells)
-        fold_record_gradient_kernel<8><<<blocks, 256, 0, s>>>(records, D, H, W, grad);
-    else
-        fold_record_gradient_kernel<4><<<blocks, 256, 0, s>>>(records, D, H, W, grad);
+    fold_record_gradient_kernel<<<blocks, 256, 0, s>>>(records, D, H, W, grad);
     DGC_LAUNCH_CHECK("fold_record_gradient");
     return DGC_OK;
 }
@@ -1539,9 +1074,10 @@ void fp_fill_layout(FpArgs& p) {
     p.zq_x = (uint32_t)(p.D + 2);
     p.zq_y = (uint32_t)(p.W + 1) * (uint32_t)(p.D + 2);
     p.zq_bias = (1u + p.zq_x + p.zq_y) - kFloorMagicBits * (1u + p.zq_x + p.zq_y);
-    // padded gradient: G[(yp*(W+2) + xp)*(D+2) + zp]
+    // level records of the volume gradient: record index of padded cell
+    // (floor+1) from the biased floors, R[(yp*(W+1) + xp)*(D+2) + zp]
     p.gz_x = (uint32_t)(p.D + 2);
-    p.gz_y = (uint32_t)(p.W + 2) * (uint32_t)(p.D + 2);
+    p.gz_y = (uint32_t)(p.W + 1) * (uint32_t)(p.D + 2);
     p.gz_bias = (1u + p.gz_x + p.gz_y) - kFloorMagicBits * (1u + p.gz_x + p.gz_y);
     p.inv_voxel = 1.0f / p.voxel_size;
 }
@@ -1570,10 +1106,6 @@ int fp_launch_backward(const FpArgs& p, const FpTile& tile, bool gradvol, cudaSt
 }
 
 int fp_mse_tile(int D, int H, int W) {
-    if (const char* e = std::getenv("DGC_MSE_TU")) {
-        const int t = std::atoi(e);
-        if (t == 8 || t == 4 || t == 2) return t;
-    }
     // 4 columns up to 256^3 voxels, 8 beyond: 51.0 vs 52.7 ms at 256^3 / 360 x
     // 384^2 and 5.84 vs 6.06 ms at 128^3 / 180 x 256^2, but 1145 vs 930 ms at
     // 512^3 / 720 x 768^2
@@ -1629,15 +1161,6 @@ int fp_reduce_partials(const double* partials, int A, long long tiles, const Geo
     DGC_TRACE("reduce_view_partials", s);
     reduce_view_partials_kernel<<<A, 256, 0, s>>>(partials, (int)tiles, out);
     DGC_LAUNCH_CHECK("reduce_view_partials");
-    return DGC_OK;
-}
-
-int fp_fold_gradient(const float* gpad, int D, int H, int W, float* grad, cudaStream_t s) {
-    DGC_TRACE("fold_padded_gradient", s);
-    const long long total = (long long)D * H * W;
-    const int blocks = (int)std::min<long long>((total + 255) / 256, 148LL * 16);
-    fold_padded_gradient_kernel<<<blocks, 256, 0, s>>>(gpad, D, H, W, grad);
-    DGC_LAUNCH_CHECK("fold_padded_gradient");
     return DGC_OK;
 }
 

@@ -17,10 +17,9 @@ struct FpArgs {
     float* projections;
     // backward
     const float* grad_projections;  // [A][U][V]
-    float* grad_pad;                // G[(yp*(W+2) + xp)*(D+2) + zp] or null
+    float* grad_pad;                // level records R[(yp*(W+1) + xp)*(D+2) + zp][4] or null
     uint32_t gz_x, gz_y, gz_bias;
     double* partials;  // [A][tiles][8]
-    int scatter;       // VolumeScatter the gradient buffer was laid out for (0: choose)
 };
 
 // Ray tile of a CTA: TU detector columns x (256/TU) rows; the 32 lanes of a
@@ -31,9 +30,7 @@ struct FpTile {
 };
 
 // One instance of a batched launch (an entry of the device-resident table).
-enum : int {
-    kBatchDiv = 1, kBatchOff = 2, kBatchMerge = 4, kBatchCells = 8, kBatchLevels = 16, kBatchRuns = 32
-};
+enum : int { kBatchDiv = 1, kBatchOff = 2 };
 constexpr int kFoldChunk = 2048;
 
 struct BatchInstance {
@@ -43,9 +40,7 @@ struct BatchInstance {
     GeometryGrad gout;     // eight [A] outputs
     int tile_fwd, tile_bwd;  // columns per CTA tile (forward 8/4/2, backward 8/4)
     int flags;             // kBatchDiv (non power-of-two voxel) | kBatchOff (non-zero ROI
-                           // offset) | kBatchMerge (lane-pair merged scatter) |
-                           // kBatchCells / kBatchLevels (lane pairs merged into
-                           // cell records of 8 / 4 floats)
+                           // offset)
     int quad_gx;           // blocks along x of the quads build
     long long tiles_bwd;   // backward tiles per view
 };
@@ -74,35 +69,19 @@ int fp_check_args(int D, int H, int W, int A, int U, int V, float pixel_size, fl
 
 void fp_fill_layout(FpArgs& p);
 long long fp_tiles_per_view(int U, int V, int tu);
-// Volume-gradient scatter of the backward.  kScatterRuns (the default) adds
-// the weights of a lane's consecutive samples in one cell in registers and
-// emits them as 16-byte vector reductions into a cell-major buffer of level
-// records (4 floats per cell); kScatterLevels and kScatterCells merge lane
-// pairs into records of 4 / 8 floats instead (fp_fill_cell_layout,
-// fp_record_buffer_floats, fp_fold_records); kScatterPlain and kScatterPairs
-// add single floats into the padded buffer (every sample alone, lane pairs
-// merged first); kScatterBrick accumulates shared-memory bricks flushed into
-// the padded buffer (single-problem backward only; the batched one scatters
-// plain).  DGC_SCATTER=runs|levels|cells|plain|pairs|brick overrides.
-enum VolumeScatter : int {
-    kScatterPlain = 1, kScatterPairs = 2, kScatterCells = 3, kScatterBrick = 4, kScatterLevels = 5,
-    kScatterRuns = 6  // level records, a lane's consecutive samples of a cell merged first
-};
-VolumeScatter fp_volume_scatter();
-// floats per cell record: 8 (cells), 4 (levels), 0 (padded-buffer scatters)
-int fp_record_floats(VolumeScatter scatter);
-size_t fp_record_buffer_floats(VolumeScatter scatter, int D, int H, int W);
-void fp_fill_cell_layout(FpArgs& p);
-int fp_fold_records(VolumeScatter scatter, const float* records, int D, int H, int W, float* grad,
-                    cudaStream_t s);
+// Volume gradient of the backward: the weights of a lane's consecutive
+// samples in one cell are added in registers and emitted as 16-byte vector
+// reductions into a cell-major buffer of level records (4 floats per cell,
+// fp_record_buffer_floats), then folded onto the voxels (fp_fold_records).
+size_t fp_record_buffer_floats(int D, int H, int W);
+int fp_fold_records(const float* records, int D, int H, int W, float* grad, cudaStream_t s);
 int build_volume_quads(const float* vol, int D, int H, int W, float4* quads, cudaStream_t s);
 int fp_launch_forward(const FpArgs& p, const FpTile& tile, cudaStream_t s);
 int fp_launch_backward(const FpArgs& p, const FpTile& tile, bool gradvol, cudaStream_t s);
 int fp_launch_counts(const FpArgs& p, int64_t* counts, cudaStream_t s);
 // Fused projection -> masked squared error -> geometry-gradient terms (8-column
 // tiles); p.partials [A][tiles][8], loss_partials [A][tiles].
-// Columns per CTA tile of the fused calibration step (by volume size;
-// DGC_MSE_TU=8|4|2 overrides).
+// Columns per CTA tile of the fused calibration step (by volume size).
 int fp_mse_tile(int D, int H, int W);
 // tile: columns per CTA (fp_mse_tile(), decided with the partials' size)
 int fp_launch_mse_grad(const FpArgs& p, int tile, const float* measured, const float* mask,
@@ -110,6 +89,5 @@ int fp_launch_mse_grad(const FpArgs& p, int tile, const float* measured, const f
 int fp_sum_partials(const double* x, long long n, double scale, double* out, cudaStream_t s);
 int fp_reduce_partials(const double* partials, int A, long long tiles, const GeometryGrad& out,
                        cudaStream_t s);
-int fp_fold_gradient(const float* gpad, int D, int H, int W, float* grad, cudaStream_t s);
 
 }  // namespace dgc

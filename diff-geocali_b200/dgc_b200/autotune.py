@@ -97,19 +97,21 @@ def time_backprojector(projections, geometry, pixel_size, volume_shape, voxel_si
     """Median device time [ms] of the backprojection (``direction`` "forward")
     or of its backward without the projection gradient ("backward") with Z
     blocking ``kz`` and forward column patch ``cta``, on the first
-    ``BP_TUNE_VIEWS`` views (set through DGC_BP_KZ / DGC_BP_CTA for the
-    measurement, restored afterwards)."""
+    ``BP_TUNE_VIEWS`` views.  The measurement replaces the library's tile
+    rules by one rule for these tiles and clears the rules afterwards
+    (``Autotuner.tune_backprojector`` registers its cached rules again)."""
     import torch
 
-    from . import _ops
+    from . import _native, _ops
 
     views = min(int(geometry[0].numel()), BP_TUNE_VIEWS)
     proj = projections[:views].contiguous()
     geom = [g[:views].contiguous() for g in geometry]
     D, H, W = (int(x) for x in volume_shape)
-    saved = {k: os.environ.get(k) for k in ("DGC_BP_KZ", "DGC_BP_CTA")}
-    os.environ["DGC_BP_KZ"] = str(int(kz))
-    os.environ["DGC_BP_CTA"] = f"{int(cta[0])},{int(cta[1])}"
+    lib = _native.lib()
+    _native.check(lib.dgc_bp_clear_tile_rules())
+    _native.check(lib.dgc_bp_add_tile_rule(1 << 30, 1 << 30, int(kz), int(kz), int(cta[0]),
+                                           int(cta[1])))
     try:
         if direction == "forward":
             def run():
@@ -131,11 +133,7 @@ def time_backprojector(projections, geometry, pixel_size, volume_shape, voxel_si
             stop.synchronize()
             times.append(start.elapsed_time(stop))
     finally:
-        for k, v in saved.items():
-            if v is None:
-                os.environ.pop(k, None)
-            else:
-                os.environ[k] = v
+        _native.check(lib.dgc_bp_clear_tile_rules())
     return sorted(times)[len(times) // 2]
 
 

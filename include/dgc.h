@@ -318,8 +318,7 @@ int dgc_reconstruct_fdk_ex(const float* projections, int A, int U, int V,
  * kz_forward / kz_backward (32*kz voxels of a column per warp; 1, 2, 4 or 8,
  * 0 = built-in choice) and a cta_x x cta_y patch of columns per CTA in the
  * forward (both 0 = built-in 8 x 1; cta_x*cta_y <= 16).  Rules are tried in
- * the order they were added (at most 16); the environment variables
- * DGC_BP_KZ / DGC_BP_CTA take precedence.  Results do not depend on the tiles
+ * the order they were added (at most 16).  Results do not depend on the tiles
  * beyond float-summation order (the forward's not at all).  No counterpart in
  * the reference. */
 int dgc_bp_add_tile_rule(int d_max, int a_max, int kz_forward, int kz_backward, int cta_x,

@@ -29,16 +29,11 @@ def _align(n):
     return (n + 255) // 256 * 256
 
 
-@pytest.mark.parametrize("scatter", [None, "pairs"])
-def test_workspace_bytes_follow_the_layout(scatter, monkeypatch):
+def test_workspace_bytes_follow_the_layout():
     """Volume-gradient buffers: 16-byte level records over (D+2)(H+1)(W+1)
-    cells by default, the padded volume with DGC_SCATTER=pairs."""
+    cells."""
     from dgc_b200 import _native
 
-    if scatter:
-        monkeypatch.setenv("DGC_SCATTER", scatter)
-    else:
-        monkeypatch.delenv("DGC_SCATTER", raising=False)
     lib = _native.lib()
     specs = [(24, 20, 16, 12, 40, 36, 8), (9, 31, 27, 7, 33, 65, 4), (5, 7, 6, 33, 12, 9, 0)]
     for gv in (True, False):
@@ -48,10 +43,8 @@ def test_workspace_bytes_follow_the_layout(scatter, monkeypatch):
             tu = tb or 8
             tiles = math.ceil(U / tu) * math.ceil(V / (256 // tu))
             per += _align(16 * (D + 2) * (H + 1) * (W + 1)) + _align(8 * 8 * A * tiles)
-            if gv and scatter is None:
+            if gv:
                 per += _align(16 * (D + 2) * (H + 1) * (W + 1))
-            elif gv:
-                per += _align(4 * (D + 2) * (H + 2) * (W + 2))
         n = len(specs)
         table = got - per - 5 * _align(8 * (n + 1)) - _align(16)
         # the n device-side instance records precede the buffers
@@ -124,20 +117,18 @@ def test_autotuner_picks_fastest_and_caches(tmp_path):
 
 
 @pytest.fixture
-def clean_bp_rules(monkeypatch):
+def clean_bp_rules():
     from dgc_b200 import _native
 
-    monkeypatch.delenv("DGC_BP_KZ", raising=False)
-    monkeypatch.delenv("DGC_BP_CTA", raising=False)
     lib = _native.lib()
     lib.dgc_bp_clear_tile_rules()
     yield lib
     lib.dgc_bp_clear_tile_rules()
 
 
-def test_backprojector_tile_rules(clean_bp_rules, monkeypatch):
+def test_backprojector_tile_rules(clean_bp_rules):
     """Built-in Z blocking, rules (first match, zero fields keep the built-in
-    choice), argument checks and the environment's precedence -- host only."""
+    choice) and argument checks -- host only."""
     from dgc_b200 import _native
     from dgc_b200.autotune import backprojector_tiles
 
@@ -150,9 +141,6 @@ def test_backprojector_tile_rules(clean_bp_rules, monkeypatch):
     assert backprojector_tiles(50, 90) == (1, 2, (8, 1))       # first rule; kz_backward built in
     assert backprojector_tiles(256, 360) == (8, 8, (4, 2))     # second rule
     assert backprojector_tiles(256, 600) == (2, 4, (8, 1))     # no rule covers A = 600
-    monkeypatch.setenv("DGC_BP_KZ", "4")
-    monkeypatch.setenv("DGC_BP_CTA", "2,4")
-    assert backprojector_tiles(256, 360) == (4, 4, (2, 4))     # environment first
     for bad in ((0, 10, 2, 2, 0, 0), (64, 10, 3, 2, 0, 0), (64, 10, 2, 2, 5, 4),
                 (64, 10, 2, 2, 4, 0)):
         with pytest.raises(RuntimeError):

@@ -176,14 +176,31 @@ def test_geometry_only_backward_skips_the_projection_gradient():
         assert torch.equal(a, b)
 
 
+@pytest.fixture
+def tile_rule():
+    """Sets one library tile rule for every backprojection (dgc_bp_add_tile_rule)
+    and clears the rules afterwards."""
+    from dgc_b200 import _native
+
+    lib = _native.lib()
+
+    def set_rule(kz=0, cta=(0, 0)):
+        _native.check(lib.dgc_bp_clear_tile_rules())
+        _native.check(lib.dgc_bp_add_tile_rule(1 << 30, 1 << 30, kz, kz, cta[0], cta[1]))
+
+    lib.dgc_bp_clear_tile_rules()
+    yield set_rule
+    lib.dgc_bp_clear_tile_rules()
+
+
 @pytest.mark.parametrize("px", [1.0, 0.9])
-@pytest.mark.parametrize("kz", ["1", "2", "4", "8"])
-def test_every_z_blocking_matches_the_oracle(kz, px, oracle, monkeypatch):
-    """DGC_BP_KZ: 32*KZ voxels of a column per warp (the defaults pick 2 for
-    the forward, 4 for the backward); every choice, with D not a multiple of
-    the warp's span and with the dividing (non power-of-two) pixel size,
-    against the FP64 oracle."""
-    monkeypatch.setenv("DGC_BP_KZ", kz)
+@pytest.mark.parametrize("kz", [1, 2, 4, 8])
+def test_every_z_blocking_matches_the_oracle(kz, px, oracle, tile_rule):
+    """32*KZ voxels of a column per warp (the defaults pick 2 for the forward,
+    4 for the backward; the autotuner may pick any): every choice, with D not
+    a multiple of the warp's span and with the dividing (non power-of-two)
+    pixel size, against the FP64 oracle."""
+    tile_rule(kz=kz)
     case = random_case(4, px=px, vs=1.0, shape=(70, 21, 19))
     vol, proj, geom = run_bp(case, requires_grad=True)
     truth = oracle.backproject(case["proj"], case["geom"], px, case["shape"], 1.0, case["off"])
@@ -197,9 +214,9 @@ def test_every_z_blocking_matches_the_oracle(kz, px, oracle, monkeypatch):
         assert rel_l2(ours[1 + k].cpu(), gg[k]) < GRAD_RTOL, name
 
 
-@pytest.mark.parametrize("cta", ["4,2", "2,4", "4,4", "16,1", "3,5"])
-def test_column_patch_shapes_are_bitwise(cta, monkeypatch):
-    """DGC_BP_CTA: the forward's CTA as a cx x cy patch of columns gives the
+@pytest.mark.parametrize("cta", [(4, 2), (2, 4), (4, 4), (16, 1), (3, 5)])
+def test_column_patch_shapes_are_bitwise(cta, tile_rule):
+    """The forward's CTA as a cx x cy patch of columns (a tile rule) gives the
     default's volume bit for bit (each voxel sums its views in one order),
     W and H not multiples of the patch included."""
     from cbct_backprojector import backproject
@@ -207,23 +224,19 @@ def test_column_patch_shapes_are_bitwise(cta, monkeypatch):
     case = random_case(6, px=1.0, vs=1.0, shape=(45, 23, 19))
     proj = cuda32(case["proj"])
     geom = [cuda32(g) for g in case["geom"]]
-    monkeypatch.delenv("DGC_BP_CTA", raising=False)
     a = backproject(proj, *geom, 1.0, case["shape"], 1.0, volume_offset=case["off"])
-    monkeypatch.setenv("DGC_BP_CTA", cta)
+    tile_rule(cta=cta)
     b = backproject(proj, *geom, 1.0, case["shape"], 1.0, volume_offset=case["off"])
     torch.cuda.synchronize()
     assert torch.equal(a, b)
 
 
-
-def test_autotuner_on_backprojector(tmp_path, monkeypatch):
+def test_autotuner_on_backprojector(tmp_path):
     """tune_backprojector on the GPU: every candidate timed, the choice
     registered as a library rule, the volume unchanged bit for bit."""
     from dgc_b200 import _native, backproject
     from dgc_b200.autotune import Autotuner, backprojector_tiles
 
-    monkeypatch.delenv("DGC_BP_KZ", raising=False)
-    monkeypatch.delenv("DGC_BP_CTA", raising=False)
     lib = _native.lib()
     lib.dgc_bp_clear_tile_rules()
     try:

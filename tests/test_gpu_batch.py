@@ -56,12 +56,10 @@ def plain(pr):
     return p.detach(), grads[0], torch.stack(grads[1:])
 
 
-@pytest.mark.parametrize("scatter", ["cells", "levels", "runs", "pairs", "plain"])
-def test_batch_matches_plain_calls(scatter, monkeypatch):
-    """Every volume-gradient scatter: batched launches against per-problem calls."""
+def test_batch_matches_plain_calls():
+    """Batched launches against per-problem calls."""
     from dgc_b200.batch import ProjectionBatch
 
-    monkeypatch.setenv("DGC_SCATTER", scatter)
     problems = make_problems()
     batch = ProjectionBatch(problems)
     batch.step()

@@ -184,13 +184,11 @@ def test_forward_matches_reference_cuda(which, golden, ref_native, oracle):
     assert rel_l2(ours.cpu(), truth) < FWD_RTOL
 
 
-@pytest.mark.parametrize("scatter", ["brick", "plain", "pairs", "cells", "levels", "runs"])
 @pytest.mark.parametrize("which", ["config1", "random_nonpow2"])
-def test_backward_matches_reference_cuda(which, scatter, golden, ref_native, oracle, monkeypatch):
-    """Every volume-gradient scatter: shared-memory bricks flushed once per
-    slab, every sample alone, lane pairs merged first, lane pairs merged into
-    per-cell records of 8 or 4 floats folded afterwards."""
-    monkeypatch.setenv("DGC_SCATTER", scatter)
+def test_backward_matches_reference_cuda(which, golden, ref_native, oracle):
+    """The volume gradient (run-merged level records folded afterwards) and
+    the eight geometry gradients against the reference's CUDA and the FP64
+    oracle."""
     ref_fp, _ = ref_native
     case = config1_case(golden("fp_config1.npz")) if which == "config1" else random_case(5)
     out, vol, geom = run_project(case, requires_grad=True)
@@ -213,13 +211,11 @@ def test_backward_matches_reference_cuda(which, scatter, golden, ref_native, ora
         assert rel_l2(ours_m[1 + k].cpu(), gg[k]) < GRAD_RTOL, name
 
 
-@pytest.mark.parametrize("scatter", ["runs", "levels", "cells", "plain"])
 @pytest.mark.parametrize("shape", [(1, 1, 1), (1, 5, 4), (3, 1, 2), (2, 3, 1)])
-def test_thin_volume_gradients(shape, scatter, oracle, monkeypatch):
+def test_thin_volume_gradients(shape, oracle):
     """Volumes one or a few voxels thick: every padded corner folds onto an
-    edge voxel, the records' z range is at its smallest.  Volume gradient of
-    every scatter against the FP64 oracle."""
-    monkeypatch.setenv("DGC_SCATTER", scatter)
+    edge voxel, the records' z range is at its smallest.  Volume gradient
+    against the FP64 oracle."""
     case = random_case(31, shape=shape, A=6, U=12, V=10, vs=1.0, step=0.25, off=(0.1, -0.2, 0.05))
     out, vol, geom = run_project(case, requires_grad=True)
     up = torch.linspace(0.2, 1.1, out.numel(), device="cuda").view_as(out)
