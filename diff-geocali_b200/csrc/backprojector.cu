@@ -127,6 +127,42 @@ __device__ __forceinline__ ColumnView column_view(const ViewRow& r, int a, float
 }
 
 // ---------------------------------------------------------------------------
+// Block order
+// ---------------------------------------------------------------------------
+
+// Tile (tx, ty) and z block of a CTA from its linear index.  Every CTA loops
+// over all views, so the projection data a CTA reads per view is re-read from
+// DRAM by each wave of CTAs unless the CTAs in flight share it: they must
+// cover a compact region of the volume, whose projections are small patches
+// of each view (a strip of rows along the whole volume width projects onto
+// whole detector rows).  Tiles are therefore taken z block by z block and,
+// inside a z block, in super-tiles of sx x sy tiles (about 64 x 64 voxels,
+// one wave of CTAs) ordered row by row; edge super-tiles are narrower.
+struct BpTile {
+    int tx, ty, zb;
+};
+
+__device__ __forceinline__ BpTile bp_tile(long long linear, int tiles_x, int tiles_y, int sx,
+                                          int sy) {
+    const long long layer = (long long)tiles_x * tiles_y;
+    BpTile t;
+    t.zb = (int)(linear / layer);
+    const long long r = linear - (long long)t.zb * layer;
+    const long long band_tiles = (long long)sy * tiles_x;
+    const int band = (int)(r / band_tiles);
+    const long long rb = r - band * band_tiles;
+    const int rows = min(sy, tiles_y - band * sy);
+    const int col = (int)(rb / ((long long)sx * rows));
+    const int rc = (int)(rb - (long long)col * sx * rows);
+    const int cols = min(sx, tiles_x - col * sx);
+    t.ty = band * sy + rc / cols;
+    t.tx = col * sx + rc % cols;
+    return t;
+}
+
+__host__ __device__ __forceinline__ int bp_super(int cta) { return cta >= 64 ? 1 : 64 / cta; }
+
+// ---------------------------------------------------------------------------
 // Forward (backprojection) kernel
 // ---------------------------------------------------------------------------
 
@@ -137,18 +173,25 @@ __global__ void __launch_bounds__(32 * kBpMaxWarps) bp_forward_kernel(BpArgs p) 
     __shared__ float s_out[32 * KZ][kBpMaxWarps + 1];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int cx = p.cta_x, cy = p.cta_y, nw = cx * cy;
-    const int tiles_x = (p.W + cx - 1) / cx;
-    const int ty = blockIdx.x / tiles_x;
-    const int xb = (blockIdx.x - ty * tiles_x) * cx, yb = ty * cy;
+    const int tiles_x = (p.W + cx - 1) / cx, tiles_y = (p.H + cy - 1) / cy;
+    const BpTile tile = bp_tile((long long)blockIdx.y * gridDim.x + blockIdx.x, tiles_x, tiles_y,
+                                bp_super(cx), bp_super(cy));
+    const int xb = tile.tx * cx, yb = tile.ty * cy;
     const int x = xb + warp % cx, y = yb + warp / cx;
-    const int zbase = blockIdx.y * 32 * KZ;
+    const int zbase = tile.zb * 32 * KZ;
     const unsigned FULL = 0xffffffffu;
 
-    float acc[KZ];
+    // FP32 sums of up to 8 views, added into FP64 totals: the FDK terms of a
+    // voxel cancel over the views (filtered projections change sign), and a
+    // running FP32 sum over hundreds of views loses 1e-5 to 1e-4 of the
+    // result to that cancellation
+    double acc[KZ];
+    float part[KZ];
     float pz[KZ];
 #pragma unroll
     for (int k = 0; k < KZ; ++k) {
-        acc[k] = 0.0f;
+        acc[k] = 0.0;
+        part[k] = 0.0f;
         const int z = zbase + lane + 32 * k;
         pz[k] = (z - p.D * 0.5f) * p.voxel_size + p.off_z;
     }
@@ -164,6 +207,13 @@ __global__ void __launch_bounds__(32 * kBpMaxWarps) bp_forward_kernel(BpArgs p) 
             const unsigned valid_mask = __ballot_sync(FULL, mine.valid);
             const int nv = min(32, p.A - a0);
             for (int j = 0; j < nv; ++j) {
+                if ((j & 7) == 0 && j > 0) {
+#pragma unroll
+                    for (int k = 0; k < KZ; ++k) {
+                        acc[k] += (double)part[k];
+                        part[k] = 0.0f;
+                    }
+                }
                 if (!((valid_mask >> j) & 1u)) continue;
                 const float t = __shfl_sync(FULL, mine.t, j);
                 const float dsv = __shfl_sync(FULL, mine.ds_v, j);
@@ -182,18 +232,22 @@ __global__ void __launch_bounds__(32 * kBpMaxWarps) bp_forward_kernel(BpArgs p) 
                         const float4 q = __ldg(rq + (int)(fs.biased - kFloorMagicBits));
                         const float interp =
                             lerpf(lerpf(q.x, q.y, fs.frac), lerpf(q.z, q.w, fs.frac), fu);
-                        acc[k] = fmaf(w, interp, acc[k]);
+                        part[k] = fmaf(w, interp, part[k]);
                     }
                 }
+            }
+#pragma unroll
+            for (int k = 0; k < KZ; ++k) {
+                acc[k] += (double)part[k];
+                part[k] = 0.0f;
             }
         }
     }
     // Transpose through shared memory; write rows along X.
 #pragma unroll
     for (int k = 0; k < KZ; ++k) {
-        float val = acc[k];
+        float val = FDK ? (float)(acc[k] * (double)p.out_scale) : (float)acc[k];
         if (FDK) {
-            val *= p.out_scale;
             if (p.clamp) val = val < 0.0f ? 0.0f : val;  // clamp_min(0); NaN propagates
         }
         s_out[lane + 32 * k][warp] = val;
@@ -211,22 +265,126 @@ __global__ void __launch_bounds__(32 * kBpMaxWarps) bp_forward_kernel(BpArgs p) 
 // Backward kernel
 // ---------------------------------------------------------------------------
 
+// Column geometry of one (x, y, view) for the backward (bp.cu:139-174; the
+// u/v indices use 1/pixel) and what the chain rule of bp.cu:213-292 needs.
+struct ColumnGrad {
+    bool ok;
+    int ui;
+    float t, w, fu, inv_q, du, m, sdn, denom, py;
+    float ds_u, ds_n, ds_v, v0, c, s;
+};
+
+__device__ __forceinline__ ColumnGrad column_grad(const ViewRow& r, float vx, float vy, bool col_ok,
+                                                  const BpArgs& p) {
+    ColumnGrad g;
+    g.c = r.c;
+    g.s = r.s;
+    g.ds_u = r.ds_u;
+    g.ds_n = r.ds_n;
+    g.ds_v = r.ds_v;
+    g.v0 = r.v0;
+    g.ui = 0;
+    g.t = g.w = g.fu = g.inv_q = g.du = g.m = 0.f;
+    const float px = vx * r.c + vy * r.s;
+    g.py = -vx * r.s + vy * r.c;
+    g.denom = r.sod + r.ds_n - g.py;
+    g.sdn = r.sid + r.ds_n;
+    g.ok = col_ok && g.denom > 1e-6f && g.sdn > 1e-6f;
+    if (g.ok) {
+        g.inv_q = 1.0f / g.denom;
+        g.t = g.sdn * g.inv_q;
+        g.du = px - r.ds_u;
+        const float u_phys = r.ds_u + g.t * g.du;
+        g.m = r.sod + r.ds_n;
+        g.w = g.m * g.m * (g.inv_q * g.inv_q);
+        const float u_idx = u_phys * p.inv_pixel + r.u0;
+        g.ok = u_idx >= 0.0f && u_idx < (p.U - 1.0f);
+        if (g.ok) {
+            g.ui = (int)floorf(u_idx);
+            g.fu = u_idx - g.ui;
+        }
+    }
+    return g;
+}
+
+// The eight per-view geometry gradients of a (column, view) from its four Z
+// sums (s_iu = sum g*Iu, s_iv = sum g*Iv, s_ivdv = sum g*Iv*dv, s_int = sum
+// g*interp): the chain-rule coefficients of bp.cu:213-292 applied once.
+__device__ __forceinline__ void column_terms(const ColumnGrad& g, float s_iu, float s_iv,
+                                             float s_ivdv, float s_int, float ip,
+                                             float (&terms)[8]) {
+    const float inv_q2 = g.inv_q * g.inv_q, inv_q3 = inv_q2 * g.inv_q;
+    const float m2 = g.m * g.m;
+    const float b_sid = g.du * s_iu + s_ivdv;
+    terms[1] = g.w * g.inv_q * ip * b_sid;
+    const float dt_sod = -g.sdn * inv_q2;
+    const float dw_sod = 2.0f * g.m * inv_q2 - 2.0f * m2 * inv_q3;
+    terms[2] = dw_sod * s_int + g.w * ip * dt_sod * b_sid;
+    const float dsu_b = g.ds_n, dsn_b = -g.ds_u, dq_b = g.du;
+    const float dt_b = (dsn_b * g.denom - g.sdn * dq_b) * inv_q2;
+    const float du_b = (1.0f - g.t) * dsu_b + g.t * g.py + g.du * dt_b;
+    const float dw_b = 2.0f * g.m * inv_q2 * dsn_b - 2.0f * m2 * inv_q3 * dq_b;
+    terms[0] = dw_b * s_int + g.w * ip * (du_b * s_iu + dt_b * s_ivdv);
+    terms[3] = g.w * s_iu;
+    terms[4] = g.w * s_iv;
+    const float dsu_x = g.c, dsn_x = -g.s;
+    const float dt_x = dsn_x * (g.denom - g.sdn) * inv_q2;
+    const float du_x = (1.0f - g.t) * dsu_x + g.du * dt_x;
+    const float dw_x = 2.0f * g.m * inv_q2 * dsn_x - 2.0f * m2 * inv_q3 * dsn_x;
+    terms[5] = dw_x * s_int + g.w * ip * (du_x * s_iu + dt_x * s_ivdv);
+    const float dsu_y = g.s, dsn_y = g.c;
+    const float dt_y = dsn_y * (g.denom - g.sdn) * inv_q2;
+    const float du_y = (1.0f - g.t) * dsu_y + g.du * dt_y;
+    const float dw_y = 2.0f * g.m * inv_q2 * dsn_y - 2.0f * m2 * inv_q3 * dsn_y;
+    terms[6] = dw_y * s_int + g.w * ip * (du_y * s_iu + dt_y * s_ivdv);
+    terms[7] = g.w * (1.0f - g.t) * ip * s_iv;
+}
+
+// Sums of 32 per-lane values over the warp, lane L receiving the sum of value
+// L: five butterfly steps, each halving the values a lane holds (31 shuffles
+// for the 32 sums instead of 5 per sum).
+__device__ __forceinline__ float warp_transpose_sum(float (&v)[32], int lane) {
+    const unsigned FULL = 0xffffffffu;
+#pragma unroll
+    for (int h = 16; h >= 1; h >>= 1) {
+        const bool up = (lane & h) != 0;
+#pragma unroll
+        for (int k = 0; k < h; ++k) {
+            const float send = up ? v[k] : v[k + h];
+            const float keep = up ? v[k + h] : v[k];
+            v[k] = keep + __shfl_xor_sync(FULL, send, h);
+        }
+    }
+    return v[0];
+}
+
 // GP: projection gradient 0 = not computed (p.grad_projections null), 1 = four
 // float reductions per voxel-view into grad_projections.
+//
+// A warp owns one (x, y) column and 32*KZ of its voxels along z.  Views go in
+// groups of 32: lane j evaluates the column geometry of view a0+j (and later
+// its chain rule), the warp walks the views of the group eight at a time
+// with that view's geometry broadcast by shuffles, each lane adding its z
+// voxels' four products per view into registers; the 4 x 8 sums are then
+// reduced over the warp at once (warp_transpose_sum) and the eight lanes that
+// own those views apply the chain rule in parallel.
 template <int KZ, int GP>
 __global__ void __launch_bounds__(256) bp_backward_kernel(BpArgs p) {
     __shared__ double s_terms[8][32][8];
+    const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int cols_x = (p.W + 7) >> 3;
-    const int y = blockIdx.x / cols_x;
-    const int x = (blockIdx.x - y * cols_x) * 8 + warp;
-    const int zbase = blockIdx.y * 32 * KZ;
     const long long block_id = (long long)blockIdx.y * gridDim.x + blockIdx.x;
+    const BpTile tile = bp_tile(block_id, cols_x, p.H, bp_super(8), bp_super(1));
+    const int y = tile.ty;
+    const int x = tile.tx * 8 + warp;
+    const int zbase = tile.zb * 32 * KZ;
     const long long nblocks = (long long)gridDim.x * gridDim.y;
     const bool col_ok = x < p.W;
     const float vx = (x - p.W * 0.5f) * p.voxel_size + p.off_x;
     const float vy = (y - p.H * 0.5f) * p.voxel_size + p.off_y;
     const float vlim = p.V - 1.0f;
+    const float ip = p.inv_pixel;
 
     float gval[KZ], pz[KZ];
 #pragma unroll
@@ -239,42 +397,48 @@ __global__ void __launch_bounds__(256) bp_backward_kernel(BpArgs p) {
 
     for (int a0 = 0; a0 < p.A; a0 += 32) {
         const int nv = min(32, p.A - a0);
-        for (int j = 0; j < nv; ++j) {
-            const int a = a0 + j;
-            const ViewRow r = p.vt[a];
-            float terms[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-            // column geometry (backward form of bp.cu:139-174: u/v idx use 1/pixel)
-            const float px = vx * r.c + vy * r.s;
-            const float py = -vx * r.s + vy * r.c;
-            const float denom = r.sod + r.ds_n - py;
-            const float sdn = r.sid + r.ds_n;
-            bool ok = col_ok && denom > 1e-6f && sdn > 1e-6f;
-            float inv_q = 0.f, t = 0.f, du = 0.f, m = 0.f, w = 0.f, fu = 0.f;
-            int ui = 0;
-            if (ok) {
-                inv_q = 1.0f / denom;
-                t = sdn * inv_q;
-                du = px - r.ds_u;
-                const float u_phys = r.ds_u + t * du;
-                m = r.sod + r.ds_n;
-                w = m * m * (inv_q * inv_q);
-                const float u_idx = u_phys * p.inv_pixel + r.u0;
-                ok = u_idx >= 0.0f && u_idx < (p.U - 1.0f);
-                if (ok) {
-                    ui = (int)floorf(u_idx);
-                    fu = u_idx - ui;
-                }
-            }
-            if (ok) {  // warp-uniform
-                float s_iu = 0.f, s_iv = 0.f, s_ivdv = 0.f, s_int = 0.f;
+        // the values the z loop needs from lane j's view (the rest of its
+        // geometry is recomputed by the same lane for the chain rule)
+        float my_t = 0.f, my_dsv = 0.f, my_v0 = 0.f, my_fu = 0.f, my_w = 0.f;
+        int my_ui = 0;
+        bool my_ok = false;
+        if (lane < nv) {
+            const ColumnGrad g = column_grad(p.vt[a0 + lane], vx, vy, col_ok, p);
+            my_ok = g.ok;
+            my_t = g.t;
+            my_dsv = g.ds_v;
+            my_v0 = g.v0;
+            my_fu = g.fu;
+            my_w = g.w;
+            my_ui = g.ui;
+        }
+        const unsigned valid_mask = __ballot_sync(FULL, my_ok);
+        for (int b = 0; b < nv; b += 8) {
+            float acc[32];
+#pragma unroll
+            for (int i = 0; i < 32; ++i) acc[i] = 0.0f;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const int j = b + i;
+                if (!((valid_mask >> j) & 1u)) continue;  // warp-uniform
+                const float t = __shfl_sync(FULL, my_t, j);
+                const float dsv = __shfl_sync(FULL, my_dsv, j);
+                const float v0 = __shfl_sync(FULL, my_v0, j);
+                const float fu = __shfl_sync(FULL, my_fu, j);
+                const int ui = __shfl_sync(FULL, my_ui, j);
+                const int a = a0 + j;
                 const float4* __restrict__ rq = p.pquads + (a * (p.U - 1) + ui) * (p.V - 1);
-                float* __restrict__ gp = GP ? p.grad_projections + ((long long)a * p.U + ui) * p.V
-                                            : nullptr;
+                float w = 0.0f;
+                float* __restrict__ gp = nullptr;
+                if (GP) {
+                    w = __shfl_sync(FULL, my_w, j);
+                    gp = p.grad_projections + ((long long)a * p.U + ui) * p.V;
+                }
 #pragma unroll
                 for (int k = 0; k < KZ; ++k) {
-                    const float dv = pz[k] - r.ds_v;
-                    const float v_phys = r.ds_v + t * dv;
-                    const float v_idx = v_phys * p.inv_pixel + r.v0;
+                    const float dv = pz[k] - dsv;
+                    const float v_phys = dsv + t * dv;
+                    const float v_idx = v_phys * ip + v0;
                     if (32 * k < zlimit && v_idx >= 0.0f && v_idx < vlim) {
                         const FloorSplit fs = floor_split(v_idx);
                         const int vi = (int)(fs.biased - kFloorMagicBits);
@@ -284,10 +448,10 @@ __global__ void __launch_bounds__(256) bp_backward_kernel(BpArgs p) {
                         const float iu = lerpf(q.z - q.x, q.w - q.y, fv);
                         const float iv = lerpf(q.y - q.x, q.w - q.z, fu);
                         const float g = gval[k];
-                        s_iu = fmaf(g, iu, s_iu);
-                        s_iv = fmaf(g, iv, s_iv);
-                        s_ivdv = fmaf(g * iv, dv, s_ivdv);
-                        s_int = fmaf(g, interp, s_int);
+                        acc[4 * i + 0] = fmaf(g, iu, acc[4 * i + 0]);
+                        acc[4 * i + 1] = fmaf(g, iv, acc[4 * i + 1]);
+                        acc[4 * i + 2] = fmaf(g * iv, dv, acc[4 * i + 2]);
+                        acc[4 * i + 3] = fmaf(g, interp, acc[4 * i + 3]);
                         if (GP) {
                             const float gb = g * w;
                             const float g0 = gb * (1.0f - fu), g1 = gb * fu;
@@ -298,44 +462,22 @@ __global__ void __launch_bounds__(256) bp_backward_kernel(BpArgs p) {
                         }
                     }
                 }
-                s_iu = warp_sum(s_iu);
-                s_iv = warp_sum(s_iv);
-                s_ivdv = warp_sum(s_ivdv);
-                s_int = warp_sum(s_int);
-                if (lane == 0) {
-                    // Chain-rule coefficients of bp.cu:213-292, applied to the
-                    // Z sums: sum g*(Iu*dU + Iv*dV) = dU*s_iu + dt*s_ivdv, etc.
-                    const float inv_q2 = inv_q * inv_q, inv_q3 = inv_q2 * inv_q;
-                    const float m2 = m * m;
-                    const float ip = p.inv_pixel;
-                    const float b_sid = du * s_iu + s_ivdv;
-                    terms[1] = w * inv_q * ip * b_sid;
-                    const float dt_sod = -sdn * inv_q2;
-                    const float dw_sod = 2.0f * m * inv_q2 - 2.0f * m2 * inv_q3;
-                    terms[2] = dw_sod * s_int + w * ip * dt_sod * b_sid;
-                    const float dsu_b = r.ds_n, dsn_b = -r.ds_u, dq_b = du;
-                    const float dt_b = (dsn_b * denom - sdn * dq_b) * inv_q2;
-                    const float du_b = (1.0f - t) * dsu_b + t * py + du * dt_b;
-                    const float dw_b = 2.0f * m * inv_q2 * dsn_b - 2.0f * m2 * inv_q3 * dq_b;
-                    terms[0] = dw_b * s_int + w * ip * (du_b * s_iu + dt_b * s_ivdv);
-                    terms[3] = w * s_iu;
-                    terms[4] = w * s_iv;
-                    const float dsu_x = r.c, dsn_x = -r.s;
-                    const float dt_x = dsn_x * (denom - sdn) * inv_q2;
-                    const float du_x = (1.0f - t) * dsu_x + du * dt_x;
-                    const float dw_x = 2.0f * m * inv_q2 * dsn_x - 2.0f * m2 * inv_q3 * dsn_x;
-                    terms[5] = dw_x * s_int + w * ip * (du_x * s_iu + dt_x * s_ivdv);
-                    const float dsu_y = r.s, dsn_y = r.c;
-                    const float dt_y = dsn_y * (denom - sdn) * inv_q2;
-                    const float du_y = (1.0f - t) * dsu_y + du * dt_y;
-                    const float dw_y = 2.0f * m * inv_q2 * dsn_y - 2.0f * m2 * inv_q3 * dsn_y;
-                    terms[6] = dw_y * s_int + w * ip * (du_y * s_iu + dt_y * s_ivdv);
-                    terms[7] = w * (1.0f - t) * ip * s_iv;
-                }
             }
-            if (lane == 0) {
+            // lane 4i+q: sum q of view b+i; the view's owner (lane b+i) gathers its four
+            const float total = warp_transpose_sum(acc, lane);
+            const int src = 4 * ((lane - b) & 7);
+            const float s_iu = __shfl_sync(FULL, total, src + 0);
+            const float s_iv = __shfl_sync(FULL, total, src + 1);
+            const float s_ivdv = __shfl_sync(FULL, total, src + 2);
+            const float s_int = __shfl_sync(FULL, total, src + 3);
+            if (lane >= b && lane < b + 8 && lane < nv) {
+                float terms[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+                if (my_ok) {
+                    const ColumnGrad g = column_grad(p.vt[a0 + lane], vx, vy, col_ok, p);
+                    column_terms(g, s_iu, s_iv, s_ivdv, s_int, ip, terms);
+                }
 #pragma unroll
-                for (int k = 0; k < 8; ++k) s_terms[warp][j][k] = (double)terms[k];
+                for (int k = 0; k < 8; ++k) s_terms[warp][lane][k] = (double)terms[k];
             }
         }
         __syncthreads();

@@ -77,24 +77,25 @@ def make_case(D, A, U, seed):
 
 def reference_filter(p, px, sod, sid, alpha=0.8):
     """filtering.py:82-104 (the reference's fdk_filter), restated with torch.fft
-    on the GPU in FP32: centred cosine preweight, zero padding along U to
-    2^bitlen(2U-1), the DFT of the discrete Ram-Lak kernel (real part) times
-    the Hann window, inverse transform, crop, * pixel * sid/sod."""
+    on the GPU in the dtype of ``p`` (FP32 as the reference; FP64 for the
+    truth): centred cosine preweight, zero padding along U to 2^bitlen(2U-1),
+    the DFT of the discrete Ram-Lak kernel (real part) times the Hann window,
+    inverse transform, crop, * pixel * sid/sod."""
     A, U, V = p.shape
-    dev = p.device
-    u = (torch.arange(U, device=dev, dtype=torch.float32) - (U - 1) / 2) * px
-    v = (torch.arange(V, device=dev, dtype=torch.float32) - (V - 1) / 2) * px
-    sid3, sod3 = sid.view(-1, 1, 1), sod.view(-1, 1, 1)
+    dev, dt = p.device, p.dtype
+    u = (torch.arange(U, device=dev, dtype=dt) - (U - 1) / 2) * px
+    v = (torch.arange(V, device=dev, dtype=dt) - (V - 1) / 2) * px
+    sid3, sod3 = sid.to(dt).view(-1, 1, 1), sod.to(dt).view(-1, 1, 1)
     dist = torch.sqrt(sid3.square() + u.view(1, -1, 1).square() + v.view(1, 1, -1).square())
     P = 1 << (2 * U - 1).bit_length()
     n = torch.arange(P, device=dev)
     n = torch.where(n > P // 2, n - P, n)
-    ramp = torch.zeros(P, device=dev, dtype=torch.float32)
+    ramp = torch.zeros(P, device=dev, dtype=dt)
     ramp[0] = 1.0 / (4.0 * px * px)
     odd = n % 2 != 0
-    ramp[odd] = -1.0 / (math.pi * n[odd].float() * px).square()
+    ramp[odd] = -1.0 / (math.pi * n[odd].to(dt) * px).square()
     response = torch.fft.rfft(ramp).real
-    f = torch.arange(P // 2 + 1, device=dev, dtype=torch.float32) / P
+    f = torch.arange(P // 2 + 1, device=dev, dtype=dt) / P
     hann = torch.where(f <= alpha * 0.5, 0.5 + 0.5 * torch.cos(2.0 * math.pi * f / alpha),
                        torch.zeros_like(f))
     spec = torch.fft.rfft(p * (sid3 / dist), n=P, dim=1) * (response * hann).view(1, -1, 1)
@@ -206,19 +207,35 @@ def test_config2_backprojection_and_gradients(cfg2, ref_native, oracle):
                                     grad_outputs=w_slab)
     truth_gp, truth_gg = oracle.backproject_backward(w[rows.start:rows.stop].cpu().numpy(), q_np,
                                                      g_np, PX, VOX, off)
+    theirs_slab = ref_bp.backward(w_slab, q0, *c["geom"], PX, VOX, *ORIGIN)
+    torch.cuda.synchronize()
     rec["vs_oracle"] = {"volume_slab": rel(vol.detach()[rows.start:rows.stop], truth_v),
                         "grad_projections_slab": rel(ours_slab[0], truth_gp),
                         **geometry_errors(ours_slab[1:], list(truth_gg))}
+    # the reference's CUDA against the same FP64 truth: its per-view sums are
+    # FP32 atomics over ~10^7 voxels
+    rec["reference_vs_oracle"] = {"grad_projections_slab": rel(theirs_slab[0], truth_gp),
+                                  **geometry_errors(theirs_slab[1:], list(truth_gg))}
     log(rec)
-    r, o = rec["vs_reference"], rec["vs_oracle"]
+    r, o, ro = rec["vs_reference"], rec["vs_oracle"], rec["reference_vs_oracle"]
     assert r["volume"] < FWD_RTOL and o["volume_slab"] < FWD_RTOL
     assert r["grad_projections"] < GRAD_RTOL and o["grad_projections_slab"] < GRAD_RTOL
     for name in GEOM_NAMES:
         assert o[name] < GRAD_RTOL, (name, o[name])
-        assert r[name] < GRAD_RTOL, (name, r[name])
+        # beyond the bar only where the reference is the one further from the truth
+        assert r[name] < GRAD_RTOL or ro[name] > o[name], (name, r[name], ro[name], o[name])
 
 
 def fdk_parity(c, ref_bp, oracle, views, rows, label):
+    """reconstruct_fdk against the reference's pipeline (its FFT filter in FP32,
+    its CUDA backprojector) and both against the FP64 truth on a slab of depth
+    rows: the FFT filter in FP64 on the GPU (checked against the oracle's
+    filter on ``views``), then the oracle's FP64 backprojection, * pi/A,
+    clamp.  The FDK sum cancels over the views (filtered projections change
+    sign), so FP32 accumulation alone leaves 1e-5..1e-4 relative error; the
+    library adds FP32 sums of 8 views in FP64.  Bars: the library within 1e-5
+    of the truth (volume slab and filter), no further from it than the
+    reference's pipeline, and within 1e-4 of that pipeline."""
     from cbct_backprojector import fdk_filter, project, reconstruct_fdk
     from dgc_b200.sharded import slab_offset
 
@@ -231,22 +248,31 @@ def fdk_parity(c, ref_bp, oracle, views, rows, label):
         theirs = reference_reconstruct(ref_bp, p, g, shape)
         filt = fdk_filter(p, PX, g[2], g[1])
         ref_filt = reference_filter(p[views], PX, g[2][views], g[1][views])
+        f64 = torch.cat([reference_filter(p[s:s + 32].double(), PX, g[2][s:s + 32],
+                                          g[1][s:s + 32]).cpu()
+                         for s in range(0, c["A"], 32)])
     torch.cuda.synchronize()
-    rec = {"case": f"{label} reconstruct_fdk",
-           "vs_reference": {"volume": rel(ours, theirs), "filter_views": rel(filt[views], ref_filt)}}
-    p_np = p[views].double().cpu().numpy()
-    truth_f = oracle.fdk_filter(p_np, PX, SOD, SID)
-    # the slab from the library's filtered projections (checked just above)
+    truth_f = oracle.fdk_filter(p[views].double().cpu().numpy(), PX, SOD, SID)
     off = slab_offset(shape, VOX, ORIGIN, rows)
-    truth_v = oracle.backproject(filt.double().cpu().numpy(), view(g, slice(None)), PX,
-                                 (len(rows), D, D), VOX, off)
+    truth_v = oracle.backproject(f64.numpy(), view(g, slice(None)), PX, (len(rows), D, D), VOX,
+                                 off)
     truth_v = np.maximum(truth_v * (math.pi / c["A"]), 0.0)
-    rec["vs_oracle"] = {"filter_views": rel(filt[views], truth_f),
-                        "volume_slab": rel(ours[rows.start:rows.stop], truth_v)}
+    sl = slice(rows.start, rows.stop)
+    rec = {"case": f"{label} reconstruct_fdk",
+           "vs_reference": {"volume": rel(ours, theirs), "volume_slab": rel(ours[sl], theirs[sl]),
+                            "filter_views": rel(filt[views], ref_filt)},
+           "vs_oracle": {"filter_views": rel(filt[views], truth_f),
+                         "volume_slab": rel(ours[sl], truth_v)},
+           "reference_vs_oracle": {"filter_views": rel(ref_filt, truth_f),
+                                   "volume_slab": rel(theirs[sl], truth_v)},
+           "fp64_fft_filter_vs_oracle": rel(f64[views], truth_f)}
     log(rec)
-    for side in ("vs_reference", "vs_oracle"):
-        for key, err in rec[side].items():
-            assert err < FWD_RTOL, (side, key, err)
+    o, ro, r = rec["vs_oracle"], rec["reference_vs_oracle"], rec["vs_reference"]
+    assert rec["fp64_fft_filter_vs_oracle"] < 1e-10
+    for key in ("filter_views", "volume_slab"):
+        assert o[key] < FWD_RTOL, (key, o[key])
+        assert o[key] <= ro[key], (key, o[key], ro[key])
+    assert r["volume"] < 1e-4 and r["filter_views"] < 1e-4
 
 
 def test_config2_reconstruct_fdk(cfg2, ref_native, oracle):
@@ -254,19 +280,20 @@ def test_config2_reconstruct_fdk(cfg2, ref_native, oracle):
                label="config2")
 
 
-def test_config3_loss_gradient_finite_differences_on_32_views(cfg2, oracle):
+def test_config3_loss_gradient_finite_differences_on_32_views(cfg2):
     """Config 3's loss at config 2's size: the fused calibration step's
     geometry gradients (``dgc_project_mse_grad``) against central differences
     on 32 random views, one parameter each.
 
     A view's parameters move only that view's rays, so each difference is
     taken on its view alone (a one-view projection, bitwise the rays of the
-    whole scan) with the whole scan's normalisation.  Rays whose trace (entry
-    face, sample count, cells; FP64 oracle and the kernel's own counts) a
-    +-eps step changes are masked out of the loss, for the analytic gradient
-    too.  The bound is relative to the summed magnitude of the per-ray
-    contributions, since a view's gradient is a sum of ray terms that largely
-    cancel (ray set-up in FP32, as the reference's)."""
+    whole scan) with the whole scan's normalisation.  Rays whose FP32 sample
+    count a +-eps step changes (the projection's only discontinuities) are
+    masked out of the loss, for the analytic gradient too; rays that cross
+    interpolation cells stay in (the projection is continuous there, its
+    derivative has kinks).  The bound is relative to the summed magnitude of
+    the per-ray contributions, since a view's gradient is a sum of ray terms
+    that largely cancel (ray set-up in FP32, as the reference's)."""
     from dgc_b200 import _ops, project
 
     c = cfg2
@@ -286,36 +313,23 @@ def test_config3_loss_gradient_finite_differences_on_32_views(cfg2, oracle):
         return [x[a:a + 1].contiguous() for x in g]
 
     def counts(g):
-        return _ops.project_sample_counts(vol.shape, g, PX, U, U, STEP, VOX).cpu().numpy()
+        return _ops.project_sample_counts(vol.shape, g, PX, U, U, STEP, VOX)
 
     for i, a in enumerate(views):
         k = i % 8
         g1 = one_view(geom, a)
-        base = oracle.ray_traces(vol.shape, [x.cpu().numpy() for x in g1], PX, U, U, STEP, VOX,
-                                 mode=1)
-        base_counts = counts(g1)
-        for eps in (eps_by_family[k] / 2**j for j in range(4)):
-            plus = [x.clone() for x in g1]
-            minus = [x.clone() for x in g1]
-            plus[k] += eps
-            minus[k] -= eps
-            tp = oracle.ray_traces(vol.shape, [x.cpu().numpy() for x in plus], PX, U, U, STEP, VOX,
-                                   mode=1)
-            tm = oracle.ray_traces(vol.shape, [x.cpu().numpy() for x in minus], PX, U, U, STEP,
-                                   VOX, mode=1)
-            ok = ((base != 0) & (base == tp) & (base == tm) &
-                  (counts(plus) == base_counts) & (counts(minus) == base_counts))
-            if ok.mean() >= 0.5:
-                break
-        keep[a] = torch.tensor(ok[0].astype(np.float32), device="cuda")
+        plus = [x.clone() for x in g1]
+        minus = [x.clone() for x in g1]
+        plus[k] += eps_by_family[k]
+        minus[k] -= eps_by_family[k]
+        base = counts(g1)
+        keep[a] = ((counts(plus) == base) & (counts(minus) == base))[0].float()
         steps[int(a)] = (k, plus, minus)
     denom = float(keep.sum())
     _, grads, _ = _ops.fp_mse_grad(vol, geom, PX, U, U, STEP, VOX, meas, keep, 1.0 / denom)
-    worst = 0.0
-    checked = 0
+    worst, kept = 0.0, []
     for a, (k, plus, minus) in steps.items():
-        if float(keep[a].mean()) < 0.5:
-            continue
+        kept.append(float(keep[a].mean()))
         with torch.no_grad():
             m1, w1 = meas[a:a + 1].double(), keep[a:a + 1].double()
             p0 = project(vol, *one_view(geom, a), PX, U, U, step_size=STEP).double()
@@ -328,10 +342,9 @@ def test_config3_loss_gradient_finite_differences_on_32_views(cfg2, oracle):
         err = abs(analytic - fd) / (scale + 1e-30)
         worst = max(worst, err)
         assert abs(analytic - fd) <= 2e-2 * scale + 1e-12, (GEOM_NAMES[k], a, analytic, fd, scale)
-        checked += 1
     log({"case": "config3 finite differences, 32 views at 256^3 / 360 x 384^2",
-         "checked": checked, "worst_error_over_scale": worst})
-    assert checked >= 28
+         "checked": len(steps), "min_rays_kept": min(kept), "worst_error_over_scale": worst})
+    assert len(steps) == 32 and min(kept) > 0.5
 
 
 # ------------------------------------------------------------------ target size
