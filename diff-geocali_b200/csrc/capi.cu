@@ -145,7 +145,8 @@ size_t dgc_project_workspace_bytes(int D, int H, int W, int A, int U, int V) {
     (void)U;
     (void)V;
     if (D <= 0 || H <= 0 || W <= 0) return 0;
-    return quad_volume_bytes(D, H, W);
+    // the quad-packed volume and the status word of the TMA arm's bounded waits
+    return quad_volume_bytes(D, H, W) + Workspace::align(sizeof(int));
 }
 
 static int project_impl(const float* volume, int D, int H, int W, const Geometry& g, int A,
@@ -176,15 +177,18 @@ static int project_impl(const float* volume, int D, int H, int W, const Geometry
     DGC_REQUIRE(volume && projections, "volume and projections must be non-null");
     Workspace ws(workspace, workspace_bytes);
     float4* quads = ws.take<float4>((size_t)(D + 2) * (H + 1) * (W + 1));
-    if (!quads) {
+    int* status = ws.take<int>(1);
+    if (!quads || !status) {
         set_error("workspace too small: dgc_project needs " +
                   std::to_string(dgc_project_workspace_bytes(D, H, W, A, U, V)) + " bytes");
         return DGC_ERR_WORKSPACE;
     }
     p.quads = quads;
     p.projections = projections;
+    p.error = status;
     rc = build_volume_quads(volume, D, H, W, quads, s);
     if (rc != DGC_OK) return rc;
+    DGC_CUDA(cudaMemsetAsync(status, 0, sizeof(int), s));
     return fp_launch_forward(p, kForwardTile, s);
 }
 
@@ -706,6 +710,33 @@ int dgc_bp_tiles(int D, int A, int* kz_forward, int* kz_backward, int* cta_x, in
     *kz_forward = bp_kz_forward(D, A);
     *kz_backward = bp_kz_backward(D, A);
     bp_forward_cta(D, A, *cta_x, *cta_y);
+    return DGC_OK;
+}
+
+int dgc_fp_add_arm_rule(long long voxels_max, int arm, int slab_cells) {
+    using namespace dgc;
+    clear_error();
+    const int rc = fp_add_arm_rule(voxels_max, arm, slab_cells);
+    if (rc == -2) {
+        set_error("dgc_fp_add_arm_rule: the rule table is full");
+        return DGC_ERR_UNSUPPORTED;
+    }
+    DGC_REQUIRE(rc == 0, "dgc_fp_add_arm_rule: need voxels_max >= 1, arm 0 (L1) or 1 (TMA) and, "
+                         "for arm 1, slab_cells 2 or 4");
+    return DGC_OK;
+}
+
+int dgc_fp_clear_arm_rules(void) {
+    dgc::clear_error();
+    dgc::fp_clear_arm_rules();
+    return DGC_OK;
+}
+
+int dgc_fp_arm(int D, int H, int W, int* arm, int* slab_cells) {
+    using namespace dgc;
+    clear_error();
+    DGC_REQUIRE(arm && slab_cells, "pointers must be non-null");
+    fp_forward_arm(D, H, W, arm, slab_cells);
     return DGC_OK;
 }
 

@@ -34,10 +34,13 @@
 //     clamped edge voxels afterwards (the sums of the reference's clamped-index
 //     atomics).
 #include <cstdlib>
+#include <mutex>
+#include <climits>
 #include <cstring>
 
 #include "common.cuh"
 #include "forward_projector.cuh"
+#include "tma.cuh"
 
 namespace dgc {
 
@@ -431,6 +434,250 @@ __global__ void __launch_bounds__(256) fp_forward_kernel(FpArgs p) {
     tile_ray<TU>(tc, u, v);
     if (u >= p.U || v >= p.V) return;
     forward_ray<DIV, OFF>(p, vg, tc.a, u, v);
+}
+
+// ---------------------------------------------------------------------------
+// Forward kernel, TMA arm: volume bricks staged in shared memory
+// ---------------------------------------------------------------------------
+//
+// The CTA's 256 rays (one view, 8 detector columns x 32 rows) form a thin
+// bundle that runs along one horizontal axis m (x or y, whichever the bundle's
+// central ray follows more).  Its march is cut into slabs of L cells along m;
+// for each slab one thread issues a 3-D cp.async.bulk.tensor copy of the
+// quads under the bundle -- L cells along m, kTmaO across, kTmaZ along z, a
+// box bounded from the bundle's four corner rays at the slab's two faces --
+// into one of two shared-memory stages, so the copy of slab i+1 overlaps the
+// samples of slab i.  Every thread marches its own ray (the same FP32
+// recurrence, cells and packed lerps as march_sum, so the integrals are
+// bitwise those of fp_forward_kernel) through the slab, reading the quads of
+// a sample from the stage, or from global memory when the cell lies outside
+// the box (rounding at its edge, or a bundle wider than the box), then meets
+// the others at a barrier before the stage is refilled.  Waits on the copies
+// are bounded: a timeout sets *error and the rays finish on global loads.
+
+constexpr int kTmaO = 12;  // box cells across the bundle's main axis
+constexpr int kTmaZ = 36;  // box quads along z (cells + 1)
+
+struct TmaCorner {
+    float o[3], d[3];  // voxel coordinates of the source and the ray direction per unit t
+};
+
+struct TmaSlab {
+    int m0, o0, z0;  // padded index of the box origin along m, across, along z
+};
+
+// Box of slab id `sid` (padded m range [sid*L, sid*L + L)) from the corner
+// rays' points on the slab's two faces, one cell of margin on each side.
+template <int L>
+__device__ __forceinline__ TmaSlab tma_slab_box(const TmaCorner* c, int m, int sid) {
+    const int o = 1 - m;
+    float omin = FLT_MAX, omax = -FLT_MAX, zmin = FLT_MAX, zmax = -FLT_MAX;
+#pragma unroll
+    for (int f = 0; f < 2; ++f) {
+        const float plane = (float)(sid * L - 1 + f * L);  // voxel coordinate of the face
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const float tau = (plane - c[k].o[m]) / c[k].d[m];
+            const float oo = fmaf(tau, c[k].d[o], c[k].o[o]);
+            const float zz = fmaf(tau, c[k].d[2], c[k].o[2]);
+            omin = fminf(omin, oo);
+            omax = fmaxf(omax, oo);
+            zmin = fminf(zmin, zz);
+            zmax = fmaxf(zmax, zz);
+        }
+    }
+    TmaSlab b;
+    b.m0 = sid * L;
+    // padded index = floor + 1; one cell of margin below
+    b.o0 = (int)floorf(omin);
+    b.z0 = (int)floorf(zmin);
+    // centre the box on the bundle when it is narrower than the box
+    const int o_need = (int)floorf(omax) + 2 - b.o0, z_need = (int)floorf(zmax) + 3 - b.z0;
+    if (o_need < kTmaO) b.o0 -= (kTmaO - o_need) / 2;
+    if (z_need < kTmaZ) b.z0 -= (kTmaZ - z_need) / 2;
+    return b;
+}
+
+template <int L>
+__device__ __forceinline__ void tma_issue_slab(const TmaCorner* c, int m, int sid, int stage,
+                                               TmaSlab* s_box_origin, ulonglong2* s_box,
+                                               uint64_t* s_full, const CUtensorMap* map_x,
+                                               const CUtensorMap* map_y) {
+    constexpr uint32_t kBytes = (uint32_t)(L * kTmaO * kTmaZ * 16);
+    const TmaSlab b = tma_slab_box<L>(c, m, sid);
+    s_box_origin[stage] = b;
+    const uint32_t bar = tma_smem_u32(&s_full[stage]);
+    const uint32_t dst = tma_smem_u32(s_box + (size_t)stage * L * kTmaO * kTmaZ);
+    tma_expect_tx(bar, kBytes);
+    // x coordinate = 4 floats per quad: a multiple of 16 bytes for every z0
+    if (m == 0) tma_load_3d(dst, map_x, 4 * b.z0, b.m0, b.o0, bar);
+    else tma_load_3d(dst, map_y, 4 * b.z0, b.o0, b.m0, bar);
+}
+
+// Samples of one ray while their cell lies in the slab [m_lo, m_hi) (padded m
+// index); returns with t at the first sample beyond it.
+template <int L, bool CLAMP, bool DIV, bool OFF>
+__device__ __forceinline__ void tma_march_slab(const RaySetup& r, const ViewGeo& vg, const FpArgs& p,
+                                               const XYPacks& k, int m, int dir, int m_lo, int m_hi,
+                                               const TmaSlab& b, const ulonglong2* __restrict__ box,
+                                               bool use_box, int nmax, float& t, int& n,
+                                               float& acc) {
+    const ulonglong2* __restrict__ Q = reinterpret_cast<const ulonglong2*>(p.quads);
+#pragma unroll 1
+    for (; t <= r.tmax && n < nmax; t += p.step_size, ++n) {
+        const Cell c = sample_cell<CLAMP, DIV, OFF, true>(t, r, vg, p, k);
+        const int px = (int)(c.bx - kFloorMagicBits) + 1, py = (int)(c.by - kFloorMagicBits) + 1;
+        const int pz = (int)(c.bz - kFloorMagicBits) + 1;
+        const int pm = m == 0 ? px : py, po = m == 0 ? py : px;
+        if (dir > 0 ? pm >= m_hi : pm < m_lo) break;
+        const int dm = pm - b.m0, dox = po - b.o0, dz = pz - b.z0;
+        ulonglong2 q0, q1;
+        if (use_box && (unsigned)dm < (unsigned)L && (unsigned)dox < (unsigned)kTmaO &&
+            (unsigned)dz < (unsigned)(kTmaZ - 1)) {
+            const int idx = (m == 0 ? (dox * L + dm) : (dm * kTmaO + dox)) * kTmaZ + dz;
+            q0 = box[idx];
+            q1 = box[idx + 1];
+        } else {
+            const uint32_t qi = quad_index(c, p);
+            q0 = __ldg(Q + qi);
+            q1 = __ldg(Q + qi + 1);
+        }
+        const f32x2 wx = pack2(c.fx, c.fx);
+        const f32x2 e0 = lerp2(q0.x, q0.y, wx);
+        const f32x2 e1 = lerp2(q1.x, q1.y, wx);
+        const float2 e = unpack2(lerp2(e0, e1, pack2(c.fz, c.fz)));
+        acc += lerpf(e.x, e.y, c.fy);
+    }
+}
+
+template <int L, bool DIV, bool OFF>
+__global__ void __launch_bounds__(256, 4) fp_forward_tma_kernel(FpArgs p,
+                                                             const __grid_constant__ CUtensorMap map_x,
+                                                             const __grid_constant__ CUtensorMap map_y,
+                                                             int* error) {
+    extern __shared__ __align__(128) ulonglong2 s_box[];  // two stages of L x kTmaO x kTmaZ quads
+    __shared__ ViewGeo s_view;
+    __shared__ __align__(8) uint64_t s_full[2];
+    __shared__ TmaSlab s_origin[2];
+    __shared__ TmaCorner s_corner[4];
+    __shared__ int s_pm[2];
+    __shared__ int s_abort;
+    constexpr int TU = 8;
+    constexpr int kBoxQuads = L * kTmaO * kTmaZ;
+    const int tiles_u = (p.U + TU - 1) / TU;
+    const TileCoord tc = tile_coord(p, tiles_u);
+    if (threadIdx.x == 0) {
+        load_view(p.g, tc.a, s_view);
+        tma_mbar_init(tma_smem_u32(&s_full[0]), 1);
+        tma_mbar_init(tma_smem_u32(&s_full[1]), 1);
+        tma_fence_init();
+        s_pm[0] = INT_MAX;
+        s_pm[1] = INT_MIN;
+        s_abort = 0;
+    }
+    __syncthreads();
+    const ViewGeo vg = s_view;
+    int u, v;
+    tile_ray<TU>(tc, u, v);
+    const bool in_range = u < p.U && v < p.V;
+    const int uc = min(u, p.U - 1), vc = min(v, p.V - 1);
+    const RaySetup r = setup_ray(vg, uc, vc, p);
+    // main axis and direction of the bundle, from its central ray (the same
+    // for every thread)
+    const RaySetup rc = setup_ray(vg, min(tc.tu * TU + TU / 2, p.U - 1),
+                                  min(tc.tv * 32 + 16, p.V - 1), p);
+    const int m = fabsf(rc.dx) >= fabsf(rc.dy) ? 0 : 1;
+    const int dir = (m == 0 ? rc.dx : rc.dy) >= 0.0f ? 1 : -1;
+    const int n_m = m == 0 ? p.W : p.H;
+    const float half_m = n_m * 0.5f;
+    const float off_m = m == 0 ? p.off_x : p.off_y;
+    const bool active = in_range && r.ok && r.hit;
+    if (active) {
+        // padded m index range of the ray's samples: between its box entry
+        // and exit points, clamped to the padded volume
+        const float om = m == 0 ? vg.ox : vg.oy, dm = m == 0 ? r.dx : r.dy;
+        const float a = to_voxel<DIV, OFF>(fmaf(r.tmin, dm, om), off_m, p.voxel_size, p.inv_voxel,
+                                           half_m);
+        const float bb = to_voxel<DIV, OFF>(fmaf(r.tmax, dm, om), off_m, p.voxel_size, p.inv_voxel,
+                                            half_m);
+        const float lo = fminf(fmaxf(fminf(a, bb), -1.0f), (float)(n_m - 1));
+        const float hi = fminf(fmaxf(fmaxf(a, bb), -1.0f), (float)(n_m - 1));
+        atomicMin(&s_pm[0], (int)floorf(lo) + 1 - 1);  // one index of margin
+        atomicMax(&s_pm[1], (int)floorf(hi) + 1 + 1);
+    }
+    // corner rays: warps 0 and 7, lanes 0 and 31
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if ((warp == 0 || warp == 7) && (lane == 0 || lane == 31)) {
+        const int ci = (warp == 7 ? 2 : 0) + (lane == 31 ? 1 : 0);
+        TmaCorner cr;
+        const float ox = to_voxel<DIV, OFF>(vg.ox, p.off_x, p.voxel_size, p.inv_voxel, p.W * 0.5f);
+        const float oy = to_voxel<DIV, OFF>(vg.oy, p.off_y, p.voxel_size, p.inv_voxel, p.H * 0.5f);
+        const float oz = to_voxel<DIV, OFF>(vg.oz, p.off_z, p.voxel_size, p.inv_voxel, p.D * 0.5f);
+        cr.o[0] = ox;
+        cr.o[1] = oy;
+        cr.o[2] = oz;
+        cr.d[0] = r.dx / p.voxel_size;
+        cr.d[1] = r.dy / p.voxel_size;
+        cr.d[2] = r.dz / p.voxel_size;
+        s_corner[ci] = cr;
+    }
+    __syncthreads();
+    int pm_min = max(s_pm[0], 0), pm_max = min(s_pm[1], n_m);
+    const int s_first = (dir > 0 ? pm_min : pm_max) / L;
+    const int n_slabs = pm_min <= pm_max ? pm_max / L - pm_min / L + 1 : 0;
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < 2 && i < n_slabs; ++i)
+            tma_issue_slab<L>(s_corner, m, s_first + dir * i, i, s_origin, s_box, s_full, &map_x,
+                              &map_y);
+    }
+    const XYPacks k = make_xy_packs(r, vg, p);
+    const bool inside = active ? ray_inside_pad<DIV>(r, vg, p) : true;
+    const int nmax = active ? step_bound(r, p.step_size) : 0;
+    float t = r.tmin, acc = 0.0f;
+    int n = 0;
+    for (int i = 0; i < n_slabs; ++i) {
+        const int stage = i & 1;
+        const int sid = s_first + dir * i;
+        bool have = tma_wait(tma_smem_u32(&s_full[stage]), (uint32_t)((i >> 1) & 1));
+        if (!have) {
+            s_abort = 1;
+            if (error) atomicExch(error, 1);
+        }
+        have = have && !s_abort;
+        if (active) {
+            const TmaSlab b = s_origin[stage];
+            const ulonglong2* box = s_box + (size_t)stage * kBoxQuads;
+            const int m_lo = sid * L, m_hi = sid * L + L;
+            if (inside)
+                tma_march_slab<L, false, DIV, OFF>(r, vg, p, k, m, dir, m_lo, m_hi, b, box, have,
+                                                   nmax, t, n, acc);
+            else
+                tma_march_slab<L, true, DIV, OFF>(r, vg, p, k, m, dir, m_lo, m_hi, b, box, have,
+                                                  nmax, t, n, acc);
+        }
+        __syncthreads();  // every thread is done with this stage
+        if (threadIdx.x == 0 && i + 2 < n_slabs && !s_abort)
+            tma_issue_slab<L>(s_corner, m, s_first + dir * (i + 2), stage, s_origin, s_box, s_full,
+                              &map_x, &map_y);
+    }
+    if (threadIdx.x == 0 && s_abort) {
+        // copies issued after a timed-out wait: wait for them (bounded) before exit
+        for (int i = max(0, n_slabs - 2); i < n_slabs; ++i)
+            tma_wait(tma_smem_u32(&s_full[i & 1]), (uint32_t)((i >> 1) & 1));
+    }
+    if (active) {
+        // samples past the last slab (none unless rounding put a cell beyond
+        // the bundle's range): global loads
+        if (inside)
+            tma_march_slab<L, false, DIV, OFF>(r, vg, p, k, m, dir, dir > 0 ? 0 : INT_MIN,
+                                               dir > 0 ? INT_MAX : INT_MAX, TmaSlab{0, 0, 0},
+                                               nullptr, false, nmax, t, n, acc);
+        else
+            tma_march_slab<L, true, DIV, OFF>(r, vg, p, k, m, dir, dir > 0 ? 0 : INT_MIN,
+                                              dir > 0 ? INT_MAX : INT_MAX, TmaSlab{0, 0, 0},
+                                              nullptr, false, nmax, t, n, acc);
+    }
+    if (in_range) p.projections[((long long)tc.a * p.U + u) * p.V + v] = active ? acc * p.step_size : 0.0f;
 }
 
 // Sample counts under the same FP32 rule (measurement support).
@@ -1082,8 +1329,108 @@ void fp_fill_layout(FpArgs& p) {
     p.inv_voxel = 1.0f / p.voxel_size;
 }
 
+namespace {
+
+// Arm rules (what the autotuner chose per volume size): the first rule with
+// D*H*W <= voxels_max applies; without one the L1 arm runs.
+struct FpArmRule {
+    long long voxels_max;
+    int arm, slab;
+};
+std::mutex g_arm_mutex;
+FpArmRule g_arm_rules[16];
+int g_arm_count = 0;
+
+template <int L, bool DIV, bool OFF>
+int launch_tma_variant(const FpArgs& p, const CUtensorMap& mx, const CUtensorMap& my,
+                       long long blocks, cudaStream_t s) {
+    constexpr int smem = 2 * L * kTmaO * kTmaZ * 16;
+    static std::atomic<unsigned long long> configured{0};
+    const int rc = once_per_device(configured, []() -> int {
+        DGC_CUDA(cudaFuncSetAttribute(fp_forward_tma_kernel<L, DIV, OFF>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        return DGC_OK;
+    });
+    if (rc != DGC_OK) return rc;
+    fp_forward_tma_kernel<L, DIV, OFF><<<(unsigned)blocks, 256, smem, s>>>(p, mx, my, p.error);
+    return DGC_OK;
+}
+
+// 3-D float map of the quad volume, innermost first: 4*(D+2) floats, W+1, H+1.
+bool quad_volume_map(CUtensorMap* map, const FpArgs& p, int box_z, int box_x, int box_y) {
+    EncodeTiledFn fn = encode_tiled();
+    if (!fn) return false;
+    const cuuint64_t dims[3] = {(cuuint64_t)4 * (p.D + 2), (cuuint64_t)(p.W + 1),
+                                (cuuint64_t)(p.H + 1)};
+    const cuuint64_t strides[2] = {(cuuint64_t)16 * (p.D + 2),
+                                   (cuuint64_t)16 * (p.D + 2) * (cuuint64_t)(p.W + 1)};
+    const cuuint32_t box[3] = {(cuuint32_t)(4 * box_z), (cuuint32_t)box_x, (cuuint32_t)box_y};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    return fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float4*>(p.quads), dims, strides,
+              box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+           CUDA_SUCCESS;
+}
+
+template <int L>
+int launch_forward_tma(const FpArgs& p, bool div, cudaStream_t s, bool* used) {
+    *used = false;
+    CUtensorMap mx, my;
+    if (!quad_volume_map(&mx, p, kTmaZ, L, kTmaO) || !quad_volume_map(&my, p, kTmaZ, kTmaO, L))
+        return DGC_OK;
+    *used = true;
+    DGC_TRACE("fp_forward_tma_kernel", s);
+    const long long blocks = fp_tiles_per_view(p.U, p.V, 8) * (long long)p.A;
+    const bool off = p.off_x != 0.0f || p.off_y != 0.0f || p.off_z != 0.0f;
+    int rc;
+    if (div) rc = off ? launch_tma_variant<L, true, true>(p, mx, my, blocks, s)
+                      : launch_tma_variant<L, true, false>(p, mx, my, blocks, s);
+    else rc = off ? launch_tma_variant<L, false, true>(p, mx, my, blocks, s)
+                  : launch_tma_variant<L, false, false>(p, mx, my, blocks, s);
+    if (rc != DGC_OK) return rc;
+    DGC_LAUNCH_CHECK("fp_forward_tma_kernel");
+    return DGC_OK;
+}
+
+}  // namespace
+
+int fp_add_arm_rule(long long voxels_max, int arm, int slab) {
+    if (voxels_max < 1 || (arm != 0 && arm != 1) || (arm == 1 && slab != 2 && slab != 4))
+        return -1;
+    std::lock_guard<std::mutex> lock(g_arm_mutex);
+    if (g_arm_count >= 16) return -2;
+    g_arm_rules[g_arm_count++] = FpArmRule{voxels_max, arm, arm == 1 ? slab : 0};
+    return 0;
+}
+
+void fp_clear_arm_rules() {
+    std::lock_guard<std::mutex> lock(g_arm_mutex);
+    g_arm_count = 0;
+}
+
+void fp_forward_arm(int D, int H, int W, int* arm, int* slab) {
+    const long long voxels = (long long)D * H * W;
+    std::lock_guard<std::mutex> lock(g_arm_mutex);
+    for (int i = 0; i < g_arm_count; ++i)
+        if (voxels <= g_arm_rules[i].voxels_max) {
+            *arm = g_arm_rules[i].arm;
+            *slab = g_arm_rules[i].slab;
+            return;
+        }
+    *arm = 0;
+    *slab = 0;
+}
+
 int fp_launch_forward(const FpArgs& p, const FpTile& tile, cudaStream_t s) {
     const bool div = !is_pow2_float(p.voxel_size);
+    int arm = 0, slab = 0;
+    fp_forward_arm(p.D, p.H, p.W, &arm, &slab);
+    if (arm == 1 && tile.tu == 8) {
+        bool used = false;
+        const int rc = slab == 2 ? launch_forward_tma<2>(p, div, s, &used)
+                                 : launch_forward_tma<4>(p, div, s, &used);
+        if (rc != DGC_OK || used) return rc;
+    }
     switch (tile.tu) {
         case 8: return launch_forward_tu<8>(p, div, s);
         case 4: return launch_forward_tu<4>(p, div, s);

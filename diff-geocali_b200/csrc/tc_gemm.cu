@@ -31,8 +31,23 @@
 
 #include "common.cuh"
 #include "tc_gemm.cuh"
+#include "tma.cuh"
 
 namespace dgc {
+
+EncodeTiledFn encode_tiled() {
+    static EncodeTiledFn fn = [] {
+        void* ptr = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) !=
+                cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return static_cast<EncodeTiledFn>(nullptr);
+        return reinterpret_cast<EncodeTiledFn>(ptr);
+    }();
+    return fn;
+}
+
 namespace {
 
 constexpr int kBM = 128;
@@ -441,26 +456,6 @@ __global__ void __launch_bounds__(128) tc_gemm_tma_kernel(const __grid_constant_
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(kCols)
                      : "memory");
     }
-}
-
-typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
-                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
-                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
-                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
-// against libcuda); null if the driver does not provide it.
-EncodeTiledFn encode_tiled() {
-    static EncodeTiledFn fn = [] {
-        void* ptr = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) !=
-                cudaSuccess ||
-            q != cudaDriverEntryPointSuccess)
-            return static_cast<EncodeTiledFn>(nullptr);
-        return reinterpret_cast<EncodeTiledFn>(ptr);
-    }();
-    return fn;
 }
 
 // 2-D bf16 map of a row-major [rows][ld] matrix with K = cols valid columns:

@@ -14,6 +14,13 @@ two (division or multiplication variant).  The view count only scales the
 number of tiles, so it is not part of the key, and a bucket is timed on its
 first ``TUNE_VIEWS`` views.
 
+The forward projector of a single problem also has two arms
+(``tune_forward_arm``): quad loads through L1 (``fp_forward_kernel``) or volume
+bricks staged in shared memory by TMA, slabs of 2 or 4 cells along the ray
+bundle (``fp_forward_tma_kernel``).  Both give bitwise the same projections;
+the faster one per volume-size bucket (voxel count rounded up to a power of
+two) is registered in the library as an arm rule (``dgc_fp_add_arm_rule``).
+
 The backprojector is tuned the same way (``tune_backprojector``): the Z
 blocking of its forward and backward (32*KZ voxels of a column per warp) and
 the forward's patch of columns per CTA, per bucket of volume depth and view
@@ -35,6 +42,8 @@ BP_KZ_FORWARD = (1, 2, 4, 8)
 BP_KZ_BACKWARD = (2, 4, 8)
 BP_CTAS = ((8, 1), (4, 2))
 BP_TUNE_VIEWS = 360
+FORWARD_ARMS = ((0, 0), (1, 2), (1, 4))  # (arm, slab cells): L1 quads; TMA bricks
+ARM_TUNE_VIEWS = 24
 
 
 def _pow2(x: float) -> bool:
@@ -83,6 +92,46 @@ def time_problem(problem, direction: str, tile: int, grad_volume=True, warmup=1,
         stop.synchronize()
         times.append(start.elapsed_time(stop))
     del batch
+    return sorted(times)[len(times) // 2]
+
+
+def arm_bucket(volume_shape) -> int:
+    """Voxel count of a forward-arm bucket: D*H*W rounded up to a power of two."""
+    D, H, W = (int(x) for x in volume_shape)
+    return 1 << max(0, (D * H * W - 1).bit_length())
+
+
+def time_forward_arm(problem, arm, slab, warmup=1, repeats=3):
+    """Median device time [ms] of ``project`` of ``problem`` restricted to its
+    first ``ARM_TUNE_VIEWS`` views with the forward arm ``arm`` (slab width
+    ``slab``).  The measurement replaces the library's arm rules by one rule
+    for this arm and clears them afterwards (``Autotuner.tune_forward_arm``
+    registers its cached rules again)."""
+    import torch
+
+    from . import _native, _ops
+
+    views = min(int(problem.geometry[0].numel()), ARM_TUNE_VIEWS)
+    geom = [g[:views].contiguous() for g in problem.geometry]
+    lib = _native.lib()
+    _native.check(lib.dgc_fp_clear_arm_rules())
+    _native.check(lib.dgc_fp_add_arm_rule(1 << 62, int(arm), int(slab)))
+    try:
+        def run():
+            _ops.fp_forward(problem.volume, *geom, problem.pixel_size, problem.U, problem.V,
+                            problem.step_size, problem.voxel_size, *problem.offset)
+        for _ in range(warmup):
+            run()
+        times = []
+        for _ in range(repeats):
+            start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            start.record()
+            run()
+            stop.record()
+            stop.synchronize()
+            times.append(start.elapsed_time(stop))
+    finally:
+        _native.check(lib.dgc_fp_clear_arm_rules())
     return sorted(times)[len(times) // 2]
 
 
@@ -143,10 +192,12 @@ class Autotuner:
     ``measure(problem, direction, tile) -> ms`` defaults to ``time_problem``.
     """
 
-    def __init__(self, cache_path=None, measure=None, grad_volume=True, measure_bp=None):
+    def __init__(self, cache_path=None, measure=None, grad_volume=True, measure_bp=None,
+                 measure_arm=None):
         self.cache_path = Path(cache_path) if cache_path else default_cache_path()
         self.measure = measure or (lambda pr, d, t: time_problem(pr, d, t, grad_volume))
         self.measure_bp = measure_bp or time_backprojector
+        self.measure_arm = measure_arm or time_forward_arm
         self.table = {}
         if self.cache_path.exists():
             try:
@@ -204,6 +255,38 @@ class Autotuner:
         self.apply_backprojector_rules()
         return self.table[key]
 
+    def tune_forward_arm(self, problem):
+        """Arm (L1 quads or TMA bricks) and slab width of the forward projector
+        for the volume-size bucket of ``problem``: every arm timed once
+        (``measure_arm(problem, arm, slab) -> ms``, default
+        ``time_forward_arm``), cached, registered (``apply_forward_arm_rules``)."""
+        key = f"fp-arm:{arm_bucket(problem.volume.shape)}"
+        if key not in self.table:
+            ms = {f"{a}/{sl}": float(self.measure_arm(problem, a, sl)) for a, sl in FORWARD_ARMS}
+            best = min(ms, key=ms.get)
+            a, sl = (int(x) for x in best.split("/"))
+            self.table[key] = {"voxels_max": arm_bucket(problem.volume.shape), "arm": a,
+                               "slab": sl, "ms": ms,
+                               "arm_name": "l1" if a == 0 else f"tma-slab{sl}"}
+            self.measured.append(key)
+            self._save()
+        self.apply_forward_arm_rules()
+        return self.table[key]
+
+    def apply_forward_arm_rules(self):
+        """Register every cached forward-arm bucket as a library arm rule,
+        smallest bucket first."""
+        from . import _native
+
+        lib = _native.lib()
+        _native.check(lib.dgc_fp_clear_arm_rules())
+        rules = sorted((e for k, e in self.table.items() if k.startswith("fp-arm:")),
+                       key=lambda e: e["voxels_max"])
+        for e in rules[:16]:
+            _native.check(lib.dgc_fp_add_arm_rule(int(e["voxels_max"]), int(e["arm"]),
+                                                  int(e["slab"])))
+        return len(rules[:16])
+
     def apply_backprojector_rules(self):
         """Register every cached backprojector bucket as a library tile rule,
         tightest bucket first."""
@@ -241,5 +324,6 @@ def backprojector_tiles(D, A):
     return out[0].value, out[1].value, (out[2].value, out[3].value)
 
 
-__all__ = ["Autotuner", "bucket", "bp_bucket", "time_problem", "time_backprojector",
-           "backprojector_tiles", "FORWARD_TILES", "BACKWARD_TILES"]
+__all__ = ["Autotuner", "bucket", "bp_bucket", "arm_bucket", "time_problem",
+           "time_backprojector", "time_forward_arm", "backprojector_tiles", "FORWARD_TILES",
+           "BACKWARD_TILES", "FORWARD_ARMS"]

@@ -177,3 +177,42 @@ def test_autotuner_tunes_backprojector(clean_bp_rules, tmp_path):
     again = Autotuner(cache_path=path, measure_bp=lambda *a: pytest.fail("cache miss"))
     assert again.tune_backprojector(None, geom, 1.0, (200, 9, 9), 1.0)["kz_forward"] == 4
     assert backprojector_tiles(256, 360) == (4, 8, (4, 2))
+
+
+def test_autotuner_tunes_forward_arm(tmp_path):
+    """Fastest forward arm (L1 quads or TMA bricks, slab 2 or 4) per
+    volume-size bucket, cached as JSON and registered as a library arm rule;
+    a second tuner answers from the cache -- host only."""
+    import ctypes
+
+    from dgc_b200 import _native
+    from dgc_b200.autotune import FORWARD_ARMS, Autotuner, arm_bucket
+
+    lib = _native.lib()
+    lib.dgc_fp_clear_arm_rules()
+    try:
+        assert arm_bucket((256, 256, 256)) == 1 << 24
+        assert arm_bucket((100, 20, 20)) == 1 << 16
+        calls = []
+
+        def fake(problem, arm, slab):
+            calls.append((arm, slab))
+            return {(0, 0): 3.0, (1, 2): 2.5, (1, 4): 2.0}[(arm, slab)]
+
+        pr = SimpleNamespace(volume=SimpleNamespace(shape=(512, 512, 512)))
+        path = tmp_path / "tiles.json"
+        e = Autotuner(cache_path=path, measure_arm=fake).tune_forward_arm(pr)
+        assert (e["arm"], e["slab"], e["arm_name"]) == (1, 4, "tma-slab4")
+        assert sorted(calls) == sorted(FORWARD_ARMS)
+        a, s = ctypes.c_int(), ctypes.c_int()
+        _native.check(lib.dgc_fp_arm(512, 512, 512, ctypes.byref(a), ctypes.byref(s)))
+        assert (a.value, s.value) == (1, 4)
+        _native.check(lib.dgc_fp_arm(600, 512, 512, ctypes.byref(a), ctypes.byref(s)))
+        assert (a.value, s.value) == (0, 0)       # beyond every bucket: the L1 arm
+        lib.dgc_fp_clear_arm_rules()
+        again = Autotuner(cache_path=path, measure_arm=lambda *x: pytest.fail("cache miss"))
+        assert again.tune_forward_arm(pr)["arm"] == 1
+        _native.check(lib.dgc_fp_arm(512, 512, 512, ctypes.byref(a), ctypes.byref(s)))
+        assert (a.value, s.value) == (1, 4)
+    finally:
+        lib.dgc_fp_clear_arm_rules()

@@ -38,7 +38,7 @@ def test_exports_every_declared_symbol(lib):
 
 def test_workspace_queries(lib):
     a = lib.dgc_project_workspace_bytes(256, 256, 256, 360, 384, 384)
-    assert a == 16 * 258 * 257 * 257 + (-(16 * 258 * 257 * 257) % 256)
+    assert a == 16 * 258 * 257 * 257 + (-(16 * 258 * 257 * 257) % 256) + 256  # quads + status word
     assert lib.dgc_project_workspace_bytes(0, 1, 1, 1, 1, 1) == 0
     b0 = lib.dgc_project_backward_workspace_bytes(64, 64, 64, 90, 128, 128, 0)
     b1 = lib.dgc_project_backward_workspace_bytes(64, 64, 64, 90, 128, 128, 1)
