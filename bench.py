@@ -74,14 +74,15 @@ def parse_args(argv=None):
     ap.add_argument("--detector", type=int, default=None, help="override the square detector size")
     ap.add_argument("--workload", default="target512",
                     choices=["target512", "fdk256", "fdk-sharded", "batch64", "calib", "tour",
-                             "gemm"],
+                             "gemm", "arms"],
                     help="target512: the FDK step at 512^3 / 720 x 768^2 (default); fdk256: the "
                          "same step at 256^3 / 360 x 384^2; fdk-sharded: one target512 object "
                          "split by views over the ranks; batch64: 64 uneven project+backward "
                          "instances, batched vs sequential; calib: calibration wall time to "
                          "0.1 px, learned warm start vs plain; tour: every kernel once on the "
                          "fdk256 instance (profiler captures); gemm: the tcgen05 GEMM at "
-                         "8192^3 and at the network's largest layer shapes")
+                         "8192^3 and at the network's largest layer shapes; arms: the forward "
+                         "projector's L1 and TMA arms timed at 256^3 and 512^3")
     ap.add_argument("--acq", choices=["half", "eval", "config3"], default="half",
                     help="calib: 256^3 x 2 mm / 360 / 384^2 x 2 mm (half), 512^3 / 720 / 768^2 "
                          "(eval) or 256^3 x 1 mm / 360 / 384^2 x 1 mm (config3)")
@@ -964,6 +965,66 @@ def run_tour(args):
     return 0
 
 
+# --------------------------------------------------------------------- arms
+
+
+def run_arms(args):
+    """The forward projector's arms -- quads through L1 and volume bricks
+    staged by TMA (slabs of 2 or 4 cells) -- on the fdk256 and target512
+    phantoms and scans, each timed on ``--views`` views (default 48) with CUDA
+    events (median of ``--steps``), checked bitwise equal, with the autotuner's
+    choice per volume bucket."""
+    import torch
+
+    from dgc_b200 import _native, _ops
+    from dgc_b200.autotune import FORWARD_ARMS
+
+    torch.cuda.set_device(0)
+    device = torch.device("cuda", 0)
+    lib = _native.lib()
+    out = {}
+    with ClockSampler(0) as clocks:
+        for key in ("fdk256", "target512"):
+            WORKLOAD.clear()
+            WORKLOAD.update(WORKLOADS[key])
+            w = WORKLOAD
+            views = args.views or 48
+            WORKLOAD["A"] = views
+            vol, geom = make_instance(device, instance_seed(0))
+            res, ref = {}, None
+            for arm, slab in FORWARD_ARMS:
+                _native.check(lib.dgc_fp_clear_arm_rules())
+                _native.check(lib.dgc_fp_add_arm_rule(1 << 62, arm, slab))
+
+                def run():
+                    return _ops.fp_forward(vol, *geom, w["pixel"], w["U"], w["V"], w["step"],
+                                           w["voxel"])
+                for _ in range(max(1, args.warmup)):
+                    p = run()
+                times = []
+                for _ in range(max(3, args.steps)):
+                    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    a.record()
+                    p = run()
+                    b.record()
+                    b.synchronize()
+                    times.append(a.elapsed_time(b))
+                ms = statistics.median(times)
+                same = None if ref is None else bool(torch.equal(p, ref))
+                if ref is None:
+                    ref = p
+                res["l1" if arm == 0 else f"tma-slab{slab}"] = {
+                    "ms": ms, "grays_per_s": views * w["U"] * w["V"] / (ms * 1e-3) / 1e9,
+                    "bitwise_equal_to_l1": same}
+            _native.check(lib.dgc_fp_clear_arm_rules())
+            out[key] = {"views": views, "volume": w["D"], "detector": w["U"], "arms": res}
+            del vol, geom, ref, p
+            torch.cuda.empty_cache()
+    print(json.dumps({"workload": "forward projector arms", "results": out,
+                      "clocks": clocks.summary()}))
+    return 0
+
+
 # --------------------------------------------------------------------- gemm
 
 
@@ -1021,6 +1082,8 @@ def main(argv=None):
     args = parse_args(argv)
     if args.workload == "gemm":
         return run_gemm(args)
+    if args.workload == "arms":
+        return run_arms(args)
     if args.workload == "tour":
         return run_tour(args)
     if args.workload == "calib":
