@@ -561,6 +561,7 @@ __global__ void __launch_bounds__(256, 4) fp_forward_tma_kernel(FpArgs p,
     __shared__ TmaSlab s_origin[2];
     __shared__ TmaCorner s_corner[4];
     __shared__ int s_pm[2];
+    __shared__ int s_issued[2];  // copies issued on each stage
     __shared__ int s_abort;
     constexpr int TU = 8;
     constexpr int kBoxQuads = L * kTmaO * kTmaZ;
@@ -573,6 +574,7 @@ __global__ void __launch_bounds__(256, 4) fp_forward_tma_kernel(FpArgs p,
         tma_fence_init();
         s_pm[0] = INT_MAX;
         s_pm[1] = INT_MIN;
+        s_issued[0] = s_issued[1] = 0;
         s_abort = 0;
     }
     __syncthreads();
@@ -626,10 +628,13 @@ __global__ void __launch_bounds__(256, 4) fp_forward_tma_kernel(FpArgs p,
     const int s_first = (dir > 0 ? pm_min : pm_max) / L;
     const int n_slabs = pm_min <= pm_max ? pm_max / L - pm_min / L + 1 : 0;
     if (threadIdx.x == 0) {
-        for (int i = 0; i < 2 && i < n_slabs; ++i)
+        for (int i = 0; i < 2 && i < n_slabs; ++i) {
             tma_issue_slab<L>(s_corner, m, s_first + dir * i, i, s_origin, s_box, s_full, &map_x,
                               &map_y);
+            s_issued[i] += 1;
+        }
     }
+    __syncthreads();
     const XYPacks k = make_xy_packs(r, vg, p);
     const bool inside = active ? ray_inside_pad<DIV>(r, vg, p) : true;
     const int nmax = active ? step_bound(r, p.step_size) : 0;
@@ -638,12 +643,15 @@ __global__ void __launch_bounds__(256, 4) fp_forward_tma_kernel(FpArgs p,
     for (int i = 0; i < n_slabs; ++i) {
         const int stage = i & 1;
         const int sid = s_first + dir * i;
-        bool have = tma_wait(tma_smem_u32(&s_full[stage]), (uint32_t)((i >> 1) & 1));
-        if (!have) {
-            s_abort = 1;
-            if (error) atomicExch(error, 1);
+        // after an abort no further copies are issued: no wait, global loads
+        bool have = false;
+        if (!s_abort) {
+            have = tma_wait(tma_smem_u32(&s_full[stage]), (uint32_t)((i >> 1) & 1));
+            if (!have) {
+                s_abort = 1;
+                if (error) atomicExch(error, 1);
+            }
         }
-        have = have && !s_abort;
         if (active) {
             const TmaSlab b = s_origin[stage];
             const ulonglong2* box = s_box + (size_t)stage * kBoxQuads;
@@ -656,14 +664,20 @@ __global__ void __launch_bounds__(256, 4) fp_forward_tma_kernel(FpArgs p,
                                                   nmax, t, n, acc);
         }
         __syncthreads();  // every thread is done with this stage
-        if (threadIdx.x == 0 && i + 2 < n_slabs && !s_abort)
+        if (threadIdx.x == 0 && i + 2 < n_slabs && !s_abort) {
             tma_issue_slab<L>(s_corner, m, s_first + dir * (i + 2), stage, s_origin, s_box, s_full,
                               &map_x, &map_y);
+            s_issued[stage] += 1;
+        }
+        __syncthreads();  // s_abort and the next stage's origin as thread 0 left them
     }
-    if (threadIdx.x == 0 && s_abort) {
-        // copies issued after a timed-out wait: wait for them (bounded) before exit
-        for (int i = max(0, n_slabs - 2); i < n_slabs; ++i)
-            tma_wait(tma_smem_u32(&s_full[i & 1]), (uint32_t)((i >> 1) & 1));
+    if (threadIdx.x == 0) {
+        // no copy may still write into this CTA's shared memory when it exits:
+        // wait (bounded) for the last copy of each stage; returns at once for
+        // copies already waited for
+        for (int st = 0; st < 2; ++st)
+            if (s_issued[st] > 0)
+                tma_wait(tma_smem_u32(&s_full[st]), (uint32_t)((s_issued[st] - 1) & 1));
     }
     if (active) {
         // samples past the last slab (none unless rounding put a cell beyond
