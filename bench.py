@@ -969,8 +969,9 @@ def run_tour(args):
 
 
 def run_arms(args):
-    """The forward projector's arms -- quads through L1 and volume bricks
-    staged by TMA (slabs of 2 or 4 cells) -- on the fdk256 and target512
+    """The forward projector's arms -- quads through L1 (march unrolled once
+    or twice) and volume bricks staged by TMA (slabs of 2 or 4 cells) -- on
+    the fdk256 and target512
     phantoms and scans, each timed on ``--views`` views (default 48) with CUDA
     events (median of ``--steps``), checked bitwise equal, with the autotuner's
     choice per volume bucket."""
@@ -992,9 +993,9 @@ def run_arms(args):
             WORKLOAD["A"] = views
             vol, geom = make_instance(device, instance_seed(0))
             res, ref = {}, None
-            for arm, slab in FORWARD_ARMS:
+            for arm, slab, unroll in FORWARD_ARMS:
                 _native.check(lib.dgc_fp_clear_arm_rules())
-                _native.check(lib.dgc_fp_add_arm_rule(1 << 62, arm, slab))
+                _native.check(lib.dgc_fp_add_arm_rule(1 << 62, arm, slab, unroll))
 
                 def run():
                     return _ops.fp_forward(vol, *geom, w["pixel"], w["U"], w["V"], w["step"],
@@ -1013,7 +1014,7 @@ def run_arms(args):
                 same = None if ref is None else bool(torch.equal(p, ref))
                 if ref is None:
                     ref = p
-                res["l1" if arm == 0 else f"tma-slab{slab}"] = {
+                res[f"l1-unroll{unroll}" if arm == 0 else f"tma-slab{slab}"] = {
                     "ms": ms, "grays_per_s": views * w["U"] * w["V"] / (ms * 1e-3) / 1e9,
                     "bitwise_equal_to_l1": same}
             _native.check(lib.dgc_fp_clear_arm_rules())

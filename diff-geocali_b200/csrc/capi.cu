@@ -713,16 +713,16 @@ int dgc_bp_tiles(int D, int A, int* kz_forward, int* kz_backward, int* cta_x, in
     return DGC_OK;
 }
 
-int dgc_fp_add_arm_rule(long long voxels_max, int arm, int slab_cells) {
+int dgc_fp_add_arm_rule(long long voxels_max, int arm, int slab_cells, int unroll) {
     using namespace dgc;
     clear_error();
-    const int rc = fp_add_arm_rule(voxels_max, arm, slab_cells);
+    const int rc = fp_add_arm_rule(voxels_max, arm, slab_cells, unroll);
     if (rc == -2) {
         set_error("dgc_fp_add_arm_rule: the rule table is full");
         return DGC_ERR_UNSUPPORTED;
     }
-    DGC_REQUIRE(rc == 0, "dgc_fp_add_arm_rule: need voxels_max >= 1, arm 0 (L1) or 1 (TMA) and, "
-                         "for arm 1, slab_cells 2 or 4");
+    DGC_REQUIRE(rc == 0, "dgc_fp_add_arm_rule: need voxels_max >= 1, arm 0 (L1) or 1 (TMA), "
+                         "for arm 1 slab_cells 2 or 4, unroll 1 or 2 (arm 1: 1)");
     return DGC_OK;
 }
 
@@ -732,11 +732,11 @@ int dgc_fp_clear_arm_rules(void) {
     return DGC_OK;
 }
 
-int dgc_fp_arm(int D, int H, int W, int* arm, int* slab_cells) {
+int dgc_fp_arm(int D, int H, int W, int* arm, int* slab_cells, int* unroll) {
     using namespace dgc;
     clear_error();
-    DGC_REQUIRE(arm && slab_cells, "pointers must be non-null");
-    fp_forward_arm(D, H, W, arm, slab_cells);
+    DGC_REQUIRE(arm && slab_cells && unroll, "pointers must be non-null");
+    fp_forward_arm(D, H, W, arm, slab_cells, unroll);
     return DGC_OK;
 }
 

@@ -344,7 +344,9 @@ __device__ __forceinline__ void load_cell(const ulonglong2* __restrict__ Q, uint
 // Sum of the trilinear samples along the ray (fp.cu:321-335).  The quads
 // hold the y-pairs of x0 and x1 as 64-bit halves, so the interpolation runs
 // as packed pairs: along x for (y0, y1) at z0 and z1, along z, then along y.
-template <bool CLAMP, bool DIV, bool OFF, bool GUARD = true>
+// UNROLL: the march loop unrolled by the compiler (1 or 2; the same samples
+// and sums either way, a tuned dimension of the forward).
+template <bool CLAMP, bool DIV, bool OFF, bool GUARD = true, int UNROLL = 1>
 __device__ __forceinline__ float march_sum(const RaySetup& r, const ViewGeo& vg, const FpArgs& p) {
     const ulonglong2* __restrict__ Q = reinterpret_cast<const ulonglong2*>(p.quads);
     const XYPacks k = make_xy_packs(r, vg, p);
@@ -353,7 +355,7 @@ __device__ __forceinline__ float march_sum(const RaySetup& r, const ViewGeo& vg,
     float t = r.tmin;
     int n = 0;
     CellQuads cq;
-#pragma unroll 1
+#pragma unroll UNROLL
     for (; t <= r.tmax && (!GUARD || n < nmax); t += p.step_size, n += GUARD ? 1 : 0) {
         const Cell c = sample_cell<CLAMP, DIV, OFF, true>(t, r, vg, p, k);
         load_cell(Q, quad_index(c, p), cq);
@@ -403,7 +405,7 @@ __device__ __forceinline__ void tile_ray(const TileCoord& tc, int& u, int& v) {
 }
 
 // Line integral of one ray, written to p.projections.
-template <bool DIV, bool OFF>
+template <bool DIV, bool OFF, int UNROLL = 1>
 __device__ __forceinline__ void forward_ray(const FpArgs& p, const ViewGeo& vg, int a, int u,
                                             int v) {
     const RaySetup r = setup_ray(vg, u, v, p);
@@ -411,18 +413,18 @@ __device__ __forceinline__ void forward_ray(const FpArgs& p, const ViewGeo& vg, 
     if (r.ok && r.hit) {
         const bool inside = ray_inside_pad<DIV>(r, vg, p);
         if (steps_advance(r, p.step_size))
-            integral = inside ? march_sum<false, DIV, OFF, false>(r, vg, p)
-                              : march_sum<true, DIV, OFF, false>(r, vg, p);
+            integral = inside ? march_sum<false, DIV, OFF, false, UNROLL>(r, vg, p)
+                              : march_sum<true, DIV, OFF, false, UNROLL>(r, vg, p);
         else
-            integral = inside ? march_sum<false, DIV, OFF>(r, vg, p)
-                              : march_sum<true, DIV, OFF>(r, vg, p);
+            integral = inside ? march_sum<false, DIV, OFF, true, UNROLL>(r, vg, p)
+                              : march_sum<true, DIV, OFF, true, UNROLL>(r, vg, p);
         integral *= p.step_size;
     }
     p.projections[((long long)a * p.U + u) * p.V + v] = integral;
 }
 
 // A CTA owns TU detector columns x (256/TU) rows of one view.
-template <int TU, bool DIV, bool OFF>
+template <int TU, bool DIV, bool OFF, int UNROLL = 1>
 __global__ void __launch_bounds__(256) fp_forward_kernel(FpArgs p) {
     __shared__ ViewGeo s_view;
     const int tiles_u = (p.U + TU - 1) / TU;
@@ -433,7 +435,7 @@ __global__ void __launch_bounds__(256) fp_forward_kernel(FpArgs p) {
     int u, v;
     tile_ray<TU>(tc, u, v);
     if (u >= p.U || v >= p.V) return;
-    forward_ray<DIV, OFF>(p, vg, tc.a, u, v);
+    forward_ray<DIV, OFF, UNROLL>(p, vg, tc.a, u, v);
 }
 
 // ---------------------------------------------------------------------------
@@ -1283,17 +1285,17 @@ __global__ void __launch_bounds__(256) batch_fold_kernel(BatchTables t) {
 
 namespace {
 
-template <int TU>
+template <int TU, int UNROLL = 1>
 int launch_forward_tu(const FpArgs& p, bool div, cudaStream_t s) {
     DGC_TRACE("fp_forward_kernel", s);
     const long long blocks = fp_tiles_per_view(p.U, p.V, TU) * (long long)p.A;
     const bool off = p.off_x != 0.0f || p.off_y != 0.0f || p.off_z != 0.0f;
     if (div) {
-        if (off) fp_forward_kernel<TU, true, true><<<(unsigned)blocks, 256, 0, s>>>(p);
-        else fp_forward_kernel<TU, true, false><<<(unsigned)blocks, 256, 0, s>>>(p);
+        if (off) fp_forward_kernel<TU, true, true, UNROLL><<<(unsigned)blocks, 256, 0, s>>>(p);
+        else fp_forward_kernel<TU, true, false, UNROLL><<<(unsigned)blocks, 256, 0, s>>>(p);
     } else {
-        if (off) fp_forward_kernel<TU, false, true><<<(unsigned)blocks, 256, 0, s>>>(p);
-        else fp_forward_kernel<TU, false, false><<<(unsigned)blocks, 256, 0, s>>>(p);
+        if (off) fp_forward_kernel<TU, false, true, UNROLL><<<(unsigned)blocks, 256, 0, s>>>(p);
+        else fp_forward_kernel<TU, false, false, UNROLL><<<(unsigned)blocks, 256, 0, s>>>(p);
     }
     DGC_LAUNCH_CHECK("fp_forward_kernel");
     return DGC_OK;
@@ -1349,7 +1351,7 @@ namespace {
 // D*H*W <= voxels_max applies; without one the L1 arm runs.
 struct FpArmRule {
     long long voxels_max;
-    int arm, slab;
+    int arm, slab, unroll;
 };
 std::mutex g_arm_mutex;
 FpArmRule g_arm_rules[16];
@@ -1408,12 +1410,13 @@ int launch_forward_tma(const FpArgs& p, bool div, cudaStream_t s, bool* used) {
 
 }  // namespace
 
-int fp_add_arm_rule(long long voxels_max, int arm, int slab) {
-    if (voxels_max < 1 || (arm != 0 && arm != 1) || (arm == 1 && slab != 2 && slab != 4))
+int fp_add_arm_rule(long long voxels_max, int arm, int slab, int unroll) {
+    if (voxels_max < 1 || (arm != 0 && arm != 1) || (arm == 1 && slab != 2 && slab != 4) ||
+        (unroll != 1 && unroll != 2) || (arm == 1 && unroll != 1))
         return -1;
     std::lock_guard<std::mutex> lock(g_arm_mutex);
     if (g_arm_count >= 16) return -2;
-    g_arm_rules[g_arm_count++] = FpArmRule{voxels_max, arm, arm == 1 ? slab : 0};
+    g_arm_rules[g_arm_count++] = FpArmRule{voxels_max, arm, arm == 1 ? slab : 0, unroll};
     return 0;
 }
 
@@ -1422,29 +1425,32 @@ void fp_clear_arm_rules() {
     g_arm_count = 0;
 }
 
-void fp_forward_arm(int D, int H, int W, int* arm, int* slab) {
+void fp_forward_arm(int D, int H, int W, int* arm, int* slab, int* unroll) {
     const long long voxels = (long long)D * H * W;
     std::lock_guard<std::mutex> lock(g_arm_mutex);
     for (int i = 0; i < g_arm_count; ++i)
         if (voxels <= g_arm_rules[i].voxels_max) {
             *arm = g_arm_rules[i].arm;
             *slab = g_arm_rules[i].slab;
+            *unroll = g_arm_rules[i].unroll;
             return;
         }
     *arm = 0;
     *slab = 0;
+    *unroll = 1;
 }
 
 int fp_launch_forward(const FpArgs& p, const FpTile& tile, cudaStream_t s) {
     const bool div = !is_pow2_float(p.voxel_size);
-    int arm = 0, slab = 0;
-    fp_forward_arm(p.D, p.H, p.W, &arm, &slab);
+    int arm = 0, slab = 0, unroll = 1;
+    fp_forward_arm(p.D, p.H, p.W, &arm, &slab, &unroll);
     if (arm == 1 && tile.tu == 8) {
         bool used = false;
         const int rc = slab == 2 ? launch_forward_tma<2>(p, div, s, &used)
                                  : launch_forward_tma<4>(p, div, s, &used);
         if (rc != DGC_OK || used) return rc;
     }
+    if (unroll == 2 && tile.tu == 8) return launch_forward_tu<8, 2>(p, div, s);
     switch (tile.tu) {
         case 8: return launch_forward_tu<8>(p, div, s);
         case 4: return launch_forward_tu<4>(p, div, s);

@@ -78,12 +78,13 @@ size_t fp_record_buffer_floats(int D, int H, int W);
 int fp_fold_records(const float* records, int D, int H, int W, float* grad, cudaStream_t s);
 int build_volume_quads(const float* vol, int D, int H, int W, float4* quads, cudaStream_t s);
 int fp_launch_forward(const FpArgs& p, const FpTile& tile, cudaStream_t s);
-// Forward arm per volume size: 0 = quads through L1 (fp_forward_kernel), 1 =
-// bricks staged by TMA (fp_forward_tma_kernel, slab of 2 or 4 cells); rules
-// registered by the autotuner (0 ok, -1 invalid, -2 table full).
-int fp_add_arm_rule(long long voxels_max, int arm, int slab);
+// Forward arm per volume size: 0 = quads through L1 (fp_forward_kernel, march
+// unrolled 1 or 2 times), 1 = bricks staged by TMA (fp_forward_tma_kernel,
+// slab of 2 or 4 cells); rules registered by the autotuner (0 ok, -1
+// invalid, -2 table full).
+int fp_add_arm_rule(long long voxels_max, int arm, int slab, int unroll);
 void fp_clear_arm_rules();
-void fp_forward_arm(int D, int H, int W, int* arm, int* slab);
+void fp_forward_arm(int D, int H, int W, int* arm, int* slab, int* unroll);
 int fp_launch_backward(const FpArgs& p, const FpTile& tile, bool gradvol, cudaStream_t s);
 int fp_launch_counts(const FpArgs& p, int64_t* counts, cudaStream_t s);
 // Fused projection -> masked squared error -> geometry-gradient terms (8-column

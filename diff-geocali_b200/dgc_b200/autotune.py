@@ -15,11 +15,12 @@ number of tiles, so it is not part of the key, and a bucket is timed on its
 first ``TUNE_VIEWS`` views.
 
 The forward projector of a single problem also has two arms
-(``tune_forward_arm``): quad loads through L1 (``fp_forward_kernel``) or volume
-bricks staged in shared memory by TMA, slabs of 2 or 4 cells along the ray
-bundle (``fp_forward_tma_kernel``).  Both give bitwise the same projections;
-the faster one per volume-size bucket (voxel count rounded up to a power of
-two) is registered in the library as an arm rule (``dgc_fp_add_arm_rule``).
+(``tune_forward_arm``): quad loads through L1 (``fp_forward_kernel``, its march
+loop unrolled once or twice) or volume bricks staged in shared memory by TMA,
+slabs of 2 or 4 cells along the ray bundle (``fp_forward_tma_kernel``).  All
+give bitwise the same projections; the fastest per volume-size bucket (voxel
+count rounded up to a power of two) is registered in the library as an arm
+rule (``dgc_fp_add_arm_rule``).
 
 The backprojector is tuned the same way (``tune_backprojector``): the Z
 blocking of its forward and backward (32*KZ voxels of a column per warp) and
@@ -42,7 +43,8 @@ BP_KZ_FORWARD = (1, 2, 4, 8)
 BP_KZ_BACKWARD = (2, 4, 8)
 BP_CTAS = ((8, 1), (4, 2))
 BP_TUNE_VIEWS = 360
-FORWARD_ARMS = ((0, 0), (1, 2), (1, 4))  # (arm, slab cells): L1 quads; TMA bricks
+# (arm, slab cells, march unroll): L1 quads unrolled once or twice; TMA bricks
+FORWARD_ARMS = ((0, 0, 1), (0, 0, 2), (1, 2, 1), (1, 4, 1))
 ARM_TUNE_VIEWS = 24
 
 
@@ -101,10 +103,10 @@ def arm_bucket(volume_shape) -> int:
     return 1 << max(0, (D * H * W - 1).bit_length())
 
 
-def time_forward_arm(problem, arm, slab, warmup=1, repeats=3):
+def time_forward_arm(problem, arm, slab, unroll=1, warmup=1, repeats=3):
     """Median device time [ms] of ``project`` of ``problem`` restricted to its
     first ``ARM_TUNE_VIEWS`` views with the forward arm ``arm`` (slab width
-    ``slab``).  The measurement replaces the library's arm rules by one rule
+    ``slab``, march unroll ``unroll``).  The measurement replaces the library's arm rules by one rule
     for this arm and clears them afterwards (``Autotuner.tune_forward_arm``
     registers its cached rules again)."""
     import torch
@@ -115,7 +117,7 @@ def time_forward_arm(problem, arm, slab, warmup=1, repeats=3):
     geom = [g[:views].contiguous() for g in problem.geometry]
     lib = _native.lib()
     _native.check(lib.dgc_fp_clear_arm_rules())
-    _native.check(lib.dgc_fp_add_arm_rule(1 << 62, int(arm), int(slab)))
+    _native.check(lib.dgc_fp_add_arm_rule(1 << 62, int(arm), int(slab), int(unroll)))
     try:
         def run():
             _ops.fp_forward(problem.volume, *geom, problem.pixel_size, problem.U, problem.V,
@@ -258,16 +260,17 @@ class Autotuner:
     def tune_forward_arm(self, problem):
         """Arm (L1 quads or TMA bricks) and slab width of the forward projector
         for the volume-size bucket of ``problem``: every arm timed once
-        (``measure_arm(problem, arm, slab) -> ms``, default
+        (``measure_arm(problem, arm, slab, unroll) -> ms``, default
         ``time_forward_arm``), cached, registered (``apply_forward_arm_rules``)."""
         key = f"fp-arm:{arm_bucket(problem.volume.shape)}"
         if key not in self.table:
-            ms = {f"{a}/{sl}": float(self.measure_arm(problem, a, sl)) for a, sl in FORWARD_ARMS}
+            ms = {f"{a}/{sl}/{un}": float(self.measure_arm(problem, a, sl, un))
+                  for a, sl, un in FORWARD_ARMS}
             best = min(ms, key=ms.get)
-            a, sl = (int(x) for x in best.split("/"))
+            a, sl, un = (int(x) for x in best.split("/"))
             self.table[key] = {"voxels_max": arm_bucket(problem.volume.shape), "arm": a,
-                               "slab": sl, "ms": ms,
-                               "arm_name": "l1" if a == 0 else f"tma-slab{sl}"}
+                               "slab": sl, "unroll": un, "ms": ms,
+                               "arm_name": f"l1-unroll{un}" if a == 0 else f"tma-slab{sl}"}
             self.measured.append(key)
             self._save()
         self.apply_forward_arm_rules()
@@ -284,7 +287,7 @@ class Autotuner:
                        key=lambda e: e["voxels_max"])
         for e in rules[:16]:
             _native.check(lib.dgc_fp_add_arm_rule(int(e["voxels_max"]), int(e["arm"]),
-                                                  int(e["slab"])))
+                                                  int(e["slab"]), int(e.get("unroll", 1))))
         return len(rules[:16])
 
     def apply_backprojector_rules(self):

@@ -329,15 +329,16 @@ int dgc_bp_tiles(int D, int A, int* kz_forward, int* kz_backward, int* cta_x, in
 
 /* Forward-projector arm rules (what the autotuner chose per volume size): a
  * dgc_project of D*H*W <= voxels_max voxels runs arm 0 (quad loads through
- * L1, fp_forward_kernel) or arm 1 (volume bricks staged in shared memory by
- * TMA, slab_cells = 2 or 4 cells per slab along the bundle's main axis).
- * Rules are tried in the order they were added (at most 16); without one,
- * arm 0.  Both arms give bitwise the same projections.  No counterpart in
+ * L1, fp_forward_kernel, its march loop unrolled `unroll` = 1 or 2 times) or
+ * arm 1 (volume bricks staged in shared memory by TMA, slab_cells = 2 or 4
+ * cells per slab along the bundle's main axis; unroll 1).  Rules are tried
+ * in the order they were added (at most 16); without one, arm 0 unrolled
+ * once.  Every arm gives bitwise the same projections.  No counterpart in
  * the reference. */
-int dgc_fp_add_arm_rule(long long voxels_max, int arm, int slab_cells);
+int dgc_fp_add_arm_rule(long long voxels_max, int arm, int slab_cells, int unroll);
 int dgc_fp_clear_arm_rules(void);
-/* The arm and slab a dgc_project of a D x H x W volume uses. */
-int dgc_fp_arm(int D, int H, int W, int* arm, int* slab_cells);
+/* The arm, slab and unroll a dgc_project of a D x H x W volume uses. */
+int dgc_fp_arm(int D, int H, int W, int* arm, int* slab_cells, int* unroll);
 
 /* volume[i] = max(volume[i], 0) in place (NaN stays NaN): the clamp that ends
  * an FDK reconstruction (filtering.py:197), after the partial volumes of a

@@ -25,10 +25,10 @@ def arm():
 
     lib = _native.lib()
 
-    def use(a, slab=0):
+    def use(a, slab=0, unroll=1):
         _native.check(lib.dgc_fp_clear_arm_rules())
         if a is not None:
-            _native.check(lib.dgc_fp_add_arm_rule(1 << 62, a, slab))
+            _native.check(lib.dgc_fp_add_arm_rule(1 << 62, a, slab, unroll))
 
     use(None)
     yield use
@@ -44,13 +44,15 @@ CASES = {
 }
 
 
-@pytest.mark.parametrize("slab", [2, 4])
+@pytest.mark.parametrize("variant", [(1, 2, 1), (1, 4, 1), (0, 0, 2)])
 @pytest.mark.parametrize("name", sorted(CASES))
-def test_tma_arm_is_bitwise_the_l1_arm(name, slab, arm):
+def test_tma_arm_is_bitwise_the_l1_arm(name, variant, arm):
+    """TMA bricks (slab 2 or 4) and the L1 arm's march unrolled twice, each
+    against the L1 arm unrolled once."""
     case = random_case(**CASES[name])
     arm(0)
     ref, _, _ = run_project(case)
-    arm(1, slab)
+    arm(*variant)
     got, _, _ = run_project(case)
     torch.cuda.synchronize()
     assert torch.isfinite(got).all()
@@ -80,15 +82,19 @@ def test_arm_rules(arm):
     from dgc_b200 import _native
 
     lib = _native.lib()
-    a, s = ctypes.c_int(), ctypes.c_int()
+    a, s, u = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+
+    def query(D, H, W):
+        _native.check(lib.dgc_fp_arm(D, H, W, ctypes.byref(a), ctypes.byref(s), ctypes.byref(u)))
+        return a.value, s.value, u.value
+
     arm(None)
-    _native.check(lib.dgc_fp_arm(64, 64, 64, ctypes.byref(a), ctypes.byref(s)))
-    assert (a.value, s.value) == (0, 0)
-    _native.check(lib.dgc_fp_add_arm_rule(100 ** 3, 1, 4))
-    _native.check(lib.dgc_fp_arm(64, 64, 64, ctypes.byref(a), ctypes.byref(s)))
-    assert (a.value, s.value) == (1, 4)
-    _native.check(lib.dgc_fp_arm(512, 512, 512, ctypes.byref(a), ctypes.byref(s)))
-    assert (a.value, s.value) == (0, 0)
-    for bad in ((0, 0, 0), (10, 2, 0), (10, 1, 3)):
+    assert query(64, 64, 64) == (0, 0, 1)
+    _native.check(lib.dgc_fp_add_arm_rule(100 ** 3, 1, 4, 1))
+    _native.check(lib.dgc_fp_add_arm_rule(600 ** 3, 0, 0, 2))
+    assert query(64, 64, 64) == (1, 4, 1)
+    assert query(512, 512, 512) == (0, 0, 2)
+    assert query(700, 700, 700) == (0, 0, 1)
+    for bad in ((0, 0, 0, 1), (10, 2, 0, 1), (10, 1, 3, 1), (10, 0, 0, 3), (10, 1, 2, 2)):
         with pytest.raises(RuntimeError):
             _native.check(lib.dgc_fp_add_arm_rule(*bad))
