@@ -304,11 +304,30 @@ class WarmStartNet(torch.nn.Module):
 # ----------------------------------------------------------------- data
 
 
-def network_input(measured, nominal_projection, mask):
-    """[A, 96, 96, 2] bf16: nominal reprojection and masked residual on the 96^2 grid."""
+def canvas_padding(acq) -> int:
+    """Detector pixels of zero padding on each side that put a scan on the
+    network's physical canvas: the training detector's extent (256 x 3 mm =
+    768 mm), which the 96^2 input grid covers at 8 mm per cell.  Zero for
+    scans of that extent (HALF, EVAL) and for ``acq`` None; a smaller
+    detector (CONFIG3: 384 mm) is centred on the canvas, so that the network
+    sees objects at the scale it was trained on (line integrals are in
+    physical units already)."""
+    if acq is None:
+        return 0
+    extent = TRAIN.detector * TRAIN.pixel
+    return max(0, int(round((extent / acq.pixel - acq.detector) / 2)))
+
+
+def network_input(measured, nominal_projection, mask, acq=None):
+    """[A, 96, 96, 2] bf16: nominal reprojection and masked residual on the
+    96^2 grid, the detector placed on the network's canvas (``canvas_padding``)."""
+    pad = canvas_padding(acq)
+    resid = (measured - nominal_projection) * mask
+    if pad:
+        nominal_projection = F.pad(nominal_projection, (pad, pad, pad, pad))
+        resid = F.pad(resid, (pad, pad, pad, pad))
     p = F.interpolate(nominal_projection[:, None], size=(INPUT_SIZE, INPUT_SIZE), mode="area")
-    r = F.interpolate(((measured - nominal_projection) * mask)[:, None],
-                      size=(INPUT_SIZE, INPUT_SIZE), mode="area")
+    r = F.interpolate(resid[:, None], size=(INPUT_SIZE, INPUT_SIZE), mode="area")
     x = torch.cat([p * 0.1, r], 1)                      # [A, 2, 96, 96]
     return x.permute(0, 2, 3, 1).contiguous().to(torch.bfloat16)
 
@@ -380,7 +399,7 @@ def train(steps=20000, lr=1e-3, seed=0, device="cuda", log_every=500, time_budge
             with torch.no_grad():
                 p_ref = project(st["volume"], *ref, scan.pixel_size, scan.U, scan.V,
                                 step_size=scan.step_size, voxel_size=scan.voxel_size)
-        x = network_input(st["measured"], p_ref, st["mask"])
+        x = network_input(st["measured"], p_ref, st["mask"], acq)
         out = net(x)
         pred, _ = predicted_geometry(out, ref, acq)
         loss = reprojection_loss(pred, st["true"], pts, acq.pixel) + 1e-4 * out.square().mean()
@@ -426,7 +445,7 @@ def predict(net, measured, nominal_projection, mask, nominal, acq: Acquisition, 
     residual (it was trained to map (reference reprojection, residual) to
     true - reference geometry).  Needs ``volume`` for stages > 1.
     """
-    out = net(network_input(measured, nominal_projection, mask))
+    out = net(network_input(measured, nominal_projection, mask, acq))
     geometry, delta = predicted_geometry(out, nominal, acq)
     scan = acq.scan
     for _ in range(1, int(stages)):
@@ -434,7 +453,7 @@ def predict(net, measured, nominal_projection, mask, nominal, acq: Acquisition, 
             raise ValueError("stages > 1 needs the volume")
         p = project(volume, *geometry, scan.pixel_size, scan.U, scan.V, step_size=scan.step_size,
                     voxel_size=scan.voxel_size)
-        out = net(network_input(measured, p, mask))
+        out = net(network_input(measured, p, mask, acq))
         geometry, _ = predicted_geometry(out, geometry, acq)
     return [g - n for g, n in zip(geometry, nominal)]
 
