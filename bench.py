@@ -331,15 +331,18 @@ def measure_ceilings(device, repeats=5):
             rate = max(rate, amount.value / (a.elapsed_time(b) * 1e-3))
         return rate
 
-    for level, key, iters in ((1, "l1_gather_gbs", 16384), (2, "l2_gather_gbs", 4096)):
-        out[key] = best(lambda ref, lv=level, it=iters: lib.dgc_ceiling_gather(
-            buf.data_ptr(), buf.numel() * 4, lv, it, 4, sink.data_ptr(), ref,
+    for level, key, iters, stride in ((1, "l1_gather_gbs", 16384, 16),
+                                      (2, "l2_gather_gbs", 4096, 16),
+                                      (1, "l1_gather_bp_pattern_gbs", 16384, 27)):
+        out[key] = best(lambda ref, lv=level, it=iters, st=stride: lib.dgc_ceiling_gather(
+            buf.data_ptr(), buf.numel() * 4, lv, it, 4, st, sink.data_ptr(), ref,
             stream.cuda_stream)) / 1e9
     out["issue_warp_inst_per_s"] = best(lambda ref: lib.dgc_ceiling_issue(
         2048, 4, sink.data_ptr(), ref, stream.cuda_stream))
     out["source"] = ("csrc/ceilings.cu, measured in this run: 16-byte warp loads of 512 "
                      "contiguous bytes from a 32 KiB (L1) or 64 MiB (L2) buffer in random "
-                     "order; independent FFMA chains")
+                     "order; the same from L1 with lanes 1.69 quads apart (the "
+                     "backprojector's spread at magnification 1.67); independent FFMA chains")
     del buf
     return out
 
@@ -618,6 +621,7 @@ def run_ours(args):
     if bp_ms is not None:
         bp_gbs = bp_bytes / (bp_ms * 1e-3) / 1e9
         rooflines[bp_key] = {"bound": "l1", "achieved": bp_gbs, "frac": bp_gbs / l1, "ms": bp_ms,
+                             "frac_of_bp_pattern": bp_gbs / ceilings["l1_gather_bp_pattern_gbs"],
                              "algorithmic_bytes": bp_bytes, "valid_voxel_views": n_valid}
 
     line = {
@@ -970,15 +974,15 @@ def run_tour(args):
 
 def run_arms(args):
     """The forward projector's arms -- quads through L1 (march unrolled once
-    or twice) and volume bricks staged by TMA (slabs of 2 or 4 cells) -- on
-    the fdk256 and target512
+    or twice, CTAs in view blocks of 0, 16 or 64), volume bricks staged by TMA
+    (slabs of 2 or 4 cells), z pairs through L1 -- on the fdk256 and target512
     phantoms and scans, each timed on ``--views`` views (default 48) with CUDA
     events (median of ``--steps``), checked bitwise equal, with the autotuner's
     choice per volume bucket."""
     import torch
 
     from dgc_b200 import _native, _ops
-    from dgc_b200.autotune import FORWARD_ARMS
+    from dgc_b200.autotune import FORWARD_ARMS, arm_name
 
     torch.cuda.set_device(0)
     device = torch.device("cuda", 0)
@@ -993,9 +997,9 @@ def run_arms(args):
             WORKLOAD["A"] = views
             vol, geom = make_instance(device, instance_seed(0))
             res, ref = {}, None
-            for arm, slab, unroll in FORWARD_ARMS:
+            for arm, slab, unroll, vb in FORWARD_ARMS:
                 _native.check(lib.dgc_fp_clear_arm_rules())
-                _native.check(lib.dgc_fp_add_arm_rule(1 << 62, arm, slab, unroll))
+                _native.check(lib.dgc_fp_add_arm_rule(1 << 62, arm, slab, unroll, vb))
 
                 def run():
                     return _ops.fp_forward(vol, *geom, w["pixel"], w["U"], w["V"], w["step"],
@@ -1014,7 +1018,7 @@ def run_arms(args):
                 same = None if ref is None else bool(torch.equal(p, ref))
                 if ref is None:
                     ref = p
-                res[f"l1-unroll{unroll}" if arm == 0 else f"tma-slab{slab}"] = {
+                res[arm_name(arm, slab, unroll, vb)] = {
                     "ms": ms, "grays_per_s": views * w["U"] * w["V"] / (ms * 1e-3) / 1e9,
                     "bitwise_equal_to_l1": same}
             _native.check(lib.dgc_fp_clear_arm_rules())

@@ -186,10 +186,14 @@ static int project_impl(const float* volume, int D, int H, int W, const Geometry
     p.quads = quads;
     p.projections = projections;
     p.error = status;
-    rc = build_volume_quads(volume, D, H, W, quads, s);
+    // the arm decided once: its layout is built into the quads' slice (the
+    // z-pair layout is smaller)
+    const FpArm arm = fp_forward_arm(D, H, W);
+    rc = arm.arm == 2 ? build_volume_pairs(volume, D, H, W, reinterpret_cast<float2*>(quads), s)
+                      : build_volume_quads(volume, D, H, W, quads, s);
     if (rc != DGC_OK) return rc;
     DGC_CUDA(cudaMemsetAsync(status, 0, sizeof(int), s));
-    return fp_launch_forward(p, kForwardTile, s);
+    return fp_launch_forward(p, kForwardTile, arm, s);
 }
 
 int dgc_project(const float* volume, int D, int H, int W, const float* angles, const float* sid,
@@ -713,16 +717,18 @@ int dgc_bp_tiles(int D, int A, int* kz_forward, int* kz_backward, int* cta_x, in
     return DGC_OK;
 }
 
-int dgc_fp_add_arm_rule(long long voxels_max, int arm, int slab_cells, int unroll) {
+int dgc_fp_add_arm_rule(long long voxels_max, int arm, int slab_cells, int unroll,
+                        int view_block) {
     using namespace dgc;
     clear_error();
-    const int rc = fp_add_arm_rule(voxels_max, arm, slab_cells, unroll);
+    const int rc = fp_add_arm_rule(voxels_max, arm, slab_cells, unroll, view_block);
     if (rc == -2) {
         set_error("dgc_fp_add_arm_rule: the rule table is full");
         return DGC_ERR_UNSUPPORTED;
     }
     DGC_REQUIRE(rc == 0, "dgc_fp_add_arm_rule: need voxels_max >= 1, arm 0 (L1) or 1 (TMA), "
-                         "for arm 1 slab_cells 2 or 4, unroll 1 or 2 (arm 1: 1)");
+                         "for arm 1 slab_cells 2 or 4, unroll 1 or 2 (arm 1: 1), "
+                         "0 <= view_block <= 65535");
     return DGC_OK;
 }
 
@@ -732,11 +738,11 @@ int dgc_fp_clear_arm_rules(void) {
     return DGC_OK;
 }
 
-int dgc_fp_arm(int D, int H, int W, int* arm, int* slab_cells, int* unroll) {
+int dgc_fp_arm(int D, int H, int W, int* arm, int* slab_cells, int* unroll, int* view_block) {
     using namespace dgc;
     clear_error();
-    DGC_REQUIRE(arm && slab_cells && unroll, "pointers must be non-null");
-    fp_forward_arm(D, H, W, arm, slab_cells, unroll);
+    DGC_REQUIRE(arm && slab_cells && unroll && view_block, "pointers must be non-null");
+    fp_forward_arm(D, H, W, arm, slab_cells, unroll, view_block);
     return DGC_OK;
 }
 

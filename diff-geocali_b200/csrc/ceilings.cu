@@ -10,7 +10,9 @@
 //
 //   * gather_ceiling_kernel: every warp issues independent 16-byte loads, one
 //     float4 per lane, a warp covering 512 contiguous bytes (four 128-byte
-//     lines) per load -- the best case for 16 bytes per lane.  With a small
+//     lines) per load -- the best case for 16 bytes per lane -- or, with a
+//     lane stride above one element, the wider spread of the backprojector's
+//     loads (lanes ~1.7 quads apart: seven lines per load).  With a small
 //     window shared by all CTAs the lines stay in each SM's L1 (the L1
 //     ceiling); with every CTA ranging over one buffer far larger
 //     than an SM's L1 but smaller than L2, in a random line order, nearly
@@ -28,14 +30,16 @@ constexpr int kGatherThreads = 256;
 constexpr int kGatherUnroll = 8;
 
 // window_mask + 1 = elements (float4) the loads range over, a power of two
-// >= 32, one window shared by all CTAs.  Each load of warp w reads elements
-// g*32 .. g*32+31 (one per lane) of the window, the 512-byte group g drawn by
-// a linear congruential sequence per warp, so consecutive loads of a warp
+// >= 64, one window shared by all CTAs.  Each load of warp w reads, lane l,
+// element g*64 + floor(l * stride16 / 16) of the window -- stride16 = 16: 32
+// contiguous elements (512 bytes); 27: lanes 1.6875 elements apart, the
+// backprojector's pattern at magnification 1.67 -- the 1 KiB group g drawn
+// by a linear congruential sequence per warp, so consecutive loads of a warp
 // touch unrelated lines.
 __global__ void __launch_bounds__(kGatherThreads)
 gather_ceiling_kernel(const float4* __restrict__ base, unsigned window_mask, int iterations,
-                      float* sink) {
-    const unsigned lane = threadIdx.x & 31;
+                      unsigned stride16, float* sink) {
+    const unsigned lane = ((threadIdx.x & 31) * stride16) >> 4;
     const unsigned warp = (blockIdx.x * (kGatherThreads / 32)) + (threadIdx.x >> 5);
     unsigned h = warp * 2654435761u + 12345u;
     float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -44,7 +48,7 @@ gather_ceiling_kernel(const float4* __restrict__ base, unsigned window_mask, int
 #pragma unroll
         for (int u = 0; u < kGatherUnroll; ++u) {
             h = h * 1664525u + 1013904223u;
-            q[u] = __ldg(base + ((((h >> 8) << 5) | lane) & window_mask));
+            q[u] = __ldg(base + ((((h >> 8) << 6) + lane) & window_mask));
         }
 #pragma unroll
         for (int u = 0; u < kGatherUnroll; ++u) {
@@ -93,7 +97,8 @@ int sm_count(int* out) {
 }  // namespace dgc
 
 extern "C" int dgc_ceiling_gather(const void* buffer, size_t buffer_bytes, int level, int iterations,
-                                  int ctas_per_sm, float* sink, double* bytes, void* stream) {
+                                  int ctas_per_sm, int lane_stride16, float* sink, double* bytes,
+                                  void* stream) {
     using namespace dgc;
     clear_error();
     DGC_REQUIRE(buffer && sink && bytes, "pointers must be non-null");
@@ -102,6 +107,8 @@ extern "C" int dgc_ceiling_gather(const void* buffer, size_t buffer_bytes, int l
                 "iterations must be a positive multiple of 8");
     DGC_REQUIRE(ctas_per_sm > 0 && ctas_per_sm <= 8, "ctas_per_sm must be in [1, 8]");
     DGC_REQUIRE(((uintptr_t)buffer & 15u) == 0, "buffer must be 16-byte aligned");
+    DGC_REQUIRE(lane_stride16 >= 16 && lane_stride16 <= 32,
+                "lane_stride16 must be in [16, 32] (lanes 1 to 2 elements apart)");
     int sms = 0;
     int rc = sm_count(&sms);
     if (rc != DGC_OK) return rc;
@@ -121,7 +128,8 @@ extern "C" int dgc_ceiling_gather(const void* buffer, size_t buffer_bytes, int l
     {
         DGC_TRACE("gather_ceiling_kernel", (cudaStream_t)stream);
         gather_ceiling_kernel<<<(unsigned)grid, kGatherThreads, 0, (cudaStream_t)stream>>>(
-            static_cast<const float4*>(buffer), window - 1u, iterations, sink);
+            static_cast<const float4*>(buffer), window - 1u, iterations, (unsigned)lane_stride16,
+            sink);
         DGC_LAUNCH_CHECK("gather_ceiling_kernel");
     }
     *bytes = (double)grid * kGatherThreads * (double)iterations * 16.0;

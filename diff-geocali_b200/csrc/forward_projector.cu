@@ -96,6 +96,47 @@ int build_volume_quads(const float* vol, int D, int H, int W, float4* quads, cud
     return DGC_OK;
 }
 
+// Z-pair layout of the forward's pair arm: P[(yq*(W+2) + xq)*(D+1) + zp] =
+// (v(z0, y, x), v(z1, y, x)) with y = yq-1, x = xq-1, z0 = zp-1, z1 = zp, all
+// clamped to the volume -- half the quads' bytes (8 per padded voxel).  A
+// cell's eight corners are four pairs (x and y neighbours at +(D+1) and
+// +(W+2)(D+1)), regrouped in registers into the two quads of the cell, so
+// the interpolation is bitwise the quad arm's.
+// grid: x = ceil((W+2)/32) * (H+2), y = ceil((D+1)/32); block (32, 8)
+__global__ void build_volume_pairs_kernel(const float* __restrict__ vol, int D, int H, int W,
+                                          float2* __restrict__ P) {
+    __shared__ float2 tile[32][33];
+    const int xtiles = (W + 2 + 31) / 32;
+    const int yq = blockIdx.x / xtiles;
+    const int xq0 = (blockIdx.x - yq * xtiles) * 32;
+    const int zp0 = blockIdx.y * 32;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    {
+        const int x = min(max(xq0 + tx - 1, 0), W - 1);
+        const int y = min(max(yq - 1, 0), H - 1);
+        for (int zl = ty; zl < 32; zl += 8) {
+            const int z0 = min(max(zp0 + zl - 1, 0), D - 1), z1 = min(zp0 + zl, D - 1);
+            tile[zl][tx] = make_float2(__ldg(vol + ((long long)z0 * H + y) * W + x),
+                                       __ldg(vol + ((long long)z1 * H + y) * W + x));
+        }
+    }
+    __syncthreads();
+    const int zp = zp0 + tx;
+    for (int xl = ty; xl < 32; xl += 8) {
+        const int xq = xq0 + xl;
+        if (xq <= W + 1 && zp <= D)
+            P[((long long)yq * (W + 2) + xq) * (D + 1) + zp] = tile[tx][xl];
+    }
+}
+
+int build_volume_pairs(const float* vol, int D, int H, int W, float2* pairs, cudaStream_t s) {
+    DGC_TRACE("build_volume_pairs", s);
+    const dim3 grid((unsigned)(ceil_div(W + 2, 32) * (long long)(H + 2)), (unsigned)ceil_div(D + 1, 32));
+    build_volume_pairs_kernel<<<grid, dim3(32, 8), 0, s>>>(vol, D, H, W, pairs);
+    DGC_LAUNCH_CHECK("build_volume_pairs");
+    return DGC_OK;
+}
+
 // ---------------------------------------------------------------------------
 // Per-view and per-ray set-up (reference arithmetic, kept expression for
 // expression so that t_min / t_max -- and with them the FP32 sample count --
@@ -378,13 +419,30 @@ __host__ __device__ __forceinline__ long long fp_tiles_per_view_dev(int U, int V
     return (long long)((U + tu - 1) / tu) * ((V + 256 / tu - 1) / (256 / tu));
 }
 
+// With p.view_block = B > 0, inside a band the views go in blocks of B and,
+// inside a block, the view runs fastest, then the u tile: the CTAs in flight
+// then cover B views of a few u tiles instead of every u tile of a few views
+// (a smaller set of volume cells, shared across views; a tuned dimension of
+// the forward).  The order changes no result.
 __device__ __forceinline__ TileCoord tile_coord(const FpArgs& p, int tiles_u) {
     int b = blockIdx.x;
     TileCoord tc;
-    tc.tu = b % tiles_u;
-    b /= tiles_u;
-    tc.a = b % p.A;
-    tc.tv = b / p.A;
+    if (p.view_block <= 0) {
+        tc.tu = b % tiles_u;
+        b /= tiles_u;
+        tc.a = b % p.A;
+        tc.tv = b / p.A;
+        return tc;
+    }
+    const int per_band = tiles_u * p.A;
+    tc.tv = b / per_band;
+    int r = b - tc.tv * per_band;
+    const int block_tiles = p.view_block * tiles_u;
+    const int vb = r / block_tiles;
+    r -= vb * block_tiles;
+    const int nv = min(p.view_block, p.A - vb * p.view_block);
+    tc.a = vb * p.view_block + r % nv;
+    tc.tu = r / nv;
     return tc;
 }
 
@@ -436,6 +494,73 @@ __global__ void __launch_bounds__(256) fp_forward_kernel(FpArgs p) {
     tile_ray<TU>(tc, u, v);
     if (u >= p.U || v >= p.V) return;
     forward_ray<DIV, OFF, UNROLL>(p, vg, tc.a, u, v);
+}
+
+// ---------------------------------------------------------------------------
+// Forward kernel, pair arm: the volume as z-pairs (half the quads' footprint)
+// ---------------------------------------------------------------------------
+
+// march_sum over the z-pair layout: the same samples, cells and packed lerps
+// (the four pairs of a cell regrouped into its two quads), four 8-byte loads
+// per new cell instead of two 16-byte ones.
+template <bool CLAMP, bool DIV, bool OFF, bool GUARD = true>
+__device__ __forceinline__ float march_sum_pairs(const RaySetup& r, const ViewGeo& vg,
+                                                 const FpArgs& p) {
+    const unsigned long long* __restrict__ P =
+        reinterpret_cast<const unsigned long long*>(p.quads);
+    const XYPacks k = make_xy_packs(r, vg, p);
+    const int nmax = step_bound(r, p.step_size);
+    const uint32_t sx = (uint32_t)(p.D + 1), sy = (uint32_t)(p.W + 2) * (uint32_t)(p.D + 1);
+    const uint32_t bias = (1u + sx + sy) - kFloorMagicBits * (1u + sx + sy);
+    float acc = 0.0f;
+    float t = r.tmin;
+    int n = 0;
+    CellQuads cq;
+#pragma unroll 1
+    for (; t <= r.tmax && (!GUARD || n < nmax); t += p.step_size, n += GUARD ? 1 : 0) {
+        const Cell c = sample_cell<CLAMP, DIV, OFF, true>(t, r, vg, p, k);
+        const uint32_t pi = c.bz + c.bx * sx + c.by * sy + bias;
+        if (pi != cq.qi) {
+            const float2 p00 = unpack2(__ldg(P + pi)), p10 = unpack2(__ldg(P + pi + sx));
+            const float2 p01 = unpack2(__ldg(P + pi + sy)), p11 = unpack2(__ldg(P + pi + sy + sx));
+            cq.q0 = make_ulonglong2(pack2(p00.x, p01.x), pack2(p10.x, p11.x));
+            cq.q1 = make_ulonglong2(pack2(p00.y, p01.y), pack2(p10.y, p11.y));
+            cq.qi = pi;
+        }
+        const ulonglong2 q0 = cq.q0, q1 = cq.q1;
+        const f32x2 wx = pack2(c.fx, c.fx);
+        const f32x2 e0 = lerp2(q0.x, q0.y, wx);
+        const f32x2 e1 = lerp2(q1.x, q1.y, wx);
+        const float2 e = unpack2(lerp2(e0, e1, pack2(c.fz, c.fz)));
+        acc += lerpf(e.x, e.y, c.fy);
+    }
+    return acc;
+}
+
+template <int TU, bool DIV, bool OFF>
+__global__ void __launch_bounds__(256) fp_forward_pairs_kernel(FpArgs p) {
+    __shared__ ViewGeo s_view;
+    const int tiles_u = (p.U + TU - 1) / TU;
+    const TileCoord tc = tile_coord(p, tiles_u);
+    if (threadIdx.x == 0) load_view(p.g, tc.a, s_view);
+    __syncthreads();
+    const ViewGeo vg = s_view;
+    int u, v;
+    tile_ray<TU>(tc, u, v);
+    if (u >= p.U || v >= p.V) return;
+    const RaySetup r = setup_ray(vg, u, v, p);
+    float integral = 0.0f;
+    if (r.ok && r.hit) {
+        const bool inside = ray_inside_pad<DIV>(r, vg, p);
+        if (steps_advance(r, p.step_size))
+            integral = inside ? march_sum_pairs<false, DIV, OFF, false>(r, vg, p)
+                              : march_sum_pairs<true, DIV, OFF, false>(r, vg, p);
+        else
+            integral = inside ? march_sum_pairs<false, DIV, OFF>(r, vg, p)
+                              : march_sum_pairs<true, DIV, OFF>(r, vg, p);
+        integral *= p.step_size;
+    }
+    p.projections[((long long)tc.a * p.U + u) * p.V + v] = integral;
 }
 
 // ---------------------------------------------------------------------------
@@ -1351,7 +1476,7 @@ namespace {
 // D*H*W <= voxels_max applies; without one the L1 arm runs.
 struct FpArmRule {
     long long voxels_max;
-    int arm, slab, unroll;
+    int arm, slab, unroll, view_block;
 };
 std::mutex g_arm_mutex;
 FpArmRule g_arm_rules[16];
@@ -1410,13 +1535,15 @@ int launch_forward_tma(const FpArgs& p, bool div, cudaStream_t s, bool* used) {
 
 }  // namespace
 
-int fp_add_arm_rule(long long voxels_max, int arm, int slab, int unroll) {
-    if (voxels_max < 1 || (arm != 0 && arm != 1) || (arm == 1 && slab != 2 && slab != 4) ||
-        (unroll != 1 && unroll != 2) || (arm == 1 && unroll != 1))
+int fp_add_arm_rule(long long voxels_max, int arm, int slab, int unroll, int view_block) {
+    if (voxels_max < 1 || arm < 0 || arm > 2 || (arm == 1 && slab != 2 && slab != 4) ||
+        (unroll != 1 && unroll != 2) || (arm != 0 && unroll != 1) || view_block < 0 ||
+        view_block > 65535)
         return -1;
     std::lock_guard<std::mutex> lock(g_arm_mutex);
     if (g_arm_count >= 16) return -2;
-    g_arm_rules[g_arm_count++] = FpArmRule{voxels_max, arm, arm == 1 ? slab : 0, unroll};
+    g_arm_rules[g_arm_count++] =
+        FpArmRule{voxels_max, arm, arm == 1 ? slab : 0, unroll, view_block};
     return 0;
 }
 
@@ -1425,7 +1552,7 @@ void fp_clear_arm_rules() {
     g_arm_count = 0;
 }
 
-void fp_forward_arm(int D, int H, int W, int* arm, int* slab, int* unroll) {
+void fp_forward_arm(int D, int H, int W, int* arm, int* slab, int* unroll, int* view_block) {
     const long long voxels = (long long)D * H * W;
     std::lock_guard<std::mutex> lock(g_arm_mutex);
     for (int i = 0; i < g_arm_count; ++i)
@@ -1433,24 +1560,47 @@ void fp_forward_arm(int D, int H, int W, int* arm, int* slab, int* unroll) {
             *arm = g_arm_rules[i].arm;
             *slab = g_arm_rules[i].slab;
             *unroll = g_arm_rules[i].unroll;
+            *view_block = g_arm_rules[i].view_block;
             return;
         }
     *arm = 0;
     *slab = 0;
     *unroll = 1;
+    *view_block = 0;
 }
 
-int fp_launch_forward(const FpArgs& p, const FpTile& tile, cudaStream_t s) {
+FpArm fp_forward_arm(int D, int H, int W) {
+    FpArm a;
+    fp_forward_arm(D, H, W, &a.arm, &a.slab, &a.unroll, &a.view_block);
+    return a;
+}
+
+int fp_launch_forward(const FpArgs& args, const FpTile& tile, const FpArm& a, cudaStream_t s) {
+    FpArgs p = args;
+    p.view_block = a.view_block;
     const bool div = !is_pow2_float(p.voxel_size);
-    int arm = 0, slab = 0, unroll = 1;
-    fp_forward_arm(p.D, p.H, p.W, &arm, &slab, &unroll);
-    if (arm == 1 && tile.tu == 8) {
+    if (a.arm == 2 && tile.tu == 8) {
+        // p.quads holds the z-pair layout (the caller built it for this arm)
+        DGC_TRACE("fp_forward_pairs_kernel", s);
+        const long long blocks = fp_tiles_per_view(p.U, p.V, 8) * (long long)p.A;
+        const bool off = p.off_x != 0.0f || p.off_y != 0.0f || p.off_z != 0.0f;
+        if (div) {
+            if (off) fp_forward_pairs_kernel<8, true, true><<<(unsigned)blocks, 256, 0, s>>>(p);
+            else fp_forward_pairs_kernel<8, true, false><<<(unsigned)blocks, 256, 0, s>>>(p);
+        } else {
+            if (off) fp_forward_pairs_kernel<8, false, true><<<(unsigned)blocks, 256, 0, s>>>(p);
+            else fp_forward_pairs_kernel<8, false, false><<<(unsigned)blocks, 256, 0, s>>>(p);
+        }
+        DGC_LAUNCH_CHECK("fp_forward_pairs_kernel");
+        return DGC_OK;
+    }
+    if (a.arm == 1 && tile.tu == 8) {
         bool used = false;
-        const int rc = slab == 2 ? launch_forward_tma<2>(p, div, s, &used)
-                                 : launch_forward_tma<4>(p, div, s, &used);
+        const int rc = a.slab == 2 ? launch_forward_tma<2>(p, div, s, &used)
+                                   : launch_forward_tma<4>(p, div, s, &used);
         if (rc != DGC_OK || used) return rc;
     }
-    if (unroll == 2 && tile.tu == 8) return launch_forward_tu<8, 2>(p, div, s);
+    if (a.unroll == 2 && tile.tu == 8) return launch_forward_tu<8, 2>(p, div, s);
     switch (tile.tu) {
         case 8: return launch_forward_tu<8>(p, div, s);
         case 4: return launch_forward_tu<4>(p, div, s);

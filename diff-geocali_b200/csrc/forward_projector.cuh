@@ -21,6 +21,7 @@ struct FpArgs {
     uint32_t gz_x, gz_y, gz_bias;
     double* partials;  // [A][tiles][8]
     int* error;        // device word set to 1 when a bounded wait gives up (TMA arm), or null
+    int view_block;    // CTA order: 0 = u tile fastest; B > 0 = views in blocks of B (tile_coord)
 };
 
 // Ray tile of a CTA: TU detector columns x (256/TU) rows; the 32 lanes of a
@@ -77,14 +78,22 @@ long long fp_tiles_per_view(int U, int V, int tu);
 size_t fp_record_buffer_floats(int D, int H, int W);
 int fp_fold_records(const float* records, int D, int H, int W, float* grad, cudaStream_t s);
 int build_volume_quads(const float* vol, int D, int H, int W, float4* quads, cudaStream_t s);
-int fp_launch_forward(const FpArgs& p, const FpTile& tile, cudaStream_t s);
+// The forward's arm, slab, unroll and CTA order for a volume (the arm rules).
+struct FpArm {
+    int arm = 0, slab = 0, unroll = 1, view_block = 0;
+};
+// With arm 2 (z pairs) p.quads must hold build_volume_pairs' layout, else the quads.
+int fp_launch_forward(const FpArgs& p, const FpTile& tile, const FpArm& arm, cudaStream_t s);
+int build_volume_pairs(const float* vol, int D, int H, int W, float2* pairs, cudaStream_t s);
 // Forward arm per volume size: 0 = quads through L1 (fp_forward_kernel, march
 // unrolled 1 or 2 times), 1 = bricks staged by TMA (fp_forward_tma_kernel,
-// slab of 2 or 4 cells); rules registered by the autotuner (0 ok, -1
-// invalid, -2 table full).
-int fp_add_arm_rule(long long voxels_max, int arm, int slab, int unroll);
+// slab of 2 or 4 cells), 2 = z pairs through L1 (fp_forward_pairs_kernel,
+// half the quads' bytes); and the CTA order (view_block, tile_coord); rules
+// registered by the autotuner (0 ok, -1 invalid, -2 table full).
+int fp_add_arm_rule(long long voxels_max, int arm, int slab, int unroll, int view_block);
 void fp_clear_arm_rules();
-void fp_forward_arm(int D, int H, int W, int* arm, int* slab, int* unroll);
+void fp_forward_arm(int D, int H, int W, int* arm, int* slab, int* unroll, int* view_block);
+FpArm fp_forward_arm(int D, int H, int W);
 int fp_launch_backward(const FpArgs& p, const FpTile& tile, bool gradvol, cudaStream_t s);
 int fp_launch_counts(const FpArgs& p, int64_t* counts, cudaStream_t s);
 // Fused projection -> masked squared error -> geometry-gradient terms (8-column

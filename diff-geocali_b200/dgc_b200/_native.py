@@ -102,10 +102,10 @@ SIGNATURES = {
     "dgc_trace_count": (_I, []),
     "dgc_trace_get": (_I, [_I, ctypes.c_char_p, _I, ctypes.POINTER(_F)]),
     "dgc_trace_clear": (None, []),
-    "dgc_fp_add_arm_rule": (_I, [ctypes.c_longlong, _I, _I, _I]),
+    "dgc_fp_add_arm_rule": (_I, [ctypes.c_longlong, _I, _I, _I, _I]),
     "dgc_fp_clear_arm_rules": (_I, []),
-    "dgc_fp_arm": (_I, [_I, _I, _I, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I)]),
-    "dgc_ceiling_gather": (_I, [_P, _S, _I, _I, _I, _P, ctypes.POINTER(_D), _P]),
+    "dgc_fp_arm": (_I, [_I, _I, _I, *[ctypes.POINTER(_I)] * 4]),
+    "dgc_ceiling_gather": (_I, [_P, _S, _I, _I, _I, _I, _P, ctypes.POINTER(_D), _P]),
     "dgc_ceiling_issue": (_I, [_I, _I, _P, ctypes.POINTER(_D), _P]),
 }
 

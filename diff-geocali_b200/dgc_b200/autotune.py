@@ -16,8 +16,10 @@ first ``TUNE_VIEWS`` views.
 
 The forward projector of a single problem also has two arms
 (``tune_forward_arm``): quad loads through L1 (``fp_forward_kernel``, its march
-loop unrolled once or twice) or volume bricks staged in shared memory by TMA,
-slabs of 2 or 4 cells along the ray bundle (``fp_forward_tma_kernel``).  All
+loop unrolled once or twice), volume bricks staged in shared memory by TMA,
+slabs of 2 or 4 cells along the ray bundle (``fp_forward_tma_kernel``), or the
+volume as z pairs, half the quads' bytes (``fp_forward_pairs_kernel``); and the
+order of the CTAs (every u tile of a view first, or views in blocks).  All
 give bitwise the same projections; the fastest per volume-size bucket (voxel
 count rounded up to a power of two) is registered in the library as an arm
 rule (``dgc_fp_add_arm_rule``).
@@ -43,8 +45,11 @@ BP_KZ_FORWARD = (1, 2, 4, 8)
 BP_KZ_BACKWARD = (2, 4, 8)
 BP_CTAS = ((8, 1), (4, 2))
 BP_TUNE_VIEWS = 360
-# (arm, slab cells, march unroll): L1 quads unrolled once or twice; TMA bricks
-FORWARD_ARMS = ((0, 0, 1), (0, 0, 2), (1, 2, 1), (1, 4, 1))
+# (arm, slab cells, march unroll, view block): L1 quads unrolled once or twice,
+# CTAs in view blocks of 0 (every u tile of a view first), 16 or 64; TMA
+# bricks; z pairs through L1
+FORWARD_ARMS = ((0, 0, 1, 0), (0, 0, 2, 0), (0, 0, 1, 16), (0, 0, 1, 64), (1, 2, 1, 0),
+                (1, 4, 1, 0), (2, 0, 1, 0), (2, 0, 1, 64))
 ARM_TUNE_VIEWS = 24
 
 
@@ -97,16 +102,22 @@ def time_problem(problem, direction: str, tile: int, grad_volume=True, warmup=1,
     return sorted(times)[len(times) // 2]
 
 
+def arm_name(arm, slab, unroll, view_block) -> str:
+    """Label of a forward arm: l1-unroll1, l1-unroll1-vb64, tma-slab4, pairs, ..."""
+    base = {0: f"l1-unroll{unroll}", 1: f"tma-slab{slab}", 2: "pairs"}[int(arm)]
+    return base + (f"-vb{view_block}" if view_block else "")
+
+
 def arm_bucket(volume_shape) -> int:
     """Voxel count of a forward-arm bucket: D*H*W rounded up to a power of two."""
     D, H, W = (int(x) for x in volume_shape)
     return 1 << max(0, (D * H * W - 1).bit_length())
 
 
-def time_forward_arm(problem, arm, slab, unroll=1, warmup=1, repeats=3):
+def time_forward_arm(problem, arm, slab, unroll=1, view_block=0, warmup=1, repeats=3):
     """Median device time [ms] of ``project`` of ``problem`` restricted to its
     first ``ARM_TUNE_VIEWS`` views with the forward arm ``arm`` (slab width
-    ``slab``, march unroll ``unroll``).  The measurement replaces the library's arm rules by one rule
+    ``slab``, march unroll ``unroll``, CTA view block ``view_block``).  The measurement replaces the library's arm rules by one rule
     for this arm and clears them afterwards (``Autotuner.tune_forward_arm``
     registers its cached rules again)."""
     import torch
@@ -117,7 +128,8 @@ def time_forward_arm(problem, arm, slab, unroll=1, warmup=1, repeats=3):
     geom = [g[:views].contiguous() for g in problem.geometry]
     lib = _native.lib()
     _native.check(lib.dgc_fp_clear_arm_rules())
-    _native.check(lib.dgc_fp_add_arm_rule(1 << 62, int(arm), int(slab), int(unroll)))
+    _native.check(lib.dgc_fp_add_arm_rule(1 << 62, int(arm), int(slab), int(unroll),
+                                          int(view_block)))
     try:
         def run():
             _ops.fp_forward(problem.volume, *geom, problem.pixel_size, problem.U, problem.V,
@@ -260,17 +272,17 @@ class Autotuner:
     def tune_forward_arm(self, problem):
         """Arm (L1 quads or TMA bricks) and slab width of the forward projector
         for the volume-size bucket of ``problem``: every arm timed once
-        (``measure_arm(problem, arm, slab, unroll) -> ms``, default
+        (``measure_arm(problem, arm, slab, unroll, view_block) -> ms``, default
         ``time_forward_arm``), cached, registered (``apply_forward_arm_rules``)."""
         key = f"fp-arm:{arm_bucket(problem.volume.shape)}"
         if key not in self.table:
-            ms = {f"{a}/{sl}/{un}": float(self.measure_arm(problem, a, sl, un))
-                  for a, sl, un in FORWARD_ARMS}
+            ms = {f"{a}/{sl}/{un}/{vb}": float(self.measure_arm(problem, a, sl, un, vb))
+                  for a, sl, un, vb in FORWARD_ARMS}
             best = min(ms, key=ms.get)
-            a, sl, un = (int(x) for x in best.split("/"))
+            a, sl, un, vb = (int(x) for x in best.split("/"))
             self.table[key] = {"voxels_max": arm_bucket(problem.volume.shape), "arm": a,
-                               "slab": sl, "unroll": un, "ms": ms,
-                               "arm_name": f"l1-unroll{un}" if a == 0 else f"tma-slab{sl}"}
+                               "slab": sl, "unroll": un, "view_block": vb, "ms": ms,
+                               "arm_name": arm_name(a, sl, un, vb)}
             self.measured.append(key)
             self._save()
         self.apply_forward_arm_rules()
@@ -287,7 +299,8 @@ class Autotuner:
                        key=lambda e: e["voxels_max"])
         for e in rules[:16]:
             _native.check(lib.dgc_fp_add_arm_rule(int(e["voxels_max"]), int(e["arm"]),
-                                                  int(e["slab"]), int(e.get("unroll", 1))))
+                                                  int(e["slab"]), int(e.get("unroll", 1)),
+                                                  int(e.get("view_block", 0))))
         return len(rules[:16])
 
     def apply_backprojector_rules(self):
@@ -328,5 +341,5 @@ def backprojector_tiles(D, A):
 
 
 __all__ = ["Autotuner", "bucket", "bp_bucket", "arm_bucket", "time_problem",
-           "time_backprojector", "time_forward_arm", "backprojector_tiles", "FORWARD_TILES",
+           "time_backprojector", "time_forward_arm", "arm_name", "backprojector_tiles", "FORWARD_TILES",
            "BACKWARD_TILES", "FORWARD_ARMS"]

@@ -329,16 +329,21 @@ int dgc_bp_tiles(int D, int A, int* kz_forward, int* kz_backward, int* cta_x, in
 
 /* Forward-projector arm rules (what the autotuner chose per volume size): a
  * dgc_project of D*H*W <= voxels_max voxels runs arm 0 (quad loads through
- * L1, fp_forward_kernel, its march loop unrolled `unroll` = 1 or 2 times) or
+ * L1, fp_forward_kernel, its march loop unrolled `unroll` = 1 or 2 times),
  * arm 1 (volume bricks staged in shared memory by TMA, slab_cells = 2 or 4
- * cells per slab along the bundle's main axis; unroll 1).  Rules are tried
- * in the order they were added (at most 16); without one, arm 0 unrolled
- * once.  Every arm gives bitwise the same projections.  No counterpart in
- * the reference. */
-int dgc_fp_add_arm_rule(long long voxels_max, int arm, int slab_cells, int unroll);
+ * cells per slab along the bundle's main axis; unroll 1) or arm 2 (the
+ * volume as z pairs, half the quads' bytes, four 8-byte loads per cell;
+ * unroll 1), with its CTAs in
+ * the order view_block: 0 = every u tile of a view, then the next view;
+ * B > 0 = inside a detector band, views in blocks of B, the view fastest
+ * inside a block.  Rules are tried in the order they were added (at most
+ * 16); without one, arm 0, unroll 1, order 0.  Every choice gives bitwise
+ * the same projections.  No counterpart in the reference. */
+int dgc_fp_add_arm_rule(long long voxels_max, int arm, int slab_cells, int unroll,
+                        int view_block);
 int dgc_fp_clear_arm_rules(void);
-/* The arm, slab and unroll a dgc_project of a D x H x W volume uses. */
-int dgc_fp_arm(int D, int H, int W, int* arm, int* slab_cells, int* unroll);
+/* The arm, slab, unroll and CTA order a dgc_project of a D x H x W volume uses. */
+int dgc_fp_arm(int D, int H, int W, int* arm, int* slab_cells, int* unroll, int* view_block);
 
 /* volume[i] = max(volume[i], 0) in place (NaN stays NaN): the clamp that ends
  * an FDK reconstruction (filtering.py:197), after the partial volumes of a
@@ -493,8 +498,10 @@ void dgc_trace_clear(void);
 /* ---------------------------------------------------------------------- */
 
 /* Launches one pass of 16-byte loads on every SM (ctas_per_sm CTAs of 256
- * threads per SM, `iterations` loads per thread, a multiple of 8): each warp
- * load covers 512 contiguous bytes, groups in a random order.  level 1: the
+ * threads per SM, `iterations` loads per thread, a multiple of 8): lane l of
+ * a warp load reads element floor(l * lane_stride16 / 16) of a 1 KiB group
+ * (lane_stride16 = 16: 512 contiguous bytes; 27: lanes 1.69 elements apart,
+ * the backprojector's spread), groups in a random order.  level 1: the
  * groups of a 32 KiB window of `buffer` (resident in every SM's L1); level 2:
  * of the largest power-of-two prefix of `buffer` (at least 16 MiB; made far
  * larger than an SM's L1 and smaller than L2, its loads are served by L2).
@@ -502,7 +509,8 @@ void dgc_trace_clear(void);
  * rate over the caller's event timing.  `buffer` should be zeroed; `sink` is
  * a float that the kernel never writes for zeroed input. */
 int dgc_ceiling_gather(const void* buffer, size_t buffer_bytes, int level, int iterations,
-                       int ctas_per_sm, float* sink, double* bytes, void* stream);
+                       int ctas_per_sm, int lane_stride16, float* sink, double* bytes,
+                       void* stream);
 
 /* Launches independent FFMA chains on every SM (ctas_per_sm CTAs of 256
  * threads per SM, 128 FFMA per iteration and thread); *warp_instructions

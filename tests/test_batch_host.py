@@ -195,28 +195,26 @@ def test_autotuner_tunes_forward_arm(tmp_path):
         assert arm_bucket((100, 20, 20)) == 1 << 16
         calls = []
 
-        def fake(problem, arm, slab, unroll):
-            calls.append((arm, slab, unroll))
-            return {(0, 0, 1): 3.0, (0, 0, 2): 3.1, (1, 2, 1): 2.5, (1, 4, 1): 2.0}[(arm, slab,
-                                                                                    unroll)]
+        def fake(problem, arm, slab, unroll, view_block):
+            calls.append((arm, slab, unroll, view_block))
+            return 2.0 if (arm, slab) == (1, 4) else 3.0 + 0.1 * arm + 0.01 * view_block
 
         pr = SimpleNamespace(volume=SimpleNamespace(shape=(512, 512, 512)))
         path = tmp_path / "tiles.json"
         e = Autotuner(cache_path=path, measure_arm=fake).tune_forward_arm(pr)
         assert (e["arm"], e["slab"], e["arm_name"]) == (1, 4, "tma-slab4")
         assert sorted(calls) == sorted(FORWARD_ARMS)
-        a, s, u = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        out = [ctypes.c_int() for _ in range(4)]
 
         def query(D, H, W):
-            _native.check(lib.dgc_fp_arm(D, H, W, ctypes.byref(a), ctypes.byref(s),
-                                         ctypes.byref(u)))
-            return a.value, s.value, u.value
+            _native.check(lib.dgc_fp_arm(D, H, W, *[ctypes.byref(x) for x in out]))
+            return tuple(x.value for x in out)
 
-        assert query(512, 512, 512) == (1, 4, 1)
-        assert query(600, 512, 512) == (0, 0, 1)  # beyond every bucket: the L1 arm
+        assert query(512, 512, 512) == (1, 4, 1, 0)
+        assert query(600, 512, 512) == (0, 0, 1, 0)  # beyond every bucket: the L1 arm
         lib.dgc_fp_clear_arm_rules()
         again = Autotuner(cache_path=path, measure_arm=lambda *x: pytest.fail("cache miss"))
         assert again.tune_forward_arm(pr)["arm"] == 1
-        assert query(512, 512, 512) == (1, 4, 1)
+        assert query(512, 512, 512) == (1, 4, 1, 0)
     finally:
         lib.dgc_fp_clear_arm_rules()

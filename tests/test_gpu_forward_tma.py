@@ -25,10 +25,10 @@ def arm():
 
     lib = _native.lib()
 
-    def use(a, slab=0, unroll=1):
+    def use(a, slab=0, unroll=1, view_block=0):
         _native.check(lib.dgc_fp_clear_arm_rules())
         if a is not None:
-            _native.check(lib.dgc_fp_add_arm_rule(1 << 62, a, slab, unroll))
+            _native.check(lib.dgc_fp_add_arm_rule(1 << 62, a, slab, unroll, view_block))
 
     use(None)
     yield use
@@ -44,11 +44,13 @@ CASES = {
 }
 
 
-@pytest.mark.parametrize("variant", [(1, 2, 1), (1, 4, 1), (0, 0, 2)])
+@pytest.mark.parametrize("variant", [(1, 2, 1, 0), (1, 4, 1, 0), (0, 0, 2, 0), (0, 0, 1, 3),
+                                     (2, 0, 1, 0), (2, 0, 1, 64)])
 @pytest.mark.parametrize("name", sorted(CASES))
 def test_tma_arm_is_bitwise_the_l1_arm(name, variant, arm):
-    """TMA bricks (slab 2 or 4) and the L1 arm's march unrolled twice, each
-    against the L1 arm unrolled once."""
+    """TMA bricks (slab 2 or 4), the L1 arm's march unrolled twice, CTAs in
+    view blocks, and the z-pair layout, each against the L1 arm unrolled once
+    in the default order."""
     case = random_case(**CASES[name])
     arm(0)
     ref, _, _ = run_project(case)
@@ -59,8 +61,8 @@ def test_tma_arm_is_bitwise_the_l1_arm(name, variant, arm):
     assert torch.equal(got, ref), float((got - ref).abs().max())
 
 
-@pytest.mark.parametrize("slab", [2, 4])
-def test_tma_arm_config2_views(slab, arm):
+@pytest.mark.parametrize("variant", [(1, 2, 1, 0), (1, 4, 1, 0), (2, 0, 1, 0), (0, 0, 1, 16)])
+def test_tma_arm_config2_views(variant, arm):
     """A 256^3 phantom, 24 views of config 2's scan (384^2, sid 1000, sod 600)."""
     from cbct_backprojector import project
     from dgc_b200.phantoms import circular_geometry, ellipsoid_phantom
@@ -70,7 +72,7 @@ def test_tma_arm_config2_views(slab, arm):
     geom[0] = geom[0] + 0.013  # off the axis-aligned angles
     arm(0)
     ref = project(vol, *geom, 1.0, 384, 384, step_size=0.5, voxel_size=1.0)
-    arm(1, slab)
+    arm(*variant)
     got = project(vol, *geom, 1.0, 384, 384, step_size=0.5, voxel_size=1.0)
     torch.cuda.synchronize()
     assert torch.equal(got, ref), float((got - ref).abs().max())
@@ -82,19 +84,20 @@ def test_arm_rules(arm):
     from dgc_b200 import _native
 
     lib = _native.lib()
-    a, s, u = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    out = [ctypes.c_int() for _ in range(4)]
 
     def query(D, H, W):
-        _native.check(lib.dgc_fp_arm(D, H, W, ctypes.byref(a), ctypes.byref(s), ctypes.byref(u)))
-        return a.value, s.value, u.value
+        _native.check(lib.dgc_fp_arm(D, H, W, *[ctypes.byref(x) for x in out]))
+        return tuple(x.value for x in out)
 
     arm(None)
-    assert query(64, 64, 64) == (0, 0, 1)
-    _native.check(lib.dgc_fp_add_arm_rule(100 ** 3, 1, 4, 1))
-    _native.check(lib.dgc_fp_add_arm_rule(600 ** 3, 0, 0, 2))
-    assert query(64, 64, 64) == (1, 4, 1)
-    assert query(512, 512, 512) == (0, 0, 2)
-    assert query(700, 700, 700) == (0, 0, 1)
-    for bad in ((0, 0, 0, 1), (10, 2, 0, 1), (10, 1, 3, 1), (10, 0, 0, 3), (10, 1, 2, 2)):
+    assert query(64, 64, 64) == (0, 0, 1, 0)
+    _native.check(lib.dgc_fp_add_arm_rule(100 ** 3, 1, 4, 1, 0))
+    _native.check(lib.dgc_fp_add_arm_rule(600 ** 3, 0, 0, 2, 64))
+    assert query(64, 64, 64) == (1, 4, 1, 0)
+    assert query(512, 512, 512) == (0, 0, 2, 64)
+    assert query(700, 700, 700) == (0, 0, 1, 0)
+    for bad in ((0, 0, 0, 1, 0), (10, 3, 0, 1, 0), (10, 1, 3, 1, 0), (10, 0, 0, 3, 0),
+                (10, 1, 2, 2, 0), (10, 2, 0, 2, 0), (10, 0, 0, 1, -1)):
         with pytest.raises(RuntimeError):
             _native.check(lib.dgc_fp_add_arm_rule(*bad))
