@@ -1015,11 +1015,13 @@ def run_arms(args):
                     b.synchronize()
                     times.append(a.elapsed_time(b))
                 ms = statistics.median(times)
+                spread = [min(times), max(times)]
                 same = None if ref is None else bool(torch.equal(p, ref))
                 if ref is None:
                     ref = p
                 res[arm_name(arm, slab, unroll, vb)] = {
-                    "ms": ms, "grays_per_s": views * w["U"] * w["V"] / (ms * 1e-3) / 1e9,
+                    "ms": ms, "ms_range": spread,
+                    "grays_per_s": views * w["U"] * w["V"] / (ms * 1e-3) / 1e9,
                     "bitwise_equal_to_l1": same}
             _native.check(lib.dgc_fp_clear_arm_rules())
             out[key] = {"views": views, "volume": w["D"], "detector": w["U"], "arms": res}

@@ -46,10 +46,10 @@ BP_KZ_BACKWARD = (2, 4, 8)
 BP_CTAS = ((8, 1), (4, 2))
 BP_TUNE_VIEWS = 360
 # (arm, slab cells, march unroll, view block): L1 quads unrolled once or twice,
-# CTAs in view blocks of 0 (every u tile of a view first), 16 or 64; TMA
+# CTAs in view blocks of 0 (every u tile of a view first), 8, 16, 32 or 64; TMA
 # bricks; z pairs through L1
-FORWARD_ARMS = ((0, 0, 1, 0), (0, 0, 2, 0), (0, 0, 1, 16), (0, 0, 1, 64), (1, 2, 1, 0),
-                (1, 4, 1, 0), (2, 0, 1, 0), (2, 0, 1, 64))
+FORWARD_ARMS = ((0, 0, 1, 0), (0, 0, 2, 0), (0, 0, 1, 8), (0, 0, 1, 16), (0, 0, 1, 32),
+                (0, 0, 1, 64), (1, 2, 1, 0), (1, 4, 1, 0), (2, 0, 1, 0), (2, 0, 1, 16))
 ARM_TUNE_VIEWS = 24
 
 
