@@ -356,6 +356,8 @@ int dgc_project_mse_grad(const float* volume, int D, int H, int W, const float* 
     p.quads = quads;
     p.partials = partials;
     p.projections = projections;
+    // the forward's CTA order for this volume (the fused step marches the same rays)
+    p.view_block = fp_forward_arm(D, H, W).view_block;
     rc = build_volume_quads(volume, D, H, W, quads, s);
     if (rc != DGC_OK) return rc;
     rc = fp_launch_mse_grad(p, tile, measured, mask, scale, lpart, s);

@@ -1563,10 +1563,13 @@ void fp_forward_arm(int D, int H, int W, int* arm, int* slab, int* unroll, int* 
             *view_block = g_arm_rules[i].view_block;
             return;
         }
+    // built-in choice: the L1 arm; above 2^26 voxels (512^3: 90.4 vs 94.1 ms
+    // for 96 views of 768^2) CTAs in view blocks of 16, below (256^3) the
+    // order makes no difference
     *arm = 0;
     *slab = 0;
     *unroll = 1;
-    *view_block = 0;
+    *view_block = voxels > (1LL << 26) ? 16 : 0;
 }
 
 FpArm fp_forward_arm(int D, int H, int W) {

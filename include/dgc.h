@@ -337,8 +337,10 @@ int dgc_bp_tiles(int D, int A, int* kz_forward, int* kz_backward, int* cta_x, in
  * the order view_block: 0 = every u tile of a view, then the next view;
  * B > 0 = inside a detector band, views in blocks of B, the view fastest
  * inside a block.  Rules are tried in the order they were added (at most
- * 16); without one, arm 0, unroll 1, order 0.  Every choice gives bitwise
- * the same projections.  No counterpart in the reference. */
+ * 16); without one, arm 0, unroll 1, and view blocks of 16 above 2^26 voxels
+ * (order 0 below).  Every choice gives bitwise the same projections; the
+ * fused calibration step (dgc_project_mse_grad) takes the same CTA order.
+ * No counterpart in the reference. */
 int dgc_fp_add_arm_rule(long long voxels_max, int arm, int slab_cells, int unroll,
                         int view_block);
 int dgc_fp_clear_arm_rules(void);
