@@ -213,7 +213,6 @@ def test_autotuner_tunes_forward_arm(tmp_path):
         assert query(512, 512, 512) == (1, 4, 1, 0)
         # beyond every bucket: the built-in choice (L1 arm; view blocks of 16 above 2^26 voxels)
         assert query(600, 512, 512) == (0, 0, 1, 16)
-        assert query(64, 64, 64) == (0, 0, 1, 0)
         lib.dgc_fp_clear_arm_rules()
         again = Autotuner(cache_path=path, measure_arm=lambda *x: pytest.fail("cache miss"))
         assert again.tune_forward_arm(pr)["arm"] == 1
