@@ -416,3 +416,63 @@ def test_target_backprojection(target, ref_native, oracle):
 def test_target_reconstruct_fdk(target, ref_native, oracle):
     fdk_parity(target, ref_native[1], oracle, views=[3], rows=range(255, 257),
                label="target 512^3 / 720 x 768^2")
+
+
+# ---------------------------------------------------- off-nominal full-size case
+
+
+def test_offnominal_projection_and_backprojection(ref_native, oracle):
+    """A full-size case away from every fast path: 200 x 224 x 184 voxels of
+    1.3 mm (a dividing voxel size), ROI offsets (5.2, -3.1, 2.4) mm, 240
+    views over 2 pi of a non-square 320 x 288 detector of 0.9 mm pixels,
+    sid 1100, sod 700, step 0.4, config-3 perturbations: projection,
+    backprojection and their gradients against the reference's CUDA, values
+    against the FP64 oracle on two whole views and a 4-row slab."""
+    from cbct_backprojector import backproject, project
+    from dgc_b200.calibration import perturb_geometry
+    from dgc_b200.phantoms import circular_geometry, ellipsoid_phantom
+    from dgc_b200.sharded import slab_offset
+
+    ref_fp, ref_bp = ref_native
+    D, H, W, A, U, V = 200, 224, 184, 240, 320, 288
+    vs, px, step, off = 1.3, 0.9, 0.4, (5.2, -3.1, 2.4)
+    vol0 = ellipsoid_phantom((D, H, W), n=12, seed=21, voxel_size=vs, offset=off, device="cuda",
+                             axis_range=(8.0, 60.0))
+    geom0 = perturb_geometry(circular_geometry(A, U, V, 1100.0, 700.0, px, device="cuda"), 22)
+    vol = vol0.clone().requires_grad_()
+    geom = [g.clone().requires_grad_() for g in geom0]
+    p = project(vol, *geom, px, U, V, step_size=step, voxel_size=vs, off_x=off[0], off_y=off[1],
+                off_z=off[2])
+    up = torch.linspace(-0.5, 1.0, p.numel(), device="cuda").view_as(p)
+    ours = torch.autograd.grad(p, [vol, *geom], grad_outputs=up)
+    theirs_p = ref_fp.forward(vol0, *geom0, px, U, V, step, vs, *off)
+    theirs = ref_fp.backward(up, vol0, *geom0, px, step, vs, True, *off)
+    q = p.detach().clone().requires_grad_()
+    geom2 = [g.clone().requires_grad_() for g in geom0]
+    b = backproject(q, *geom2, px, (D, H, W), vs, volume_offset=off)
+    wv = (vol0 - 0.05).contiguous()
+    ours_b = torch.autograd.grad(b, [q, *geom2], grad_outputs=wv)
+    theirs_b = ref_bp.forward(p.detach(), *geom0, px, D, H, W, vs, *off)
+    theirs_bb = ref_bp.backward(wv, p.detach(), *geom0, px, vs, *off)
+    torch.cuda.synchronize()
+    ks = [17, 133]
+    truth_p = oracle.project(vol0.double().cpu().numpy(), view(geom0, ks), px, U, V, step, vs, off,
+                             mode=1)
+    rows = range(90, 94)
+    truth_b = oracle.backproject(p.detach().double().cpu().numpy(), view(geom0, slice(None)), px,
+                                 (len(rows), H, W), vs, slab_offset((D, H, W), vs, off, rows))
+    rec = {"case": "off-nominal 200x224x184 x 1.3 mm, 240 x 320x288 x 0.9 mm, offsets",
+           "vs_reference": {"projection": rel(p.detach(), theirs_p),
+                            "grad_volume": rel(ours[0], theirs[0]),
+                            **{f"fp_{k}": v for k, v in geometry_errors(ours[1:], theirs[1:]).items()},
+                            "backprojection": rel(b.detach(), theirs_b),
+                            "bp_grad_projections": rel(ours_b[0], theirs_bb[0])},
+           "vs_oracle": {"projection_views": rel(p.detach()[ks], truth_p),
+                         "backprojection_slab": rel(b.detach()[rows.start:rows.stop], truth_b)}}
+    log(rec)
+    r, o = rec["vs_reference"], rec["vs_oracle"]
+    assert r["projection"] < FWD_RTOL and o["projection_views"] < FWD_RTOL
+    assert r["backprojection"] < FWD_RTOL and o["backprojection_slab"] < FWD_RTOL
+    assert r["grad_volume"] < GRAD_RTOL and r["bp_grad_projections"] < GRAD_RTOL
+    for name in GEOM_NAMES:
+        assert r[f"fp_{name}"] < GRAD_RTOL, (name, r[f"fp_{name}"])
