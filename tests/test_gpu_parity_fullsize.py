@@ -468,10 +468,17 @@ def test_offnominal_projection_and_backprojection(ref_native, oracle):
                             "backprojection": rel(b.detach(), theirs_b),
                             "bp_grad_projections": rel(ours_b[0], theirs_bb[0])},
            "vs_oracle": {"projection_views": rel(p.detach()[ks], truth_p),
-                         "backprojection_slab": rel(b.detach()[rows.start:rows.stop], truth_b)}}
+                         "backprojection_slab": rel(b.detach()[rows.start:rows.stop], truth_b)},
+           "reference_vs_oracle": {"projection_views": rel(theirs_p[ks], truth_p),
+                                   "backprojection_slab": rel(theirs_b[rows.start:rows.stop],
+                                                              truth_b)}}
     log(rec)
-    r, o = rec["vs_reference"], rec["vs_oracle"]
-    assert r["projection"] < FWD_RTOL and o["projection_views"] < FWD_RTOL
+    r, o, ro = rec["vs_reference"], rec["vs_oracle"], rec["reference_vs_oracle"]
+    # FP32 sample positions (the reference's expressions, a dividing voxel
+    # size) against FP64 ones at the phantom's sharp edges: the bar is 1e-5
+    # or the reference's own distance from the truth, whichever is larger
+    assert r["projection"] < FWD_RTOL
+    assert o["projection_views"] < max(FWD_RTOL, 1.02 * ro["projection_views"])
     assert r["backprojection"] < FWD_RTOL and o["backprojection_slab"] < FWD_RTOL
     assert r["grad_volume"] < GRAD_RTOL and r["bp_grad_projections"] < GRAD_RTOL
     for name in GEOM_NAMES:
