@@ -906,8 +906,9 @@ def run_calib(args):
 def run_tour(args):
     """Every kernel of the library on the fdk256 instance (honouring --views /
     --volume / --detector), ``--steps`` times: project, its backward with the
-    volume gradient, the fused calibration step, backproject and its backward,
-    reconstruct_fdk, the filter's backward, a two-instance batched step and one warm-start network
+    volume gradient, the fused calibration step, backproject and its backward
+    (all nine gradients, then the geometry's alone), reconstruct_fdk, the
+    filter's backward, a two-instance batched step and one warm-start network
     forward/backward (tensor-core GEMMs).  Prints the per-kernel device times
     of the last pass; meant for profiler captures of small cases."""
     import torch
@@ -943,6 +944,9 @@ def run_tour(args):
         g2 = [t.detach().requires_grad_() for t in geom]
         b = cb.backproject(pr, *g2, w["pixel"], shape, w["voxel"])
         torch.autograd.grad(b, [pr, *g2], grad_outputs=torch.ones_like(b))
+        g3 = [t.detach().requires_grad_() for t in geom]  # geometry only (self-calibration)
+        b = cb.backproject(p.detach(), *g3, w["pixel"], shape, w["voxel"])
+        torch.autograd.grad(b, g3, grad_outputs=torch.ones_like(b))
         cb.reconstruct_fdk(p.detach(), *geom, w["pixel"], shape, w["voxel"], alpha=w["alpha"])
         pf = p.detach().requires_grad_()
         sid = geom[1].detach().requires_grad_()

@@ -340,13 +340,15 @@ __device__ __forceinline__ void column_terms(const ColumnGrad& g, float s_iu, fl
     terms[7] = g.w * (1.0f - g.t) * ip * s_iv;
 }
 
-// Sums of 32 per-lane values over the warp, lane L receiving the sum of value
-// L: five butterfly steps, each halving the values a lane holds (31 shuffles
-// for the 32 sums instead of 5 per sum).
-__device__ __forceinline__ float warp_transpose_sum(float (&v)[32], int lane) {
+// Sums of N (16 or 32) per-lane values over the warp, lane L receiving the
+// sum of value L mod N: log2(N) butterfly steps, each halving the values a
+// lane holds (N-1 shuffles for the N sums instead of 5 per sum), then the
+// halves of the warp added.
+template <int N>
+__device__ __forceinline__ float warp_transpose_sum(float (&v)[N], int lane) {
     const unsigned FULL = 0xffffffffu;
 #pragma unroll
-    for (int h = 16; h >= 1; h >>= 1) {
+    for (int h = N / 2; h >= 1; h >>= 1) {
         const bool up = (lane & h) != 0;
 #pragma unroll
         for (int k = 0; k < h; ++k) {
@@ -355,21 +357,31 @@ __device__ __forceinline__ float warp_transpose_sum(float (&v)[32], int lane) {
             v[k] = keep + __shfl_xor_sync(FULL, send, h);
         }
     }
-    return v[0];
+    float x = v[0];
+#pragma unroll
+    for (int o = N; o < 32; o <<= 1) x += __shfl_xor_sync(FULL, x, o);
+    return x;
 }
+
+// Views whose four z-sums are reduced together (16 accumulators per lane).
+constexpr int kBpGroup = 4;
 
 // GP: projection gradient 0 = not computed (p.grad_projections null), 1 = four
 // float reductions per voxel-view into grad_projections.
 //
 // A warp owns one (x, y) column and 32*KZ of its voxels along z.  Views go in
-// groups of 32: lane j evaluates the column geometry of view a0+j (and later
-// its chain rule), the warp walks the views of the group eight at a time
-// with that view's geometry broadcast by shuffles, each lane adding its z
-// voxels' four products per view into registers; the 4 x 8 sums are then
-// reduced over the warp at once (warp_transpose_sum) and the eight lanes that
-// own those views apply the chain rule in parallel.
+// passes of 32: lane j evaluates the column geometry of view a0+j (and, at
+// the end of the pass, its chain rule).  The warp walks the pass's views
+// kBpGroup at a time with that view's geometry broadcast by shuffles; per
+// view every lane first issues the loads of its KZ taps together (an
+// out-of-range tap loads the row's first quad and is masked), then adds its
+// voxels' four products into registers.  The group's 4 x kBpGroup sums are
+// reduced over the warp at once (warp_transpose_sum) and kept by the lane
+// that owns the view; after the pass all 32 lanes apply the chain rule at
+// once.
 template <int KZ, int GP>
 __global__ void __launch_bounds__(256) bp_backward_kernel(BpArgs p) {
+    constexpr int G = kBpGroup;
     __shared__ double s_terms[8][32][8];
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -413,12 +425,14 @@ __global__ void __launch_bounds__(256) bp_backward_kernel(BpArgs p) {
             my_ui = g.ui;
         }
         const unsigned valid_mask = __ballot_sync(FULL, my_ok);
-        for (int b = 0; b < nv; b += 8) {
-            float acc[32];
+        // this lane's view: its four z-sums over the warp's voxels
+        float m_iu = 0.f, m_iv = 0.f, m_ivdv = 0.f, m_int = 0.f;
+        for (int b = 0; b < nv; b += G) {
+            float acc[4 * G];
 #pragma unroll
-            for (int i = 0; i < 32; ++i) acc[i] = 0.0f;
+            for (int i = 0; i < 4 * G; ++i) acc[i] = 0.0f;
 #pragma unroll
-            for (int i = 0; i < 8; ++i) {
+            for (int i = 0; i < G; ++i) {
                 const int j = b + i;
                 if (!((valid_mask >> j) & 1u)) continue;  // warp-uniform
                 const float t = __shfl_sync(FULL, my_t, j);
@@ -434,19 +448,31 @@ __global__ void __launch_bounds__(256) bp_backward_kernel(BpArgs p) {
                     w = __shfl_sync(FULL, my_w, j);
                     gp = p.grad_projections + ((long long)a * p.U + ui) * p.V;
                 }
+                float4 q[KZ];
+                float fvk[KZ], dvk[KZ];
+                int vik[KZ];
+                bool okk[KZ];
 #pragma unroll
                 for (int k = 0; k < KZ; ++k) {
                     const float dv = pz[k] - dsv;
                     const float v_phys = dsv + t * dv;
                     const float v_idx = v_phys * ip + v0;
-                    if (32 * k < zlimit && v_idx >= 0.0f && v_idx < vlim) {
-                        const FloorSplit fs = floor_split(v_idx);
-                        const int vi = (int)(fs.biased - kFloorMagicBits);
-                        const float fv = fs.frac;
-                        const float4 q = __ldg(rq + vi);
-                        const float interp = lerpf(lerpf(q.x, q.y, fv), lerpf(q.z, q.w, fv), fu);
-                        const float iu = lerpf(q.z - q.x, q.w - q.y, fv);
-                        const float iv = lerpf(q.y - q.x, q.w - q.z, fu);
+                    okk[k] = 32 * k < zlimit && v_idx >= 0.0f && v_idx < vlim;
+                    const FloorSplit fs = floor_split(v_idx);
+                    vik[k] = okk[k] ? (int)(fs.biased - kFloorMagicBits) : 0;
+                    fvk[k] = fs.frac;
+                    dvk[k] = dv;
+                    q[k] = __ldg(rq + vik[k]);
+                }
+#pragma unroll
+                for (int k = 0; k < KZ; ++k) {
+                    if (okk[k]) {
+                        const float fv = fvk[k], dv = dvk[k];
+                        const int vi = vik[k];
+                        const float4 c = q[k];
+                        const float interp = lerpf(lerpf(c.x, c.y, fv), lerpf(c.z, c.w, fv), fu);
+                        const float iu = lerpf(c.z - c.x, c.w - c.y, fv);
+                        const float iv = lerpf(c.y - c.x, c.w - c.z, fu);
                         const float g = gval[k];
                         acc[4 * i + 0] = fmaf(g, iu, acc[4 * i + 0]);
                         acc[4 * i + 1] = fmaf(g, iv, acc[4 * i + 1]);
@@ -463,23 +489,27 @@ __global__ void __launch_bounds__(256) bp_backward_kernel(BpArgs p) {
                     }
                 }
             }
-            // lane 4i+q: sum q of view b+i; the view's owner (lane b+i) gathers its four
-            const float total = warp_transpose_sum(acc, lane);
-            const int src = 4 * ((lane - b) & 7);
+            // lane 4i+q: sum q of view b+i; the view's owner (lane b+i) keeps its four
+            const float total = warp_transpose_sum<4 * G>(acc, lane);
+            const int src = 4 * ((lane - b) & (G - 1));
             const float s_iu = __shfl_sync(FULL, total, src + 0);
             const float s_iv = __shfl_sync(FULL, total, src + 1);
             const float s_ivdv = __shfl_sync(FULL, total, src + 2);
             const float s_int = __shfl_sync(FULL, total, src + 3);
-            if (lane >= b && lane < b + 8 && lane < nv) {
-                float terms[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-                if (my_ok) {
-                    const ColumnGrad g = column_grad(p.vt[a0 + lane], vx, vy, col_ok, p);
-                    column_terms(g, s_iu, s_iv, s_ivdv, s_int, ip, terms);
-                }
-#pragma unroll
-                for (int k = 0; k < 8; ++k) s_terms[warp][lane][k] = (double)terms[k];
+            if (lane >= b && lane < b + G) {
+                m_iu = s_iu;
+                m_iv = s_iv;
+                m_ivdv = s_ivdv;
+                m_int = s_int;
             }
         }
+        float terms[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        if (my_ok) {
+            const ColumnGrad g = column_grad(p.vt[a0 + lane], vx, vy, col_ok, p);
+            column_terms(g, m_iu, m_iv, m_ivdv, m_int, ip, terms);
+        }
+#pragma unroll
+        for (int k = 0; k < 8; ++k) s_terms[warp][lane][k] = (double)terms[k];
         __syncthreads();
         {
             const int j = threadIdx.x >> 3, k = threadIdx.x & 7;
@@ -514,10 +544,10 @@ __global__ void __launch_bounds__(256) bp_reduce_partials_kernel(const double* _
 // they stay in L1; more amortise the per-(column, view) geometry.  Measured
 // (sid 1000, sod 600; 256^3 / 360 x 384^2, 128^3 / 180 x 256^2, 512^3 / 90 x
 // 512^2), forward KZ = 1 / 2 / 4 / 8: 9.07 / 8.18 / 11.6 / 14.1 ms,
-// 0.46 / 0.36 / 0.52 / 0.52 ms, 17.0 / 13.7 / 14.5 / 15.5 ms; backward
-// without the projection gradient: 45.9 / 28.7 / 21.3 / 28.2 ms,
-// 2.38 / 1.43 / 1.04 / 1.34 ms, 96.0 / 56.2 / 37.1 / 45.6 ms (with it
-// 36.1-36.9 ms at KZ 2-4 for 256^3, 62.0 ms at KZ 4 for 512^3).
+// 0.46 / 0.36 / 0.52 / 0.52 ms, 17.0 / 13.7 / 14.5 / 15.5 ms (before the
+// super-tile order).  Backward at 256^3 / 360 x 384^2 (current kernel),
+// KZ = 2 / 4 / 8: 13.1 / 11.2 / 11.4 ms without the projection gradient,
+// 23.3 / 24.7 / 28.5 ms with it.
 // Tile rules registered by the autotuner (dgc_bp_add_tile_rule): the first
 // rule with D <= d_max and A <= a_max applies; a zero field keeps the
 // built-in choice.
@@ -633,7 +663,7 @@ int bp_launch_forward(const BpArgs& args, bool fdk, cudaStream_t s) {
 }
 
 int bp_launch_backward(const BpArgs& p, cudaStream_t s) {
-    DGC_TRACE("bp_backward_kernel", s);
+    DGC_TRACE(p.grad_projections ? "bp_backward_kernel<gp>" : "bp_backward_kernel", s);
     // the Z blocking the caller sized the partials for (a rule added by another
     // thread in between must not change the grid)
     const int kz = p.kz_backward ? p.kz_backward : bp_kz_backward(p.D, p.A);
