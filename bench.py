@@ -53,10 +53,11 @@ WORKLOADS["fdk-sharded"] = dict(
 WORKLOAD = dict(WORKLOADS["target512"])
 METRIC = "fwd Grays/s, backproj Gvoxel-views/s; calib time to 0.1 px reproj, NN vs plain"
 UNIT = "Grays/s"
-# DRAM bytes (read + write) of one fp_forward_kernel launch of a workload: an
-# ncu capture of a few of its views, scaled by the view count (the profile
-# summaries under profiles/ give the commands and the captured figures).
-FWD_DRAM_BYTES = {"fdk256": (351.7e6 + 17.9e6) * 15, "target512": None}
+# DRAM bytes (read + write) of one fp_forward_kernel launch of a workload at
+# its nominal view count: an ncu capture of a few of its views, scaled by the
+# view count (the profile summaries under profiles/ give the commands and the
+# captured figures; target512: 48 views = 3 view blocks of 16).
+FWD_DRAM_BYTES = {"fdk256": (351.7e6 + 17.9e6) * 15, "target512": (25.811e9 + 0.344e9) * 15}
 FALLBACK_HBM_GBS = 6650.0
 FALLBACK_BF16_TFLOPS = 1590.0
 
@@ -607,8 +608,11 @@ def run_ours(args):
     fwd_bytes = 32 * S + 4 * R_local  # two 16-byte quads per sample + projection writes
     fwd_gbs = fwd_bytes / (fwd_ms * 1e-3) / 1e9
     traffic = FWD_DRAM_BYTES.get(w.get("key", ""))
-    if traffic is not None and sharded:
-        traffic = traffic * A_local / w["A"]
+    nominal = WORKLOADS.get(w.get("key", ""), {})
+    if traffic is not None and all(w[k] == nominal[k] for k in ("D", "H", "W", "U", "V")):
+        traffic = traffic * A_local / nominal["A"]  # this rank's views (sharded or --views)
+    else:
+        traffic = None
     roofline = {"bound": "l1", "kernel": "fp_forward_kernel", "achieved": fwd_gbs, "peak": l1,
                 "unit": "GB/s", "frac": fwd_gbs / l1,
                 "peak_source": "l1_gather_gbs of this run's ceilings (csrc/ceilings.cu)",
