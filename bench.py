@@ -75,7 +75,7 @@ def parse_args(argv=None):
     ap.add_argument("--detector", type=int, default=None, help="override the square detector size")
     ap.add_argument("--workload", default="target512",
                     choices=["target512", "fdk256", "fdk-sharded", "batch64", "calib", "tour",
-                             "gemm", "arms"],
+                             "gemm", "arms", "refcuda"],
                     help="target512: the FDK step at 512^3 / 720 x 768^2 (default); fdk256: the "
                          "same step at 256^3 / 360 x 384^2; fdk-sharded: one target512 object "
                          "split by views over the ranks; batch64: 64 uneven project+backward "
@@ -83,7 +83,8 @@ def parse_args(argv=None):
                          "0.1 px, learned warm start vs plain; tour: every kernel once on the "
                          "fdk256 instance (profiler captures); gemm: the tcgen05 GEMM at "
                          "8192^3 and at the network's largest layer shapes; arms: the forward "
-                         "projector's L1 and TMA arms timed at 256^3 and 512^3")
+                         "projector's L1 and TMA arms timed at 256^3 and 512^3; refcuda: the "
+                         "reference's own CUDA operators (baseline/_ref) against this library's")
     ap.add_argument("--acq", choices=["half", "eval", "config3"], default="half",
                     help="calib: 256^3 x 2 mm / 360 / 384^2 x 2 mm (half), 512^3 / 720 / 768^2 "
                          "(eval) or 256^3 x 1 mm / 360 / 384^2 x 1 mm (config3)")
@@ -1043,6 +1044,121 @@ def run_arms(args):
 # --------------------------------------------------------------------- gemm
 
 
+def load_reference_cuda():
+    """The reference's own native operators, from its pip installation under
+    ``baseline/_ref`` (built for sm_100 from its sources), loaded by file path
+    under their module names without entering ``sys.modules`` (the names are
+    this package's shims too).  None when the installation is absent."""
+    import importlib.machinery
+    import importlib.util
+
+    root = ROOT / "baseline" / "_ref"
+    mods = []
+    for name in ("src_cbct_forwardprojector_cuda", "src_cbct_backprojector_cuda"):
+        found = sorted(root.glob(name + ".*.so"))
+        if not found:
+            return None
+        loader = importlib.machinery.ExtensionFileLoader(name, str(found[0]))
+        spec = importlib.util.spec_from_file_location(name, str(found[0]), loader=loader)
+        mod = importlib.util.module_from_spec(spec)
+        loader.exec_module(mod)
+        mods.append(mod)
+    return mods
+
+
+def run_refcuda(args):
+    """The GPU bar: the reference's own CUDA operators (``load_reference_cuda``)
+    against this library's on the same instance, stream and GPU -- forward
+    projection, its backward with all nine gradients, backprojection, its
+    backward with all nine -- on the fdk256 instance (honouring --views), and
+    the forward projection and backprojection of the target512 instance
+    (one timed call each).  CUDA events, median of ``--steps`` after
+    ``--warmup`` calls, clocks sampled; every operator's output is compared
+    with the reference's (max relative L2 over its outputs)."""
+    import statistics
+
+    import torch
+
+    from dgc_b200 import _ops
+
+    ref = load_reference_cuda()
+    if ref is None:
+        print(json.dumps({"workload": "refcuda", "unavailable": "baseline/_ref is not installed"}))
+        return 0
+    ref_fp, ref_bp = ref
+    torch.cuda.set_device(0)
+    device = torch.device("cuda", 0)
+
+    def timed(fn, warmup, steps):
+        out = None
+        for _ in range(max(1, warmup)):
+            out = fn()
+        torch.cuda.synchronize(device)
+        ts = []
+        for _ in range(max(1, steps)):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            fn()
+            b.record()
+            b.synchronize()
+            ts.append(a.elapsed_time(b))
+        return statistics.median(ts), out
+
+    def rel(x, y):
+        xs = x if isinstance(x, (list, tuple)) else [x]
+        ys = y if isinstance(y, (list, tuple)) else [y]
+        worst = 0.0
+        for a, b in zip(xs, ys):
+            if a is None or b is None or b.numel() == 0:
+                continue
+            n = float(b.double().norm())
+            worst = max(worst, float((a.double() - b.double()).norm()) / n if n > 0 else 0.0)
+        return worst
+
+    out = {}
+    with ClockSampler(0) as clocks:
+        for key in ("fdk256", "target512"):
+            WORKLOAD.clear()
+            WORKLOAD.update(WORKLOADS[key])
+            if key == "fdk256" and args.views:
+                WORKLOAD["A"] = args.views
+            w = WORKLOAD
+            vol, geom = make_instance(device, instance_seed(0))
+            px, U, V, st, vx = w["pixel"], w["U"], w["V"], w["step"], w["voxel"]
+            D, H, W = w["D"], w["H"], w["W"]
+            full = key == "fdk256"
+            warm, steps = (args.warmup, args.steps) if full else (1, 1)
+            ops = {
+                "project": (lambda: _ops.fp_forward(vol, *geom, px, U, V, st, vx),
+                            lambda: ref_fp.forward(vol, *geom, px, U, V, st, vx, 0.0, 0.0, 0.0)),
+            }
+            proj = _ops.fp_forward(vol, *geom, px, U, V, st, vx)
+            ops["backproject"] = (lambda: _ops.bp_forward(proj, *geom, px, D, H, W, vx),
+                                  lambda: ref_bp.forward(proj, *geom, px, D, H, W, vx, 0.0, 0.0,
+                                                         0.0))
+            if full:
+                ops["project_backward"] = (
+                    lambda: _ops.fp_backward(proj, vol, *geom, px, st, vx, True),
+                    lambda: ref_fp.backward(proj, vol, *geom, px, st, vx, True, 0.0, 0.0, 0.0))
+                ops["backproject_backward"] = (
+                    lambda: _ops.bp_backward(vol, proj, *geom, px, vx),
+                    lambda: ref_bp.backward(vol, proj, *geom, px, vx, 0.0, 0.0, 0.0))
+            res = {}
+            for name, (mine, theirs) in ops.items():
+                t_ours, o_ours = timed(mine, warm, steps)
+                t_ref, o_ref = timed(theirs, warm, steps)
+                res[name] = {"ours_ms": t_ours, "reference_ms": t_ref, "speedup": t_ref / t_ours,
+                             "max_rel_l2_vs_reference": rel(o_ours, o_ref)}
+                del o_ours, o_ref
+            out[w["name"]] = res
+            del vol, geom, proj, ops
+            torch.cuda.empty_cache()
+    print(json.dumps({"workload": "refcuda: the reference's own CUDA operators (baseline/_ref) "
+                                  "vs this library, same GPU and stream", "results": out,
+                      "clocks": clocks.summary()}))
+    return 0
+
+
 def run_gemm(args):
     """TFLOP/s of the tcgen05 BF16 GEMM (fp32 out) against the measured cuBLAS
     bf16 peak: 8192^3, and the forward / weight-gradient products of the
@@ -1101,6 +1217,8 @@ def main(argv=None):
         return run_arms(args)
     if args.workload == "tour":
         return run_tour(args)
+    if args.workload == "refcuda":
+        return run_refcuda(args)
     if args.workload == "calib":
         return run_calib(args)
     if args.impl == "reference":
