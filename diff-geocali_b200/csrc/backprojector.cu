@@ -15,7 +15,9 @@
 //     warp, lane j evaluates the column geometry of view a0+j and the warp
 //     broadcasts it with shuffles, so no lane recomputes it.
 //   * Projections are re-laid out as quads PQ[a][u][v] = float4(P[u][v],
-//     P[u][v+1], P[u+1][v], P[u+1][v+1]): one 16-byte load per voxel-view.
+//     P[u+1][v], P[u][v+1], P[u+1][v+1]) -- two column pairs, so the lerp
+//     along v runs as one packed f32x2 lerp over rows u and u+1: one 16-byte
+//     load per voxel-view.
 //   * Outputs go through a shared-memory transpose so the volume is written
 //     along X (coalesced).
 //   * The backward sums the per-voxel terms over Z in four accumulators and
@@ -71,7 +73,7 @@ __global__ void build_proj_quads_kernel(const float* __restrict__ P, int A, int 
         const int u = (int)(r % QU);
         const int a = (int)(r / QU);
         const float* row = P + ((long long)a * U + u) * V + v;
-        PQ[i] = make_float4(__ldg(row), __ldg(row + 1), __ldg(row + V), __ldg(row + V + 1));
+        PQ[i] = make_float4(__ldg(row), __ldg(row + V), __ldg(row + 1), __ldg(row + V + 1));
     }
 }
 
@@ -168,8 +170,13 @@ __host__ __device__ __forceinline__ int bp_super(int cta) { return cta >= 64 ? 1
 
 // A CTA owns a cta_x x cta_y patch of (x, y) columns, one warp per column
 // (at most kBpMaxWarps warps), and 32*KZ voxels of each along z.
+//
+// Register caps by z depth (in place of launch bounds, which cannot express
+// "five 256-thread CTAs per SM"): at KZ = 2 the compiler's own choice (49
+// registers) leaves four CTAs per SM and runs 1.5x slower than 48 registers
+// and five CTAs.  Any CTA of up to kBpMaxWarps warps fits under each cap.
 template <int KZ, bool PIXDIV, bool FDK>
-__global__ void __launch_bounds__(32 * kBpMaxWarps) bp_forward_kernel(BpArgs p) {
+__global__ void __maxnreg__(KZ == 1 ? 40 : KZ == 2 ? 48 : KZ == 4 ? 64 : 96) bp_forward_kernel(BpArgs p) {
     __shared__ float s_out[32 * KZ][kBpMaxWarps + 1];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int cx = p.cta_x, cy = p.cta_y, nw = cx * cy;
@@ -198,48 +205,74 @@ __global__ void __launch_bounds__(32 * kBpMaxWarps) bp_forward_kernel(BpArgs p) 
     if (x < p.W && y < p.H) {
         const float vx = (x - p.W * 0.5f) * p.voxel_size + p.off_x;
         const float vy = (y - p.H * 0.5f) * p.voxel_size + p.off_y;
-        const float vlim = p.V - 1.0f;
         const int zlimit = p.D - zbase - lane;  // k valid while 32k < zlimit
+        // a tap is valid iff 0 <= v_idx < V-1, i.e. its floor (exact from the
+        // magic-number split, which maps NaN, infinities and values beyond
+        // 2^22 outside [0, V-2]) as an unsigned index is below V-1
+        const uint32_t vcount = (uint32_t)max(p.V - 1, 0);
+        f32x2 pz2[KZ / 2 > 0 ? KZ / 2 : 1];
+#pragma unroll
+        for (int k = 0; k + 1 < KZ; k += 2) pz2[k / 2] = pack2(pz[k], pz[k + 1]);
+        const f32x2 ip2 = pack2(p.inv_pixel, p.inv_pixel);
+        const f32x2 magic2 = pack2(kFloorMagic, kFloorMagic);
         for (int a0 = 0; a0 < p.A; a0 += 32) {
             ColumnView mine;
             mine.valid = false;
             if (a0 + lane < p.A) mine = column_view<PIXDIV>(p.vt[a0 + lane], a0 + lane, vx, vy, p);
             const unsigned valid_mask = __ballot_sync(FULL, mine.valid);
             const int nv = min(32, p.A - a0);
-            for (int j = 0; j < nv; ++j) {
-                if ((j & 7) == 0 && j > 0) {
+            // views in chunks of 8, each chunk's FP32 partial sums added into
+            // the FP64 totals after it
+            for (int jb = 0; jb < nv; jb += 8) {
+                const int je = min(jb + 8, nv);
+                for (int j = jb; j < je; ++j) {
+                    if (!((valid_mask >> j) & 1u)) continue;
+                    const float t = __shfl_sync(FULL, mine.t, j);
+                    const float dsv = __shfl_sync(FULL, mine.ds_v, j);
+                    const float v0 = __shfl_sync(FULL, mine.v0, j);
+                    const float w = __shfl_sync(FULL, mine.w, j);
+                    const float fu = __shfl_sync(FULL, mine.fu, j);
+                    const int row = __shfl_sync(FULL, mine.row, j);
+                    const ulonglong2* __restrict__ rq =
+                        reinterpret_cast<const ulonglong2*>(p.pquads) + row;
+                    // one tap: v_idx's floor split -> validity, column pair lerp
+                    // along v (packed: rows u and u+1), then along u
+                    auto tap = [&](int k, uint32_t biased, float fv) {
+                        const uint32_t vi = biased - kFloorMagicBits;
+                        if (32 * k < zlimit && vi < vcount) {
+                            const ulonglong2 q = __ldg(rq + vi);
+                            const float2 e = unpack2(lerp2(q.x, q.y, pack2(fv, fv)));
+                            part[k] = fmaf(w, lerpf(e.x, e.y, fu), part[k]);
+                        }
+                    };
+                    if constexpr (!PIXDIV && KZ % 2 == 0) {
+                        const f32x2 t2 = pack2(t, t), d2 = pack2(dsv, dsv), o2 = pack2(v0, v0);
 #pragma unroll
-                    for (int k = 0; k < KZ; ++k) {
-                        acc[k] += (double)part[k];
-                        part[k] = 0.0f;
+                        for (int k = 0; k < KZ; k += 2) {
+                            const f32x2 vp = fma2(t2, sub2(pz2[k / 2], d2), d2);
+                            const f32x2 vx2 = fma2(vp, ip2, o2);
+                            const f32x2 f2 = add2_rd(vx2, magic2);
+                            const float2 fr = unpack2(sub2(vx2, sub2(f2, magic2)));
+                            const uint2 bits = unpack2_bits(f2);
+                            tap(k, bits.x, fr.x);
+                            tap(k + 1, bits.y, fr.y);
+                        }
+                    } else {
+#pragma unroll
+                        for (int k = 0; k < KZ; ++k) {
+                            const float v_phys = dsv + t * (pz[k] - dsv);
+                            const float v_idx =
+                                PIXDIV ? v_phys / p.pixel_size + v0 : fmaf(v_phys, p.inv_pixel, v0);
+                            const FloorSplit fs = floor_split(v_idx);
+                            tap(k, fs.biased, fs.frac);
+                        }
                     }
                 }
-                if (!((valid_mask >> j) & 1u)) continue;
-                const float t = __shfl_sync(FULL, mine.t, j);
-                const float dsv = __shfl_sync(FULL, mine.ds_v, j);
-                const float v0 = __shfl_sync(FULL, mine.v0, j);
-                const float w = __shfl_sync(FULL, mine.w, j);
-                const float fu = __shfl_sync(FULL, mine.fu, j);
-                const int row = __shfl_sync(FULL, mine.row, j);
-                const float4* __restrict__ rq = p.pquads + row;
 #pragma unroll
                 for (int k = 0; k < KZ; ++k) {
-                    const float v_phys = dsv + t * (pz[k] - dsv);
-                    const float v_idx =
-                        PIXDIV ? v_phys / p.pixel_size + v0 : fmaf(v_phys, p.inv_pixel, v0);
-                    if (32 * k < zlimit && v_idx >= 0.0f && v_idx < vlim) {
-                        const FloorSplit fs = floor_split(v_idx);
-                        const float4 q = __ldg(rq + (int)(fs.biased - kFloorMagicBits));
-                        const float interp =
-                            lerpf(lerpf(q.x, q.y, fs.frac), lerpf(q.z, q.w, fs.frac), fu);
-                        part[k] = fmaf(w, interp, part[k]);
-                    }
+                    acc[k] += (double)part[k];
+                    part[k] = 0.0f;
                 }
-            }
-#pragma unroll
-            for (int k = 0; k < KZ; ++k) {
-                acc[k] += (double)part[k];
-                part[k] = 0.0f;
             }
         }
     }
@@ -470,9 +503,9 @@ __global__ void __launch_bounds__(256) bp_backward_kernel(BpArgs p) {
                         const float fv = fvk[k], dv = dvk[k];
                         const int vi = vik[k];
                         const float4 c = q[k];
-                        const float interp = lerpf(lerpf(c.x, c.y, fv), lerpf(c.z, c.w, fv), fu);
-                        const float iu = lerpf(c.z - c.x, c.w - c.y, fv);
-                        const float iv = lerpf(c.y - c.x, c.w - c.z, fu);
+                        const float interp = lerpf(lerpf(c.x, c.z, fv), lerpf(c.y, c.w, fv), fu);
+                        const float iu = lerpf(c.y - c.x, c.w - c.z, fv);
+                        const float iv = lerpf(c.z - c.x, c.w - c.y, fu);
                         const float g = gval[k];
                         acc[4 * i + 0] = fmaf(g, iu, acc[4 * i + 0]);
                         acc[4 * i + 1] = fmaf(g, iv, acc[4 * i + 1]);
