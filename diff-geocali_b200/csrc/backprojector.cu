@@ -428,7 +428,6 @@ __global__ void __launch_bounds__(256) bp_backward_kernel(BpArgs p) {
     const bool col_ok = x < p.W;
     const float vx = (x - p.W * 0.5f) * p.voxel_size + p.off_x;
     const float vy = (y - p.H * 0.5f) * p.voxel_size + p.off_y;
-    const float vlim = p.V - 1.0f;
     const float ip = p.inv_pixel;
 
     float gval[KZ], pz[KZ];
@@ -439,6 +438,12 @@ __global__ void __launch_bounds__(256) bp_backward_kernel(BpArgs p) {
         gval[k] = (col_ok && z < p.D) ? p.grad_volume[((long long)z * p.H + y) * p.W + x] : 0.0f;
     }
     const int zlimit = p.D - zbase - lane;
+    const uint32_t vcount = (uint32_t)max(p.V - 1, 0);
+    f32x2 pz2[KZ / 2 > 0 ? KZ / 2 : 1];
+#pragma unroll
+    for (int k = 0; k + 1 < KZ; k += 2) pz2[k / 2] = pack2(pz[k], pz[k + 1]);
+    const f32x2 ip2 = pack2(p.inv_pixel, p.inv_pixel);
+    const f32x2 magic2 = pack2(kFloorMagic, kFloorMagic);
 
     for (int a0 = 0; a0 < p.A; a0 += 32) {
         const int nv = min(32, p.A - a0);
@@ -474,38 +479,63 @@ __global__ void __launch_bounds__(256) bp_backward_kernel(BpArgs p) {
                 const float fu = __shfl_sync(FULL, my_fu, j);
                 const int ui = __shfl_sync(FULL, my_ui, j);
                 const int a = a0 + j;
-                const float4* __restrict__ rq = p.pquads + (a * (p.U - 1) + ui) * (p.V - 1);
+                const ulonglong2* __restrict__ rq =
+                    reinterpret_cast<const ulonglong2*>(p.pquads) + (a * (p.U - 1) + ui) * (p.V - 1);
                 float w = 0.0f;
                 float* __restrict__ gp = nullptr;
                 if (GP) {
                     w = __shfl_sync(FULL, my_w, j);
                     gp = p.grad_projections + ((long long)a * p.U + ui) * p.V;
                 }
-                float4 q[KZ];
+                ulonglong2 q[KZ];
                 float fvk[KZ], dvk[KZ];
                 int vik[KZ];
                 bool okk[KZ];
-#pragma unroll
-                for (int k = 0; k < KZ; ++k) {
-                    const float dv = pz[k] - dsv;
-                    const float v_phys = dsv + t * dv;
-                    const float v_idx = v_phys * ip + v0;
-                    okk[k] = 32 * k < zlimit && v_idx >= 0.0f && v_idx < vlim;
-                    const FloorSplit fs = floor_split(v_idx);
-                    vik[k] = okk[k] ? (int)(fs.biased - kFloorMagicBits) : 0;
-                    fvk[k] = fs.frac;
+                // z voxels in pairs: v_idx and its floor split as packed f32x2;
+                // a tap is valid iff its floor, as an unsigned index, is below V-1
+                auto setup = [&](int k, float dv, uint32_t biased, float fv) {
+                    const uint32_t vi = biased - kFloorMagicBits;
+                    okk[k] = 32 * k < zlimit && vi < vcount;
+                    vik[k] = okk[k] ? (int)vi : 0;
+                    fvk[k] = fv;
                     dvk[k] = dv;
                     q[k] = __ldg(rq + vik[k]);
+                };
+                if constexpr (KZ % 2 == 0) {
+                    const f32x2 t2 = pack2(t, t), d2 = pack2(dsv, dsv), o2 = pack2(v0, v0);
+#pragma unroll
+                    for (int k = 0; k < KZ; k += 2) {
+                        const f32x2 dv2 = sub2(pz2[k / 2], d2);
+                        const f32x2 vx2 = fma2(fma2(t2, dv2, d2), ip2, o2);
+                        const f32x2 f2 = add2_rd(vx2, magic2);
+                        const float2 fr = unpack2(sub2(vx2, sub2(f2, magic2)));
+                        const uint2 bits = unpack2_bits(f2);
+                        const float2 dv = unpack2(dv2);
+                        setup(k, dv.x, bits.x, fr.x);
+                        setup(k + 1, dv.y, bits.y, fr.y);
+                    }
+                } else {
+#pragma unroll
+                    for (int k = 0; k < KZ; ++k) {
+                        const float dv = pz[k] - dsv;
+                        const float v_phys = dsv + t * dv;
+                        const FloorSplit fs = floor_split(v_phys * ip + v0);
+                        setup(k, dv, fs.biased, fs.frac);
+                    }
                 }
 #pragma unroll
                 for (int k = 0; k < KZ; ++k) {
                     if (okk[k]) {
                         const float fv = fvk[k], dv = dvk[k];
                         const int vi = vik[k];
-                        const float4 c = q[k];
-                        const float interp = lerpf(lerpf(c.x, c.z, fv), lerpf(c.y, c.w, fv), fu);
-                        const float iu = lerpf(c.y - c.x, c.w - c.z, fv);
-                        const float iv = lerpf(c.z - c.x, c.w - c.y, fu);
+                        // column pairs (rows u, u+1) at v and v+1: the lerp along v
+                        // and the difference along v as packed pairs
+                        const float2 e = unpack2(lerp2(q[k].x, q[k].y, pack2(fv, fv)));
+                        const float2 d = unpack2(sub2(q[k].y, q[k].x));
+                        const float2 c0 = unpack2(q[k].x), c1 = unpack2(q[k].y);
+                        const float interp = lerpf(e.x, e.y, fu);
+                        const float iu = lerpf(c0.y - c0.x, c1.y - c1.x, fv);
+                        const float iv = lerpf(d.x, d.y, fu);
                         const float g = gval[k];
                         acc[4 * i + 0] = fmaf(g, iu, acc[4 * i + 0]);
                         acc[4 * i + 1] = fmaf(g, iv, acc[4 * i + 1]);
@@ -579,8 +609,8 @@ __global__ void __launch_bounds__(256) bp_reduce_partials_kernel(const double* _
 // 512^2), forward KZ = 1 / 2 / 4 / 8: 9.07 / 8.18 / 11.6 / 14.1 ms,
 // 0.46 / 0.36 / 0.52 / 0.52 ms, 17.0 / 13.7 / 14.5 / 15.5 ms (before the
 // super-tile order).  Backward at 256^3 / 360 x 384^2 (current kernel),
-// KZ = 2 / 4 / 8: 13.1 / 11.2 / 11.4 ms without the projection gradient,
-// 23.3 / 24.7 / 28.5 ms with it.
+// KZ = 2 / 4 / 8: 12.6 / 10.5 / 10.9 ms without the projection gradient,
+// 22.9 / 25.1 / 28.7 ms with it.
 // Tile rules registered by the autotuner (dgc_bp_add_tile_rule): the first
 // rule with D <= d_max and A <= a_max applies; a zero field keeps the
 // built-in choice.
