@@ -99,9 +99,9 @@ constexpr int FBK = 16;   // reduction slice
 // frame centre in length units, dist^2 = D^2 + u_c^2 + v_c^2, and
 // dw/dD = (u_c^2 + v_c^2)/dist^3.
 template <bool ADJ, bool CG = false>
-__global__ void __launch_bounds__(256) fdk_filter_kernel(FdkArgs p) {
+__global__ void __launch_bounds__(256, 2) fdk_filter_kernel(FdkArgs p) {
     __shared__ __align__(16) float ws[FBK][FBN];
-    __shared__ float gw[FBM + FBK];
+    __shared__ f32x2 gw2[FBM + FBK];  // taps, each duplicated into a packed pair
     __shared__ double s_part[8][kFdkPartials];
     const int a = blockIdx.z;
     const int m0 = blockIdx.y * FBM;
@@ -116,11 +116,13 @@ __global__ void __launch_bounds__(256) fdk_filter_kernel(FdkArgs p) {
     const float cu = p.frame_u ? p.frame_u[a] : 0.5f * (p.U - 1);
     const float cv = p.frame_v ? p.frame_v[a] : 0.5f * (p.V - 1);
 
-    float acc[8][8];
+    // 8 x 8 outputs per thread as packed pairs along v: one fma.rn.f32x2 per
+    // two outputs (lane by lane the scalar FMA, in the same order)
+    f32x2 acc2[8][4];
 #pragma unroll
     for (int i = 0; i < 8; ++i)
 #pragma unroll
-        for (int j = 0; j < 8; ++j) acc[i][j] = 0.0f;
+        for (int j = 0; j < 4; ++j) acc2[i][j] = pack2(0.0f, 0.0f);
 
     for (int k0 = 0; k0 < p.U; k0 += FBK) {
         {   // stage the cosine-weighted input slice w[k0..k0+FBK) x [n0..n0+FBN)
@@ -152,23 +154,33 @@ __global__ void __launch_bounds__(256) fdk_filter_kernel(FdkArgs p) {
         for (int i = tid; i < FBM + FBK - 1; i += 256) {
             int d = m0 - k0 - (FBK - 1) + i;
             d = d < 0 ? -d : d;
-            gw[i] = p.taps[min(d, p.U - 1)];
+            const float h = p.taps[min(d, p.U - 1)];
+            gw2[i] = pack2(h, h);
         }
         __syncthreads();
 #pragma unroll
         for (int kk = 0; kk < FBK; ++kk) {
-            const float4 b0 = *reinterpret_cast<const float4*>(&ws[kk][tx * 8]);
-            const float4 b1 = *reinterpret_cast<const float4*>(&ws[kk][tx * 8 + 4]);
-            const float b[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+            const ulonglong2 b0 = *reinterpret_cast<const ulonglong2*>(&ws[kk][tx * 8]);
+            const ulonglong2 b1 = *reinterpret_cast<const ulonglong2*>(&ws[kk][tx * 8 + 4]);
+            const f32x2 b[4] = {b0.x, b0.y, b1.x, b1.y};
 #pragma unroll
             for (int i = 0; i < 8; ++i) {
-                const float av = gw[ty * 8 + i - kk + FBK - 1];
+                const f32x2 av = gw2[ty * 8 + i - kk + FBK - 1];
 #pragma unroll
-                for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(av, b[j], acc[i][j]);
+                for (int j = 0; j < 4; ++j) acc2[i][j] = fma2(av, b[j], acc2[i][j]);
             }
         }
         __syncthreads();
     }
+    float acc[8][8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const float2 e = unpack2(acc2[i][j]);
+            acc[i][2 * j] = e.x;
+            acc[i][2 * j + 1] = e.y;
+        }
     // filtering.py:104: filtered * pixel_size * (sid / sod)
     const float ratio = sid / sod;
     if (!ADJ) {
