@@ -216,26 +216,35 @@ def test_config2_backprojection_and_gradients(cfg2, ref_native, oracle):
     # FP32 atomics over ~10^7 voxels
     rec["reference_vs_oracle"] = {"grad_projections_slab": rel(theirs_slab[0], truth_gp),
                                   **geometry_errors(theirs_slab[1:], list(truth_gg))}
-    # three views' geometry gradients over the WHOLE volume against their FP64
-    # truth: a view's gradient sums every voxel's term, which is where the
-    # reference's FP32 atomics lose digits (the slab holds 1/64 of the terms)
-    ks = [37, 151, 299]
+    # where this library and the reference disagree most (per gradient family,
+    # the view with the largest difference), the geometry gradients over the
+    # WHOLE volume against their FP64 truth: a view's gradient sums every
+    # voxel's term, which is where the reference's FP32 atomics lose digits
+    # (the slab holds 1/64 of the terms)
+    worst = [int(torch.argmax((a - b).abs())) for a, b in zip(ours[1:], theirs[1:])]
+    ks = sorted(set(worst))
     _, truth_views = oracle.backproject_backward(w.cpu().numpy(), q_np[ks], view(c["geom"], ks),
                                                  PX, VOX, ORIGIN)
     for key, grads in (("vs_oracle", ours[1:]), ("reference_vs_oracle", theirs[1:])):
         errs = geometry_errors([g[ks] for g in grads], list(truth_views))
         rec[key].update({f"{name}_views": e for name, e in errs.items()})
+    at_worst = {}
+    for i, name in enumerate(GEOM_NAMES):
+        j = ks.index(worst[i])
+        t = float(truth_views[i][j])
+        at_worst[name] = (abs(float(ours[1 + i][worst[i]]) - t), abs(float(theirs[1 + i][worst[i]]) - t))
+    rec["worst_view_abs_error_ours_reference"] = at_worst
     log(rec)
-    r, o, ro = rec["vs_reference"], rec["vs_oracle"], rec["reference_vs_oracle"]
+    r, o = rec["vs_reference"], rec["vs_oracle"]
     assert r["volume"] < FWD_RTOL and o["volume_slab"] < FWD_RTOL
     assert r["grad_projections"] < GRAD_RTOL and o["grad_projections_slab"] < GRAD_RTOL
     for name in GEOM_NAMES:
         assert o[name] < GRAD_RTOL, (name, o[name])
         assert o[f"{name}_views"] < GRAD_RTOL, (name, o[f"{name}_views"])
-        # beyond the bar against the reference only where the reference is the
-        # one further from the whole-volume truth
-        assert r[name] < GRAD_RTOL or ro[f"{name}_views"] > o[f"{name}_views"], (
-            name, r[name], ro[f"{name}_views"], o[f"{name}_views"])
+        # beyond the bar against the reference only where, at the view of
+        # their largest difference, the reference is the one off the truth
+        mine, ref = at_worst[name]
+        assert r[name] < GRAD_RTOL or mine < ref, (name, r[name], mine, ref)
 
 
 def fdk_parity(c, ref_bp, oracle, views, rows, label):
