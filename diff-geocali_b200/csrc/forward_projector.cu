@@ -450,16 +450,24 @@ __device__ __forceinline__ TileCoord tile_coord(const FpArgs& p, int tiles_u) {
 // Forward kernel
 // ---------------------------------------------------------------------------
 
-// Ray of this thread in a TU x (256/TU) tile: warps run along V (32
-// consecutive rows of one column).
-template <int TU>
+// Ray of this thread in a TU x (256/TU) tile.  WU = 1: warps run along V (32
+// consecutive rows of one column).  WU > 1: a warp takes a patch of WU
+// columns x 32/WU rows (lanes along V first).
+template <int TU, int WU = 1>
 __device__ __forceinline__ void tile_ray(const TileCoord& tc, int& u, int& v) {
     constexpr int TV = 256 / TU;
     constexpr int WARPS_V = TV / 32;
     static_assert(TV % 32 == 0, "rows per CTA must be whole warps");
+    static_assert(TU % WU == 0 && 32 % WU == 0, "warp patches must tile the CTA");
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    u = tc.tu * TU + warp / WARPS_V;
-    v = tc.tv * TV + (warp % WARPS_V) * 32 + lane;
+    if constexpr (WU == 1) {
+        u = tc.tu * TU + warp / WARPS_V;
+        v = tc.tv * TV + (warp % WARPS_V) * 32 + lane;
+    } else {
+        constexpr int ROWS = 32 / WU;
+        u = tc.tu * TU + (warp % (TU / WU)) * WU + lane / ROWS;
+        v = tc.tv * TV + (warp / (TU / WU)) * ROWS + lane % ROWS;
+    }
 }
 
 // Line integral of one ray, written to p.projections.
@@ -491,7 +499,13 @@ __global__ void __launch_bounds__(256) fp_forward_kernel(FpArgs p) {
     __syncthreads();
     const ViewGeo vg = s_view;
     int u, v;
-    tile_ray<TU>(tc, u, v);
+    // with view blocks (the order for volumes beyond L2) warps take 4 x 8 ray
+    // patches: 671.3 -> 658.9 ms at 512^3 / 720 x 768^2, while at 256^3 /
+    // 720 x 384^2 the 4 x 8 patches are 1.3 % slower than 1 x 32 columns (the
+    // autotuner's view-block arms carry the patches, so its timings include
+    // them; the projections are the same)
+    if (TU % 4 == 0 && p.view_block > 0) tile_ray<TU, (TU % 4 == 0 ? 4 : 1)>(tc, u, v);
+    else tile_ray<TU>(tc, u, v);
     if (u >= p.U || v >= p.V) return;
     forward_ray<DIV, OFF, UNROLL>(p, vg, tc.a, u, v);
 }

@@ -21,7 +21,8 @@ struct FpArgs {
     uint32_t gz_x, gz_y, gz_bias;
     double* partials;  // [A][tiles][8]
     int* error;        // device word set to 1 when a bounded wait gives up (TMA arm), or null
-    int view_block;    // CTA order: 0 = u tile fastest; B > 0 = views in blocks of B (tile_coord)
+    int view_block;    // CTA order: 0 = u tile fastest; B > 0 = views in blocks of B (tile_coord),
+                       // and the L1 forward's warps as 4 x 8 ray patches (tile_ray)
 };
 
 // Ray tile of a CTA: TU detector columns x (256/TU) rows; the 32 lanes of a

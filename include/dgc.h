@@ -336,7 +336,8 @@ int dgc_bp_tiles(int D, int A, int* kz_forward, int* kz_backward, int* cta_x, in
  * unroll 1), with its CTAs in
  * the order view_block: 0 = every u tile of a view, then the next view;
  * B > 0 = inside a detector band, views in blocks of B, the view fastest
- * inside a block.  Rules are tried in the order they were added (at most
+ * inside a block, and arm 0's warps as patches of 4 detector columns x 8
+ * rows instead of 32 rows of one column.  Rules are tried in the order they were added (at most
  * 16); without one, arm 0, unroll 1, and view blocks of 16 above 2^26 voxels
  * (order 0 below).  Every choice gives bitwise the same projections; the
  * fused calibration step (dgc_project_mse_grad) takes the same CTA order.
