@@ -57,7 +57,7 @@ UNIT = "Grays/s"
 # its nominal view count: an ncu capture of a few of its views, scaled by the
 # view count (the profile summaries under profiles/ give the commands and the
 # captured figures; target512: 48 views = 3 view blocks of 16).
-FWD_DRAM_BYTES = {"fdk256": (351.7e6 + 17.9e6) * 15, "target512": (25.811e9 + 0.344e9) * 15}
+FWD_DRAM_BYTES = {"fdk256": (351.7e6 + 17.9e6) * 15, "target512": (24.812e9 + 0.120e9) * 15}
 FALLBACK_HBM_GBS = 6650.0
 FALLBACK_BF16_TFLOPS = 1590.0
 
