@@ -459,6 +459,17 @@ def run_reference(args):
     return 0
 
 
+def forward_traffic(w, views):
+    """Measured DRAM bytes of one forward launch over ``views`` views of
+    workload ``w`` (FWD_DRAM_BYTES scaled by the view count), or None when
+    none was measured for its volume and detector sizes."""
+    traffic = FWD_DRAM_BYTES.get(w.get("key", ""))
+    nominal = WORKLOADS.get(w.get("key", ""), {})
+    if traffic is None or any(w[k] != nominal[k] for k in ("D", "H", "W", "U", "V")):
+        return None
+    return traffic * views / nominal["A"]
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -608,12 +619,7 @@ def run_ours(args):
     l1 = ceilings["l1_gather_gbs"]
     fwd_bytes = 32 * S + 4 * R_local  # two 16-byte quads per sample + projection writes
     fwd_gbs = fwd_bytes / (fwd_ms * 1e-3) / 1e9
-    traffic = FWD_DRAM_BYTES.get(w.get("key", ""))
-    nominal = WORKLOADS.get(w.get("key", ""), {})
-    if traffic is not None and all(w[k] == nominal[k] for k in ("D", "H", "W", "U", "V")):
-        traffic = traffic * A_local / nominal["A"]  # this rank's views (sharded or --views)
-    else:
-        traffic = None
+    traffic = forward_traffic(w, A_local)
     roofline = {"bound": "l1", "kernel": "fp_forward_kernel", "achieved": fwd_gbs, "peak": l1,
                 "unit": "GB/s", "frac": fwd_gbs / l1,
                 "peak_source": "l1_gather_gbs of this run's ceilings (csrc/ceilings.cu)",
