@@ -160,8 +160,10 @@ __global__ void __launch_bounds__(256, 2) fdk_filter_kernel(FdkArgs p) {
         __syncthreads();
 #pragma unroll
         for (int kk = 0; kk < FBK; ++kk) {
-            const ulonglong2 b0 = *reinterpret_cast<const ulonglong2*>(&ws[kk][tx * 8]);
-            const ulonglong2 b1 = *reinterpret_cast<const ulonglong2*>(&ws[kk][tx * 8 + 4]);
+            // a thread's columns: tx*4..+3 and FBN/2 + tx*4..+3, so the 16 lanes of
+            // a load read contiguous 16-byte chunks (no bank conflicts)
+            const ulonglong2 b0 = *reinterpret_cast<const ulonglong2*>(&ws[kk][tx * 4]);
+            const ulonglong2 b1 = *reinterpret_cast<const ulonglong2*>(&ws[kk][FBN / 2 + tx * 4]);
             const f32x2 b[4] = {b0.x, b0.y, b1.x, b1.y};
 #pragma unroll
             for (int i = 0; i < 8; ++i) {
@@ -191,7 +193,7 @@ __global__ void __launch_bounds__(256, 2) fdk_filter_kernel(FdkArgs p) {
             if (u >= p.U) continue;
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
-                const int v = n0 + tx * 8 + j;
+                const int v = n0 + (j < 4 ? tx * 4 + j : FBN / 2 + tx * 4 + j - 4);
                 if (v < p.V) Oa[(long long)u * p.V + v] = (acc[i][j] * p.pixel_size) * ratio;
             }
         }
@@ -207,7 +209,7 @@ __global__ void __launch_bounds__(256, 2) fdk_filter_kernel(FdkArgs p) {
         const float uu = ((float)u - cu) * p.pixel_size;
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
-            const int v = n0 + tx * 8 + j;
+            const int v = n0 + (j < 4 ? tx * 4 + j : FBN / 2 + tx * 4 + j - 4);
             if (v >= p.V) continue;
             const long long idx = (long long)u * p.V + v;
             const float vv = ((float)v - cv) * p.pixel_size;
